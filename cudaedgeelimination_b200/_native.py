@@ -1,0 +1,116 @@
+"""ctypes binding of libcee.so (include/cee.h). Loading fails loudly when the library is absent:
+there is no CPU fallback for any entry point."""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+
+PKG = pathlib.Path(__file__).resolve().parent
+LIB_PATH = PKG / "libcee.so"
+
+c_i32p = ctypes.POINTER(ctypes.c_int32)
+c_i64p = ctypes.POINTER(ctypes.c_int64)
+c_u8p = ctypes.POINTER(ctypes.c_uint8)
+c_u64p = ctypes.POINTER(ctypes.c_uint64)
+
+CEE_OK = 0
+CEE_ERR_INVALID = -1
+CEE_ERR_RANGE = -2
+CEE_ERR_CUDA = -3
+CEE_ERR_NOMEM = -4
+CEE_ERR_NODEVICE = -5
+CEE_ERR_TIMEOUT = -6
+CEE_ERR_STATE = -7
+
+
+class GraphView(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int32), ("dist_type", ctypes.c_int32),
+        ("x", c_i64p), ("y", c_i64p),
+        ("m", ctypes.c_int64),
+        ("edge_u", c_i32p), ("edge_v", c_i32p), ("edge_w", c_i64p), ("active", c_u8p),
+        ("adjacency", ctypes.c_int64),
+        ("row_offsets", c_i32p), ("neighbors", c_i32p), ("csr_edge_ids", c_i32p),
+    ]
+
+
+class JvStats(ctypes.Structure):
+    _fields_ = [
+        ("static_hit", ctypes.c_int32), ("workspace_hit", ctypes.c_int32),
+        ("resident_bytes", ctypes.c_uint64),
+        ("h2d_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double), ("d2h_ms", ctypes.c_double),
+        ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64), ("edges_screened", ctypes.c_int64),
+    ]
+
+
+class KoptStats(ctypes.Structure):
+    _fields_ = [
+        ("snapshot_hit", ctypes.c_int32), ("template_hit", ctypes.c_int32), ("workspace_hit", ctypes.c_int32),
+        ("resident_bytes", ctypes.c_uint64),
+        ("h2d_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double), ("d2h_ms", ctypes.c_double),
+        ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
+    ]
+
+
+class NativeError(RuntimeError):
+    """A non-zero status from libcee; `code` is the CEE_ERR_* value."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"libcee error {code}: {message}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m cudaedgeelimination_b200.build`")
+        L = ctypes.CDLL(str(LIB_PATH))
+        vp = ctypes.c_void_p
+        sig = {
+            "cee_abi_version": (ctypes.c_int, []),
+            "cee_device_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
+            "cee_select_device": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
+            "cee_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(vp)]),
+            "cee_destroy": (None, [vp]),
+            "cee_last_error": (ctypes.c_char_p, [vp]),
+            "cee_ctx_device": (ctypes.c_int, [vp]),
+            "cee_ctx_stream": (vp, [vp]),
+            "cee_ctx_synchronize": (ctypes.c_int, [vp]),
+            "cee_ctx_resident_bytes": (ctypes.c_uint64, [vp]),
+            "cee_ctx_clear": (ctypes.c_int, [vp, ctypes.c_uint]),
+            "cee_jv_screen": (ctypes.c_int, [vp, ctypes.POINTER(GraphView), c_i32p, ctypes.POINTER(JvStats)]),
+            "cee_jv_prepare": (ctypes.c_int, [vp, ctypes.POINTER(GraphView), ctypes.POINTER(JvStats)]),
+            "cee_jv_launch": (ctypes.c_int, [vp]),
+            "cee_jv_fetch": (ctypes.c_int, [vp, c_i32p]),
+            "cee_kopt_templates": (ctypes.c_int, [ctypes.c_uint32, c_u8p, c_u64p]),
+            "cee_kopt_costs": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, c_i64p, c_i64p, ctypes.c_uint32,
+                                              c_u8p, ctypes.c_int32, ctypes.c_uint64, vp, ctypes.c_int64, c_i64p,
+                                              ctypes.POINTER(KoptStats)]),
+            "cee_kopt_costs_multi": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, c_i64p, c_i64p,
+                                                    ctypes.c_int32, ctypes.POINTER(ctypes.c_uint32),
+                                                    ctypes.POINTER(vp), c_i64p, ctypes.POINTER(vp),
+                                                    ctypes.POINTER(KoptStats)]),
+            "cee_kopt_prepare_multi": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, c_i64p, c_i64p,
+                                                      ctypes.c_int32, ctypes.POINTER(ctypes.c_uint32),
+                                                      ctypes.POINTER(vp), c_i64p, ctypes.POINTER(KoptStats)]),
+            "cee_kopt_launch": (ctypes.c_int, [vp]),
+            "cee_kopt_fetch": (ctypes.c_int, [vp, ctypes.POINTER(vp)]),
+            "cee_cd_screen": (ctypes.c_int, [vp, ctypes.POINTER(GraphView), ctypes.c_int32, ctypes.c_int32, vp,
+                                             ctypes.c_int64, ctypes.c_int32, c_u8p]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(ctx, status: int) -> None:
+    if status != CEE_OK:
+        message = lib().cee_last_error(ctx)
+        raise NativeError(status, message.decode() if message else "")

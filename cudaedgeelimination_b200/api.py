@@ -1,0 +1,247 @@
+"""Python mirror of the reference's CUDA-backend seam, calling the B200 kernels via the C ABI.
+
+Names, argument meaning and error behaviour follow the reference's C++ entry points:
+  CudaBackendAvailable / FindJvCandidatesCuda / ClearJvCudaCache
+      include/cuda_edge_elimination/elimination.hpp:333-338
+  KOptCostCudaAvailable / EvaluateKOptTemplateCostsCuda / ClearKOptCostCudaCache /
+  BuildKOptReconnectTable
+      include/cuda_edge_elimination/local_search.hpp:49, 235-242
+  HtCdCudaAvailable / ScreenHtCdCandidatesCuda
+      include/cuda_edge_elimination/hamilton_tutte.hpp:527-531
+Caches live in one context per (host thread, device), as the reference keeps thread-local
+per-device caches (src/cuda/jv_cuda.cu:138-139). Errors raise NativeError (a RuntimeError).
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native
+from .snapshot import GraphSnapshot
+
+KOPT_TASK_DTYPE = np.dtype([("port_nodes", np.int32, (10,)), ("deleted_cost", np.int64)])
+CD_TASK_DTYPE = np.dtype([("c", np.int32), ("d", np.int32), ("active", np.uint8), ("pad", np.uint8, (3,))])
+assert KOPT_TASK_DTYPE.itemsize == 48 and CD_TASK_DTYPE.itemsize == 12
+
+INVALID_KOPT_COST = np.iinfo(np.int64).max
+KOPT_TEMPLATE_COUNTS = {3: 4, 4: 25, 5: 208}
+
+
+class Context:
+    """One cee_ctx: a device, a stream and the resident caches."""
+
+    def __init__(self, device: int = -1):
+        L = _native.lib()
+        handle = ctypes.c_void_p()
+        _native.check(None, L.cee_create(device, ctypes.byref(handle)))
+        self.handle = handle
+        self.device = L.cee_ctx_device(handle)
+
+    def close(self) -> None:
+        if self.handle:
+            _native.lib().cee_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return _native.lib().cee_ctx_stream(self.handle) or 0
+
+    def synchronize(self) -> None:
+        _native.check(self.handle, _native.lib().cee_ctx_synchronize(self.handle))
+
+    def resident_bytes(self) -> int:
+        return int(_native.lib().cee_ctx_resident_bytes(self.handle))
+
+    def clear(self, what: int = 0xF) -> None:
+        _native.check(self.handle, _native.lib().cee_ctx_clear(self.handle, what))
+
+    # ---- JV -------------------------------------------------------------------------
+    def jv_screen(self, graph: GraphSnapshot) -> tuple[np.ndarray, _native.JvStats]:
+        witness = np.empty(graph.m, np.int32)
+        stats = _native.JvStats()
+        view = graph.view()
+        _native.check(self.handle, _native.lib().cee_jv_screen(
+            self.handle, ctypes.byref(view), witness.ctypes.data_as(_native.c_i32p), ctypes.byref(stats)))
+        return witness, stats
+
+    def jv_prepare(self, graph: GraphSnapshot) -> _native.JvStats:
+        stats = _native.JvStats()
+        view = graph.view()
+        _native.check(self.handle, _native.lib().cee_jv_prepare(self.handle, ctypes.byref(view), ctypes.byref(stats)))
+        return stats
+
+    def jv_launch(self) -> None:
+        _native.check(self.handle, _native.lib().cee_jv_launch(self.handle))
+
+    def jv_fetch(self, m: int) -> np.ndarray:
+        witness = np.empty(m, np.int32)
+        _native.check(self.handle, _native.lib().cee_jv_fetch(self.handle, witness.ctypes.data_as(_native.c_i32p)))
+        return witness
+
+    # ---- k-opt ----------------------------------------------------------------------
+    def kopt_costs(self, graph: GraphSnapshot, table: "KOptReconnectTable", tasks: np.ndarray):
+        tasks = np.ascontiguousarray(tasks, dtype=KOPT_TASK_DTYPE)
+        rows = int(tasks.shape[0])
+        T = len(table.templates)
+        costs = np.empty((rows, T), np.int64)
+        mates = np.ascontiguousarray(table.templates, dtype=np.uint8)
+        stats = _native.KoptStats()
+        _native.check(self.handle, _native.lib().cee_kopt_costs(
+            self.handle, graph.n, graph.dist_type, graph.x.ctypes.data_as(_native.c_i64p),
+            graph.y.ctypes.data_as(_native.c_i64p), table.k, mates.ctypes.data_as(_native.c_u8p), T,
+            table.generator_hash, tasks.ctypes.data_as(ctypes.c_void_p), rows,
+            costs.ctypes.data_as(_native.c_i64p), ctypes.byref(stats)))
+        return costs, stats
+
+    def _multi_args(self, ks, task_lists):
+        n = len(ks)
+        tasks = [np.ascontiguousarray(t, dtype=KOPT_TASK_DTYPE) for t in task_lists]
+        karr = (ctypes.c_uint32 * n)(*ks)
+        tptr = (ctypes.c_void_p * n)(*[t.ctypes.data for t in tasks])
+        rows = np.array([t.shape[0] for t in tasks], np.int64)
+        return tasks, karr, tptr, rows
+
+    def kopt_costs_multi(self, graph: GraphSnapshot, ks, task_lists):
+        tasks, karr, tptr, rows = self._multi_args(ks, task_lists)
+        outs = [np.empty((int(r), KOPT_TEMPLATE_COUNTS[k]), np.int64) for k, r in zip(ks, rows)]
+        optr = (ctypes.c_void_p * len(ks))(*[o.ctypes.data for o in outs])
+        stats = _native.KoptStats()
+        _native.check(self.handle, _native.lib().cee_kopt_costs_multi(
+            self.handle, graph.n, graph.dist_type, graph.x.ctypes.data_as(_native.c_i64p),
+            graph.y.ctypes.data_as(_native.c_i64p), len(ks), karr, tptr, rows.ctypes.data_as(_native.c_i64p),
+            optr, ctypes.byref(stats)))
+        return outs, stats
+
+    def kopt_prepare_multi(self, graph: GraphSnapshot, ks, task_lists) -> _native.KoptStats:
+        tasks, karr, tptr, rows = self._multi_args(ks, task_lists)
+        stats = _native.KoptStats()
+        _native.check(self.handle, _native.lib().cee_kopt_prepare_multi(
+            self.handle, graph.n, graph.dist_type, graph.x.ctypes.data_as(_native.c_i64p),
+            graph.y.ctypes.data_as(_native.c_i64p), len(ks), karr, tptr, rows.ctypes.data_as(_native.c_i64p),
+            ctypes.byref(stats)))
+        return stats
+
+    def kopt_launch(self) -> None:
+        _native.check(self.handle, _native.lib().cee_kopt_launch(self.handle))
+
+    def kopt_fetch(self, outs) -> None:
+        optr = (ctypes.c_void_p * len(outs))(*[o.ctypes.data for o in outs])
+        _native.check(self.handle, _native.lib().cee_kopt_fetch(self.handle, optr))
+
+    # ---- c,d ------------------------------------------------------------------------
+    def cd_screen(self, graph: GraphSnapshot, target, tasks: np.ndarray, mode: int) -> np.ndarray:
+        tasks = np.ascontiguousarray(tasks, dtype=CD_TASK_DTYPE)
+        flags = np.empty(tasks.shape[0], np.uint8)
+        view = graph.view()
+        _native.check(self.handle, _native.lib().cee_cd_screen(
+            self.handle, ctypes.byref(view), int(target[0]), int(target[1]),
+            tasks.ctypes.data_as(ctypes.c_void_p), int(tasks.shape[0]), int(mode),
+            flags.ctypes.data_as(_native.c_u8p)))
+        return flags
+
+
+# ---- the reference seam, one context per (thread, device) ------------------------------
+
+_tls = threading.local()
+
+
+def _context(device: int = -1) -> Context:
+    contexts = getattr(_tls, "contexts", None)
+    if contexts is None:
+        contexts = _tls.contexts = {}
+    if device < 0:
+        device = getattr(_tls, "preferred", -1)
+    if device < 0 or device not in contexts:
+        ctx = Context(device)
+        contexts[ctx.device] = ctx
+        _tls.preferred = ctx.device
+        return ctx
+    return contexts[device]
+
+
+def device_count() -> int:
+    count = ctypes.c_int(0)
+    _native.lib().cee_device_count(ctypes.byref(count))
+    return int(count.value)
+
+
+def CudaBackendAvailable() -> tuple[bool, str]:
+    if device_count() == 0:
+        return False, "no visible CUDA device"
+    return True, ""
+
+
+KOptCostCudaAvailable = CudaBackendAvailable
+HtCdCudaAvailable = CudaBackendAvailable
+
+
+@dataclass
+class Candidate:
+    edge_id: int
+    witness: int
+    method: int = 1  # EliminationMethod::kJv
+
+
+@dataclass
+class JvCudaCacheUsage:
+    static_hit: bool
+    workspace_hit: bool
+    resident_bytes: int
+    h2d_ms: float
+    kernel_ms: float
+    d2h_ms: float
+
+
+def FindJvCandidatesCuda(graph: GraphSnapshot) -> tuple[list[Candidate], int, JvCudaCacheUsage]:
+    """Candidates in ascending edge id, the selected device and the cache usage."""
+    ctx = _context()
+    witness, stats = ctx.jv_screen(graph)
+    ids = np.flatnonzero(witness >= 0)
+    usage = JvCudaCacheUsage(bool(stats.static_hit), bool(stats.workspace_hit), int(stats.resident_bytes),
+                             stats.h2d_ms, stats.kernel_ms, stats.d2h_ms)
+    return [Candidate(int(e), int(witness[e])) for e in ids], ctx.device, usage
+
+
+def ClearJvCudaCache() -> None:
+    for ctx in getattr(_tls, "contexts", {}).values():
+        ctx.clear(1)
+
+
+@dataclass
+class KOptReconnectTable:
+    k: int
+    templates: np.ndarray  # uint8 [T, 14]
+    generator_hash: int
+
+
+def BuildKOptReconnectTable(k: int) -> KOptReconnectTable:
+    mates = np.full((208, 14), 0xFF, np.uint8)
+    h = ctypes.c_uint64(0)
+    count = _native.lib().cee_kopt_templates(k, mates.ctypes.data_as(_native.c_u8p), ctypes.byref(h))
+    if count <= 0:
+        raise ValueError("k must lie in [3,5]")
+    return KOptReconnectTable(k, mates[:count].copy(), int(h.value))
+
+
+def EvaluateKOptTemplateCostsCuda(graph: GraphSnapshot, table: KOptReconnectTable, tasks: np.ndarray):
+    """Row-major int64 cost matrix [rows, T] (INVALID_KOPT_COST for invalid cells)."""
+    costs, stats = _context().kopt_costs(graph, table, tasks)
+    return costs, stats
+
+
+def ClearKOptCostCudaCache() -> None:
+    for ctx in getattr(_tls, "contexts", {}).values():
+        ctx.clear(2)
+
+
+def ScreenHtCdCandidatesCuda(graph: GraphSnapshot, target, tasks: np.ndarray, mode: int) -> np.ndarray:
+    return _context().cd_screen(graph, target, tasks, mode)

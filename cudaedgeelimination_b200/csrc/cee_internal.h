@@ -1,0 +1,137 @@
+// Host-side state behind the C ABI (shared by the translation units of libcee.so).
+#pragma once
+
+#include "cee.h"
+#include "kopt_cost.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace cee {
+
+// A device allocation that only grows.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t capacity = 0;
+  cudaError_t Reserve(size_t bytes, bool* grew);
+  void Release();
+};
+
+struct JvState {
+  // static key, compared element-wise like the reference (src/cuda/jv_cuda.cu:360-382)
+  bool has_static = false;
+  int32_t n = 0, dist_type = 0;
+  int64_t m = 0;
+  std::vector<int64_t> hx, hy, hw;
+  std::vector<int32_t> heu, hev;
+  DevBuf xy, uv, w32;
+  // dynamic workspace, refreshed every call
+  DevBuf active, ro, nbr, ids, slotw, witness;
+  int64_t adjacency = 0;
+  int64_t edges_screened = 0;
+  int64_t last_h2d_bytes = 0;
+  bool prepared = false;
+  void Release() {
+    for (DevBuf* b : {&xy, &uv, &w32, &active, &ro, &nbr, &ids, &slotw, &witness}) b->Release();
+    has_static = false;
+    prepared = false;
+    hx.clear();
+    hy.clear();
+    hw.clear();
+    heu.clear();
+    hev.clear();
+  }
+};
+
+struct KoptTable {
+  uint32_t k = 0;
+  uint64_t hash = 0;
+  int32_t T = 0;
+  std::vector<uint8_t> mates;
+  DevBuf pairs;  // T x k pair indices
+  void Release() {
+    pairs.Release();
+    k = 0;
+    T = 0;
+    mates.clear();
+  }
+};
+
+struct KoptState {
+  bool has_coords = false;
+  int32_t n = 0, dist_type = 0;
+  std::vector<int64_t> hx, hy;
+  DevBuf xy;
+  KoptTable user[3];   // caller templates per k (the reference's template cache)
+  KoptTable canon[3];  // this library's proper templates per k
+  DevBuf tasks, costs;
+  KoptLaunch launch{};
+  int32_t segments = 0, tiles = 0;
+  int64_t seg_rows[kKoptMaxSegments] = {};
+  int32_t seg_T[kKoptMaxSegments] = {};
+  int64_t last_h2d_bytes = 0, last_d2h_bytes = 0;
+  bool prepared = false;
+  void Release() {
+    xy.Release();
+    tasks.Release();
+    costs.Release();
+    for (KoptTable& t : user) t.Release();
+    for (KoptTable& t : canon) t.Release();
+    has_coords = false;
+    prepared = false;
+    hx.clear();
+    hy.clear();
+  }
+};
+
+struct CdState {
+  bool has_coords = false;
+  int32_t n = 0, dist_type = 0;
+  std::vector<int64_t> hx, hy;
+  DevBuf xy, tasks, flags;
+  void Release() {
+    xy.Release();
+    tasks.Release();
+    flags.Release();
+    has_coords = false;
+    hx.clear();
+    hy.clear();
+  }
+};
+
+struct BatchState;
+
+}  // namespace cee
+
+struct cee_ctx {
+  int device = -1;
+  int sm_count = 148;
+  int jv_blocks_per_sm = 8;
+  int kopt_rows_per_tile[3] = {0, 0, 0};  // 0 = default tile for k = 3, 4, 5
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[6] = {};
+  int32_t* d_error = nullptr;  // device bounds-check word
+  int32_t* h_error = nullptr;  // pinned copy
+  std::string error;
+  cee::JvState jv;
+  cee::KoptState kopt;
+  cee::CdState cd;
+  cee::BatchState* batch = nullptr;
+};
+
+namespace cee {
+
+int Fail(cee_ctx* ctx, int code, const std::string& message);
+int CudaFail(cee_ctx* ctx, cudaError_t status, const char* what);
+int Activate(cee_ctx* ctx);
+int PackCoordinates(cee_ctx* ctx, int32_t n, const int64_t* x, const int64_t* y, std::vector<int2>* out);
+int GridFor(int64_t work, int per_block, int max_blocks);
+float EventMs(cudaEvent_t a, cudaEvent_t b);
+int CheckDeviceError(cee_ctx* ctx, const char* what);
+void ReleaseBatch(cee_ctx* ctx);
+uint64_t BatchResident(const cee_ctx* ctx);
+
+}  // namespace cee

@@ -1,0 +1,168 @@
+// Jonker-Volgenant fast-elimination screen, one warp per edge.
+//
+// Semantics (the reference's CPU oracle, src/cpu/jv_elimination.cpp:45-117, 209-224):
+//   for every active edge (a,b) with deg(a) > 2 and deg(b) > 2
+//     candidates = the 10 smallest (score, node) over
+//                    c in N(a)\{a,b}:              score = w(a,c) + C(c,b)
+//                    c in N(b)\{a,b}, c not in N(a): score = w(b,c) + C(c,a)
+//     witness    = the first candidate c (in that order) such that every
+//                  d in N(c)\{a,b} is incompatible:  w(a,b) + w(c,d) > C(a,c) + C(d,b)
+//                                                and w(a,b) + w(c,d) > C(a,d) + C(b,c)
+// where w are the snapshot's CSR slot weights and C the exact TSPLIB distance.
+//
+// B200 mapping: the 32 lanes score up to 32 candidates at once and keep the running
+// top-10 as a warp-wide bitonic-sorted list (one 64-bit key (score << 32 | node) per lane);
+// the witness search flattens the (c, d) pairs of all candidates, in candidate order,
+// over the lanes. Lanes may test pairs of later candidates speculatively, but a candidate
+// is only accepted once every pair of it has been tested and every earlier candidate is
+// known to have a compatible d, so the chosen witness is exactly the sequential one.
+#pragma once
+
+#include "device_common.cuh"
+
+namespace cee {
+
+constexpr int kJvMaxCandidates = 10;  // src/cpu/jv_elimination.cpp:28
+constexpr int kJvWarpsPerBlock = 8;
+
+// Device view of a snapshot (coordinates relative to the bounding-box corner).
+struct JvGraph {
+  int32_t n;
+  int32_t dist_type;
+  int64_t m;
+  const int2* __restrict__ xy;          // [n]
+  const int2* __restrict__ edge_uv;     // [m] (u, v) of the stable edge list
+  const int32_t* __restrict__ edge_w;   // [m]
+  const uint8_t* __restrict__ active;   // [m]
+  const int32_t* __restrict__ row_offsets;  // [n + 1]
+  const int32_t* __restrict__ nbr;      // [adjacency], rows ascending
+  const int32_t* __restrict__ slot_w;   // [adjacency], weight of the CSR slot's edge
+};
+
+struct JvWarpScratch {
+  int32_t c[kJvMaxCandidates];
+  int32_t row[kJvMaxCandidates];   // first CSR slot of N(c)
+  int32_t begin[kJvMaxCandidates]; // first flattened pair index of candidate i
+  int32_t end[kJvMaxCandidates];   // one past its last pair index
+  uint32_t cac[kJvMaxCandidates];  // C(a, c)
+  uint32_t cbc[kJvMaxCandidates];  // C(b, c)
+};
+
+// Screens edge e with the calling (full) warp; returns the witness or -1 on every lane.
+// Bad node indices (outside [0, n)) are recorded in *error and skipped.
+__device__ __forceinline__ int32_t jv_screen_edge(const JvGraph& g, int64_t e,
+                                                  JvWarpScratch& s, int lane,
+                                                  int32_t* __restrict__ error) {
+  if (g.active[e] == 0) return -1;
+  const int2 uv = g.edge_uv[e];
+  const int32_t a = uv.x, b = uv.y;
+  const int32_t ra0 = __ldg(g.row_offsets + a), ra1 = __ldg(g.row_offsets + a + 1);
+  const int32_t rb0 = __ldg(g.row_offsets + b), rb1 = __ldg(g.row_offsets + b + 1);
+  const int32_t da = ra1 - ra0, db = rb1 - rb0;
+  if (da <= 2 || db <= 2) return -1;
+  const int2 pa = __ldg(g.xy + a), pb = __ldg(g.xy + b);
+  const int64_t cab = __ldg(g.edge_w + e);
+
+  // ---- candidate scoring: warp-wide sorted top list -----------------------------------
+  uint64_t top = kEmptyKey;
+  const int total = da + db;
+  for (int base = 0; base < total; base += 32) {
+    const int i = base + lane;
+    uint64_t key = kEmptyKey;
+    if (i < total) {
+      const bool second = i >= da;
+      const int32_t slot = second ? rb0 + (i - da) : ra0 + i;
+      const int32_t c = __ldg(g.nbr + slot);
+      bool ok = c != a && c != b;
+      if (ok && static_cast<uint32_t>(c) >= static_cast<uint32_t>(g.n)) {
+        atomicOr(error, 1);
+        ok = false;
+      }
+      // second row: nodes already reached through N(a) are not scored again
+      if (ok && second) ok = !row_contains(g.nbr, ra0, ra1, c);
+      if (ok) {
+        const uint64_t score = static_cast<uint64_t>(static_cast<uint32_t>(__ldg(g.slot_w + slot))) +
+                               exact_distance(__ldg(g.xy + c), second ? pa : pb, g.dist_type);
+        key = (score << 32) | static_cast<uint32_t>(c);
+      }
+    }
+    key = warp_sort_asc(key, lane);
+    top = base == 0 ? key : warp_merge_smallest(top, key, lane);
+  }
+  const int nc = __popc(__ballot_sync(kFullMask, lane < kJvMaxCandidates && top != kEmptyKey));
+  if (nc == 0) return -1;
+
+  // ---- candidate table: row ranges and flattened pair numbering ------------------------
+  int deg = 0;
+  if (lane < nc) {
+    const int32_t c = static_cast<int32_t>(top & 0xffffffffu);
+    const int32_t rc0 = __ldg(g.row_offsets + c), rc1 = __ldg(g.row_offsets + c + 1);
+    const int2 pc = __ldg(g.xy + c);
+    deg = rc1 - rc0;
+    s.c[lane] = c;
+    s.row[lane] = rc0;
+    s.cac[lane] = exact_distance(pa, pc, g.dist_type);
+    s.cbc[lane] = exact_distance(pb, pc, g.dist_type);
+  }
+  const int incl = warp_inclusive_sum(deg, lane);
+  if (lane < nc) {
+    s.begin[lane] = incl - deg;
+    s.end[lane] = incl;
+  }
+  const int pairs = __shfl_sync(kFullMask, incl, nc - 1);
+  __syncwarp();
+
+  // ---- witness search ------------------------------------------------------------------
+  const uint32_t all = (nc == 32) ? kFullMask : ((1u << nc) - 1u);
+  uint32_t compatible = 0;  // candidates known to have a compatible d (warp-uniform)
+  int base = 0;
+  while (true) {
+    const int p = base + lane;
+    uint32_t bit = 0;
+    if (p < pairs) {
+      int ci = 0;
+#pragma unroll
+      for (int i = 1; i < kJvMaxCandidates; ++i) ci += (i < nc && s.begin[i] <= p) ? 1 : 0;
+      if (((compatible >> ci) & 1u) == 0) {
+        const int32_t slot = s.row[ci] + (p - s.begin[ci]);
+        const int32_t d = __ldg(g.nbr + slot);
+        if (d != a && d != b) {
+          if (static_cast<uint32_t>(d) >= static_cast<uint32_t>(g.n)) {
+            atomicOr(error, 1);
+          } else {
+            const int2 pd = __ldg(g.xy + d);
+            const int64_t left = cab + __ldg(g.slot_w + slot);
+            const int64_t first = static_cast<int64_t>(s.cac[ci]) + exact_distance(pd, pb, g.dist_type);
+            const int64_t second = static_cast<int64_t>(exact_distance(pa, pd, g.dist_type)) + s.cbc[ci];
+            if (left <= first || left <= second) bit = 1u << ci;
+          }
+        }
+      }
+    }
+    compatible |= __reduce_or_sync(kFullMask, bit);
+    const uint32_t open = all & ~compatible;
+    if (open == 0) return -1;  // every candidate has a compatible neighbour
+    const int first_open = __ffs(open) - 1;
+    const int chunk_end = base + 32;
+    if (s.end[first_open] <= chunk_end) return s.c[first_open];
+    base = max(chunk_end, s.begin[first_open]);
+  }
+}
+
+// Grid-stride over edges [first, last): one warp per edge, witness[e] always written.
+static __global__ void __launch_bounds__(kJvWarpsPerBlock * 32)
+    jv_screen_kernel(JvGraph g, int64_t first, int64_t last, int32_t* __restrict__ witness,
+                     int32_t* __restrict__ error) {
+  __shared__ JvWarpScratch scratch[kJvWarpsPerBlock];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * kJvWarpsPerBlock;
+  for (int64_t e = first + static_cast<int64_t>(blockIdx.x) * kJvWarpsPerBlock + warp; e < last;
+       e += warps) {
+    const int32_t w = jv_screen_edge(g, e, scratch[warp], lane, error);
+    if (lane == 0) witness[e] = w;
+    __syncwarp();
+  }
+}
+
+}  // namespace cee

@@ -1,0 +1,115 @@
+"""Seeded synthetic workloads (libcee_synth.so, csrc/synth.cpp). The reference's own inputs
+(TSPLIB pcb3038 / rl5915 / d15112 with ElimTSP edge sets) do not ship with it; these seeded
+instances of the same shapes stand in for them.
+
+  jv_small()        300 nodes in [0,10^4)^2, union of 10-NN, EUC_2D          (CPU-runnable JV case)
+  jv_clustered()    3,000 nodes: 30 Gaussian clusters (sigma 300) + 600 uniform in [0,10^5)^2,
+                    8-NN plus 2 nearest per quadrant, EUC_2D                  (multi-epoch JV)
+  kopt_instance()   15,000 nodes uniform in [0,10^6)^2, 10-NN, CEIL_2D, with 200,000 leaf rows
+                    of k in {3,4,5} in thirds                                 (k-opt cost matrix)
+  batch_instance(i) instance i of the 4,096-instance mix (n log-uniform in [100,5000])
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+
+import numpy as np
+
+from .api import KOPT_TASK_DTYPE
+from .snapshot import CEIL_2D, EUC_2D, GraphSnapshot
+
+_LIB_PATH = pathlib.Path(__file__).resolve().parent / "libcee_synth.so"
+_lib = None
+
+SEED_BASE = 0x5EED0000
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not _LIB_PATH.exists():
+            raise ImportError(f"{_LIB_PATH} is missing: build it with `python -m cudaedgeelimination_b200.build`")
+        L = ctypes.CDLL(str(_LIB_PATH))
+        vp = ctypes.c_void_p
+        L.cees_uniform_knn.restype = vp
+        L.cees_uniform_knn.argtypes = [ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64]
+        L.cees_clustered_knn.restype = vp
+        L.cees_clustered_knn.argtypes = [ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, ctypes.c_double,
+                                         ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                         ctypes.c_uint64]
+        L.cees_batch_instance.restype = vp
+        L.cees_batch_instance.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_double, ctypes.c_double]
+        L.cees_free.argtypes = [vp]
+        L.cees_n.restype = ctypes.c_int32
+        L.cees_n.argtypes = [vp]
+        L.cees_m.restype = ctypes.c_int64
+        L.cees_m.argtypes = [vp]
+        L.cees_dist_type.restype = ctypes.c_int32
+        L.cees_dist_type.argtypes = [vp]
+        L.cees_copy.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.cees_kopt_rows.restype = ctypes.c_int32
+        L.cees_kopt_rows.argtypes = [vp, ctypes.c_int64, vp, ctypes.c_uint64, vp]
+        _lib = L
+    return _lib
+
+
+class _Handle:
+    def __init__(self, handle):
+        if not handle:
+            raise RuntimeError("synthetic generator failed")
+        self.handle = handle
+
+    def snapshot(self) -> GraphSnapshot:
+        L = lib()
+        n, m = L.cees_n(self.handle), L.cees_m(self.handle)
+        x = np.empty(n, np.int64)
+        y = np.empty(n, np.int64)
+        eu = np.empty(m, np.int32)
+        ev = np.empty(m, np.int32)
+        w = np.empty(m, np.int64)
+        L.cees_copy(self.handle, x.ctypes.data, y.ctypes.data, eu.ctypes.data, ev.ctypes.data, w.ctypes.data)
+        return GraphSnapshot(n, L.cees_dist_type(self.handle), x, y, eu, ev, w, np.ones(m, np.uint8))
+
+    def kopt_rows(self, ks: np.ndarray, seed: int) -> np.ndarray:
+        ks = np.ascontiguousarray(ks, np.uint8)
+        out = np.zeros(ks.shape[0], KOPT_TASK_DTYPE)
+        rc = lib().cees_kopt_rows(self.handle, ks.shape[0], ks.ctypes.data, seed, out.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"k-opt row generation failed ({rc})")
+        return out
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib().cees_free(self.handle)
+            self.handle = None
+
+
+def uniform_knn(n: int, coord_range: int, k: int, dist_type: int, seed: int) -> GraphSnapshot:
+    return _Handle(lib().cees_uniform_knn(n, coord_range, k, dist_type, seed)).snapshot()
+
+
+def jv_small(seed: int = SEED_BASE + 0) -> GraphSnapshot:
+    return uniform_knn(300, 10_000, 10, EUC_2D, seed)
+
+
+def jv_clustered(seed: int = SEED_BASE + 1) -> GraphSnapshot:
+    return _Handle(lib().cees_clustered_knn(3000, 100_000, 30, 300.0, 600, 8, 2, EUC_2D, seed)).snapshot()
+
+
+def kopt_instance(rows: int = 200_000, n: int = 15_000, seed: int = SEED_BASE + 2):
+    """The instance and its rows grouped by k: returns (snapshot, {k: tasks})."""
+    h = _Handle(lib().cees_uniform_knn(n, 1_000_000, 10, CEIL_2D, seed))
+    third = -(-rows // 3)
+    counts = {3: third, 4: third, 5: rows - 2 * third}
+    ks = np.concatenate([np.full(c, k, np.uint8) for k, c in counts.items()])
+    tasks = h.kopt_rows(ks, seed + 1)
+    out, start = {}, 0
+    for k, c in counts.items():
+        out[k] = tasks[start:start + c]
+        start += c
+    return h.snapshot(), out
+
+
+def batch_instance(index: int, seed: int = SEED_BASE + 3, n_lo: float = 100.0, n_hi: float = 5000.0) -> GraphSnapshot:
+    return _Handle(lib().cees_batch_instance(seed, index, n_lo, n_hi)).snapshot()

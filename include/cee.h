@@ -1,0 +1,203 @@
+/* cee.h -- C ABI of the B200 edge-elimination screen (libcee.so).
+ *
+ * Plain pointers and sizes only; no C++ or torch types cross this boundary. Each entry point
+ * names the reference interface it replaces (paths inside the reference project). The C++
+ * shim in cudaedgeelimination_b200/shim/cudaee_seam.cpp maps the reference's CUDA-backend
+ * symbols onto these calls so that the reference's CPU code drives the B200 kernels.
+ *
+ * Conventions
+ *   - Every int-returning function returns CEE_OK (0) or a negative CEE_ERR_* code; the text
+ *     of the last error is available from cee_last_error(ctx) (ctx may be NULL for errors
+ *     raised before a context exists).
+ *   - A cee_ctx belongs to one host thread and one device, owns a CUDA stream and all device
+ *     buffers it allocates; calls on one ctx are serialised on its stream. Caller buffers are
+ *     borrowed for the duration of the call only.
+ *   - Host-buffer entry points copy inputs to the device, run, copy results back and
+ *     synchronise before returning. Pinned host buffers are copied directly; pageable ones
+ *     go through the CUDA driver's staging.
+ *   - There is no CPU fallback: without a usable device the calls fail with CEE_ERR_NODEVICE.
+ *   - Exact-arithmetic range: coordinates are stored as int32 offsets from the snapshot's
+ *     bounding-box corner, so every snapshot must have max-min < 2^30 on both axes (every
+ *     distance then fits int32 and every squared distance fits 2^61); edge weights must lie in
+ *     [0, 2^31). Inputs outside this range fail with CEE_ERR_RANGE before any launch.
+ */
+#ifndef CEE_H
+#define CEE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CEE_ABI_VERSION 1
+
+enum cee_status {
+  CEE_OK = 0,
+  CEE_ERR_INVALID = -1,  /* malformed input (reference: std::invalid_argument / runtime_error) */
+  CEE_ERR_RANGE = -2,    /* outside the exact-arithmetic range (reference: std::overflow_error) */
+  CEE_ERR_CUDA = -3,     /* CUDA runtime or launch failure */
+  CEE_ERR_NOMEM = -4,    /* device or pinned host allocation failed */
+  CEE_ERR_NODEVICE = -5, /* no usable CUDA device */
+  CEE_ERR_TIMEOUT = -6,  /* a bounded device-side wait ran out */
+  CEE_ERR_STATE = -7     /* call out of order (e.g. launch before prepare) */
+};
+
+enum cee_distance_type { CEE_EUC_2D = 0, CEE_CEIL_2D = 1 };
+
+/* HtCdMode, include/cuda_edge_elimination/hamilton_tutte.hpp:21-24 */
+enum cee_cd_mode { CEE_CD_ACTIVE_INCOMPATIBLE = 0, CEE_CD_MISSING_OR_INCOMPATIBLE = 1 };
+
+/* kInvalidKOptTemplateCost, include/cuda_edge_elimination/local_search.hpp:52 */
+#define CEE_INVALID_KOPT_COST INT64_MAX
+
+typedef struct cee_ctx cee_ctx;
+
+/* ---- library / device ------------------------------------------------------------- */
+
+int cee_abi_version(void);
+/* Number of visible CUDA devices (0 when none; never fails for "no device"). */
+int cee_device_count(int* count);
+/* Picks the visible device with the most free memory, as the reference's SelectDevice does
+ * when no device is forced (src/cuda/jv_cuda.cu:290-346). */
+int cee_select_device(int* device);
+/* Creates a context on `device` (-1: cee_select_device). */
+int cee_create(int device, cee_ctx** out);
+void cee_destroy(cee_ctx* ctx);
+const char* cee_last_error(const cee_ctx* ctx);
+int cee_ctx_device(const cee_ctx* ctx);
+/* The cudaStream_t every launch of this context goes to. */
+void* cee_ctx_stream(cee_ctx* ctx);
+int cee_ctx_synchronize(cee_ctx* ctx);
+/* Device bytes currently held by the context's caches and workspaces. */
+uint64_t cee_ctx_resident_bytes(const cee_ctx* ctx);
+/* Frees cached device state: bit 1 = JV, bit 2 = k-opt, bit 4 = c,d, bit 8 = batch.
+ * Replaces ClearJvCudaCache (include/cuda_edge_elimination/elimination.hpp:338) and
+ * ClearKOptCostCudaCache (include/cuda_edge_elimination/local_search.hpp:242). */
+int cee_ctx_clear(cee_ctx* ctx, unsigned what);
+
+/* ---- snapshot view ------------------------------------------------------------------ */
+
+/* Host view of a GraphSnapshot (include/cuda_edge_elimination/graph.hpp:13-37): integer
+ * coordinates, the stable edge list (edge ids are positions in it) and the active-only CSR
+ * over it with rows ascending by neighbour (GraphSnapshot::RebuildCsr,
+ * src/common/graph.cpp:230-282). */
+typedef struct {
+  int32_t n;
+  int32_t dist_type;          /* cee_distance_type */
+  const int64_t* x;           /* [n] */
+  const int64_t* y;           /* [n] */
+  int64_t m;
+  const int32_t* edge_u;      /* [m] */
+  const int32_t* edge_v;      /* [m] */
+  const int64_t* edge_w;      /* [m] */
+  const uint8_t* active;      /* [m] 0/1 */
+  int64_t adjacency;          /* row_offsets[n] = 2 x active edges */
+  const int32_t* row_offsets; /* [n + 1] */
+  const int32_t* neighbors;   /* [adjacency] */
+  const int32_t* csr_edge_ids;/* [adjacency] */
+} cee_graph_view;
+
+/* ---- JV fast-elimination screen ------------------------------------------------------ */
+
+/* JvCudaCacheUsage (include/cuda_edge_elimination/elimination.hpp:41-49) plus byte counts. */
+typedef struct {
+  int32_t static_hit;     /* coordinates, distance type and every edge (u, v, w) unchanged */
+  int32_t workspace_hit;  /* no device buffer had to grow */
+  uint64_t resident_bytes;
+  double h2d_ms;          /* CUDA-event times on the context stream */
+  double kernel_ms;
+  double d2h_ms;
+  int64_t h2d_bytes;
+  int64_t d2h_bytes;
+  int64_t edges_screened; /* active edges of the snapshot */
+} cee_jv_stats;
+
+/* Replaces FindJvCandidatesCuda (include/cuda_edge_elimination/elimination.hpp:335-337,
+ * src/cuda/jv_cuda.cu:488-566). witness_out[e] = the first JV witness of edge e in the
+ * reference's candidate order (src/cpu/jv_elimination.cpp:45-117, 209-224) or -1; the
+ * candidate list is the edges with witness >= 0 in ascending edge id. Static data are
+ * cached per context with the reference's exact element-wise key (src/cuda/jv_cuda.cu:360-430);
+ * active bits and the CSR are uploaded on every call. */
+int cee_jv_screen(cee_ctx* ctx, const cee_graph_view* graph, int32_t* witness_out,
+                  cee_jv_stats* stats);
+/* The three phases of cee_jv_screen, for callers that keep the snapshot resident and time
+ * the kernel alone: prepare uploads, launch enqueues the screen on the context stream
+ * (no synchronisation), fetch copies the witnesses back and checks the device error word. */
+int cee_jv_prepare(cee_ctx* ctx, const cee_graph_view* graph, cee_jv_stats* stats);
+int cee_jv_launch(cee_ctx* ctx);
+int cee_jv_fetch(cee_ctx* ctx, int32_t* witness_out);
+
+/* ---- k-opt leaf cost matrix ----------------------------------------------------------- */
+
+/* KOptCostTask, include/cuda_edge_elimination/local_search.hpp:54-57 (48 bytes). */
+typedef struct {
+  int32_t port_nodes[10];
+  int64_t deleted_cost;
+} cee_kopt_task;
+
+/* KOptCudaCacheUsage (include/cuda_edge_elimination/local_search.hpp:59-64) plus timings. */
+typedef struct {
+  int32_t snapshot_hit;
+  int32_t template_hit;
+  int32_t workspace_hit;
+  uint64_t resident_bytes;
+  double h2d_ms;
+  double kernel_ms;
+  double d2h_ms;
+  int64_t h2d_bytes;
+  int64_t d2h_bytes;
+} cee_kopt_stats;
+
+/* The proper k-opt reconnect templates (BuildKOptReconnectTable,
+ * src/cpu/kopt_search.cpp:1143-1193): writes mates[t * 14 + p] for t < count (14 bytes per
+ * template, unused entries 0xff) and the generator hash pinned in
+ * configs/kopt_reconnect_hashes_v1.txt. Returns the template count (4 / 25 / 208) or < 0. */
+int cee_kopt_templates(uint32_t k, uint8_t* mates, uint64_t* generator_hash);
+
+/* Replaces EvaluateKOptTemplateCostsCuda (include/cuda_edge_elimination/local_search.hpp:
+ * 237-240, src/cuda/kopt_cost.cu:415-470). costs_out[row * template_count + t] is the exact
+ * added cost of template t on the row, or CEE_INVALID_KOPT_COST. Templates are the caller's
+ * (mates as above); the cache hits follow the reference (coordinates + type; k + hash +
+ * template bytes; workspace capacities). */
+int cee_kopt_costs(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x,
+                   const int64_t* y, uint32_t k, const uint8_t* mates, int32_t template_count,
+                   uint64_t template_hash, const cee_kopt_task* tasks, int64_t rows,
+                   int64_t* costs_out, cee_kopt_stats* stats);
+
+/* Several k buckets (each with the library's own proper templates) in one launch: segment s
+ * has k = ks[s], rows[s] rows at tasks[s] and writes costs_out[s]. At most 8 segments. */
+int cee_kopt_costs_multi(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x,
+                         const int64_t* y, int32_t segments, const uint32_t* ks,
+                         const cee_kopt_task* const* tasks, const int64_t* rows,
+                         int64_t* const* costs_out, cee_kopt_stats* stats);
+/* Phases of cee_kopt_costs_multi (prepare = upload, launch = enqueue, fetch = copy back). */
+int cee_kopt_prepare_multi(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x,
+                           const int64_t* y, int32_t segments, const uint32_t* ks,
+                           const cee_kopt_task* const* tasks, const int64_t* rows,
+                           cee_kopt_stats* stats);
+int cee_kopt_launch(cee_ctx* ctx);
+int cee_kopt_fetch(cee_ctx* ctx, int64_t* const* costs_out);
+
+/* ---- HT c,d root screen --------------------------------------------------------------- */
+
+/* HtCdScreenTask, include/cuda_edge_elimination/hamilton_tutte.hpp:42-46 (12 bytes). */
+typedef struct {
+  int32_t c;
+  int32_t d;
+  uint8_t active;
+  uint8_t reserved[3];
+} cee_cd_task;
+
+/* Replaces ScreenHtCdCandidatesCuda (include/cuda_edge_elimination/hamilton_tutte.hpp:528-531,
+ * src/cuda/ht_cd.cu:384-442): flags_out[i] in {0,1} for target (u,v), u < v. Tasks are
+ * validated as the reference does (c < d, no target endpoint, active bit equal to the CSR). */
+int cee_cd_screen(cee_ctx* ctx, const cee_graph_view* graph, int32_t u, int32_t v,
+                  const cee_cd_task* tasks, int64_t count, int32_t mode, uint8_t* flags_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CEE_H */

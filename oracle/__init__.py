@@ -1,0 +1,370 @@
+"""Test infrastructure: ctypes access to the CPU checkers.
+
+  Port       -- oracle/_build/libcee_oracle.so, the plain-C restatement (cee_oracle.c)
+  Reference  -- oracle/_ref/libcudaee_ref.so, the reference's own CPU sources compiled by
+                oracle/Makefile (CUDA seam = the reference's stubs), or, with dropin=True,
+                oracle/_ref/libcudaee_dropin.so (CUDA seam = this project's shim over libcee.so)
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this package, and only
+as the checker or as the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+import subprocess
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+PORT_LIB = HERE / "_build" / "libcee_oracle.so"
+REF_LIB = HERE / "_ref" / "libcudaee_ref.so"
+DROPIN_LIB = HERE / "_ref" / "libcudaee_dropin.so"
+
+i32p = ctypes.POINTER(ctypes.c_int32)
+i64p = ctypes.POINTER(ctypes.c_int64)
+u8p = ctypes.POINTER(ctypes.c_uint8)
+u64p = ctypes.POINTER(ctypes.c_uint64)
+vp = ctypes.c_void_p
+
+
+def _p(a: np.ndarray, t):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+class CeoGraph(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32), ("dist_type", ctypes.c_int32), ("x", i64p), ("y", i64p),
+                ("m", ctypes.c_int64), ("edge_u", i32p), ("edge_v", i32p), ("edge_w", i64p), ("active", u8p),
+                ("row_offsets", i32p), ("neighbors", i32p), ("csr_edge_ids", i32p), ("csr_weights", i64p)]
+
+
+def build_port() -> None:
+    """Builds the C restatement if it is missing (gcc is part of the image)."""
+    if not PORT_LIB.exists():
+        subprocess.run(["make", "-C", str(HERE), "port"], check=True, capture_output=True)
+
+
+class Port:
+    """The plain-C oracle over a snapshot-like object (n, dist_type, x, y, edge_u/v/w, active,
+    row_offsets, neighbors, csr_edge_ids, csr_weights)."""
+
+    def __init__(self):
+        build_port()
+        L = ctypes.CDLL(str(PORT_LIB))
+        G = ctypes.POINTER(CeoGraph)
+        L.ceo_isqrt.restype = ctypes.c_uint64
+        L.ceo_isqrt.argtypes = [ctypes.c_uint64]
+        L.ceo_distance.restype = ctypes.c_int64
+        L.ceo_distance.argtypes = [ctypes.c_int64] * 4 + [ctypes.c_int32]
+        L.ceo_rebuild_csr.argtypes = [ctypes.c_int32, ctypes.c_int64, i32p, i32p, i64p, u8p, i32p, i32p, i32p, i64p]
+        L.ceo_jv_screen.restype = ctypes.c_int64
+        L.ceo_jv_screen.argtypes = [G, i32p, i64p]
+        L.ceo_jv_screen_range.restype = ctypes.c_int64
+        L.ceo_jv_screen_range.argtypes = [G, ctypes.c_int64, ctypes.c_int64, i32p, i64p]
+        L.ceo_jv_verify.argtypes = [G, ctypes.c_int32, ctypes.c_int32]
+        L.ceo_content_hash.restype = ctypes.c_uint64
+        L.ceo_content_hash.argtypes = [G]
+        L.ceo_jv_commit.restype = ctypes.c_int64
+        L.ceo_jv_commit.argtypes = [G, i32p, i32p, ctypes.c_int64, i32p, i32p, u8p]
+        L.ceo_jv_eliminate.restype = ctypes.c_int32
+        L.ceo_jv_eliminate.argtypes = [ctypes.c_int32, ctypes.c_int32, i64p, i64p, ctypes.c_int64, i32p, i32p, i64p,
+                                       u8p, ctypes.c_uint32, i64p, i64p, u64p]
+        L.ceo_kopt_templates.restype = ctypes.c_int32
+        L.ceo_kopt_templates.argtypes = [ctypes.c_uint32, u8p, u64p]
+        L.ceo_kopt_costs.argtypes = [ctypes.c_int32, i64p, i64p, ctypes.c_uint32, vp, ctypes.c_int64, u8p,
+                                     ctypes.c_int32, i64p]
+        L.ceo_cd_tasks.restype = ctypes.c_int64
+        L.ceo_cd_tasks.argtypes = [G, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32, i32p, i32p, u8p]
+        L.ceo_cd_screen.argtypes = [G, ctypes.c_int32, ctypes.c_int32, i32p, i32p, u8p, ctypes.c_int64,
+                                    ctypes.c_int32, u8p]
+        L.ceo_ht_targets.restype = ctypes.c_int64
+        L.ceo_ht_targets.argtypes = [G, ctypes.c_int32, i32p]
+        self.L = L
+
+    def graph(self, g) -> CeoGraph:
+        s = CeoGraph()
+        s.n, s.dist_type = g.n, g.dist_type
+        s.x, s.y = _p(g.x, ctypes.c_int64), _p(g.y, ctypes.c_int64)
+        s.m = g.edge_u.shape[0]
+        s.edge_u, s.edge_v = _p(g.edge_u, ctypes.c_int32), _p(g.edge_v, ctypes.c_int32)
+        s.edge_w, s.active = _p(g.edge_w, ctypes.c_int64), _p(g.active, ctypes.c_uint8)
+        s.row_offsets, s.neighbors = _p(g.row_offsets, ctypes.c_int32), _p(g.neighbors, ctypes.c_int32)
+        s.csr_edge_ids, s.csr_weights = _p(g.csr_edge_ids, ctypes.c_int32), _p(g.csr_weights, ctypes.c_int64)
+        s._keep = g
+        return s
+
+    def isqrt(self, v: int) -> int:
+        return int(self.L.ceo_isqrt(v))
+
+    def distance(self, x1, y1, x2, y2, t) -> int:
+        return int(self.L.ceo_distance(x1, y1, x2, y2, t))
+
+    def csr(self, n, edge_u, edge_v, edge_w, active):
+        m = edge_u.shape[0]
+        slots = int(2 * np.count_nonzero(active))
+        ro = np.empty(n + 1, np.int32)
+        nb = np.empty(slots, np.int32)
+        ids = np.empty(slots, np.int32)
+        ws = np.empty(slots, np.int64)
+        self.L.ceo_rebuild_csr(n, m, _p(edge_u, ctypes.c_int32), _p(edge_v, ctypes.c_int32),
+                               _p(edge_w, ctypes.c_int64), _p(active, ctypes.c_uint8), _p(ro, ctypes.c_int32),
+                               _p(nb, ctypes.c_int32), _p(ids, ctypes.c_int32), _p(ws, ctypes.c_int64))
+        return ro, nb, ids, ws
+
+    def jv_screen(self, g, with_evals: bool = False, first: int = 0, last: int | None = None):
+        m = g.edge_u.shape[0]
+        last = m if last is None else last
+        witness = np.full(m, -1, np.int32)
+        evals = np.zeros(m, np.int64) if with_evals else None
+        self.L.ceo_jv_screen_range(self.graph(g), first, last, _p(witness, ctypes.c_int32),
+                                   _p(evals, ctypes.c_int64) if with_evals else None)
+        return (witness, evals) if with_evals else witness
+
+    def jv_verify(self, g, edge_id: int, witness: int) -> bool:
+        return bool(self.L.ceo_jv_verify(self.graph(g), edge_id, witness))
+
+    def content_hash(self, g) -> int:
+        return int(self.L.ceo_content_hash(self.graph(g)))
+
+    def jv_commit(self, g, cand_edges: np.ndarray, cand_witness: np.ndarray):
+        cand_edges = np.ascontiguousarray(cand_edges, np.int32)
+        cand_witness = np.ascontiguousarray(cand_witness, np.int32)
+        out_e = np.empty(cand_edges.shape[0], np.int32)
+        out_w = np.empty(cand_edges.shape[0], np.int32)
+        active = np.empty_like(g.active)
+        k = self.L.ceo_jv_commit(self.graph(g), _p(cand_edges, ctypes.c_int32), _p(cand_witness, ctypes.c_int32),
+                                 cand_edges.shape[0], _p(out_e, ctypes.c_int32), _p(out_w, ctypes.c_int32),
+                                 _p(active, ctypes.c_uint8))
+        return out_e[:k], out_w[:k], active
+
+    def jv_eliminate(self, g, max_rounds: int = 100):
+        """Returns (final active, per-epoch edges_before, per-epoch committed, final hash)."""
+        active = g.active.copy()
+        before = np.zeros(max_rounds, np.int64)
+        committed = np.zeros(max_rounds, np.int64)
+        h = ctypes.c_uint64(0)
+        epochs = self.L.ceo_jv_eliminate(g.n, g.dist_type, _p(g.x, ctypes.c_int64), _p(g.y, ctypes.c_int64),
+                                         g.edge_u.shape[0], _p(g.edge_u, ctypes.c_int32), _p(g.edge_v, ctypes.c_int32),
+                                         _p(g.edge_w, ctypes.c_int64), _p(active, ctypes.c_uint8), max_rounds,
+                                         _p(before, ctypes.c_int64), _p(committed, ctypes.c_int64), ctypes.byref(h))
+        return active, before[:epochs], committed[:epochs], int(h.value)
+
+    def kopt_templates(self, k: int):
+        mates = np.full((208, 14), 0xFF, np.uint8)
+        h = ctypes.c_uint64(0)
+        count = self.L.ceo_kopt_templates(k, _p(mates, ctypes.c_uint8), ctypes.byref(h))
+        return mates[:count].copy(), int(h.value)
+
+    def kopt_costs(self, g, k: int, tasks: np.ndarray, mates: np.ndarray | None = None) -> np.ndarray:
+        if mates is None:
+            mates, _ = self.kopt_templates(k)
+        mates = np.ascontiguousarray(mates, np.uint8)
+        tasks = np.ascontiguousarray(tasks)
+        costs = np.empty((tasks.shape[0], mates.shape[0]), np.int64)
+        self.L.ceo_kopt_costs(g.dist_type, _p(g.x, ctypes.c_int64), _p(g.y, ctypes.c_int64), k,
+                              tasks.ctypes.data, tasks.shape[0], _p(mates, ctypes.c_uint8), mates.shape[0],
+                              _p(costs, ctypes.c_int64))
+        return costs
+
+    def cd_tasks(self, g, u: int, v: int, max_neighborhood: int = 25, max_degree: int = 50):
+        cap = max(1, g.n * (g.n - 1) // 2) if max_neighborhood == 0 else max_neighborhood * (max_neighborhood - 1) // 2 + 1
+        c = np.empty(cap, np.int32)
+        d = np.empty(cap, np.int32)
+        a = np.empty(cap, np.uint8)
+        count = self.L.ceo_cd_tasks(self.graph(g), u, v, max_neighborhood, max_degree, _p(c, ctypes.c_int32),
+                                    _p(d, ctypes.c_int32), _p(a, ctypes.c_uint8))
+        return c[:count].copy(), d[:count].copy(), a[:count].copy()
+
+    def cd_screen(self, g, u: int, v: int, c, d, active, mode: int) -> np.ndarray:
+        c = np.ascontiguousarray(c, np.int32)
+        d = np.ascontiguousarray(d, np.int32)
+        active = np.ascontiguousarray(active, np.uint8)
+        flags = np.empty(c.shape[0], np.uint8)
+        self.L.ceo_cd_screen(self.graph(g), u, v, _p(c, ctypes.c_int32), _p(d, ctypes.c_int32),
+                             _p(active, ctypes.c_uint8), c.shape[0], mode, _p(flags, ctypes.c_uint8))
+        return flags
+
+    def ht_targets(self, g, order: int = 1) -> np.ndarray:
+        out = np.empty(max(1, g.edge_u.shape[0]), np.int32)
+        count = self.L.ceo_ht_targets(self.graph(g), order, _p(out, ctypes.c_int32))
+        return out[:count].copy()
+
+
+def reference_available(dropin: bool = False) -> bool:
+    return (DROPIN_LIB if dropin else REF_LIB).exists()
+
+
+class Reference:
+    """The reference library itself (compiled from its sources by oracle/Makefile)."""
+
+    def __init__(self, dropin: bool = False):
+        path = DROPIN_LIB if dropin else REF_LIB
+        if not path.exists():
+            raise FileNotFoundError(f"{path} is not built (oracle/Makefile needs the reference sources)")
+        L = ctypes.CDLL(str(path))
+        L.ref_last_error.restype = ctypes.c_char_p
+        L.ref_isqrt.restype = ctypes.c_uint64
+        L.ref_isqrt.argtypes = [ctypes.c_uint64]
+        L.ref_exact_distance.argtypes = [ctypes.c_int64] * 4 + [ctypes.c_int, i64p]
+        L.ref_graph_new.argtypes = [ctypes.c_int32, ctypes.c_int, i64p, i64p, ctypes.c_int64, i32p, i32p, i64p, u8p,
+                                    ctypes.POINTER(vp)]
+        L.ref_graph_free.argtypes = [vp]
+        L.ref_graph_set_active.argtypes = [vp, u8p]
+        L.ref_graph_sizes.argtypes = [vp, i64p, i64p]
+        L.ref_graph_csr.argtypes = [vp, i32p, i32p, i32p, i64p]
+        L.ref_graph_active.argtypes = [vp, u8p]
+        L.ref_graph_hash.restype = ctypes.c_uint64
+        L.ref_graph_hash.argtypes = [vp]
+        L.ref_jv_cpu.argtypes = [vp, i32p]
+        L.ref_jv_cuda.argtypes = [vp, i32p, i32p, u64p]
+        L.ref_cuda_available.argtypes = [ctypes.c_char_p, ctypes.c_int]
+        L.ref_jv_verify.argtypes = [vp, ctypes.c_int32, ctypes.c_int32]
+        L.ref_run_jv.argtypes = [vp, ctypes.c_int, ctypes.c_uint32, i64p, ctypes.c_int32, i32p, ctypes.c_int64, i64p,
+                                 u64p, u64p]
+        L.ref_kopt_table.argtypes = [ctypes.c_uint32, u8p, u64p]
+        L.ref_kopt_costs.argtypes = [vp, ctypes.c_uint32, vp, ctypes.c_int64, ctypes.c_int, i64p, i64p]
+        L.ref_cd_candidates.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32,
+                                        ctypes.c_uint32, ctypes.c_int, ctypes.c_int, i64p, ctypes.c_int32]
+        L.ref_ht_targets.argtypes = [vp, ctypes.c_int, i32p, ctypes.c_int32]
+        L.ref_cd_tasks.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32, i32p, i32p,
+                                   u8p, ctypes.c_int64]
+        L.ref_cd_screen_cpu.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, i32p, i32p, u8p, ctypes.c_int64,
+                                        ctypes.c_int, u8p]
+        self.L = L
+
+    def error(self) -> str:
+        return self.L.ref_last_error().decode()
+
+    def _check(self, rc: int) -> int:
+        if rc < 0:
+            raise RuntimeError(self.error())
+        return rc
+
+    def graph(self, g) -> "RefGraph":
+        return RefGraph(self, g)
+
+    def isqrt(self, v: int) -> int:
+        return int(self.L.ref_isqrt(v))
+
+    def distance(self, x1, y1, x2, y2, t) -> int:
+        out = ctypes.c_int64(0)
+        self._check(self.L.ref_exact_distance(x1, y1, x2, y2, t, ctypes.byref(out)))
+        return int(out.value)
+
+    def kopt_table(self, k: int):
+        mates = np.full((208, 14), 0xFF, np.uint8)
+        h = ctypes.c_uint64(0)
+        count = self._check(self.L.ref_kopt_table(k, _p(mates, ctypes.c_uint8), ctypes.byref(h)))
+        return mates[:count].copy(), int(h.value)
+
+
+class RefGraph:
+    """A GraphSnapshot owned by the reference library."""
+
+    def __init__(self, ref: Reference, g):
+        self.ref = ref
+        self.m = int(g.edge_u.shape[0])
+        handle = vp()
+        ref._check(ref.L.ref_graph_new(g.n, g.dist_type, _p(g.x, ctypes.c_int64), _p(g.y, ctypes.c_int64), self.m,
+                                       _p(g.edge_u, ctypes.c_int32), _p(g.edge_v, ctypes.c_int32),
+                                       _p(g.edge_w, ctypes.c_int64), _p(g.active, ctypes.c_uint8), ctypes.byref(handle)))
+        self.handle = handle
+        self.n = g.n
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            self.ref.L.ref_graph_free(self.handle)
+            self.handle = None
+
+    def set_active(self, active: np.ndarray) -> None:
+        active = np.ascontiguousarray(active, np.uint8)
+        self.ref._check(self.ref.L.ref_graph_set_active(self.handle, _p(active, ctypes.c_uint8)))
+
+    def csr(self):
+        m, adj = ctypes.c_int64(0), ctypes.c_int64(0)
+        self.ref.L.ref_graph_sizes(self.handle, ctypes.byref(m), ctypes.byref(adj))
+        ro = np.empty(self.n + 1, np.int32)
+        nb = np.empty(adj.value, np.int32)
+        ids = np.empty(adj.value, np.int32)
+        ws = np.empty(adj.value, np.int64)
+        self.ref.L.ref_graph_csr(self.handle, _p(ro, ctypes.c_int32), _p(nb, ctypes.c_int32), _p(ids, ctypes.c_int32),
+                                 _p(ws, ctypes.c_int64))
+        return ro, nb, ids, ws
+
+    def active(self) -> np.ndarray:
+        out = np.empty(self.m, np.uint8)
+        self.ref.L.ref_graph_active(self.handle, _p(out, ctypes.c_uint8))
+        return out
+
+    def content_hash(self) -> int:
+        return int(self.ref.L.ref_graph_hash(self.handle))
+
+    def jv_cpu(self) -> np.ndarray:
+        w = np.empty(self.m, np.int32)
+        self.ref._check(self.ref.L.ref_jv_cpu(self.handle, _p(w, ctypes.c_int32)))
+        return w
+
+    def jv_cuda(self):
+        w = np.empty(self.m, np.int32)
+        usage = np.zeros(3, np.int32)
+        resident = ctypes.c_uint64(0)
+        self.ref._check(self.ref.L.ref_jv_cuda(self.handle, _p(w, ctypes.c_int32), _p(usage, ctypes.c_int32),
+                                               ctypes.byref(resident)))
+        return w, usage, int(resident.value)
+
+    def jv_verify(self, edge_id: int, witness: int) -> bool:
+        return bool(self.ref.L.ref_jv_verify(self.handle, edge_id, witness))
+
+    def run_jv(self, backend: int, max_rounds: int = 100):
+        """RunJvElimination in place; backend 1 = CPU, 2 = CUDA. Returns (epoch stats [e,3],
+        proof records [r,3] = (epoch, edge_id, witness), initial hash, final hash)."""
+        stats = np.zeros((max_rounds, 3), np.int64)
+        cap = max(1, self.m)
+        records = np.zeros((cap, 3), np.int32)
+        count = ctypes.c_int64(0)
+        h0, h1 = ctypes.c_uint64(0), ctypes.c_uint64(0)
+        epochs = self.ref._check(self.ref.L.ref_run_jv(self.handle, backend, max_rounds, _p(stats, ctypes.c_int64),
+                                                       max_rounds, _p(records, ctypes.c_int32), cap,
+                                                       ctypes.byref(count), ctypes.byref(h0), ctypes.byref(h1)))
+        return stats[:epochs].copy(), records[:count.value].copy(), int(h0.value), int(h1.value)
+
+    def kopt_costs(self, k: int, tasks: np.ndarray, backend: int = 1):
+        tasks = np.ascontiguousarray(tasks)
+        T = {3: 4, 4: 25, 5: 208}[k]
+        costs = np.empty((tasks.shape[0], T), np.int64)
+        meta = np.zeros(5, np.int64)
+        self.ref._check(self.ref.L.ref_kopt_costs(self.handle, k, tasks.ctypes.data, tasks.shape[0], backend,
+                                                  _p(costs, ctypes.c_int64), _p(meta, ctypes.c_int64)))
+        return costs, meta
+
+    def cd_tasks(self, u: int, v: int, max_neighborhood: int = 25, max_degree: int = 50):
+        cap = max(1, self.n * (self.n - 1) // 2)
+        c = np.empty(cap, np.int32)
+        d = np.empty(cap, np.int32)
+        a = np.empty(cap, np.uint8)
+        count = self.ref._check(self.ref.L.ref_cd_tasks(self.handle, u, v, max_neighborhood, max_degree,
+                                                        _p(c, ctypes.c_int32), _p(d, ctypes.c_int32),
+                                                        _p(a, ctypes.c_uint8), cap))
+        return c[:count].copy(), d[:count].copy(), a[:count].copy()
+
+    def cd_screen(self, u, v, c, d, active, mode: int) -> np.ndarray:
+        c = np.ascontiguousarray(c, np.int32)
+        d = np.ascontiguousarray(d, np.int32)
+        active = np.ascontiguousarray(active, np.uint8)
+        flags = np.empty(c.shape[0], np.uint8)
+        self.ref._check(self.ref.L.ref_cd_screen_cpu(self.handle, u, v, _p(c, ctypes.c_int32), _p(d, ctypes.c_int32),
+                                                     _p(active, ctypes.c_uint8), c.shape[0], mode,
+                                                     _p(flags, ctypes.c_uint8)))
+        return flags
+
+    def cd_candidates(self, u, v, max_neighborhood=25, max_cd=5, max_degree=50, mode=0, backend=1):
+        cap = 1 << 16
+        out = np.empty((cap, 3), np.int64)
+        count = self.ref._check(self.ref.L.ref_cd_candidates(self.handle, u, v, max_neighborhood, max_cd, max_degree,
+                                                             mode, backend, _p(out, ctypes.c_int64), cap))
+        return out[:count].copy()
+
+    def ht_targets(self, order: int = 1) -> np.ndarray:
+        out = np.empty(max(1, self.m), np.int32)
+        count = self.ref._check(self.ref.L.ref_ht_targets(self.handle, order, _p(out, ctypes.c_int32), out.shape[0]))
+        return out[:count].copy()
