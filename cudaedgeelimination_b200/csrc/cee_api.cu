@@ -452,7 +452,7 @@ int KoptCoords(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x, con
   return CEE_OK;
 }
 
-int DefaultRowsPerTile(uint32_t k) { return k == 3 ? 512 : (k == 4 ? 128 : 32); }
+int DefaultRowsPerTile(uint32_t k) { return k == 3 ? 256 : (k == 4 ? 160 : 32); }
 
 // Uploads the rows of every segment and records the launch description.
 int KoptPrepareSegments(cee_ctx* ctx, int32_t segments, const uint32_t* ks, const KoptTable* const* tables,

@@ -11,11 +11,13 @@
 // where w are the snapshot's CSR slot weights and C the exact TSPLIB distance.
 //
 // B200 mapping: the 32 lanes score up to 32 candidates at once and keep the running
-// top-10 as a warp-wide bitonic-sorted list (one 64-bit key (score << 32 | node) per lane);
-// the witness search flattens the (c, d) pairs of all candidates, in candidate order,
-// over the lanes. Lanes may test pairs of later candidates speculatively, but a candidate
-// is only accepted once every pair of it has been tested and every earlier candidate is
-// known to have a compatible d, so the chosen witness is exactly the sequential one.
+// top-10 as a warp-wide bitonic-sorted list (one 64-bit key (score << 32 | node) per lane).
+// The witness search first tests the first three neighbours of all ten candidates at once
+// (30 lanes; most candidates meet a compatible d there), then flattens the remaining (c, d)
+// pairs of the still-open candidates, in candidate order, over the lanes. Lanes may test
+// pairs of later candidates speculatively, but a candidate is only accepted once every pair
+// of it has been tested and every earlier candidate is known to have a compatible d, so the
+// chosen witness is exactly the sequential one.
 #pragma once
 
 #include "device_common.cuh"
@@ -42,8 +44,8 @@ struct JvGraph {
 struct JvWarpScratch {
   int32_t c[kJvMaxCandidates];
   int32_t row[kJvMaxCandidates];   // first CSR slot of N(c)
-  int32_t begin[kJvMaxCandidates]; // first flattened pair index of candidate i
-  int32_t end[kJvMaxCandidates];   // one past its last pair index
+  int32_t begin[kJvMaxCandidates]; // first flattened index of candidate i's remaining pairs
+  int32_t end[kJvMaxCandidates];   // one past its last one (row end while the table is built)
   uint32_t cac[kJvMaxCandidates];  // C(a, c)
   uint32_t cbc[kJvMaxCandidates];  // C(b, c)
 };
@@ -92,30 +94,71 @@ __device__ __forceinline__ int32_t jv_screen_edge(const JvGraph& g, int64_t e,
   const int nc = __popc(__ballot_sync(kFullMask, lane < kJvMaxCandidates && top != kEmptyKey));
   if (nc == 0) return -1;
 
-  // ---- candidate table: row ranges and flattened pair numbering ------------------------
-  int deg = 0;
-  if (lane < nc) {
-    const int32_t c = static_cast<int32_t>(top & 0xffffffffu);
-    const int32_t rc0 = __ldg(g.row_offsets + c), rc1 = __ldg(g.row_offsets + c + 1);
-    const int2 pc = __ldg(g.xy + c);
-    deg = rc1 - rc0;
-    s.c[lane] = c;
-    s.row[lane] = rc0;
-    s.cac[lane] = exact_distance(pa, pc, g.dist_type);
-    s.cbc[lane] = exact_distance(pb, pc, g.dist_type);
+  // ---- candidate table: C(a,c) on lanes 0..9, C(b,c) on lanes 10..19 ------------------
+  {
+    const int ci = lane < kJvMaxCandidates ? lane : lane - kJvMaxCandidates;
+    const uint64_t key = __shfl_sync(kFullMask, top, ci);
+    if (lane < 2 * kJvMaxCandidates && ci < nc) {
+      const int32_t c = static_cast<int32_t>(key & 0xffffffffu);
+      const uint32_t dist = exact_distance(lane < kJvMaxCandidates ? pa : pb, __ldg(g.xy + c), g.dist_type);
+      if (lane < kJvMaxCandidates) {
+        s.c[ci] = c;
+        s.row[ci] = __ldg(g.row_offsets + c);
+        s.end[ci] = __ldg(g.row_offsets + c + 1);  // row end, replaced by pair numbering below
+        s.cac[ci] = dist;
+      } else {
+        s.cbc[ci] = dist;
+      }
+    }
   }
-  const int incl = warp_inclusive_sum(deg, lane);
+  __syncwarp();
+
+  // Tests pair (candidate ci, CSR slot); true when d is compatible with (a,b).
+  auto compatible_pair = [&](int ci, int32_t slot) -> bool {
+    const int32_t d = __ldg(g.nbr + slot);
+    if (d == a || d == b) return false;
+    if (static_cast<uint32_t>(d) >= static_cast<uint32_t>(g.n)) {
+      atomicOr(error, 1);
+      return false;
+    }
+    const int2 pd = __ldg(g.xy + d);
+    const int64_t left = cab + __ldg(g.slot_w + slot);
+    const int64_t first = static_cast<int64_t>(s.cac[ci]) + exact_distance(pd, pb, g.dist_type);
+    const int64_t second = static_cast<int64_t>(exact_distance(pa, pd, g.dist_type)) + s.cbc[ci];
+    return left <= first || left <= second;
+  };
+
+  // ---- witness search, breadth first: the first kHead neighbours of every candidate -----
+  // (most candidates meet a compatible d among their first neighbours)
+  constexpr int kHead = 3;
+  const int deg = lane < nc ? s.end[lane] - s.row[lane] : 0;
+  uint32_t compatible = 0;  // candidates known to have a compatible d (warp-uniform)
+  {
+    const int hi = lane / kHead, hj = lane - hi * kHead;
+    bool hit = false;
+    if (hi < nc) {
+      const int32_t row = s.row[hi];
+      if (hj < s.end[hi] - row) hit = compatible_pair(hi, row + hj);
+    }
+    compatible = __reduce_or_sync(kFullMask, hit ? 1u << hi : 0u);
+  }
+  const uint32_t all = (1u << nc) - 1u;
+  uint32_t open = all & ~compatible;
+  if (open == 0) return -1;
+
+  // ---- then the remaining neighbours of the open candidates, flattened in candidate order --
+  const int rest = ((open >> lane) & 1u) != 0 ? max(deg - kHead, 0) : 0;
+  const int incl = warp_inclusive_sum(rest, lane);
+  __syncwarp();
   if (lane < nc) {
-    s.begin[lane] = incl - deg;
+    s.begin[lane] = incl - rest;
     s.end[lane] = incl;
   }
   const int pairs = __shfl_sync(kFullMask, incl, nc - 1);
   __syncwarp();
-
-  // ---- witness search ------------------------------------------------------------------
-  const uint32_t all = (nc == 32) ? kFullMask : ((1u << nc) - 1u);
-  uint32_t compatible = 0;  // candidates known to have a compatible d (warp-uniform)
-  int base = 0;
+  int first_open = __ffs(open) - 1;
+  if (s.end[first_open] == s.begin[first_open]) return s.c[first_open];
+  int base = s.begin[first_open];
   while (true) {
     const int p = base + lane;
     uint32_t bit = 0;
@@ -123,26 +166,14 @@ __device__ __forceinline__ int32_t jv_screen_edge(const JvGraph& g, int64_t e,
       int ci = 0;
 #pragma unroll
       for (int i = 1; i < kJvMaxCandidates; ++i) ci += (i < nc && s.begin[i] <= p) ? 1 : 0;
-      if (((compatible >> ci) & 1u) == 0) {
-        const int32_t slot = s.row[ci] + (p - s.begin[ci]);
-        const int32_t d = __ldg(g.nbr + slot);
-        if (d != a && d != b) {
-          if (static_cast<uint32_t>(d) >= static_cast<uint32_t>(g.n)) {
-            atomicOr(error, 1);
-          } else {
-            const int2 pd = __ldg(g.xy + d);
-            const int64_t left = cab + __ldg(g.slot_w + slot);
-            const int64_t first = static_cast<int64_t>(s.cac[ci]) + exact_distance(pd, pb, g.dist_type);
-            const int64_t second = static_cast<int64_t>(exact_distance(pa, pd, g.dist_type)) + s.cbc[ci];
-            if (left <= first || left <= second) bit = 1u << ci;
-          }
-        }
+      if (((compatible >> ci) & 1u) == 0 && compatible_pair(ci, s.row[ci] + kHead + (p - s.begin[ci]))) {
+        bit = 1u << ci;
       }
     }
     compatible |= __reduce_or_sync(kFullMask, bit);
-    const uint32_t open = all & ~compatible;
+    open = all & ~compatible;
     if (open == 0) return -1;  // every candidate has a compatible neighbour
-    const int first_open = __ffs(open) - 1;
+    first_open = __ffs(open) - 1;
     const int chunk_end = base + 32;
     if (s.end[first_open] <= chunk_end) return s.c[first_open];
     base = max(chunk_end, s.begin[first_open]);

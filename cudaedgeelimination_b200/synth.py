@@ -113,3 +113,49 @@ def kopt_instance(rows: int = 200_000, n: int = 15_000, seed: int = SEED_BASE + 
 
 def batch_instance(index: int, seed: int = SEED_BASE + 3, n_lo: float = 100.0, n_hi: float = 5000.0) -> GraphSnapshot:
     return _Handle(lib().cees_batch_instance(seed, index, n_lo, n_hi)).snapshot()
+
+
+class BatchUnion:
+    """The 4,096-instance batching mix as one disjoint-union snapshot: global node and edge ids,
+    per-instance offsets node_begin / edge_begin, and the union CSR."""
+
+    def __init__(self, count: int = 4096, seed: int = SEED_BASE + 3, n_lo: float = 100.0, n_hi: float = 5000.0):
+        L = lib()
+        L.cees_batch_build.restype = ctypes.c_void_p
+        L.cees_batch_build.argtypes = [ctypes.c_uint64, ctypes.c_int32, ctypes.c_double, ctypes.c_double]
+        L.cees_batch_free.argtypes = [ctypes.c_void_p]
+        L.cees_batch_sizes.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.cees_batch_copy.argtypes = [ctypes.c_void_p] * 11
+        handle = L.cees_batch_build(seed, count, n_lo, n_hi)
+        if not handle:
+            raise RuntimeError("batch generation failed")
+        try:
+            nodes, edges = ctypes.c_int64(0), ctypes.c_int64(0)
+            L.cees_batch_sizes(handle, ctypes.byref(nodes), ctypes.byref(edges))
+            n, m = nodes.value, edges.value
+            if n >= 2**31 or 2 * m >= 2**31:
+                raise ValueError("batch exceeds the int32 id range")
+            self.count = count
+            self.node_begin = np.empty(count + 1, np.int64)
+            self.edge_begin = np.empty(count + 1, np.int64)
+            x, y = np.empty(n, np.int64), np.empty(n, np.int64)
+            eu, ev, w = np.empty(m, np.int32), np.empty(m, np.int32), np.empty(m, np.int64)
+            ro, nb, ids = np.empty(n + 1, np.int32), np.empty(2 * m, np.int32), np.empty(2 * m, np.int32)
+            L.cees_batch_copy(handle, *(a.ctypes.data for a in (self.node_begin, self.edge_begin, x, y, eu, ev, w,
+                                                                  ro, nb, ids)))
+        finally:
+            L.cees_batch_free(handle)
+        g = GraphSnapshot.__new__(GraphSnapshot)
+        g.n, g.dist_type, g.x, g.y = int(n), EUC_2D, x, y
+        g.edge_u, g.edge_v, g.edge_w, g.active = eu, ev, w, np.ones(m, np.uint8)
+        g.row_offsets, g.neighbors, g.csr_edge_ids = ro, nb, ids
+        g.csr_weights = None
+        self.graph = g
+
+    def instance(self, i: int) -> GraphSnapshot:
+        """Instance i as a standalone snapshot (local ids)."""
+        n0, n1 = int(self.node_begin[i]), int(self.node_begin[i + 1])
+        e0, e1 = int(self.edge_begin[i]), int(self.edge_begin[i + 1])
+        g = self.graph
+        return GraphSnapshot(n1 - n0, g.dist_type, g.x[n0:n1], g.y[n0:n1], g.edge_u[e0:e1] - n0,
+                             g.edge_v[e0:e1] - n0, g.edge_w[e0:e1], g.active[e0:e1])

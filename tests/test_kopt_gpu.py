@@ -1,0 +1,98 @@
+"""k-opt leaf cost matrices on the B200 against the CPU oracle: int64 cells bit-exact."""
+import numpy as np
+import pytest
+
+from cudaedgeelimination_b200 import KOPT_TASK_DTYPE, BuildKOptReconnectTable, GraphSnapshot, synth
+from cudaedgeelimination_b200._native import NativeError
+
+pytestmark = pytest.mark.gpu
+
+INVALID = np.iinfo(np.int64).max
+
+
+def coords_only(xs, ys, dist_type=0):
+    return GraphSnapshot.from_edges(xs, ys, np.zeros((0, 2), np.int64), dist_type)
+
+
+def make_tasks(g, k, ports_rows):
+    tasks = np.zeros(len(ports_rows), KOPT_TASK_DTYPE)
+    for r, ports in enumerate(ports_rows):
+        tasks[r]["port_nodes"][:len(ports)] = ports
+        tasks[r]["deleted_cost"] = sum(g.distance(ports[2 * e], ports[2 * e + 1]) for e in range(k))
+    return tasks
+
+
+def seventeen():
+    # the small point set of the reference's matrix test: x = 7i mod 23, y = (i^2 + 3i) mod 19
+    i = np.arange(17)
+    return (7 * i) % 23, (i * i + 3 * i) % 19
+
+
+@pytest.mark.parametrize("dist_type", [0, 1])
+def test_consecutive_adjacent_and_strided_ports(ctx, port, dist_type):
+    g = coords_only(*seventeen(), dist_type)
+    for k in (3, 4, 5):
+        rows = [list(range(2 * k)), [0, 1, 1, 2, 3, 4, 5, 6, 7, 8][:2 * k],
+                [(3 * p + 2) % 17 for p in range(2 * k)]]
+        tasks = make_tasks(g, k, rows)
+        table = BuildKOptReconnectTable(k)
+        gpu, _ = ctx.kopt_costs(g, table, tasks)
+        cpu = port.kopt_costs(g, k, tasks, table.templates)
+        np.testing.assert_array_equal(gpu, cpu)
+        assert (gpu[1] == INVALID).any()  # shared ports produce invalid cells
+
+
+def test_repeated_rows(ctx, port):
+    g = coords_only(*seventeen())
+    tasks = make_tasks(g, 5, [list(range(10))] * 40)
+    table = BuildKOptReconnectTable(5)
+    gpu, _ = ctx.kopt_costs(g, table, tasks)
+    np.testing.assert_array_equal(gpu, port.kopt_costs(g, 5, tasks))
+    assert (gpu == gpu[0]).all()
+
+
+@pytest.mark.parametrize("dist_type", [0, 1])
+def test_walk_rows_all_k(ctx, port, dist_type):
+    g, tasks = synth.kopt_instance(rows=6001, n=3000)
+    if dist_type == 0:
+        g = GraphSnapshot(g.n, 0, g.x, g.y, g.edge_u, g.edge_v, g.edge_w, g.active)
+    for k in (3, 4, 5):
+        table = BuildKOptReconnectTable(k)
+        gpu, _ = ctx.kopt_costs(g, table, tasks[k])
+        np.testing.assert_array_equal(gpu, port.kopt_costs(g, k, tasks[k]))
+
+
+def test_multi_segment_matches_single(ctx, port):
+    g, tasks = synth.kopt_instance(rows=3001, n=2000)
+    outs, stats = ctx.kopt_costs_multi(g, [3, 4, 5], [tasks[3], tasks[4], tasks[5]])
+    for k, out in zip((3, 4, 5), outs):
+        np.testing.assert_array_equal(out, port.kopt_costs(g, k, tasks[k]))
+    # odd row counts and a single row
+    outs, _ = ctx.kopt_costs_multi(g, [5, 3], [tasks[5][:1], tasks[3][:7]])
+    np.testing.assert_array_equal(outs[0], port.kopt_costs(g, 5, tasks[5][:1]))
+    np.testing.assert_array_equal(outs[1], port.kopt_costs(g, 3, tasks[3][:7]))
+
+
+def test_cache_contract(ctx, port):
+    """Snapshot / template / workspace hits as the reference's test_kopt.cpp:224-234, 322-324."""
+    ctx.clear(2)
+    g = coords_only(*seventeen())
+    rows = {k: make_tasks(g, k, [list(range(2 * k))] * 3) for k in (3, 4, 5)}
+    for k in (3, 4, 5):
+        _, s = ctx.kopt_costs(g, BuildKOptReconnectTable(k), rows[k])
+        assert s.snapshot_hit == (k != 3) and not s.template_hit and s.resident_bytes > 0
+    _, s = ctx.kopt_costs(g, BuildKOptReconnectTable(5), rows[5])
+    assert s.snapshot_hit and s.template_hit and s.workspace_hit
+    ceil = GraphSnapshot(g.n, 1, g.x, g.y, g.edge_u, g.edge_v, g.edge_w, g.active)
+    gpu, s = ctx.kopt_costs(ceil, BuildKOptReconnectTable(5), rows[5])
+    np.testing.assert_array_equal(gpu, port.kopt_costs(ceil, 5, rows[5]))
+    assert not s.snapshot_hit and s.template_hit and s.workspace_hit
+
+
+def test_bad_template_rejected(ctx):
+    g = coords_only(*seventeen())
+    table = BuildKOptReconnectTable(3)
+    table.templates = table.templates.copy()
+    table.templates[0, 0] = table.templates[0, 1]  # no longer a perfect matching
+    with pytest.raises(NativeError):
+        ctx.kopt_costs(g, table, make_tasks(g, 3, [list(range(6))]))
