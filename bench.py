@@ -169,9 +169,11 @@ def reference_jv_rate(batch, budget_s: float, threads: int):
 # ---------------------------------------------------------------- our arm -----------------
 
 def pinned_copy(arr: np.ndarray):
+    """A page-locked copy of `arr` (any dtype) and a numpy view of it."""
     import torch
-    t = torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()
-    return t, t.numpy()
+    arr = np.ascontiguousarray(arr)
+    t = torch.from_numpy(arr.view(np.uint8).reshape(-1)).pin_memory()
+    return t, t.numpy().view(arr.dtype).reshape(arr.shape)
 
 
 def run_ours(args, rank: int, world: int, device: int):
@@ -336,8 +338,8 @@ def run_kopt(args, ctx, stream, device, world):
     outs = [np.empty((t.shape[0], KOPT_TEMPLATE_COUNTS[k]), np.int64) for k, t in zip(ks, lists)]
     ctx.kopt_fetch(outs)
     # end to end: H2D of the rows, launch, D2H of the full matrices into pinned buffers
-    pinned = [pinned_copy(o)[1] for o in outs]
-    ptasks = [pinned_copy(t)[1] for t in lists]
+    keep = [pinned_copy(t) for t in lists]
+    ptasks = [k[1] for k in keep]
     t0 = time.perf_counter()
     for _ in range(args.steps):
         out_arrays, stats = ctx.kopt_costs_multi(g, ks, ptasks)

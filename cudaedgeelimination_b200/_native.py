@@ -22,6 +22,12 @@ CEE_ERR_NODEVICE = -5
 CEE_ERR_TIMEOUT = -6
 CEE_ERR_STATE = -7
 
+OPT_JV_KERNEL = 1
+OPT_JV_WAVES = 2
+OPT_KOPT_ROWS_K3 = 3
+OPT_KOPT_ROWS_K4 = 4
+OPT_KOPT_ROWS_K5 = 5
+
 
 class GraphView(ctypes.Structure):
     _fields_ = [
@@ -82,6 +88,7 @@ def lib() -> ctypes.CDLL:
             "cee_ctx_synchronize": (ctypes.c_int, [vp]),
             "cee_ctx_resident_bytes": (ctypes.c_uint64, [vp]),
             "cee_ctx_clear": (ctypes.c_int, [vp, ctypes.c_uint]),
+            "cee_ctx_set_option": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int64]),
             "cee_jv_screen": (ctypes.c_int, [vp, ctypes.POINTER(GraphView), c_i32p, ctypes.POINTER(JvStats)]),
             "cee_jv_prepare": (ctypes.c_int, [vp, ctypes.POINTER(GraphView), ctypes.POINTER(JvStats)]),
             "cee_jv_launch": (ctypes.c_int, [vp]),

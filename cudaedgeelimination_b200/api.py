@@ -61,6 +61,10 @@ class Context:
     def resident_bytes(self) -> int:
         return int(_native.lib().cee_ctx_resident_bytes(self.handle))
 
+    def set_option(self, option: int, value: int) -> None:
+        """Launch-shape option (cee_ctx_set_option); results never depend on it."""
+        _native.check(self.handle, _native.lib().cee_ctx_set_option(self.handle, option, value))
+
     def clear(self, what: int = 0xF) -> None:
         _native.check(self.handle, _native.lib().cee_ctx_clear(self.handle, what))
 

@@ -68,7 +68,8 @@ int Activate(cee_ctx* ctx) {
 
 // Coordinates as int32 offsets from the bounding-box corner; rejects spans >= 2^30.
 int PackCoordinates(cee_ctx* ctx, int32_t n, const int64_t* x, const int64_t* y,
-                    std::vector<int2>* out) {
+                    std::vector<int2>* out, bool* narrow) {
+  *narrow = true;
   if (n <= 0) {
     out->clear();
     return CEE_OK;
@@ -87,6 +88,7 @@ int PackCoordinates(cee_ctx* ctx, int32_t n, const int64_t* x, const int64_t* y,
     return Fail(ctx, CEE_ERR_RANGE,
                 "coordinate span >= 2^30: outside the exact int32 distance range of the kernels");
   }
+  *narrow = span_x < kNarrowSpan && span_y < kNarrowSpan;
   out->resize(static_cast<size_t>(n));
   for (int32_t i = 0; i < n; ++i) {
     (*out)[i] = make_int2(static_cast<int32_t>(x[i] - min_x), static_cast<int32_t>(y[i] - min_y));
@@ -174,6 +176,23 @@ float EventMs(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
+// Resident blocks per SM of every kernel variant (grid sizing).
+int QueryOccupancyOne(const void* kernel, int threads, int smem, int* out) {
+  int blocks = 0;
+  const cudaError_t status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, smem);
+  *out = std::max(1, blocks);
+  return status;
+}
+
+cudaError_t QueryOccupancy(cee_ctx* ctx) {
+  int bad = 0;
+  bad |= QueryOccupancyOne(reinterpret_cast<const void*>(jv_screen_thread_kernel<false>), kJvThreadBlock, 0, &ctx->occ_jv_thread[0]);
+  bad |= QueryOccupancyOne(reinterpret_cast<const void*>(jv_screen_thread_kernel<true>), kJvThreadBlock, 0, &ctx->occ_jv_thread[1]);
+  bad |= QueryOccupancyOne(reinterpret_cast<const void*>(jv_screen_warp_kernel<false>), kJvWarpsPerBlock * 32, 0, &ctx->occ_jv_warp[0]);
+  bad |= QueryOccupancyOne(reinterpret_cast<const void*>(jv_screen_warp_kernel<true>), kJvWarpsPerBlock * 32, 0, &ctx->occ_jv_warp[1]);
+  return bad ? cudaErrorInvalidValue : cudaSuccess;
+}
+
 // ---------------------------------------------------------------- JV --------------------
 
 int JvPrepare(cee_ctx* ctx, const cee_graph_view* g, cee_jv_stats* stats) {
@@ -191,7 +210,7 @@ int JvPrepare(cee_ctx* ctx, const cee_graph_view* g, cee_jv_stats* stats) {
   if (!static_hit) {
     s.has_static = false;
     std::vector<int2> xy;
-    rc = PackCoordinates(ctx, g->n, g->x, g->y, &xy);
+    rc = PackCoordinates(ctx, g->n, g->x, g->y, &xy, &s.narrow);
     if (rc != CEE_OK) return rc;
     std::vector<int2> uv(static_cast<size_t>(g->m));
     std::vector<int32_t> w32(static_cast<size_t>(g->m));
@@ -283,9 +302,24 @@ int JvLaunch(cee_ctx* ctx) {
   graph.row_offsets = static_cast<const int32_t*>(s.ro.ptr);
   graph.nbr = static_cast<const int32_t*>(s.nbr.ptr);
   graph.slot_w = static_cast<const int32_t*>(s.slotw.ptr);
-  const int blocks = GridFor(s.m, kJvWarpsPerBlock, ctx->sm_count * ctx->jv_blocks_per_sm);
-  jv_screen_kernel<<<blocks, kJvWarpsPerBlock * 32, 0, ctx->stream>>>(
-      graph, 0, s.m, static_cast<int32_t*>(s.witness.ptr), ctx->d_error);
+  int32_t* witness = static_cast<int32_t*>(s.witness.ptr);
+  if (ctx->jv_kernel == 1) {
+    const int per_sm = s.narrow ? ctx->occ_jv_warp[0] : ctx->occ_jv_warp[1];
+    const int blocks = GridFor(s.m, kJvWarpsPerBlock, ctx->sm_count * per_sm);
+    if (s.narrow) {
+      jv_screen_warp_kernel<false><<<blocks, kJvWarpsPerBlock * 32, 0, ctx->stream>>>(graph, 0, s.m, witness, ctx->d_error);
+    } else {
+      jv_screen_warp_kernel<true><<<blocks, kJvWarpsPerBlock * 32, 0, ctx->stream>>>(graph, 0, s.m, witness, ctx->d_error);
+    }
+  } else {
+    const int per_sm = s.narrow ? ctx->occ_jv_thread[0] : ctx->occ_jv_thread[1];
+    const int blocks = GridFor(s.m, kJvThreadBlock, ctx->sm_count * per_sm * ctx->jv_waves);
+    if (s.narrow) {
+      jv_screen_thread_kernel<false><<<blocks, kJvThreadBlock, 0, ctx->stream>>>(graph, 0, s.m, witness, ctx->d_error);
+    } else {
+      jv_screen_thread_kernel<true><<<blocks, kJvThreadBlock, 0, ctx->stream>>>(graph, 0, s.m, witness, ctx->d_error);
+    }
+  }
   const cudaError_t status = cudaGetLastError();
   if (status != cudaSuccess) return CudaFail(ctx, status, "jv_screen_kernel launch");
   return CEE_OK;
@@ -438,7 +472,7 @@ int KoptCoords(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x, con
   *hit = false;
   s.has_coords = false;
   std::vector<int2> xy;
-  int rc = PackCoordinates(ctx, n, x, y, &xy);
+  int rc = PackCoordinates(ctx, n, x, y, &xy, &s.narrow);
   if (rc != CEE_OK) return rc;
   cudaError_t status = s.xy.Reserve(xy.size() * sizeof(int2) + 16, nullptr);
   if (status != cudaSuccess) return CudaFail(ctx, status, "k-opt coordinate allocation");
@@ -452,7 +486,9 @@ int KoptCoords(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x, con
   return CEE_OK;
 }
 
-int DefaultRowsPerTile(uint32_t k) { return k == 3 ? 256 : (k == 4 ? 160 : 32); }
+int KoptTemplatesFor(int k) { return k == 3 ? 4 : (k == 4 ? 25 : 208); }
+
+int DefaultRowsPerTile(uint32_t k) { return k == 3 ? 128 : (k == 4 ? 128 : 32); }
 
 // Uploads the rows of every segment and records the launch description.
 int KoptPrepareSegments(cee_ctx* ctx, int32_t segments, const uint32_t* ks, const KoptTable* const* tables,
@@ -528,7 +564,11 @@ int KoptLaunchPrepared(cee_ctx* ctx) {
     smem = std::max(smem, kopt_tile_smem(s.launch.seg[i].k, s.launch.seg[i].rows_per_tile));
   }
   if (smem > kKoptSmemBytes) return Fail(ctx, CEE_ERR_INVALID, "k-opt tile exceeds shared memory");
-  kopt_cost_kernel<<<s.tiles, kKoptThreads, smem, ctx->stream>>>(s.launch, ctx->d_error);
+  if (s.narrow) {
+    kopt_cost_kernel<false><<<s.tiles, kKoptThreads, smem, ctx->stream>>>(s.launch, ctx->d_error);
+  } else {
+    kopt_cost_kernel<true><<<s.tiles, kKoptThreads, smem, ctx->stream>>>(s.launch, ctx->d_error);
+  }
   const cudaError_t status = cudaGetLastError();
   if (status != cudaSuccess) return CudaFail(ctx, status, "kopt_cost_kernel launch");
   return CEE_OK;
@@ -641,11 +681,7 @@ int cee_create(int device, cee_ctx** out) {
   if (status == cudaSuccess) status = cudaMalloc(&ctx->d_error, sizeof(int32_t));
   if (status == cudaSuccess) status = cudaHostAlloc(&ctx->h_error, sizeof(int32_t), cudaHostAllocDefault);
   if (status == cudaSuccess) status = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
-  if (status == cudaSuccess) {
-    int blocks = 0;
-    status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, jv_screen_kernel, kJvWarpsPerBlock * 32, 0);
-    ctx->jv_blocks_per_sm = std::max(1, blocks);
-  }
+  if (status == cudaSuccess) status = QueryOccupancy(ctx);
   if (status != cudaSuccess) {
     const std::string message = std::string("context creation: ") + cudaGetErrorString(status);
     cudaGetLastError();
@@ -706,6 +742,33 @@ int cee_ctx_clear(cee_ctx* ctx, unsigned what) {
   if (what & 4u) ctx->cd.Release();
   if (what & 8u) ReleaseBatch(ctx);
   return CEE_OK;
+}
+
+int cee_ctx_set_option(cee_ctx* ctx, int32_t option, int64_t value) {
+  if (ctx == nullptr) return Fail(nullptr, CEE_ERR_INVALID, "null context");
+  switch (option) {
+    case CEE_OPT_JV_KERNEL:
+      if (value != 0 && value != 1) return Fail(ctx, CEE_ERR_INVALID, "JV kernel must be 0 (thread) or 1 (warp)");
+      ctx->jv_kernel = static_cast<int>(value);
+      return CEE_OK;
+    case CEE_OPT_JV_WAVES:
+      if (value < 1 || value > 64) return Fail(ctx, CEE_ERR_INVALID, "JV waves must lie in [1,64]");
+      ctx->jv_waves = static_cast<int>(value);
+      return CEE_OK;
+    case CEE_OPT_KOPT_ROWS_K3:
+    case CEE_OPT_KOPT_ROWS_K4:
+    case CEE_OPT_KOPT_ROWS_K5: {
+      const int k = option - CEE_OPT_KOPT_ROWS_K3 + 3;
+      if (value != 0 && (value < 2 || value % 2 != 0 || kopt_tile_smem(k, static_cast<int>(value)) > kKoptSmemBytes ||
+                         value * KoptTemplatesFor(k) > (int64_t{1} << 20))) {
+        return Fail(ctx, CEE_ERR_INVALID, "k-opt rows per tile must be even and fit the shared-memory tile");
+      }
+      ctx->kopt_rows_per_tile[k - 3] = static_cast<int>(value);
+      return CEE_OK;
+    }
+    default:
+      return Fail(ctx, CEE_ERR_INVALID, "unknown option");
+  }
 }
 
 // ---- JV ----
@@ -886,7 +949,7 @@ int cee_cd_screen(cee_ctx* ctx, const cee_graph_view* graph, int32_t u, int32_t 
         SameArray(s.hy, graph->y, graph->n))) {
     s.has_coords = false;
     std::vector<int2> xy;
-    rc = PackCoordinates(ctx, graph->n, graph->x, graph->y, &xy);
+    rc = PackCoordinates(ctx, graph->n, graph->x, graph->y, &xy, &s.narrow);
     if (rc != CEE_OK) return rc;
     cudaError_t status = s.xy.Reserve(xy.size() * sizeof(int2) + 16, nullptr);
     if (status == cudaSuccess) status = cudaMemcpy(s.xy.ptr, xy.data(), xy.size() * sizeof(int2), cudaMemcpyHostToDevice);
@@ -903,9 +966,15 @@ int cee_cd_screen(cee_ctx* ctx, const cee_graph_view* graph, int32_t u, int32_t 
   cudaStream_t st = ctx->stream;
   cudaMemsetAsync(ctx->d_error, 0, sizeof(int32_t), st);
   cudaMemcpyAsync(s.tasks.ptr, tasks, static_cast<size_t>(count) * sizeof(cee_cd_task), cudaMemcpyHostToDevice, st);
-  cd_screen_kernel<<<GridFor(count, 256, 1 << 30), 256, 0, st>>>(
-      u, v, static_cast<const CdTask*>(s.tasks.ptr), count, static_cast<const int2*>(s.xy.ptr), s.n, s.dist_type,
-      mode, static_cast<uint8_t*>(s.flags.ptr), ctx->d_error);
+  if (s.narrow) {
+    cd_screen_kernel<false><<<GridFor(count, 256, 1 << 30), 256, 0, st>>>(
+        u, v, static_cast<const CdTask*>(s.tasks.ptr), count, static_cast<const int2*>(s.xy.ptr), s.n,
+        s.dist_type, mode, static_cast<uint8_t*>(s.flags.ptr), ctx->d_error);
+  } else {
+    cd_screen_kernel<true><<<GridFor(count, 256, 1 << 30), 256, 0, st>>>(
+        u, v, static_cast<const CdTask*>(s.tasks.ptr), count, static_cast<const int2*>(s.xy.ptr), s.n,
+        s.dist_type, mode, static_cast<uint8_t*>(s.flags.ptr), ctx->d_error);
+  }
   status = cudaGetLastError();
   if (status != cudaSuccess) return CudaFail(ctx, status, "cd_screen_kernel launch");
   cudaMemcpyAsync(flags_out, s.flags.ptr, static_cast<size_t>(count), cudaMemcpyDeviceToHost, st);

@@ -28,6 +28,7 @@ struct JvState {
   std::vector<int64_t> hx, hy, hw;
   std::vector<int32_t> heu, hev;
   DevBuf xy, uv, w32;
+  bool narrow = true;  // coordinate span < 2^26: FP64 distance path
   // dynamic workspace, refreshed every call
   DevBuf active, ro, nbr, ids, slotw, witness;
   int64_t adjacency = 0;
@@ -65,6 +66,7 @@ struct KoptState {
   int32_t n = 0, dist_type = 0;
   std::vector<int64_t> hx, hy;
   DevBuf xy;
+  bool narrow = true;
   KoptTable user[3];   // caller templates per k (the reference's template cache)
   KoptTable canon[3];  // this library's proper templates per k
   DevBuf tasks, costs;
@@ -92,6 +94,7 @@ struct CdState {
   int32_t n = 0, dist_type = 0;
   std::vector<int64_t> hx, hy;
   DevBuf xy, tasks, flags;
+  bool narrow = true;
   void Release() {
     xy.Release();
     tasks.Release();
@@ -109,7 +112,10 @@ struct BatchState;
 struct cee_ctx {
   int device = -1;
   int sm_count = 148;
-  int jv_blocks_per_sm = 8;
+  int jv_kernel = 1;                  // 0 = thread per edge, 1 = warp per edge (default)
+  int jv_waves = 4;                   // grid = SMs x resident blocks x waves (thread kernel)
+  int occ_jv_thread[2] = {1, 1};      // resident blocks per SM, [narrow, wide]
+  int occ_jv_warp[2] = {1, 1};
   int kopt_rows_per_tile[3] = {0, 0, 0};  // 0 = default tile for k = 3, 4, 5
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[6] = {};
@@ -127,7 +133,8 @@ namespace cee {
 int Fail(cee_ctx* ctx, int code, const std::string& message);
 int CudaFail(cee_ctx* ctx, cudaError_t status, const char* what);
 int Activate(cee_ctx* ctx);
-int PackCoordinates(cee_ctx* ctx, int32_t n, const int64_t* x, const int64_t* y, std::vector<int2>* out);
+int PackCoordinates(cee_ctx* ctx, int32_t n, const int64_t* x, const int64_t* y, std::vector<int2>* out,
+                    bool* narrow);
 int GridFor(int64_t work, int per_block, int max_blocks);
 float EventMs(cudaEvent_t a, cudaEvent_t b);
 int CheckDeviceError(cee_ctx* ctx, const char* what);

@@ -10,30 +10,56 @@ constexpr unsigned kFullMask = 0xffffffffu;
 constexpr uint64_t kEmptyKey = ~uint64_t{0};
 
 // Exact TSPLIB distance between two points whose coordinates are stored relative to the
-// snapshot's bounding-box corner, so 0 <= x, y < 2^30 and the result fits int32.
+// snapshot's bounding-box corner (0 <= x, y < 2^30, so the result fits int32).
 //
-// The reference computes floor(sqrt(s)) with an integer restoring square root
-// (src/common/distance.cpp:9-27) and then rounds: EUC_2D adds 1 when s - q^2 > q (nearest
-// integer, ties impossible for integer s), CEIL_2D adds 1 when q^2 != s (:44-52). Here the
-// root estimate is the correctly rounded FP64 sqrt of s (s < 2^61, so double(s) carries a
-// relative error <= 2^-53 and the estimate lies within 2^-21 of sqrt(s)); truncating it can
-// therefore only be one too high (sqrt(s) just below an integer) or one too low (s a
-// perfect square just above the estimate), which the two integer comparisons correct, so q
-// equals floor(sqrt(s)) exactly and the rounding below is the reference's, bit for bit.
+// The reference computes q = floor(sqrt(s)) of the squared distance s with an integer
+// restoring square root (src/common/distance.cpp:9-27) and rounds: EUC_2D adds 1 when
+// s - q^2 > q (nearest integer; s is an integer so there are no ties), CEIL_2D adds 1 when
+// q^2 != s (:44-52). Both variants below return exactly that value.
+//
+// kWide = false (coordinate span < 2^26, so s < 2^53): everything in FP64. dx, dy, s and
+// q^2 - s are exact in double below 2^53; q = trunc(sqrt(s)) with the correctly rounded FP64
+// square root; the two fma residuals then move q by one step if the root landed on the wrong
+// side of an integer (provably never for s < 2^52, kept as a check), and give s - q^2 exactly
+// for the rounding decision.
+// kWide = true (span up to 2^30, s < 2^61): s in uint64, FP64 root estimate within 2^-21 of
+// sqrt(s) (double(s) has relative error <= 2^-53), integer fix-up by one step either way.
+template <bool kWide>
 __device__ __forceinline__ uint32_t exact_distance(int2 p, int2 q, int dist_type) {
-  const int64_t dx = static_cast<int64_t>(p.x) - q.x;
-  const int64_t dy = static_cast<int64_t>(p.y) - q.y;
-  const uint64_t s = static_cast<uint64_t>(dx * dx + dy * dy);
-  uint64_t r = static_cast<uint64_t>(sqrt(static_cast<double>(s)));
-  if (r * r > s) {
-    --r;
-  } else if ((r + 1) * (r + 1) <= s) {
-    ++r;
+  if constexpr (kWide) {
+    const int64_t dx = static_cast<int64_t>(p.x) - q.x;
+    const int64_t dy = static_cast<int64_t>(p.y) - q.y;
+    const uint64_t s = static_cast<uint64_t>(dx * dx + dy * dy);
+    uint64_t r = static_cast<uint64_t>(sqrt(static_cast<double>(s)));
+    if (r * r > s) {
+      --r;
+    } else if ((r + 1) * (r + 1) <= s) {
+      ++r;
+    }
+    const uint64_t rem = s - r * r;
+    const uint64_t up = dist_type == 0 ? (rem > r ? 1u : 0u) : (rem != 0 ? 1u : 0u);
+    return static_cast<uint32_t>(r + up);
+  } else {
+    const double dx = static_cast<double>(p.x - q.x);
+    const double dy = static_cast<double>(p.y - q.y);
+    const double s = fma(dx, dx, dy * dy);
+    double r = trunc(sqrt(s));
+    double below = fma(r, r, -s);  // r^2 - s
+    if (below > 0.0) {
+      r -= 1.0;
+      below = fma(r, r, -s);
+    } else if (fma(r + 1.0, r + 1.0, -s) <= 0.0) {
+      r += 1.0;
+      below = fma(r, r, -s);
+    }
+    const double rem = -below;  // s - r^2 >= 0
+    const bool up = dist_type == 0 ? rem > r : rem != 0.0;
+    return static_cast<uint32_t>(r) + (up ? 1u : 0u);
   }
-  const uint64_t rem = s - r * r;
-  const uint64_t up = dist_type == 0 ? (rem > r ? 1u : 0u) : (rem != 0 ? 1u : 0u);
-  return static_cast<uint32_t>(r + up);
 }
+
+// Distances with a span below this bound are evaluated with exact_distance<false>.
+constexpr int64_t kNarrowSpan = int64_t{1} << 26;
 
 // Ascending bitonic sort of one 64-bit key per lane across a full warp.
 __device__ __forceinline__ uint64_t warp_sort_asc(uint64_t key, int lane) {

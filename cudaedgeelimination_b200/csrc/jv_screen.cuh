@@ -1,23 +1,27 @@
-// Jonker-Volgenant fast-elimination screen, one warp per edge.
+// Jonker-Volgenant fast-elimination screen.
 //
 // Semantics (the reference's CPU oracle, src/cpu/jv_elimination.cpp:45-117, 209-224):
 //   for every active edge (a,b) with deg(a) > 2 and deg(b) > 2
 //     candidates = the 10 smallest (score, node) over
-//                    c in N(a)\{a,b}:              score = w(a,c) + C(c,b)
-//                    c in N(b)\{a,b}, c not in N(a): score = w(b,c) + C(c,a)
+//                    c in N(a)\{a,b}:                 score = w(a,c) + C(c,b)
+//                    c in N(b)\{a,b}, c not in N(a):  score = w(b,c) + C(c,a)
 //     witness    = the first candidate c (in that order) such that every
 //                  d in N(c)\{a,b} is incompatible:  w(a,b) + w(c,d) > C(a,c) + C(d,b)
 //                                                and w(a,b) + w(c,d) > C(a,d) + C(b,c)
-// where w are the snapshot's CSR slot weights and C the exact TSPLIB distance.
+// where w are the snapshot's CSR slot weights and C the exact TSPLIB distance. Scores and the
+// comparison sums fit 33 bits here (int32 weights and distances) and are kept in 64 bits.
 //
-// B200 mapping: the 32 lanes score up to 32 candidates at once and keep the running
-// top-10 as a warp-wide bitonic-sorted list (one 64-bit key (score << 32 | node) per lane).
-// The witness search first tests the first three neighbours of all ten candidates at once
-// (30 lanes; most candidates meet a compatible d there), then flattens the remaining (c, d)
-// pairs of the still-open candidates, in candidate order, over the lanes. Lanes may test
-// pairs of later candidates speculatively, but a candidate is only accepted once every pair
-// of it has been tested and every earlier candidate is known to have a compatible d, so the
-// chosen witness is exactly the sequential one.
+// Two mappings of the same screen, chosen per launch:
+//   * jv_screen_thread_kernel, one thread per edge: the top-10 list lives in ten 64-bit
+//     registers (key = score << 32 | node) and takes new keys through a branch-free
+//     compare-exchange chain; N(b) is filtered against N(a) by a merge walk over the two
+//     sorted rows; the witness scan is the sequential early-exit loop. Few instructions per
+//     edge; lanes of a warp diverge on loop lengths.
+//   * jv_screen_warp_kernel, one warp per edge: the lanes score up to 32 candidates at once and
+//     keep the top-10 as a warp-wide bitonic-sorted list; the witness search tests the first
+//     three neighbours of all ten candidates at once, then flattens the remaining pairs of the
+//     still-open candidates over the lanes, accepting a candidate only once all of its pairs
+//     are tested and every earlier candidate is closed (so the sequential choice is kept).
 #pragma once
 
 #include "device_common.cuh"
@@ -26,35 +30,135 @@ namespace cee {
 
 constexpr int kJvMaxCandidates = 10;  // src/cpu/jv_elimination.cpp:28
 constexpr int kJvWarpsPerBlock = 8;
+constexpr int kJvThreadBlock = 128;
 
 // Device view of a snapshot (coordinates relative to the bounding-box corner).
 struct JvGraph {
   int32_t n;
   int32_t dist_type;
   int64_t m;
-  const int2* __restrict__ xy;          // [n]
-  const int2* __restrict__ edge_uv;     // [m] (u, v) of the stable edge list
-  const int32_t* __restrict__ edge_w;   // [m]
-  const uint8_t* __restrict__ active;   // [m]
+  const int2* __restrict__ xy;              // [n]
+  const int2* __restrict__ edge_uv;         // [m] (u, v) of the stable edge list
+  const int32_t* __restrict__ edge_w;       // [m]
+  const uint8_t* __restrict__ active;       // [m]
   const int32_t* __restrict__ row_offsets;  // [n + 1]
-  const int32_t* __restrict__ nbr;      // [adjacency], rows ascending
-  const int32_t* __restrict__ slot_w;   // [adjacency], weight of the CSR slot's edge
+  const int32_t* __restrict__ nbr;          // [adjacency], rows ascending
+  const int32_t* __restrict__ slot_w;       // [adjacency], weight of the CSR slot's edge
 };
+
+// ------------------------------------------------------------------ thread per edge -----
+
+// Keeps list[0..9] the ten smallest keys seen, ascending: each slot keeps the smaller of
+// (slot, carried key) and passes the larger on; the key left after slot 9 is dropped.
+__device__ __forceinline__ void top10_insert(uint64_t (&list)[kJvMaxCandidates], uint64_t key) {
+#pragma unroll
+  for (int i = 0; i < kJvMaxCandidates; ++i) {
+    const uint64_t lo = min(list[i], key);
+    key = max(list[i], key);
+    list[i] = lo;
+  }
+}
+
+template <bool kWide>
+__device__ __forceinline__ int32_t jv_screen_edge_thread(const JvGraph& g, int64_t e,
+                                                         int32_t* __restrict__ error) {
+  if (g.active[e] == 0) return -1;
+  const int2 uv = __ldg(g.edge_uv + e);
+  const int32_t a = uv.x, b = uv.y;
+  const int32_t ra0 = __ldg(g.row_offsets + a), ra1 = __ldg(g.row_offsets + a + 1);
+  const int32_t rb0 = __ldg(g.row_offsets + b), rb1 = __ldg(g.row_offsets + b + 1);
+  if (ra1 - ra0 <= 2 || rb1 - rb0 <= 2) return -1;
+  const int2 pa = __ldg(g.xy + a), pb = __ldg(g.xy + b);
+  const int64_t cab = __ldg(g.edge_w + e);
+  const uint32_t n = static_cast<uint32_t>(g.n);
+
+  uint64_t top[kJvMaxCandidates];
+#pragma unroll
+  for (int i = 0; i < kJvMaxCandidates; ++i) top[i] = kEmptyKey;
+  for (int32_t off = ra0; off < ra1; ++off) {
+    const int32_t c = __ldg(g.nbr + off);
+    if (c == a || c == b) continue;
+    if (static_cast<uint32_t>(c) >= n) {
+      atomicOr(error, 1);
+      continue;
+    }
+    const uint64_t score = static_cast<uint64_t>(static_cast<uint32_t>(__ldg(g.slot_w + off))) +
+                           exact_distance<kWide>(__ldg(g.xy + c), pb, g.dist_type);
+    top10_insert(top, (score << 32) | static_cast<uint32_t>(c));
+  }
+  // N(b) ascending, skipping nodes already reached through N(a) (merge walk over N(a))
+  int32_t walk = ra0;
+  int32_t next_a = walk < ra1 ? __ldg(g.nbr + walk) : INT32_MAX;
+  for (int32_t off = rb0; off < rb1; ++off) {
+    const int32_t c = __ldg(g.nbr + off);
+    while (next_a < c) {
+      ++walk;
+      next_a = walk < ra1 ? __ldg(g.nbr + walk) : INT32_MAX;
+    }
+    if (c == a || c == b || next_a == c) continue;
+    if (static_cast<uint32_t>(c) >= n) {
+      atomicOr(error, 1);
+      continue;
+    }
+    const uint64_t score = static_cast<uint64_t>(static_cast<uint32_t>(__ldg(g.slot_w + off))) +
+                           exact_distance<kWide>(__ldg(g.xy + c), pa, g.dist_type);
+    top10_insert(top, (score << 32) | static_cast<uint32_t>(c));
+  }
+
+#pragma unroll
+  for (int i = 0; i < kJvMaxCandidates; ++i) {
+    if (top[i] == kEmptyKey) return -1;
+    const int32_t c = static_cast<int32_t>(top[i] & 0xffffffffu);
+    const int2 pc = __ldg(g.xy + c);
+    const int64_t cac = exact_distance<kWide>(pa, pc, g.dist_type);
+    const int64_t cbc = exact_distance<kWide>(pb, pc, g.dist_type);
+    const int32_t rc1 = __ldg(g.row_offsets + c + 1);
+    bool witness = true;
+    for (int32_t off = __ldg(g.row_offsets + c); off < rc1; ++off) {
+      const int32_t d = __ldg(g.nbr + off);
+      if (d == a || d == b) continue;
+      if (static_cast<uint32_t>(d) >= n) {
+        atomicOr(error, 1);
+        continue;
+      }
+      const int2 pd = __ldg(g.xy + d);
+      const int64_t left = cab + __ldg(g.slot_w + off);
+      if (left <= cac + exact_distance<kWide>(pd, pb, g.dist_type) ||
+          left <= exact_distance<kWide>(pa, pd, g.dist_type) + cbc) {
+        witness = false;  // d is compatible with (a,b)
+        break;
+      }
+    }
+    if (witness) return c;
+  }
+  return -1;
+}
+
+template <bool kWide>
+static __global__ void __launch_bounds__(kJvThreadBlock)
+    jv_screen_thread_kernel(JvGraph g, int64_t first, int64_t last, int32_t* __restrict__ witness,
+                            int32_t* __restrict__ error) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t e = first + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < last; e += stride) {
+    witness[e] = jv_screen_edge_thread<kWide>(g, e, error);
+  }
+}
+
+// ------------------------------------------------------------------ warp per edge -------
 
 struct JvWarpScratch {
   int32_t c[kJvMaxCandidates];
-  int32_t row[kJvMaxCandidates];   // first CSR slot of N(c)
-  int32_t begin[kJvMaxCandidates]; // first flattened index of candidate i's remaining pairs
-  int32_t end[kJvMaxCandidates];   // one past its last one (row end while the table is built)
-  uint32_t cac[kJvMaxCandidates];  // C(a, c)
-  uint32_t cbc[kJvMaxCandidates];  // C(b, c)
+  int32_t row[kJvMaxCandidates];    // first CSR slot of N(c)
+  int32_t begin[kJvMaxCandidates];  // first flattened index of candidate i's remaining pairs
+  int32_t end[kJvMaxCandidates];    // one past its last one (row end while the table is built)
+  uint32_t cac[kJvMaxCandidates];   // C(a, c)
+  uint32_t cbc[kJvMaxCandidates];   // C(b, c)
 };
 
 // Screens edge e with the calling (full) warp; returns the witness or -1 on every lane.
-// Bad node indices (outside [0, n)) are recorded in *error and skipped.
-__device__ __forceinline__ int32_t jv_screen_edge(const JvGraph& g, int64_t e,
-                                                  JvWarpScratch& s, int lane,
-                                                  int32_t* __restrict__ error) {
+template <bool kWide>
+__device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t e, JvWarpScratch& s,
+                                                       int lane, int32_t* __restrict__ error) {
   if (g.active[e] == 0) return -1;
   const int2 uv = g.edge_uv[e];
   const int32_t a = uv.x, b = uv.y;
@@ -65,7 +169,6 @@ __device__ __forceinline__ int32_t jv_screen_edge(const JvGraph& g, int64_t e,
   const int2 pa = __ldg(g.xy + a), pb = __ldg(g.xy + b);
   const int64_t cab = __ldg(g.edge_w + e);
 
-  // ---- candidate scoring: warp-wide sorted top list -----------------------------------
   uint64_t top = kEmptyKey;
   const int total = da + db;
   for (int base = 0; base < total; base += 32) {
@@ -80,11 +183,10 @@ __device__ __forceinline__ int32_t jv_screen_edge(const JvGraph& g, int64_t e,
         atomicOr(error, 1);
         ok = false;
       }
-      // second row: nodes already reached through N(a) are not scored again
       if (ok && second) ok = !row_contains(g.nbr, ra0, ra1, c);
       if (ok) {
         const uint64_t score = static_cast<uint64_t>(static_cast<uint32_t>(__ldg(g.slot_w + slot))) +
-                               exact_distance(__ldg(g.xy + c), second ? pa : pb, g.dist_type);
+                               exact_distance<kWide>(__ldg(g.xy + c), second ? pa : pb, g.dist_type);
         key = (score << 32) | static_cast<uint32_t>(c);
       }
     }
@@ -94,17 +196,16 @@ __device__ __forceinline__ int32_t jv_screen_edge(const JvGraph& g, int64_t e,
   const int nc = __popc(__ballot_sync(kFullMask, lane < kJvMaxCandidates && top != kEmptyKey));
   if (nc == 0) return -1;
 
-  // ---- candidate table: C(a,c) on lanes 0..9, C(b,c) on lanes 10..19 ------------------
-  {
+  {  // candidate table: C(a,c) on lanes 0..9, C(b,c) on lanes 10..19
     const int ci = lane < kJvMaxCandidates ? lane : lane - kJvMaxCandidates;
     const uint64_t key = __shfl_sync(kFullMask, top, ci);
     if (lane < 2 * kJvMaxCandidates && ci < nc) {
       const int32_t c = static_cast<int32_t>(key & 0xffffffffu);
-      const uint32_t dist = exact_distance(lane < kJvMaxCandidates ? pa : pb, __ldg(g.xy + c), g.dist_type);
+      const uint32_t dist = exact_distance<kWide>(lane < kJvMaxCandidates ? pa : pb, __ldg(g.xy + c), g.dist_type);
       if (lane < kJvMaxCandidates) {
         s.c[ci] = c;
         s.row[ci] = __ldg(g.row_offsets + c);
-        s.end[ci] = __ldg(g.row_offsets + c + 1);  // row end, replaced by pair numbering below
+        s.end[ci] = __ldg(g.row_offsets + c + 1);
         s.cac[ci] = dist;
       } else {
         s.cbc[ci] = dist;
@@ -113,7 +214,6 @@ __device__ __forceinline__ int32_t jv_screen_edge(const JvGraph& g, int64_t e,
   }
   __syncwarp();
 
-  // Tests pair (candidate ci, CSR slot); true when d is compatible with (a,b).
   auto compatible_pair = [&](int ci, int32_t slot) -> bool {
     const int32_t d = __ldg(g.nbr + slot);
     if (d == a || d == b) return false;
@@ -123,16 +223,13 @@ __device__ __forceinline__ int32_t jv_screen_edge(const JvGraph& g, int64_t e,
     }
     const int2 pd = __ldg(g.xy + d);
     const int64_t left = cab + __ldg(g.slot_w + slot);
-    const int64_t first = static_cast<int64_t>(s.cac[ci]) + exact_distance(pd, pb, g.dist_type);
-    const int64_t second = static_cast<int64_t>(exact_distance(pa, pd, g.dist_type)) + s.cbc[ci];
-    return left <= first || left <= second;
+    return left <= static_cast<int64_t>(s.cac[ci]) + exact_distance<kWide>(pd, pb, g.dist_type) ||
+           left <= static_cast<int64_t>(exact_distance<kWide>(pa, pd, g.dist_type)) + s.cbc[ci];
   };
 
-  // ---- witness search, breadth first: the first kHead neighbours of every candidate -----
-  // (most candidates meet a compatible d among their first neighbours)
   constexpr int kHead = 3;
   const int deg = lane < nc ? s.end[lane] - s.row[lane] : 0;
-  uint32_t compatible = 0;  // candidates known to have a compatible d (warp-uniform)
+  uint32_t compatible = 0;
   {
     const int hi = lane / kHead, hj = lane - hi * kHead;
     bool hit = false;
@@ -146,7 +243,6 @@ __device__ __forceinline__ int32_t jv_screen_edge(const JvGraph& g, int64_t e,
   uint32_t open = all & ~compatible;
   if (open == 0) return -1;
 
-  // ---- then the remaining neighbours of the open candidates, flattened in candidate order --
   const int rest = ((open >> lane) & 1u) != 0 ? max(deg - kHead, 0) : 0;
   const int incl = warp_inclusive_sum(rest, lane);
   __syncwarp();
@@ -172,7 +268,7 @@ __device__ __forceinline__ int32_t jv_screen_edge(const JvGraph& g, int64_t e,
     }
     compatible |= __reduce_or_sync(kFullMask, bit);
     open = all & ~compatible;
-    if (open == 0) return -1;  // every candidate has a compatible neighbour
+    if (open == 0) return -1;
     first_open = __ffs(open) - 1;
     const int chunk_end = base + 32;
     if (s.end[first_open] <= chunk_end) return s.c[first_open];
@@ -180,17 +276,16 @@ __device__ __forceinline__ int32_t jv_screen_edge(const JvGraph& g, int64_t e,
   }
 }
 
-// Grid-stride over edges [first, last): one warp per edge, witness[e] always written.
+template <bool kWide>
 static __global__ void __launch_bounds__(kJvWarpsPerBlock * 32)
-    jv_screen_kernel(JvGraph g, int64_t first, int64_t last, int32_t* __restrict__ witness,
-                     int32_t* __restrict__ error) {
+    jv_screen_warp_kernel(JvGraph g, int64_t first, int64_t last, int32_t* __restrict__ witness,
+                          int32_t* __restrict__ error) {
   __shared__ JvWarpScratch scratch[kJvWarpsPerBlock];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int64_t warps = static_cast<int64_t>(gridDim.x) * kJvWarpsPerBlock;
-  for (int64_t e = first + static_cast<int64_t>(blockIdx.x) * kJvWarpsPerBlock + warp; e < last;
-       e += warps) {
-    const int32_t w = jv_screen_edge(g, e, scratch[warp], lane, error);
+  for (int64_t e = first + static_cast<int64_t>(blockIdx.x) * kJvWarpsPerBlock + warp; e < last; e += warps) {
+    const int32_t w = jv_screen_edge_warp<kWide>(g, e, scratch[warp], lane, error);
     if (lane == 0) witness[e] = w;
     __syncwarp();
   }

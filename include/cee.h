@@ -72,6 +72,16 @@ void* cee_ctx_stream(cee_ctx* ctx);
 int cee_ctx_synchronize(cee_ctx* ctx);
 /* Device bytes currently held by the context's caches and workspaces. */
 uint64_t cee_ctx_resident_bytes(const cee_ctx* ctx);
+/* Tuning options (defaults are the autotuned choices for B200; see cee_ctx_set_option). */
+enum cee_option {
+  CEE_OPT_JV_KERNEL = 1,    /* 0 = one thread per edge, 1 = one warp per edge (default) */
+  CEE_OPT_JV_WAVES = 2,     /* grid of the thread-per-edge screen, in waves of resident blocks */
+  CEE_OPT_KOPT_ROWS_K3 = 3, /* rows per k-opt tile for k = 3 / 4 / 5 (0 = default, even) */
+  CEE_OPT_KOPT_ROWS_K4 = 4,
+  CEE_OPT_KOPT_ROWS_K5 = 5
+};
+/* Sets a launch-shape option of this context; results never depend on it. */
+int cee_ctx_set_option(cee_ctx* ctx, int32_t option, int64_t value);
 /* Frees cached device state: bit 1 = JV, bit 2 = k-opt, bit 4 = c,d, bit 8 = batch.
  * Replaces ClearJvCudaCache (include/cuda_edge_elimination/elimination.hpp:338) and
  * ClearKOptCostCudaCache (include/cuda_edge_elimination/local_search.hpp:242). */

@@ -4,10 +4,19 @@ import numpy as np
 import pytest
 
 from cudaedgeelimination_b200 import GraphSnapshot, synth
+from cudaedgeelimination_b200 import _native
 from cudaedgeelimination_b200._native import NativeError, CEE_ERR_RANGE
 from helpers import commit, complete_graph, knn_graph, random_graph
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(params=[0, 1], ids=["thread", "warp"])
+def jv(ctx, request):
+    """The context with the JV screen mapped one thread per edge, then one warp per edge."""
+    ctx.set_option(_native.OPT_JV_KERNEL, request.param)
+    yield ctx
+    ctx.set_option(_native.OPT_JV_KERNEL, 1)
 
 
 def check_epochs(ctx, port, g, max_rounds=100):
@@ -27,60 +36,60 @@ def check_epochs(ctx, port, g, max_rounds=100):
     return g, epochs
 
 
-def test_small_uniform_fixed_point(ctx, port):
+def test_small_uniform_fixed_point(jv, port):
     g = synth.jv_small()
-    final, epochs = check_epochs(ctx, port, g)
+    final, epochs = check_epochs(jv, port, g)
     active, before, committed, final_hash = port.jv_eliminate(g)
     np.testing.assert_array_equal(final.active, active)
     assert epochs == len(before)
 
 
-def test_clustered_multi_epoch(ctx, port):
+def test_clustered_multi_epoch(jv, port):
     g = synth.jv_clustered()
-    final, epochs = check_epochs(ctx, port, g)
+    final, epochs = check_epochs(jv, port, g)
     assert epochs >= 2
     assert port.content_hash(final) == port.jv_eliminate(g)[3]
 
 
 @pytest.mark.parametrize("seed", range(4))
-def test_random_knn(ctx, port, seed):
-    check_epochs(ctx, port, knn_graph(400, 6 + 2 * seed, seed, dist_type=seed % 2))
+def test_random_knn(jv, port, seed):
+    check_epochs(jv, port, knn_graph(400, 6 + 2 * seed, seed, dist_type=seed % 2))
 
 
 @pytest.mark.parametrize("seed", range(3))
-def test_dense_rows_multi_pass(ctx, port, seed):
+def test_dense_rows_multi_pass(jv, port, seed):
     # degrees well above 32: several scoring passes and long witness scans
     g = random_graph(90, 1800, 100 + seed)
     assert g.degree().max() > 32
-    check_epochs(ctx, port, g, max_rounds=3)
+    check_epochs(jv, port, g, max_rounds=3)
 
 
-def test_unsorted_edges_and_inactive(ctx, port):
+def test_unsorted_edges_and_inactive(jv, port):
     g = random_graph(300, 2500, 7, shuffle=True, active_frac=0.8)
-    check_epochs(ctx, port, g, max_rounds=3)
+    check_epochs(jv, port, g, max_rounds=3)
 
 
-def test_k4_and_complete_graphs(ctx, port):
+def test_k4_and_complete_graphs(jv, port):
     k4 = complete_graph([0, 10, 0, 10], [0, 0, 10, 10])
-    gpu, _ = ctx.jv_screen(k4)
+    gpu, _ = jv.jv_screen(k4)
     np.testing.assert_array_equal(gpu, port.jv_screen(k4))
     rng = np.random.default_rng(3)
     for n in (5, 9, 12):
         g = complete_graph(rng.permutation(1000)[:n], rng.permutation(1000)[:n], dist_type=n % 2)
-        check_epochs(ctx, port, g)
+        check_epochs(jv, port, g)
 
 
-def test_low_degree_gate_and_empty(ctx, port):
+def test_low_degree_gate_and_empty(jv, port):
     # a path: every degree <= 2, so no edge is screened
     g = GraphSnapshot.from_edges([0, 5, 9, 20], [0, 3, 1, 4], [(0, 1), (1, 2), (2, 3)])
-    gpu, _ = ctx.jv_screen(g)
+    gpu, _ = jv.jv_screen(g)
     assert (gpu == -1).all()
     empty = GraphSnapshot.from_edges([0, 1, 2], [0, 1, 2], np.zeros((0, 2), np.int64))
-    gpu, _ = ctx.jv_screen(empty)
+    gpu, _ = jv.jv_screen(empty)
     assert gpu.shape == (0,)
 
 
-def test_large_coordinates_exact(ctx, port):
+def test_large_coordinates_exact(jv, port):
     # spans close to 2^30: squared distances near 2^61 exercise the FP64 root + integer fix-up
     rng = np.random.default_rng(11)
     span = (1 << 30) - 1
@@ -91,7 +100,7 @@ def test_large_coordinates_exact(ctx, port):
         g = GraphSnapshot.from_edges(xs + (1 << 40), ys - (1 << 35),
                                      [(i, j) for i in range(64) for j in range(i + 1, 64) if (i * 7 + j) % 5 < 2],
                                      dist_type=t)
-        gpu, _ = ctx.jv_screen(g)
+        gpu, _ = jv.jv_screen(g)
         np.testing.assert_array_equal(gpu, port.jv_screen(g))
 
 

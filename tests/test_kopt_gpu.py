@@ -3,9 +3,21 @@ import numpy as np
 import pytest
 
 from cudaedgeelimination_b200 import KOPT_TASK_DTYPE, BuildKOptReconnectTable, GraphSnapshot, synth
+from cudaedgeelimination_b200 import _native
 from cudaedgeelimination_b200._native import NativeError
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(params=[0, 2], ids=["default-tiles", "small-tiles"])
+def kc(ctx, request):
+    """The context with the default k-opt tiles, then with small tiles (many partial tiles)."""
+    for opt, rows in zip((_native.OPT_KOPT_ROWS_K3, _native.OPT_KOPT_ROWS_K4, _native.OPT_KOPT_ROWS_K5),
+                         (request.param * 4, request.param * 3, request.param)):
+        ctx.set_option(opt, rows)
+    yield ctx
+    for opt in (_native.OPT_KOPT_ROWS_K3, _native.OPT_KOPT_ROWS_K4, _native.OPT_KOPT_ROWS_K5):
+        ctx.set_option(opt, 0)
 
 INVALID = np.iinfo(np.int64).max
 
@@ -29,46 +41,46 @@ def seventeen():
 
 
 @pytest.mark.parametrize("dist_type", [0, 1])
-def test_consecutive_adjacent_and_strided_ports(ctx, port, dist_type):
+def test_consecutive_adjacent_and_strided_ports(kc, port, dist_type):
     g = coords_only(*seventeen(), dist_type)
     for k in (3, 4, 5):
         rows = [list(range(2 * k)), [0, 1, 1, 2, 3, 4, 5, 6, 7, 8][:2 * k],
                 [(3 * p + 2) % 17 for p in range(2 * k)]]
         tasks = make_tasks(g, k, rows)
         table = BuildKOptReconnectTable(k)
-        gpu, _ = ctx.kopt_costs(g, table, tasks)
+        gpu, _ = kc.kopt_costs(g, table, tasks)
         cpu = port.kopt_costs(g, k, tasks, table.templates)
         np.testing.assert_array_equal(gpu, cpu)
         assert (gpu[1] == INVALID).any()  # shared ports produce invalid cells
 
 
-def test_repeated_rows(ctx, port):
+def test_repeated_rows(kc, port):
     g = coords_only(*seventeen())
     tasks = make_tasks(g, 5, [list(range(10))] * 40)
     table = BuildKOptReconnectTable(5)
-    gpu, _ = ctx.kopt_costs(g, table, tasks)
+    gpu, _ = kc.kopt_costs(g, table, tasks)
     np.testing.assert_array_equal(gpu, port.kopt_costs(g, 5, tasks))
     assert (gpu == gpu[0]).all()
 
 
 @pytest.mark.parametrize("dist_type", [0, 1])
-def test_walk_rows_all_k(ctx, port, dist_type):
+def test_walk_rows_all_k(kc, port, dist_type):
     g, tasks = synth.kopt_instance(rows=6001, n=3000)
     if dist_type == 0:
         g = GraphSnapshot(g.n, 0, g.x, g.y, g.edge_u, g.edge_v, g.edge_w, g.active)
     for k in (3, 4, 5):
         table = BuildKOptReconnectTable(k)
-        gpu, _ = ctx.kopt_costs(g, table, tasks[k])
+        gpu, _ = kc.kopt_costs(g, table, tasks[k])
         np.testing.assert_array_equal(gpu, port.kopt_costs(g, k, tasks[k]))
 
 
-def test_multi_segment_matches_single(ctx, port):
+def test_multi_segment_matches_single(kc, port):
     g, tasks = synth.kopt_instance(rows=3001, n=2000)
-    outs, stats = ctx.kopt_costs_multi(g, [3, 4, 5], [tasks[3], tasks[4], tasks[5]])
+    outs, stats = kc.kopt_costs_multi(g, [3, 4, 5], [tasks[3], tasks[4], tasks[5]])
     for k, out in zip((3, 4, 5), outs):
         np.testing.assert_array_equal(out, port.kopt_costs(g, k, tasks[k]))
     # odd row counts and a single row
-    outs, _ = ctx.kopt_costs_multi(g, [5, 3], [tasks[5][:1], tasks[3][:7]])
+    outs, _ = kc.kopt_costs_multi(g, [5, 3], [tasks[5][:1], tasks[3][:7]])
     np.testing.assert_array_equal(outs[0], port.kopt_costs(g, 5, tasks[5][:1]))
     np.testing.assert_array_equal(outs[1], port.kopt_costs(g, 3, tasks[3][:7]))
 
@@ -96,3 +108,17 @@ def test_bad_template_rejected(ctx):
     table.templates[0, 0] = table.templates[0, 1]  # no longer a perfect matching
     with pytest.raises(NativeError):
         ctx.kopt_costs(g, table, make_tasks(g, 3, [list(range(6))]))
+
+
+def test_heavily_repeated_ports(kc, port):
+    """Nodes shared by several deleted edges: a node in three deleted edges (k=3), a closed
+    5-cycle where every node repeats (k=5, the maximum number of duplicate sets), and runs."""
+    g = coords_only(*seventeen())
+    cases = {3: [[0, 1, 1, 2, 1, 3], [5, 6, 6, 7, 7, 5], [2, 9, 9, 4, 4, 11]],
+             4: [[0, 1, 1, 2, 1, 3, 1, 4], [0, 1, 1, 2, 2, 3, 3, 0], [3, 4, 4, 5, 6, 7, 7, 8]],
+             5: [[0, 1, 1, 2, 2, 3, 3, 4, 4, 0], [0, 1, 1, 2, 1, 3, 1, 4, 1, 5], [2, 3, 3, 4, 4, 5, 9, 10, 10, 11]]}
+    for k, rows in cases.items():
+        tasks = make_tasks(g, k, rows)
+        table = BuildKOptReconnectTable(k)
+        gpu, _ = kc.kopt_costs(g, table, tasks)
+        np.testing.assert_array_equal(gpu, port.kopt_costs(g, k, tasks))
