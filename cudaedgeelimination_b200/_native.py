@@ -40,6 +40,15 @@ class GraphView(ctypes.Structure):
     ]
 
 
+class DeviceGraph(ctypes.Structure):
+    """cee_device_graph: a snapshot in device memory (all pointers are device addresses)."""
+    _fields_ = [
+        ("n", ctypes.c_int32), ("dist_type", ctypes.c_int32), ("m", ctypes.c_int64), ("adjacency", ctypes.c_int64),
+        ("xy", ctypes.c_void_p), ("edge_uv", ctypes.c_void_p), ("edge_w", ctypes.c_void_p), ("active", ctypes.c_void_p),
+        ("row_offsets", ctypes.c_void_p), ("neighbors", ctypes.c_void_p), ("csr_edge_ids", ctypes.c_void_p),
+    ]
+
+
 class JvStats(ctypes.Structure):
     _fields_ = [
         ("static_hit", ctypes.c_int32), ("workspace_hit", ctypes.c_int32),
@@ -93,6 +102,7 @@ def lib() -> ctypes.CDLL:
             "cee_jv_prepare": (ctypes.c_int, [vp, ctypes.POINTER(GraphView), ctypes.POINTER(JvStats)]),
             "cee_jv_launch": (ctypes.c_int, [vp]),
             "cee_jv_fetch": (ctypes.c_int, [vp, c_i32p]),
+            "cee_jv_screen_noalloc": (ctypes.c_int, [ctypes.POINTER(DeviceGraph), vp, vp]),
             "cee_kopt_templates": (ctypes.c_int, [ctypes.c_uint32, c_u8p, c_u64p]),
             "cee_kopt_costs": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, c_i64p, c_i64p, ctypes.c_uint32,
                                               c_u8p, ctypes.c_int32, ctypes.c_uint64, vp, ctypes.c_int64, c_i64p,

@@ -139,6 +139,43 @@ int cee_jv_prepare(cee_ctx* ctx, const cee_graph_view* graph, cee_jv_stats* stat
 int cee_jv_launch(cee_ctx* ctx);
 int cee_jv_fetch(cee_ctx* ctx, int32_t* witness_out);
 
+/* A snapshot already resident in the caller's device memory, in this library's device layout:
+ * coordinates as int32 (x, y) pairs in [0, 2^30) (offsets from a common corner), the stable
+ * edge list as int32 (u, v) pairs plus int32 weights in [0, 2^31) and 0/1 active bytes, and
+ * the active-only CSR (rows ascending by neighbour). All pointers are device pointers;
+ * xy and edge_uv must be 8-byte aligned. */
+typedef struct {
+  int32_t n;
+  int32_t dist_type;
+  int64_t m;
+  int64_t adjacency;
+  const int32_t* xy;           /* [2n] */
+  const int32_t* edge_uv;      /* [2m] */
+  const int32_t* edge_w;       /* [m] */
+  const uint8_t* active;       /* [m] */
+  const int32_t* row_offsets;  /* [n + 1] */
+  const int32_t* neighbors;    /* [adjacency] */
+  const int32_t* csr_edge_ids; /* [adjacency] */
+} cee_device_graph;
+
+/* JV screen that allocates nothing. No counterpart in the reference: it exists for callers
+ * that cannot call cudaMalloc -- hosts whose own pool or arena owns all device memory and
+ * forbids library allocations, and paths that must not allocate while they run (latency-
+ * critical loops that reserved their memory up front, processes under a hard device-memory
+ * quota). The caller passes its snapshot and the witness output (int32 [m], same meaning as
+ * cee_jv_screen's witness_out) in device memory and a cudaStream_t (NULL = legacy default
+ * stream); the call runs on the calling thread's current device and returns after the
+ * stream has finished the screen. It calls no cudaMalloc, cudaFree or other allocating
+ * routine: its working memory (the per-slot edge weights and a status word) lives in
+ * file-scope device arrays of fixed size that every GPU loading the library holds until the
+ * process exits (16 MiB + 256 B). Limit: adjacency <= 4,194,304 CSR slots; larger snapshots
+ * fail with CEE_ERR_RANGE before any launch. The first call on a device looks up the arrays'
+ * device addresses (once per device), so make it before any stream capture. All calls share
+ * the arrays: each call rewrites what it reads, but calls that overlap on the GPU race and must
+ * be serialised by the caller. The snapshot is validated on the device first (CEE_ERR_INVALID
+ * on failure); errors are reported through cee_last_error(NULL). */
+int cee_jv_screen_noalloc(const cee_device_graph* graph, int32_t* witness_out, void* stream);
+
 /* ---- k-opt leaf cost matrix ----------------------------------------------------------- */
 
 /* KOptCostTask, include/cuda_edge_elimination/local_search.hpp:54-57 (48 bytes). */
