@@ -370,11 +370,13 @@ def barrier(world: int):
 
 
 def max_over_ranks(value: float, world: int) -> float:
+    """The slowest rank's time (every rank gets it)."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

@@ -98,8 +98,19 @@ class GraphSnapshot:
             return r + (1 if s - r * r > r else 0)
         return r + (1 if r * r != s else 0)
 
+    def check_layout(self) -> None:
+        """Raw pointers are handed to native code: every array must be C-contiguous with the
+        documented dtype."""
+        for name, dtype in (("x", np.int64), ("y", np.int64), ("edge_u", np.int32), ("edge_v", np.int32),
+                            ("edge_w", np.int64), ("active", np.uint8), ("row_offsets", np.int32),
+                            ("neighbors", np.int32), ("csr_edge_ids", np.int32)):
+            a = getattr(self, name)
+            if a.dtype != dtype or not a.flags.c_contiguous:
+                raise ValueError(f"snapshot array {name} must be C-contiguous {np.dtype(dtype).name}")
+
     def view(self) -> _native.GraphView:
         """cee_graph_view over this snapshot's arrays (valid while the snapshot lives)."""
+        self.check_layout()
         g = _native.GraphView()
         g.n = self.n
         g.dist_type = self.dist_type
@@ -128,6 +139,6 @@ class GraphSnapshot:
         if weights is None:
             g.edge_w = np.array([g.distance(int(a), int(b)) for a, b in edges], np.int64)
         else:
-            g.edge_w = np.asarray(weights, np.int64)
+            g.edge_w = np.ascontiguousarray(weights, dtype=np.int64)
         g.rebuild_csr()
         return g

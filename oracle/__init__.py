@@ -82,6 +82,10 @@ class Port:
         self.L = L
 
     def graph(self, g) -> CeoGraph:
+        for name in ("x", "y", "edge_u", "edge_v", "edge_w", "active", "row_offsets", "neighbors", "csr_edge_ids",
+                     "csr_weights"):
+            if not getattr(g, name).flags.c_contiguous:
+                raise ValueError(f"oracle input {name} must be C-contiguous")
         s = CeoGraph()
         s.n, s.dist_type = g.n, g.dist_type
         s.x, s.y = _p(g.x, ctypes.c_int64), _p(g.y, ctypes.c_int64)
@@ -262,6 +266,9 @@ class RefGraph:
     """A GraphSnapshot owned by the reference library."""
 
     def __init__(self, ref: Reference, g):
+        for name in ("x", "y", "edge_u", "edge_v", "edge_w", "active"):
+            if not getattr(g, name).flags.c_contiguous:
+                raise ValueError(f"reference input {name} must be C-contiguous")
         self.ref = ref
         self.m = int(g.edge_u.shape[0])
         handle = vp()
