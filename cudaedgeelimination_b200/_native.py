@@ -67,6 +67,27 @@ class KoptStats(ctypes.Structure):
     ]
 
 
+class BatchView(ctypes.Structure):
+    _fields_ = [("instances", ctypes.c_int32), ("node_begin", c_i64p), ("edge_begin", c_i64p), ("graph", GraphView)]
+
+
+class BatchOptions(ctypes.Structure):
+    _fields_ = [("targets", ctypes.c_int32), ("max_neighborhood", ctypes.c_int32),
+                ("max_candidate_degree", ctypes.c_int32), ("cd_mode", ctypes.c_int32)]
+
+
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("jv_tile", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32), ("chunks", ctypes.c_int32)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.c_int64), ("edges", ctypes.c_int64), ("adjacency", ctypes.c_int64),
+                ("targets", ctypes.c_int64), ("pairs", ctypes.c_int64), ("flag_words", ctypes.c_int64),
+                ("resident_bytes", ctypes.c_uint64), ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
+                ("h2d_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double), ("d2h_ms", ctypes.c_double),
+                ("total_ms", ctypes.c_double)]
+
+
 class NativeError(RuntimeError):
     """A non-zero status from libcee; `code` is the CEE_ERR_* value."""
 
@@ -118,6 +139,16 @@ def lib() -> ctypes.CDLL:
             "cee_kopt_fetch": (ctypes.c_int, [vp, ctypes.POINTER(vp)]),
             "cee_cd_screen": (ctypes.c_int, [vp, ctypes.POINTER(GraphView), ctypes.c_int32, ctypes.c_int32, vp,
                                              ctypes.c_int64, ctypes.c_int32, c_u8p]),
+            "cee_batch_prepare": (ctypes.c_int, [vp, ctypes.POINTER(BatchView), ctypes.POINTER(BatchOptions),
+                                                 ctypes.POINTER(BatchStats)]),
+            "cee_batch_launch": (ctypes.c_int, [vp]),
+            "cee_batch_launch_plain": (ctypes.c_int, [vp]),
+            "cee_batch_fetch": (ctypes.c_int, [vp, vp, vp, vp, vp, vp]),
+            "cee_batch_screen": (ctypes.c_int, [vp, ctypes.POINTER(BatchView), ctypes.POINTER(BatchOptions),
+                                                vp, vp, vp, vp, vp, ctypes.POINTER(BatchStats)]),
+            "cee_batch_set_tuning": (ctypes.c_int, [vp, ctypes.POINTER(BatchTuning)]),
+            "cee_batch_get_tuning": (ctypes.c_int, [vp, ctypes.POINTER(BatchTuning)]),
+            "cee_batch_autotune": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.POINTER(BatchTuning)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

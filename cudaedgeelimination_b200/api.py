@@ -30,7 +30,112 @@ INVALID_KOPT_COST = np.iinfo(np.int64).max
 KOPT_TEMPLATE_COUNTS = {3: 4, 4: 25, 5: 208}
 
 
-class Context:
+# ---- batched screen ----------------------------------------------------------------------
+
+@dataclass
+class BatchOptions:
+    """Per-instance work of the batched screen: HT targets per instance and the c,d screen's
+    HtShallowOptions (neighbourhood, degree cap, mode); the reference defaults are 64/25/50/0."""
+    targets: int = 64
+    max_neighborhood: int = 25
+    max_candidate_degree: int = 50
+    cd_mode: int = 0
+
+    def native(self) -> _native.BatchOptions:
+        return _native.BatchOptions(self.targets, self.max_neighborhood, self.max_candidate_degree, self.cd_mode)
+
+    @property
+    def flag_words(self) -> int:
+        return (self.max_neighborhood * (self.max_neighborhood - 1) // 2 + 31) // 32
+
+
+@dataclass
+class BatchResult:
+    witness: np.ndarray       # [m] JV witness (global node id) or -1
+    target_ids: np.ndarray    # [I, T] global edge ids, -1 padding
+    target_count: np.ndarray  # [I]
+    nbhd: np.ndarray          # [I, T, NB] global node ids, -1 padding
+    flags: np.ndarray         # [I, T, flag_words] uint32 bit sets over the pair order i < j
+
+    def pair_flags(self, i: int, t: int) -> np.ndarray:
+        """The flags of target t of instance i as 0/1 bytes in task order."""
+        size = int((self.nbhd[i, t] >= 0).sum())
+        pairs = size * (size - 1) // 2
+        bits = np.unpackbits(self.flags[i, t].view(np.uint8), bitorder="little")
+        return bits[:pairs].astype(np.uint8)
+
+
+def batch_view(batch, graph: GraphSnapshot):
+    """cee_batch_view over a batch (node_begin / edge_begin arrays) and its union snapshot."""
+    view = _native.BatchView()
+    view.instances = int(batch.node_begin.shape[0] - 1)
+    view.node_begin = batch.node_begin.ctypes.data_as(_native.c_i64p)
+    view.edge_begin = batch.edge_begin.ctypes.data_as(_native.c_i64p)
+    view.graph = graph.view()
+    return view
+
+
+def _batch_outputs(m: int, instances: int, opt: BatchOptions) -> BatchResult:
+    T, NB = opt.targets, opt.max_neighborhood
+    return BatchResult(np.empty(m, np.int32), np.empty((instances, T), np.int32), np.empty(instances, np.int32),
+                       np.empty((instances, T, NB), np.int32), np.empty((instances, T, opt.flag_words), np.uint32))
+
+
+def _ptrs(r: BatchResult):
+    return [ctypes.c_void_p(a.ctypes.data) for a in (r.witness, r.target_ids, r.target_count, r.nbhd, r.flags)]
+
+
+class BatchMixin:
+    def batch_prepare(self, batch, opt: BatchOptions, graph: GraphSnapshot | None = None) -> _native.BatchStats:
+        graph = batch.graph if graph is None else graph
+        self._batch = (batch, graph, opt)
+        view = batch_view(batch, graph)
+        stats = _native.BatchStats()
+        _native.check(self.handle, _native.lib().cee_batch_prepare(self.handle, ctypes.byref(view),
+                                                                   ctypes.byref(opt.native()), ctypes.byref(stats)))
+        return stats
+
+    def batch_launch(self) -> None:
+        _native.check(self.handle, _native.lib().cee_batch_launch(self.handle))
+
+    def batch_launch_plain(self) -> None:
+        _native.check(self.handle, _native.lib().cee_batch_launch_plain(self.handle))
+
+    def batch_fetch(self) -> BatchResult:
+        batch, graph, opt = self._batch
+        out = _batch_outputs(graph.m, int(batch.node_begin.shape[0] - 1), opt)
+        _native.check(self.handle, _native.lib().cee_batch_fetch(self.handle, *_ptrs(out)))
+        return out
+
+    def batch_screen(self, batch, opt: BatchOptions, graph: GraphSnapshot | None = None, out: BatchResult | None = None):
+        graph = batch.graph if graph is None else graph
+        self._batch = (batch, graph, opt)
+        if out is None:
+            out = _batch_outputs(graph.m, int(batch.node_begin.shape[0] - 1), opt)
+        view = batch_view(batch, graph)
+        stats = _native.BatchStats()
+        _native.check(self.handle, _native.lib().cee_batch_screen(self.handle, ctypes.byref(view),
+                                                                  ctypes.byref(opt.native()), *_ptrs(out),
+                                                                  ctypes.byref(stats)))
+        return out, stats
+
+    def batch_tuning(self) -> _native.BatchTuning:
+        t = _native.BatchTuning()
+        _native.check(self.handle, _native.lib().cee_batch_get_tuning(self.handle, ctypes.byref(t)))
+        return t
+
+    def set_batch_tuning(self, jv_tile: int, blocks_per_sm: int, chunks: int) -> None:
+        t = _native.BatchTuning(jv_tile, blocks_per_sm, chunks)
+        _native.check(self.handle, _native.lib().cee_batch_set_tuning(self.handle, ctypes.byref(t)))
+
+    def batch_autotune(self, reps: int = 3) -> _native.BatchTuning:
+        t = _native.BatchTuning()
+        _native.check(self.handle, _native.lib().cee_batch_autotune(self.handle, reps, ctypes.byref(t)))
+        return t
+
+
+
+class Context(BatchMixin):
     """One cee_ctx: a device, a stream and the resident caches."""
 
     def __init__(self, device: int = -1):

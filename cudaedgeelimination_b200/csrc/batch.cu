@@ -1,15 +1,638 @@
-// Batched screen runtime (filled in below the single-instance kernels).
+// Batched screen runtime: many instances in one persistent, CUDA-graph-captured launch
+// (batch_screen.cuh), the one-launch-per-instance comparison path, the chunked end-to-end call
+// with copy/compute overlap, and the launch-shape autotuner. Contract in include/cee.h.
+#include "cee.h"
 #include "cee_internal.h"
+
+#include "batch_screen.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
 
 namespace cee {
 
-struct BatchState {};
+constexpr int kMaxChunks = 64;
+
+struct BatchState {
+  cee_batch_options opt{};
+  cee_batch_tuning tune{64, 0, 8};
+  int32_t instances = 0;
+  int64_t n = 0, m = 0, adj = 0;
+  int32_t dist_type = 0;
+  bool narrow = true;
+  int32_t flag_words = 0;
+  std::vector<int64_t> node_begin, edge_begin;
+  // the union snapshot in the kernels' layout
+  DevBuf d_node_begin, d_edge_begin, xy, uv, w32, active, ro, nbr, ids, slotw;
+  // raw uploads of the end-to-end call (converted on the device)
+  DevBuf raw_x, raw_y, raw_u, raw_v, raw_w;
+  // outputs and work-queue state
+  DevBuf witness, target_ids, target_count, nbhd, flags, counter, ready;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t up[kMaxChunks] = {}, done[kMaxChunks] = {};
+  int occupancy[2] = {1, 1};
+  bool prepared = false;
+
+  void ReleaseGraph() {
+    if (exec != nullptr) cudaGraphExecDestroy(exec);
+    if (graph != nullptr) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+  void Release() {
+    ReleaseGraph();
+    for (DevBuf* b : {&d_node_begin, &d_edge_begin, &xy, &uv, &w32, &active, &ro, &nbr, &ids, &slotw, &raw_x, &raw_y,
+                      &raw_u, &raw_v, &raw_w, &witness, &target_ids, &target_count, &nbhd, &flags, &counter, &ready}) {
+      b->Release();
+    }
+    for (int i = 0; i < kMaxChunks; ++i) {
+      if (up[i] != nullptr) cudaEventDestroy(up[i]);
+      if (done[i] != nullptr) cudaEventDestroy(done[i]);
+      up[i] = done[i] = nullptr;
+    }
+    if (h2d != nullptr) cudaStreamDestroy(h2d);
+    if (d2h != nullptr) cudaStreamDestroy(d2h);
+    h2d = d2h = nullptr;
+    prepared = false;
+  }
+};
 
 void ReleaseBatch(cee_ctx* ctx) {
-  delete ctx->batch;
-  ctx->batch = nullptr;
+  if (ctx->batch != nullptr) {
+    ctx->batch->Release();
+    delete ctx->batch;
+    ctx->batch = nullptr;
+  }
 }
 
-uint64_t BatchResident(const cee_ctx*) { return 0; }
+uint64_t BatchResident(const cee_ctx* ctx) {
+  const BatchState* s = ctx->batch;
+  if (s == nullptr) return 0;
+  uint64_t bytes = 0;
+  for (const DevBuf* b : {&s->d_node_begin, &s->d_edge_begin, &s->xy, &s->uv, &s->w32, &s->active, &s->ro, &s->nbr,
+                          &s->ids, &s->slotw, &s->raw_x, &s->raw_y, &s->raw_u, &s->raw_v, &s->raw_w, &s->witness,
+                          &s->target_ids, &s->target_count, &s->nbhd, &s->flags, &s->counter, &s->ready}) {
+    bytes += b->capacity;
+  }
+  return bytes;
+}
 
+namespace {
+
+BatchState* State(cee_ctx* ctx) {
+  if (ctx->batch == nullptr) ctx->batch = new BatchState();
+  return ctx->batch;
+}
+
+int ValidateOptions(cee_ctx* ctx, const cee_batch_options* o) {
+  if (o == nullptr) return Fail(ctx, CEE_ERR_INVALID, "null batch options");
+  if (o->targets < 1 || o->targets > kBatchMaxTargets) return Fail(ctx, CEE_ERR_INVALID, "targets must lie in [1,64]");
+  if (o->max_neighborhood < 2 || o->max_neighborhood > kBatchMaxNeighborhood) {
+    return Fail(ctx, CEE_ERR_INVALID, "max_neighborhood must lie in [2,32] for the batched screen");
+  }
+  if (o->max_candidate_degree < 0) return Fail(ctx, CEE_ERR_INVALID, "negative degree cap");
+  if (o->cd_mode != CEE_CD_ACTIVE_INCOMPATIBLE && o->cd_mode != CEE_CD_MISSING_OR_INCOMPATIBLE) {
+    return Fail(ctx, CEE_ERR_INVALID, "unknown c,d mode");
+  }
+  return CEE_OK;
+}
+
+// Structural checks: offsets, CSR row offsets (both O(n + instances)).
+int ValidateShape(cee_ctx* ctx, const cee_batch_view* b) {
+  if (b == nullptr || b->instances < 1 || b->node_begin == nullptr || b->edge_begin == nullptr) {
+    return Fail(ctx, CEE_ERR_INVALID, "bad batch description");
+  }
+  const cee_graph_view& g = b->graph;
+  if (g.n < 0 || g.m < 0 || g.m > INT32_MAX || (g.dist_type != CEE_EUC_2D && g.dist_type != CEE_CEIL_2D)) {
+    return Fail(ctx, CEE_ERR_INVALID, "bad union snapshot");
+  }
+  if (b->node_begin[0] != 0 || b->edge_begin[0] != 0 || b->node_begin[b->instances] != g.n ||
+      b->edge_begin[b->instances] != g.m) {
+    return Fail(ctx, CEE_ERR_INVALID, "instance offsets must cover the union exactly");
+  }
+  for (int32_t i = 0; i < b->instances; ++i) {
+    if (b->node_begin[i + 1] < b->node_begin[i] || b->edge_begin[i + 1] < b->edge_begin[i]) {
+      return Fail(ctx, CEE_ERR_INVALID, "instance offsets must be non-decreasing");
+    }
+  }
+  if (g.adjacency < 0 || g.adjacency > INT32_MAX || g.row_offsets == nullptr || g.row_offsets[0] != 0 ||
+      g.row_offsets[g.n] != g.adjacency) {
+    return Fail(ctx, CEE_ERR_INVALID, "bad union CSR");
+  }
+  for (int64_t v = 0; v < g.n; ++v) {
+    if (g.row_offsets[v + 1] < g.row_offsets[v]) return Fail(ctx, CEE_ERR_INVALID, "row_offsets not non-decreasing");
+  }
+  if (g.m > 0 && (g.x == nullptr || g.y == nullptr || g.edge_u == nullptr || g.edge_v == nullptr ||
+                  g.edge_w == nullptr || g.active == nullptr)) {
+    return Fail(ctx, CEE_ERR_INVALID, "null union arrays");
+  }
+  return CEE_OK;
+}
+
+int Reserve(cee_ctx* ctx, DevBuf& buf, size_t bytes) {
+  const cudaError_t status = buf.Reserve(bytes + 16, nullptr);
+  if (status != cudaSuccess) return CudaFail(ctx, status, "batch allocation");
+  return CEE_OK;
+}
+
+int ReserveAll(cee_ctx* ctx, BatchState& s) {
+  const size_t I = static_cast<size_t>(s.instances), T = static_cast<size_t>(s.opt.targets);
+  const size_t n = static_cast<size_t>(s.n), m = static_cast<size_t>(s.m), adj = static_cast<size_t>(s.adj);
+  const size_t NB = static_cast<size_t>(s.opt.max_neighborhood);
+  int rc = CEE_OK;
+  const std::pair<DevBuf*, size_t> wants[] = {
+      {&s.d_node_begin, (I + 1) * 8}, {&s.d_edge_begin, (I + 1) * 8}, {&s.xy, n * 8}, {&s.uv, m * 8},
+      {&s.w32, m * 4}, {&s.active, m}, {&s.ro, (n + 1) * 4}, {&s.nbr, adj * 4}, {&s.ids, adj * 4},
+      {&s.slotw, adj * 4}, {&s.witness, m * 4}, {&s.target_ids, I * T * 4}, {&s.target_count, I * 4},
+      {&s.nbhd, I * T * NB * 4}, {&s.flags, I * T * static_cast<size_t>(s.flag_words) * 4},
+      {&s.counter, kMaxChunks * 8}, {&s.ready, I * 4}};
+  for (const auto& [buf, bytes] : wants) {
+    rc = Reserve(ctx, *buf, bytes);
+    if (rc != CEE_OK) return rc;
+  }
+  return CEE_OK;
+}
+
+void SetShape(BatchState& s, const cee_batch_view* b, const cee_batch_options* o) {
+  s.opt = *o;
+  s.instances = b->instances;
+  s.n = b->graph.n;
+  s.m = b->graph.m;
+  s.adj = b->graph.adjacency;
+  s.dist_type = b->graph.dist_type;
+  const int pairs = o->max_neighborhood * (o->max_neighborhood - 1) / 2;
+  s.flag_words = (pairs + 31) / 32;
+  s.node_begin.assign(b->node_begin, b->node_begin + b->instances + 1);
+  s.edge_begin.assign(b->edge_begin, b->edge_begin + b->instances + 1);
+}
+
+BatchArgs MakeArgs(cee_ctx* ctx, BatchState& s, int32_t first, int32_t count, int chunk) {
+  BatchArgs A{};
+  A.g.n = static_cast<int32_t>(s.n);
+  A.g.dist_type = s.dist_type;
+  A.g.m = s.m;
+  A.g.xy = static_cast<const int2*>(s.xy.ptr);
+  A.g.edge_uv = static_cast<const int2*>(s.uv.ptr);
+  A.g.edge_w = static_cast<const int32_t*>(s.w32.ptr);
+  A.g.active = static_cast<const uint8_t*>(s.active.ptr);
+  A.g.row_offsets = static_cast<const int32_t*>(s.ro.ptr);
+  A.g.nbr = static_cast<const int32_t*>(s.nbr.ptr);
+  A.g.slot_w = static_cast<const int32_t*>(s.slotw.ptr);
+  A.node_begin = static_cast<const int64_t*>(s.d_node_begin.ptr);
+  A.edge_begin = static_cast<const int64_t*>(s.d_edge_begin.ptr);
+  A.first_instance = first;
+  A.instances = count;
+  A.targets = s.opt.targets;
+  A.nb = s.opt.max_neighborhood;
+  A.max_degree = s.opt.max_candidate_degree;
+  A.mode = s.opt.cd_mode;
+  A.jv_tile = s.tune.jv_tile;
+  A.flag_words = s.flag_words;
+  A.jv_first = s.edge_begin[first];
+  A.jv_last = s.edge_begin[first + count];
+  A.jv_items = (A.jv_last - A.jv_first + A.jv_tile - 1) / A.jv_tile;
+  A.witness = static_cast<int32_t*>(s.witness.ptr);
+  A.target_ids = static_cast<int32_t*>(s.target_ids.ptr);
+  A.target_count = static_cast<int32_t*>(s.target_count.ptr);
+  A.nbhd = static_cast<int32_t*>(s.nbhd.ptr);
+  A.flags = static_cast<uint32_t*>(s.flags.ptr);
+  A.counter = static_cast<unsigned long long*>(s.counter.ptr) + chunk;
+  A.ready = static_cast<int32_t*>(s.ready.ptr);
+  A.error = ctx->d_error;
+  A.wait_limit = 1ll << 24;  // ~1 s of 64 ns naps
+  return A;
+}
+
+int Grid(cee_ctx* ctx, const BatchState& s, int64_t items) {
+  const int per_sm = std::max(1, std::min(s.tune.blocks_per_sm > 0 ? s.tune.blocks_per_sm : 64,
+                                          s.occupancy[s.narrow ? 0 : 1]));
+  const int64_t want = (items + kBatchWarps - 1) / kBatchWarps;
+  return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(want, static_cast<int64_t>(ctx->sm_count) * per_sm)));
+}
+
+int LaunchRange(cee_ctx* ctx, BatchState& s, int32_t first, int32_t count, int chunk, cudaStream_t stream) {
+  const BatchArgs A = MakeArgs(ctx, s, first, count, chunk);
+  const int64_t items = static_cast<int64_t>(count) * (1 + s.opt.targets) + A.jv_items;
+  cudaMemsetAsync(A.counter, 0, sizeof(unsigned long long), stream);
+  cudaMemsetAsync(A.ready + first, 0, static_cast<size_t>(count) * 4, stream);
+  const int blocks = Grid(ctx, s, items);
+  if (s.narrow) {
+    batch_screen_kernel<false><<<blocks, kBatchWarps * 32, 0, stream>>>(A);
+  } else {
+    batch_screen_kernel<true><<<blocks, kBatchWarps * 32, 0, stream>>>(A);
+  }
+  const cudaError_t status = cudaGetLastError();
+  if (status != cudaSuccess) return CudaFail(ctx, status, "batch_screen_kernel launch");
+  return CEE_OK;
+}
+
+int Capture(cee_ctx* ctx, BatchState& s) {
+  s.ReleaseGraph();
+  cudaError_t status = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+  if (status != cudaSuccess) return CudaFail(ctx, status, "batch graph capture");
+  const int rc = LaunchRange(ctx, s, 0, s.instances, 0, ctx->stream);
+  status = cudaStreamEndCapture(ctx->stream, &s.graph);
+  if (rc != CEE_OK) return rc;
+  if (status != cudaSuccess) return CudaFail(ctx, status, "batch graph capture");
+  status = cudaGraphInstantiate(&s.exec, s.graph, 0);
+  if (status != cudaSuccess) return CudaFail(ctx, status, "batch graph instantiate");
+  return CEE_OK;
+}
+
+// slot_w[s] = edge_w[ids[s]] over slots [s0, s1); bad ids are recorded and read as 0.
+__global__ void batch_gather(const int32_t* __restrict__ ids, int64_t s0, int64_t s1, const int32_t* __restrict__ w32,
+                             int64_t m, int32_t* __restrict__ slotw, int32_t* __restrict__ error) {
+  for (int64_t s = s0 + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; s < s1;
+       s += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t id = ids[s];
+    if (static_cast<uint64_t>(static_cast<uint32_t>(id)) >= static_cast<uint64_t>(m)) {
+      atomicOr(error, 2);
+      slotw[s] = 0;
+    } else {
+      slotw[s] = __ldg(w32 + id);
+    }
+  }
+}
+
+// Raw host layout -> kernel layout for nodes [n0, n1) and edges [e0, e1): coordinates relative to
+// (min_x, min_y), (u, v) pairs, int32 weights. Out-of-range values are recorded in *error and
+// replaced by harmless ones (node 0, weight 0) so that no later access leaves its array.
+__global__ void batch_pack(const int64_t* __restrict__ x, const int64_t* __restrict__ y, int64_t n0, int64_t n1,
+                           int64_t min_x, int64_t min_y, int2* __restrict__ xy, const int32_t* __restrict__ u,
+                           const int32_t* __restrict__ v, const int64_t* __restrict__ w, int64_t e0, int64_t e1,
+                           int64_t n, int2* __restrict__ uv, int32_t* __restrict__ w32, int32_t* __restrict__ error) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t first = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (int64_t i = n0 + first; i < n1; i += stride) {
+    const int64_t dx = x[i] - min_x, dy = y[i] - min_y;
+    if (dx < 0 || dy < 0 || dx >= (int64_t{1} << 30) || dy >= (int64_t{1} << 30)) {
+      atomicOr(error, 16);
+      xy[i] = make_int2(0, 0);
+    } else {
+      xy[i] = make_int2(static_cast<int32_t>(dx), static_cast<int32_t>(dy));
+    }
+  }
+  for (int64_t e = e0 + first; e < e1; e += stride) {
+    int32_t a = u[e], b = v[e];
+    const int64_t wt = w[e];
+    if (static_cast<uint64_t>(static_cast<uint32_t>(a)) >= static_cast<uint64_t>(n) ||
+        static_cast<uint64_t>(static_cast<uint32_t>(b)) >= static_cast<uint64_t>(n) || a >= b) {
+      atomicOr(error, 32);
+      a = b = 0;
+    }
+    if (e > 0) {  // canonical order (u, v) ascending over the union
+      const int32_t pa = u[e - 1], pb = v[e - 1];
+      if (pa > a || (pa == a && pb >= b)) atomicOr(error, 32);
+    }
+    uv[e] = make_int2(a, b);
+    if (wt < 0 || wt > INT32_MAX) {
+      atomicOr(error, 64);
+      w32[e] = 0;
+    } else {
+      w32[e] = static_cast<int32_t>(wt);
+    }
+  }
+}
+
+}  // namespace
 }  // namespace cee
+
+using namespace cee;
+
+extern "C" {
+
+int cee_batch_prepare(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_options* options, cee_batch_stats* stats) {
+  int rc = Activate(ctx);
+  if (rc != CEE_OK) return rc;
+  rc = ValidateOptions(ctx, options);
+  if (rc == CEE_OK) rc = ValidateShape(ctx, b);
+  if (rc != CEE_OK) return rc;
+  const cee_graph_view& g = b->graph;
+  // every edge canonical, inside its own instance, instance-sorted by (u, v)
+  for (int32_t i = 0; i < b->instances; ++i) {
+    const int64_t n0 = b->node_begin[i], n1 = b->node_begin[i + 1];
+    for (int64_t e = b->edge_begin[i]; e < b->edge_begin[i + 1]; ++e) {
+      const int32_t u = g.edge_u[e], v = g.edge_v[e];
+      if (u < n0 || v >= n1 || u >= v) return Fail(ctx, CEE_ERR_INVALID, "edge outside its instance or not canonical");
+      if (e > b->edge_begin[i] && (g.edge_u[e - 1] > u || (g.edge_u[e - 1] == u && g.edge_v[e - 1] >= v))) {
+        return Fail(ctx, CEE_ERR_INVALID, "instance edges must be sorted by (u, v)");
+      }
+      if (g.edge_w[e] < 0 || g.edge_w[e] > INT32_MAX) return Fail(ctx, CEE_ERR_RANGE, "edge weight outside [0, 2^31)");
+    }
+  }
+  BatchState& s = *State(ctx);
+  s.prepared = false;
+  std::vector<int2> xy;
+  rc = PackCoordinates(ctx, g.n, g.x, g.y, &xy, &s.narrow);
+  if (rc != CEE_OK) return rc;
+  SetShape(s, b, options);
+  rc = ReserveAll(ctx, s);
+  if (rc != CEE_OK) return rc;
+  std::vector<int2> uv(static_cast<size_t>(g.m));
+  std::vector<int32_t> w32(static_cast<size_t>(g.m));
+  for (int64_t e = 0; e < g.m; ++e) {
+    uv[e] = make_int2(g.edge_u[e], g.edge_v[e]);
+    w32[e] = static_cast<int32_t>(g.edge_w[e]);
+  }
+  cudaStream_t st = ctx->stream;
+  cudaEventRecord(ctx->ev[0], st);
+  cudaMemcpyAsync(s.d_node_begin.ptr, b->node_begin, (b->instances + 1) * 8, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s.d_edge_begin.ptr, b->edge_begin, (b->instances + 1) * 8, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s.xy.ptr, xy.data(), xy.size() * 8, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s.uv.ptr, uv.data(), uv.size() * 8, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s.w32.ptr, w32.data(), w32.size() * 4, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s.active.ptr, g.active, static_cast<size_t>(g.m), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s.ro.ptr, g.row_offsets, (static_cast<size_t>(g.n) + 1) * 4, cudaMemcpyHostToDevice, st);
+  if (g.adjacency > 0) {
+    cudaMemcpyAsync(s.nbr.ptr, g.neighbors, static_cast<size_t>(g.adjacency) * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(s.ids.ptr, g.csr_edge_ids, static_cast<size_t>(g.adjacency) * 4, cudaMemcpyHostToDevice, st);
+  }
+  cudaMemsetAsync(ctx->d_error, 0, sizeof(int32_t), st);
+  if (g.adjacency > 0) {
+    batch_gather<<<GridFor(g.adjacency, 256, ctx->sm_count * 8), 256, 0, st>>>(
+        static_cast<const int32_t*>(s.ids.ptr), 0, g.adjacency, static_cast<const int32_t*>(s.w32.ptr), g.m,
+        static_cast<int32_t*>(s.slotw.ptr), ctx->d_error);
+  }
+  cudaError_t status = cudaStreamSynchronize(st);  // host staging vectors die at return
+  if (status != cudaSuccess) return CudaFail(ctx, status, "batch upload");
+  cudaEventRecord(ctx->ev[1], st);
+  for (int wide = 0; wide < 2; ++wide) {
+    int blocks = 0;
+    status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &blocks, wide ? batch_screen_kernel<true> : batch_screen_kernel<false>, kBatchWarps * 32, 0);
+    if (status != cudaSuccess) return CudaFail(ctx, status, "batch occupancy");
+    s.occupancy[wide] = std::max(1, blocks);
+  }
+  rc = Capture(ctx, s);
+  if (rc != CEE_OK) return rc;
+  s.prepared = true;
+  if (stats != nullptr) {
+    *stats = cee_batch_stats{};
+    stats->nodes = s.n;
+    stats->edges = s.m;
+    stats->adjacency = s.adj;
+    stats->targets = static_cast<int64_t>(s.instances) * s.opt.targets;
+    stats->flag_words = s.flag_words;
+    stats->resident_bytes = BatchResident(ctx);
+    stats->h2d_bytes = static_cast<int64_t>((b->instances + 1) * 16 + xy.size() * 8 + uv.size() * 12 + g.m +
+                                            (g.n + 1) * 4 + g.adjacency * 8);
+  }
+  return CEE_OK;
+}
+
+int cee_batch_launch(cee_ctx* ctx) {
+  int rc = Activate(ctx);
+  if (rc != CEE_OK) return rc;
+  BatchState* s = ctx->batch;
+  if (s == nullptr || !s->prepared || s->exec == nullptr) return Fail(ctx, CEE_ERR_STATE, "batch not prepared");
+  const cudaError_t status = cudaGraphLaunch(s->exec, ctx->stream);
+  if (status != cudaSuccess) return CudaFail(ctx, status, "batch graph launch");
+  return CEE_OK;
+}
+
+int cee_batch_launch_plain(cee_ctx* ctx) {
+  int rc = Activate(ctx);
+  if (rc != CEE_OK) return rc;
+  BatchState* s = ctx->batch;
+  if (s == nullptr || !s->prepared) return Fail(ctx, CEE_ERR_STATE, "batch not prepared");
+  for (int32_t i = 0; i < s->instances; ++i) {
+    rc = LaunchRange(ctx, *s, i, 1, 0, ctx->stream);
+    if (rc != CEE_OK) return rc;
+    const cudaError_t status = cudaStreamSynchronize(ctx->stream);
+    if (status != cudaSuccess) return CudaFail(ctx, status, "plain batch launch");
+  }
+  return CEE_OK;
+}
+
+int cee_batch_fetch(cee_ctx* ctx, int32_t* witness, int32_t* target_ids, int32_t* target_count, int32_t* nbhd,
+                    uint32_t* flags) {
+  int rc = Activate(ctx);
+  if (rc != CEE_OK) return rc;
+  BatchState* s = ctx->batch;
+  if (s == nullptr || !s->prepared) return Fail(ctx, CEE_ERR_STATE, "batch not prepared");
+  const size_t IT = static_cast<size_t>(s->instances) * s->opt.targets;
+  cudaStream_t st = ctx->stream;
+  if (witness != nullptr) cudaMemcpyAsync(witness, s->witness.ptr, s->m * 4, cudaMemcpyDeviceToHost, st);
+  if (target_ids != nullptr) cudaMemcpyAsync(target_ids, s->target_ids.ptr, IT * 4, cudaMemcpyDeviceToHost, st);
+  if (target_count != nullptr) {
+    cudaMemcpyAsync(target_count, s->target_count.ptr, s->instances * 4, cudaMemcpyDeviceToHost, st);
+  }
+  if (nbhd != nullptr) {
+    cudaMemcpyAsync(nbhd, s->nbhd.ptr, IT * s->opt.max_neighborhood * 4, cudaMemcpyDeviceToHost, st);
+  }
+  if (flags != nullptr) cudaMemcpyAsync(flags, s->flags.ptr, IT * s->flag_words * 4, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(ctx->h_error, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+  const cudaError_t status = cudaStreamSynchronize(st);
+  if (status != cudaSuccess) return CudaFail(ctx, status, "batch fetch");
+  return CheckDeviceError(ctx, "batched screen");
+}
+
+int cee_batch_set_tuning(cee_ctx* ctx, const cee_batch_tuning* t) {
+  int rc = Activate(ctx);
+  if (rc != CEE_OK) return rc;
+  if (t == nullptr || t->jv_tile < 1 || t->jv_tile > 4096 || t->blocks_per_sm < 0 || t->blocks_per_sm > 64 ||
+      t->chunks < 1 || t->chunks > kMaxChunks) {
+    return Fail(ctx, CEE_ERR_INVALID, "bad batch tuning");
+  }
+  BatchState& s = *State(ctx);
+  s.tune = *t;
+  if (s.prepared) return Capture(ctx, s);
+  return CEE_OK;
+}
+
+int cee_batch_get_tuning(const cee_ctx* ctx, cee_batch_tuning* t) {
+  if (ctx == nullptr || t == nullptr) return Fail(nullptr, CEE_ERR_INVALID, "null argument");
+  *t = ctx->batch != nullptr ? ctx->batch->tune : cee_batch_tuning{64, 0, 8};
+  return CEE_OK;
+}
+
+int cee_batch_autotune(cee_ctx* ctx, int32_t reps, cee_batch_tuning* chosen) {
+  int rc = Activate(ctx);
+  if (rc != CEE_OK) return rc;
+  BatchState* s = ctx->batch;
+  if (s == nullptr || !s->prepared) return Fail(ctx, CEE_ERR_STATE, "batch not prepared");
+  reps = std::max(1, reps);
+  const cee_batch_tuning start = s->tune;
+  cee_batch_tuning best = start;
+  float best_ms = 1e30f;
+  const int occ = s->occupancy[s->narrow ? 0 : 1];
+  for (const int tile : {16, 32, 64, 128, 256}) {
+    for (const int per_sm : {occ, std::max(1, occ / 2)}) {
+      cee_batch_tuning t = start;
+      t.jv_tile = tile;
+      t.blocks_per_sm = per_sm;
+      rc = cee_batch_set_tuning(ctx, &t);
+      if (rc != CEE_OK) return rc;
+      rc = cee_batch_launch(ctx);  // warm-up
+      if (rc != CEE_OK) return rc;
+      cudaEventRecord(ctx->ev[2], ctx->stream);
+      for (int r = 0; r < reps; ++r) {
+        rc = cee_batch_launch(ctx);
+        if (rc != CEE_OK) return rc;
+      }
+      cudaEventRecord(ctx->ev[3], ctx->stream);
+      const cudaError_t status = cudaEventSynchronize(ctx->ev[3]);
+      if (status != cudaSuccess) return CudaFail(ctx, status, "batch autotune");
+      const float ms = EventMs(ctx->ev[2], ctx->ev[3]) / reps;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = t;
+      }
+    }
+  }
+  rc = cee_batch_set_tuning(ctx, &best);
+  if (rc != CEE_OK) return rc;
+  if (chosen != nullptr) *chosen = best;
+  return CEE_OK;
+}
+
+int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_options* options, int32_t* witness,
+                     int32_t* target_ids, int32_t* target_count, int32_t* nbhd, uint32_t* flags,
+                     cee_batch_stats* stats) {
+  int rc = Activate(ctx);
+  if (rc != CEE_OK) return rc;
+  rc = ValidateOptions(ctx, options);
+  if (rc == CEE_OK) rc = ValidateShape(ctx, b);
+  if (rc != CEE_OK) return rc;
+  const cee_graph_view& g = b->graph;
+  BatchState& s = *State(ctx);
+  s.prepared = false;
+  s.ReleaseGraph();
+  int64_t min_x = 0, min_y = 0, max_x = 0, max_y = 0;
+  for (int64_t i = 0; i < g.n; ++i) {
+    min_x = i == 0 ? g.x[i] : std::min(min_x, g.x[i]);
+    max_x = i == 0 ? g.x[i] : std::max(max_x, g.x[i]);
+    min_y = i == 0 ? g.y[i] : std::min(min_y, g.y[i]);
+    max_y = i == 0 ? g.y[i] : std::max(max_y, g.y[i]);
+  }
+  if (static_cast<__int128>(max_x) - min_x >= (__int128{1} << 30) ||
+      static_cast<__int128>(max_y) - min_y >= (__int128{1} << 30)) {
+    return Fail(ctx, CEE_ERR_RANGE, "coordinate span >= 2^30: outside the exact int32 distance range of the kernels");
+  }
+  s.narrow = max_x - min_x < kNarrowSpan && max_y - min_y < kNarrowSpan;
+  SetShape(s, b, options);
+  rc = ReserveAll(ctx, s);
+  for (const auto& [buf, bytes] : {std::pair<DevBuf*, size_t>{&s.raw_x, g.n * 8ull}, {&s.raw_y, g.n * 8ull},
+                                   {&s.raw_u, g.m * 4ull}, {&s.raw_v, g.m * 4ull}, {&s.raw_w, g.m * 8ull}}) {
+    if (rc == CEE_OK) rc = Reserve(ctx, *buf, bytes);
+  }
+  if (rc != CEE_OK) return rc;
+  cudaError_t status = cudaSuccess;
+  if (s.h2d == nullptr) status = cudaStreamCreateWithFlags(&s.h2d, cudaStreamNonBlocking);
+  if (status == cudaSuccess && s.d2h == nullptr) status = cudaStreamCreateWithFlags(&s.d2h, cudaStreamNonBlocking);
+  for (int i = 0; i < kMaxChunks && status == cudaSuccess; ++i) {
+    if (s.up[i] == nullptr) status = cudaEventCreateWithFlags(&s.up[i], cudaEventDisableTiming);
+    if (status == cudaSuccess && s.done[i] == nullptr) status = cudaEventCreateWithFlags(&s.done[i], cudaEventDisableTiming);
+  }
+  if (status != cudaSuccess) return CudaFail(ctx, status, "batch streams");
+  for (int wide = 0; wide < 2; ++wide) {
+    int blocks = 0;
+    status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &blocks, wide ? batch_screen_kernel<true> : batch_screen_kernel<false>, kBatchWarps * 32, 0);
+    if (status != cudaSuccess) return CudaFail(ctx, status, "batch occupancy");
+    s.occupancy[wide] = std::max(1, blocks);
+  }
+  const int chunks = std::max(1, std::min<int>(s.tune.chunks, b->instances));
+  cudaStream_t cs = ctx->stream;
+  cudaEventRecord(ctx->ev[0], cs);
+  cudaStreamWaitEvent(s.h2d, ctx->ev[0], 0);
+  cudaMemsetAsync(ctx->d_error, 0, sizeof(int32_t), cs);
+  cudaMemcpyAsync(s.d_node_begin.ptr, b->node_begin, (b->instances + 1) * 8, cudaMemcpyHostToDevice, cs);
+  cudaMemcpyAsync(s.d_edge_begin.ptr, b->edge_begin, (b->instances + 1) * 8, cudaMemcpyHostToDevice, cs);
+  const size_t T = static_cast<size_t>(s.opt.targets), NB = static_cast<size_t>(s.opt.max_neighborhood);
+  const size_t FW = static_cast<size_t>(s.flag_words);
+  int64_t h2d_bytes = (b->instances + 1) * 16, d2h_bytes = 0;
+  for (int c = 0; c < chunks; ++c) {
+    const int32_t i0 = static_cast<int32_t>(static_cast<int64_t>(b->instances) * c / chunks);
+    const int32_t i1 = static_cast<int32_t>(static_cast<int64_t>(b->instances) * (c + 1) / chunks);
+    if (i1 == i0) continue;
+    const int64_t n0 = b->node_begin[i0], n1 = b->node_begin[i1], e0 = b->edge_begin[i0], e1 = b->edge_begin[i1];
+    const int64_t s0 = g.row_offsets[n0], s1 = g.row_offsets[n1];
+    // upload the chunk (copy engine stream)
+    cudaMemcpyAsync(static_cast<int64_t*>(s.raw_x.ptr) + n0, g.x + n0, (n1 - n0) * 8, cudaMemcpyHostToDevice, s.h2d);
+    cudaMemcpyAsync(static_cast<int64_t*>(s.raw_y.ptr) + n0, g.y + n0, (n1 - n0) * 8, cudaMemcpyHostToDevice, s.h2d);
+    cudaMemcpyAsync(static_cast<int32_t*>(s.ro.ptr) + n0, g.row_offsets + n0, (n1 - n0 + 1) * 4, cudaMemcpyHostToDevice, s.h2d);
+    cudaMemcpyAsync(static_cast<int32_t*>(s.raw_u.ptr) + e0, g.edge_u + e0, (e1 - e0) * 4, cudaMemcpyHostToDevice, s.h2d);
+    cudaMemcpyAsync(static_cast<int32_t*>(s.raw_v.ptr) + e0, g.edge_v + e0, (e1 - e0) * 4, cudaMemcpyHostToDevice, s.h2d);
+    cudaMemcpyAsync(static_cast<int64_t*>(s.raw_w.ptr) + e0, g.edge_w + e0, (e1 - e0) * 8, cudaMemcpyHostToDevice, s.h2d);
+    cudaMemcpyAsync(static_cast<uint8_t*>(s.active.ptr) + e0, g.active + e0, e1 - e0, cudaMemcpyHostToDevice, s.h2d);
+    if (s1 > s0) {
+      cudaMemcpyAsync(static_cast<int32_t*>(s.nbr.ptr) + s0, g.neighbors + s0, (s1 - s0) * 4, cudaMemcpyHostToDevice, s.h2d);
+      cudaMemcpyAsync(static_cast<int32_t*>(s.ids.ptr) + s0, g.csr_edge_ids + s0, (s1 - s0) * 4, cudaMemcpyHostToDevice, s.h2d);
+    }
+    h2d_bytes += (n1 - n0) * 20 + 4 + (e1 - e0) * 17 + (s1 - s0) * 8;
+    cudaEventRecord(s.up[c], s.h2d);
+    // convert and screen (compute stream)
+    cudaStreamWaitEvent(cs, s.up[c], 0);
+    batch_pack<<<GridFor(std::max(n1 - n0, e1 - e0), 256, ctx->sm_count * 8), 256, 0, cs>>>(
+        static_cast<const int64_t*>(s.raw_x.ptr), static_cast<const int64_t*>(s.raw_y.ptr), n0, n1, min_x, min_y,
+        static_cast<int2*>(s.xy.ptr), static_cast<const int32_t*>(s.raw_u.ptr), static_cast<const int32_t*>(s.raw_v.ptr),
+        static_cast<const int64_t*>(s.raw_w.ptr), e0, e1, g.n, static_cast<int2*>(s.uv.ptr),
+        static_cast<int32_t*>(s.w32.ptr), ctx->d_error);
+    if (s1 > s0) {
+      batch_gather<<<GridFor(s1 - s0, 256, ctx->sm_count * 8), 256, 0, cs>>>(
+          static_cast<const int32_t*>(s.ids.ptr), s0, s1, static_cast<const int32_t*>(s.w32.ptr), g.m,
+          static_cast<int32_t*>(s.slotw.ptr), ctx->d_error);
+    }
+    rc = LaunchRange(ctx, s, i0, i1 - i0, c, cs);
+    if (rc != CEE_OK) return rc;
+    cudaEventRecord(s.done[c], cs);
+    // download the chunk's results (second copy stream)
+    cudaStreamWaitEvent(s.d2h, s.done[c], 0);
+    const size_t t0 = static_cast<size_t>(i0) * T, t1 = static_cast<size_t>(i1) * T;
+    if (witness != nullptr) {
+      cudaMemcpyAsync(witness + e0, static_cast<int32_t*>(s.witness.ptr) + e0, (e1 - e0) * 4, cudaMemcpyDeviceToHost, s.d2h);
+      d2h_bytes += (e1 - e0) * 4;
+    }
+    if (target_ids != nullptr) {
+      cudaMemcpyAsync(target_ids + t0, static_cast<int32_t*>(s.target_ids.ptr) + t0, (t1 - t0) * 4,
+                      cudaMemcpyDeviceToHost, s.d2h);
+      d2h_bytes += (t1 - t0) * 4;
+    }
+    if (target_count != nullptr) {
+      cudaMemcpyAsync(target_count + i0, static_cast<int32_t*>(s.target_count.ptr) + i0, (i1 - i0) * 4,
+                      cudaMemcpyDeviceToHost, s.d2h);
+      d2h_bytes += (i1 - i0) * 4;
+    }
+    if (nbhd != nullptr) {
+      cudaMemcpyAsync(nbhd + t0 * NB, static_cast<int32_t*>(s.nbhd.ptr) + t0 * NB, (t1 - t0) * NB * 4,
+                      cudaMemcpyDeviceToHost, s.d2h);
+      d2h_bytes += (t1 - t0) * NB * 4;
+    }
+    if (flags != nullptr) {
+      cudaMemcpyAsync(flags + t0 * FW, static_cast<uint32_t*>(s.flags.ptr) + t0 * FW, (t1 - t0) * FW * 4,
+                      cudaMemcpyDeviceToHost, s.d2h);
+      d2h_bytes += (t1 - t0) * FW * 4;
+    }
+  }
+  cudaEventRecord(ctx->ev[4], s.d2h);
+  cudaStreamWaitEvent(cs, ctx->ev[4], 0);
+  cudaMemcpyAsync(ctx->h_error, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost, cs);
+  cudaEventRecord(ctx->ev[5], cs);
+  status = cudaStreamSynchronize(cs);
+  if (status != cudaSuccess) return CudaFail(ctx, status, "batched screen");
+  rc = CheckDeviceError(ctx, "batched screen");
+  if (rc != CEE_OK) return rc;
+  s.prepared = true;  // the resident copy now holds this batch
+  rc = Capture(ctx, s);
+  if (rc != CEE_OK) return rc;
+  if (stats != nullptr) {
+    *stats = cee_batch_stats{};
+    stats->nodes = s.n;
+    stats->edges = s.m;
+    stats->adjacency = s.adj;
+    stats->targets = static_cast<int64_t>(s.instances) * s.opt.targets;
+    stats->flag_words = s.flag_words;
+    stats->resident_bytes = BatchResident(ctx);
+    stats->h2d_bytes = h2d_bytes;
+    stats->d2h_bytes = d2h_bytes;
+    stats->total_ms = EventMs(ctx->ev[0], ctx->ev[5]);
+  }
+  return CEE_OK;
+}
+
+}  // extern "C"

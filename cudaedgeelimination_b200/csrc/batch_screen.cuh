@@ -1,0 +1,313 @@
+// Batched screen: many instances (disjoint snapshots packed into one union snapshot with
+// global ids) screened by one persistent kernel. Warps pull work items from an atomic counter:
+//
+//   [0, I)            target selection of instance i: the first T edges of
+//                     SelectHtTargetEdgeIds (src/cpu/ht_scan.cpp:316-345) -- active edges with
+//                     both degrees > 2, weight descending, then (u, v, id) ascending;
+//   [I, I + J)        JV tiles: `jv_tile` consecutive union edges screened one warp per edge
+//                     (jv_screen_edge_warp, same semantics as the single-snapshot screen);
+//   [I + J, I + J + I*T)  one HT c,d root screen per target (u, v): BuildCdScreenTasks
+//                     (src/cpu/hamilton_tutte.cpp:168-216) -- the `nb` nodes of the instance
+//                     other than u, v with degree <= max_degree (0 = no cap) nearest to the
+//                     doubled midpoint 2p - p_u - p_v, ties by node -- then every pair i < j of
+//                     that neighbourhood as (c, d) = (min, max) screened as ScreenHtCdKernel
+//                     (src/cuda/ht_cd.cu:157-178).
+//
+// The c,d items of an instance wait (bounded, with an error on timeout) for that instance's
+// target-selection item; those items come first in the queue and take a few microseconds, so
+// the wait is normally never observed. All CTAs of the grid are resident (the grid is sized
+// from the occupancy), so every claimed item runs to completion.
+#pragma once
+
+#include "cd_screen.cuh"
+#include "jv_screen.cuh"
+
+namespace cee {
+
+constexpr int kBatchWarps = 8;
+constexpr int kBatchMaxTargets = 64;
+constexpr int kBatchMaxNeighborhood = 32;
+constexpr int kBatchMaxPairs = kBatchMaxNeighborhood * (kBatchMaxNeighborhood - 1) / 2;  // 496
+constexpr int kBatchFlagWords = (kBatchMaxPairs + 31) / 32;                              // 16
+constexpr int32_t kBatchWaitError = 8;
+
+struct BatchArgs {
+  JvGraph g;                          // the union snapshot (global node and edge ids)
+  const int64_t* __restrict__ node_begin;  // [instances + 1]
+  const int64_t* __restrict__ edge_begin;  // [instances + 1]
+  int32_t first_instance, instances;  // this launch covers instances [first, first + instances)
+  int32_t targets;                    // T <= 64
+  int32_t nb;                         // neighbourhood size, 2..32
+  int32_t max_degree;                 // 0 = no cap
+  int32_t mode;                       // HtCdMode
+  int32_t jv_tile;                    // edges per JV work item
+  int32_t flag_words;                 // ceil(nb (nb - 1) / 2 / 32)
+  int64_t jv_first, jv_items;         // JV tiles cover union edges [jv_first, jv_first + items * tile) clipped
+  int64_t jv_last;
+  int32_t* __restrict__ witness;      // [m]
+  int32_t* __restrict__ target_ids;   // [I * T] global edge ids, -1 padding
+  int32_t* __restrict__ target_count; // [I]
+  int32_t* __restrict__ nbhd;         // [I * T * nb] global node ids, -1 padding
+  uint32_t* __restrict__ flags;       // [I * T * flag_words] bit p = flag of pair p
+  unsigned long long* __restrict__ counter;  // work counter, zero at launch
+  int32_t* __restrict__ ready;        // [I] set when the instance's targets are written, zero at launch
+  int32_t* __restrict__ error;
+  long long wait_limit;               // spin iterations before an item gives up
+};
+
+struct BatchWarpScratch {
+  JvWarpScratch jv;
+};
+
+// ---- warp top lists ------------------------------------------------------------------
+
+__device__ __forceinline__ uint64_t warp_bitonic_clean(uint64_t key, int lane) {
+#pragma unroll
+  for (int j = 16; j > 0; j >>= 1) {
+    const uint64_t other = __shfl_xor_sync(kFullMask, key, j);
+    key = (lane & j) == 0 ? min(key, other) : max(key, other);
+  }
+  return key;
+}
+
+// (score, node) pairs ordered lexicographically.
+__device__ __forceinline__ bool pair_less(uint64_t sa, int32_t na, uint64_t sb, int32_t nb) {
+  return sa < sb || (sa == sb && na < nb);
+}
+
+__device__ __forceinline__ void warp_sort_pairs(uint64_t& score, int32_t& node, int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const uint64_t os = __shfl_xor_sync(kFullMask, score, j);
+      const int32_t on = __shfl_xor_sync(kFullMask, node, j);
+      const bool ascending = (lane & k) == 0;
+      const bool lower = (lane & j) == 0;
+      const bool other_smaller = pair_less(os, on, score, node);
+      if ((lower == ascending) == other_smaller) {
+        score = os;
+        node = on;
+      }
+    }
+  }
+}
+
+// The 32 smallest pairs of two ascending lists, ascending.
+__device__ __forceinline__ void warp_merge_pairs(uint64_t& score, int32_t& node, uint64_t bs, int32_t bn, int lane) {
+  const uint64_t rs = __shfl_sync(kFullMask, bs, 31 - lane);
+  const int32_t rn = __shfl_sync(kFullMask, bn, 31 - lane);
+  if (pair_less(rs, rn, score, node)) {
+    score = rs;
+    node = rn;
+  }
+#pragma unroll
+  for (int j = 16; j > 0; j >>= 1) {
+    const uint64_t os = __shfl_xor_sync(kFullMask, score, j);
+    const int32_t on = __shfl_xor_sync(kFullMask, node, j);
+    const bool other_smaller = pair_less(os, on, score, node);
+    if (((lane & j) == 0) == other_smaller) {
+      score = os;
+      node = on;
+    }
+  }
+}
+
+// ---- work items ----------------------------------------------------------------------
+
+template <bool kWide>
+__device__ void batch_select_targets(const BatchArgs& A, int32_t inst, int lane) {
+  const JvGraph& g = A.g;
+  const int64_t e0 = A.edge_begin[inst], e1 = A.edge_begin[inst + 1];
+  const int K = A.targets;
+  uint64_t l1 = kEmptyKey, l2 = kEmptyKey;  // ascending ranks 0..31 and 32..63
+  for (int64_t base = e0; base < e1; base += 32) {
+    const int64_t e = base + lane;
+    uint64_t key = kEmptyKey;
+    if (e < e1 && g.active[e] != 0) {
+      const int2 uv = g.edge_uv[e];
+      const int32_t du = __ldg(g.row_offsets + uv.x + 1) - __ldg(g.row_offsets + uv.x);
+      const int32_t dv = __ldg(g.row_offsets + uv.y + 1) - __ldg(g.row_offsets + uv.y);
+      if (du > 2 && dv > 2) {
+        // weight descending, then the instance's edge order (= (u, v) order, edges canonical)
+        key = (static_cast<uint64_t>(0x7fffffffu - static_cast<uint32_t>(__ldg(g.edge_w + e))) << 32) |
+              static_cast<uint32_t>(e - e0);
+      }
+    }
+    const uint64_t threshold = K <= 32 ? __shfl_sync(kFullMask, l1, K - 1) : __shfl_sync(kFullMask, l2, K - 33);
+    if (!__any_sync(kFullMask, key < threshold)) continue;
+    const uint64_t batch = warp_sort_asc(key, lane);
+    const uint64_t reversed = __shfl_sync(kFullMask, batch, 31 - lane);
+    const uint64_t lo = min(l1, reversed), hi = max(l1, reversed);
+    l1 = warp_bitonic_clean(lo, lane);
+    if (K > 32) l2 = warp_merge_smallest(l2, warp_bitonic_clean(hi, lane), lane);
+  }
+  int32_t* out = A.target_ids + static_cast<int64_t>(inst) * K;
+  const int32_t id1 = l1 == kEmptyKey ? -1 : static_cast<int32_t>(e0 + (l1 & 0xffffffffu));
+  const int32_t id2 = l2 == kEmptyKey ? -1 : static_cast<int32_t>(e0 + (l2 & 0xffffffffu));
+  if (lane < K) out[lane] = id1;
+  if (lane + 32 < K) out[lane + 32] = id2;
+  const int count = __popc(__ballot_sync(kFullMask, lane < K && id1 >= 0)) +
+                    __popc(__ballot_sync(kFullMask, lane + 32 < K && id2 >= 0));
+  __syncwarp();
+  if (lane == 0) {
+    A.target_count[inst] = count;
+    __threadfence();
+    atomicExch(A.ready + inst, 1);
+  }
+}
+
+template <bool kWide>
+__device__ void batch_cd_target(const BatchArgs& A, int32_t inst, int32_t t, const uint8_t* pair_i,
+                                 const uint8_t* pair_j, int lane) {
+  const JvGraph& g = A.g;
+  const int64_t slot = static_cast<int64_t>(inst) * A.targets + t;
+  int32_t* nbhd_out = A.nbhd + slot * A.nb;
+  uint32_t* flags_out = A.flags + slot * A.flag_words;
+  // wait for the instance's targets (bounded)
+  if (lane == 0) {
+    long long spins = 0;
+    while (atomicAdd(A.ready + inst, 0) == 0 && spins < A.wait_limit) {
+      __nanosleep(64);
+      ++spins;
+    }
+    if (spins >= A.wait_limit) atomicOr(A.error, kBatchWaitError);
+  }
+  __syncwarp();
+  const int32_t count = *reinterpret_cast<volatile int32_t*>(A.target_count + inst);
+  const int32_t target = t < count ? *reinterpret_cast<volatile int32_t*>(A.target_ids + slot) : -1;
+  if (target < 0) {
+    for (int r = lane; r < A.nb; r += 32) nbhd_out[r] = -1;
+    for (int w = lane; w < A.flag_words; w += 32) flags_out[w] = 0;
+    return;
+  }
+  const int2 uv = g.edge_uv[target];
+  const int32_t u = uv.x, v = uv.y;
+  const int2 pu = __ldg(g.xy + u), pv = __ldg(g.xy + v);
+  const int64_t n0 = A.node_begin[inst], n1 = A.node_begin[inst + 1];
+  const int64_t mx = static_cast<int64_t>(pu.x) + pv.x, my = static_cast<int64_t>(pu.y) + pv.y;
+  const int NB = A.nb;
+
+  // neighbourhood: the NB smallest (doubled-midpoint squared distance, node)
+  uint64_t ls = kEmptyKey;
+  int32_t ln = INT32_MAX;
+  for (int64_t base = n0; base < n1; base += 32) {
+    const int64_t x = base + lane;
+    uint64_t s = kEmptyKey;
+    int32_t node = INT32_MAX;
+    if (x < n1 && x != u && x != v) {
+      const int32_t deg = __ldg(g.row_offsets + x + 1) - __ldg(g.row_offsets + x);
+      if (A.max_degree == 0 || deg <= A.max_degree) {
+        const int2 p = __ldg(g.xy + x);
+        const int64_t dx = 2 * static_cast<int64_t>(p.x) - mx, dy = 2 * static_cast<int64_t>(p.y) - my;
+        s = static_cast<uint64_t>(dx * dx) + static_cast<uint64_t>(dy * dy);
+        node = static_cast<int32_t>(x);
+      }
+    }
+    const uint64_t ts = __shfl_sync(kFullMask, ls, NB - 1);
+    const int32_t tn = __shfl_sync(kFullMask, ln, NB - 1);
+    if (!__any_sync(kFullMask, pair_less(s, node, ts, tn))) continue;
+    warp_sort_pairs(s, node, lane);
+    warp_merge_pairs(ls, ln, s, node, lane);
+  }
+  const bool have = lane < NB && ln != INT32_MAX;
+  if (lane < NB) nbhd_out[lane] = have ? ln : -1;
+  const int size = __popc(__ballot_sync(kFullMask, have));
+  // C(u, x) and C(v, x) of every neighbourhood node
+  uint32_t cu = 0, cv = 0;
+  int2 px = make_int2(0, 0);
+  if (have) {
+    px = __ldg(g.xy + ln);
+    cu = exact_distance<kWide>(pu, px, g.dist_type);
+    cv = exact_distance<kWide>(pv, px, g.dist_type);
+  }
+  const uint32_t cuv = exact_distance<kWide>(pu, pv, g.dist_type);
+  const int pairs = size * (size - 1) / 2;
+  // pair p of the neighbourhood is (i, j), i < j, in the reference's order (i major); the smem
+  // table holds that order for the full size NB, a smaller neighbourhood (a small instance)
+  // inverts p for its own size
+  for (int base = 0; base < A.flag_words * 32; base += 32) {
+    const int p = base + lane;
+    bool flag = false;
+    int i = 0, j = 1;
+    if (p < pairs) {
+      if (size == NB) {
+        i = pair_i[p];
+        j = pair_j[p];
+      } else {
+        i = 0;
+        int rest = p;
+        while (rest >= size - 1 - i) {
+          rest -= size - 1 - i;
+          ++i;
+        }
+        j = i + 1 + rest;
+      }
+    }
+    const int32_t ni = __shfl_sync(kFullMask, ln, i), nj = __shfl_sync(kFullMask, ln, j);
+    const uint32_t cui = __shfl_sync(kFullMask, cu, i), cuj = __shfl_sync(kFullMask, cu, j);
+    const uint32_t cvi = __shfl_sync(kFullMask, cv, i), cvj = __shfl_sync(kFullMask, cv, j);
+    const int2 pi = make_int2(__shfl_sync(kFullMask, px.x, i), __shfl_sync(kFullMask, px.y, i));
+    const int2 pj = make_int2(__shfl_sync(kFullMask, px.x, j), __shfl_sync(kFullMask, px.y, j));
+    if (p < pairs) {
+      const bool i_is_c = ni < nj;
+      const int32_t c = i_is_c ? ni : nj, d = i_is_c ? nj : ni;
+      const uint32_t cuc = i_is_c ? cui : cuj, cud = i_is_c ? cuj : cui;
+      const uint32_t cvc = i_is_c ? cvi : cvj, cvd = i_is_c ? cvj : cvi;
+      const bool active = row_contains(g.nbr, __ldg(g.row_offsets + c), __ldg(g.row_offsets + c + 1), d);
+      const uint64_t original = static_cast<uint64_t>(cuv) + exact_distance<kWide>(pi, pj, g.dist_type);
+      const uint64_t orient0 = static_cast<uint64_t>(cud) + cvc;
+      const uint64_t orient1 = static_cast<uint64_t>(cuc) + cvd;
+      const bool incompatible = orient0 < original && orient1 < original;
+      flag = A.mode == 0 ? (active && incompatible) : (!active || incompatible);
+    }
+    const uint32_t word = __ballot_sync(kFullMask, flag);
+    if (lane == 0) flags_out[base >> 5] = word;
+  }
+}
+
+template <bool kWide>
+static __global__ void __launch_bounds__(kBatchWarps * 32) batch_screen_kernel(BatchArgs A) {
+  __shared__ BatchWarpScratch scratch[kBatchWarps];
+  __shared__ uint8_t pair_i[kBatchMaxPairs], pair_j[kBatchMaxPairs];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int p = threadIdx.x; p < A.nb * (A.nb - 1) / 2; p += blockDim.x) {
+    int i = 0, rest = p;
+    while (rest >= A.nb - 1 - i) {
+      rest -= A.nb - 1 - i;
+      ++i;
+    }
+    pair_i[p] = static_cast<uint8_t>(i);
+    pair_j[p] = static_cast<uint8_t>(i + 1 + rest);
+  }
+  __syncthreads();
+  const int64_t n_select = A.instances;
+  const int64_t n_jv = A.jv_items;
+  const int64_t n_cd = static_cast<int64_t>(A.instances) * A.targets;
+  const int64_t total = n_select + n_jv + n_cd;
+  while (true) {
+    unsigned long long item = 0;
+    if (lane == 0) item = atomicAdd(A.counter, 1ull);
+    item = __shfl_sync(kFullMask, item, 0);
+    if (static_cast<int64_t>(item) >= total) break;
+    const int64_t q = static_cast<int64_t>(item);
+    if (q < n_select) {
+      batch_select_targets<kWide>(A, A.first_instance + static_cast<int32_t>(q), lane);
+    } else if (q < n_select + n_jv) {
+      const int64_t e0 = A.jv_first + (q - n_select) * A.jv_tile;
+      const int64_t e1 = min(e0 + A.jv_tile, A.jv_last);
+      for (int64_t e = e0; e < e1; ++e) {
+        const int32_t w = jv_screen_edge_warp<kWide>(A.g, e, scratch[warp].jv, lane, A.error);
+        if (lane == 0) A.witness[e] = w;
+        __syncwarp();
+      }
+    } else {
+      const int64_t s = q - n_select - n_jv;
+      batch_cd_target<kWide>(A, A.first_instance + static_cast<int32_t>(s / A.targets),
+                             static_cast<int32_t>(s % A.targets), pair_i, pair_j, lane);
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace cee

@@ -149,7 +149,7 @@ class BatchUnion:
         g.n, g.dist_type, g.x, g.y = int(n), EUC_2D, x, y
         g.edge_u, g.edge_v, g.edge_w, g.active = eu, ev, w, np.ones(m, np.uint8)
         g.row_offsets, g.neighbors, g.csr_edge_ids = ro, nb, ids
-        g.csr_weights = None
+        g.csr_weights = np.ascontiguousarray(w[ids])
         self.graph = g
 
     def instance(self, i: int) -> GraphSnapshot:

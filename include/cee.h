@@ -243,6 +243,72 @@ typedef struct {
 int cee_cd_screen(cee_ctx* ctx, const cee_graph_view* graph, int32_t u, int32_t v,
                   const cee_cd_task* tasks, int64_t count, int32_t mode, uint8_t* flags_out);
 
+/* ---- batched screen (many instances, one persistent graph-captured launch) ---------------- */
+
+/* Many snapshots packed into one: instance i owns nodes [node_begin[i], node_begin[i+1]) and
+ * edges [edge_begin[i], edge_begin[i+1]) of `graph`, which uses global node and edge ids; every
+ * edge joins two nodes of its own instance and each instance's edges are sorted by (u, v) (the
+ * order GraphSnapshot::Load produces, src/common/graph.cpp:223-226). */
+typedef struct {
+  int32_t instances;
+  const int64_t* node_begin; /* [instances + 1] */
+  const int64_t* edge_begin; /* [instances + 1] */
+  cee_graph_view graph;
+} cee_batch_view;
+
+/* What the batch computes per instance: the JV screen of every active edge, and the HT c,d root
+ * screen of the first `targets` edges of SelectHtTargetEdgeIds(kWeightDescending)
+ * (src/cpu/ht_scan.cpp:316-345) with HtShallowOptions' neighbourhood / degree cap / mode
+ * (include/cuda_edge_elimination/hamilton_tutte.hpp:95-108; defaults 64, 25, 50, active-incompatible). */
+typedef struct {
+  int32_t targets;              /* 1..64 */
+  int32_t max_neighborhood;     /* 2..32 */
+  int32_t max_candidate_degree; /* 0 = no cap */
+  int32_t cd_mode;              /* cee_cd_mode */
+} cee_batch_options;
+
+/* Launch shape of the batch kernel (chosen by cee_batch_autotune; results never depend on it). */
+typedef struct {
+  int32_t jv_tile;         /* edges per JV work item */
+  int32_t blocks_per_sm;   /* resident 256-thread blocks per SM (<= occupancy) */
+  int32_t chunks;          /* instance chunks of the end-to-end call (copy/compute overlap) */
+} cee_batch_tuning;
+
+typedef struct {
+  int64_t nodes, edges, adjacency, targets;
+  int64_t pairs;            /* c,d pairs screened (sum over targets of s (s - 1) / 2) */
+  int64_t flag_words;       /* per target */
+  uint64_t resident_bytes;
+  int64_t h2d_bytes, d2h_bytes;
+  double h2d_ms, kernel_ms, d2h_ms, total_ms;
+} cee_batch_stats;
+
+/* Uploads the batch, plans the work items and captures the launch as a CUDA graph. */
+int cee_batch_prepare(cee_ctx* ctx, const cee_batch_view* batch, const cee_batch_options* options,
+                      cee_batch_stats* stats);
+/* One graph launch of the persistent kernel over the prepared batch (no synchronisation). */
+int cee_batch_launch(cee_ctx* ctx);
+/* The same work as one synchronous launch per instance (the unbatched comparison path). */
+int cee_batch_launch_plain(cee_ctx* ctx);
+/* Copies the results back: witness[m] (as cee_jv_screen), target_ids[I * T] (global edge ids,
+ * -1 padding) and target_count[I], nbhd[I * T * max_neighborhood] (global node ids, -1 padding;
+ * the c,d task list of a target is every pair i < j of its neighbourhood as (min, max), in the
+ * order of BuildCdScreenTasks, src/cpu/hamilton_tutte.cpp:204-214) and flags[I * T * flag_words]
+ * (bit p of the target's words = ScreenCdTasksCpu flag of task p). Any pointer may be NULL. */
+int cee_batch_fetch(cee_ctx* ctx, int32_t* witness, int32_t* target_ids, int32_t* target_count,
+                    int32_t* nbhd, uint32_t* flags);
+/* End to end from host buffers: uploads, screens and downloads chunk by chunk, overlapping the
+ * copies of one chunk with the screen of another (pinned buffers overlap; pageable ones too,
+ * at the driver's staging speed). Output pointers as in cee_batch_fetch. */
+int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* batch, const cee_batch_options* options,
+                     int32_t* witness, int32_t* target_ids, int32_t* target_count, int32_t* nbhd,
+                     uint32_t* flags, cee_batch_stats* stats);
+int cee_batch_set_tuning(cee_ctx* ctx, const cee_batch_tuning* tuning);
+int cee_batch_get_tuning(const cee_ctx* ctx, cee_batch_tuning* tuning);
+/* Times every candidate launch shape on the prepared batch (`reps` graph launches each, CUDA
+ * events) and keeps the fastest; writes it to *chosen. */
+int cee_batch_autotune(cee_ctx* ctx, int32_t reps, cee_batch_tuning* chosen);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,117 @@
+"""Batched screen (many instances, one persistent graph-captured launch) against the CPU oracle:
+per instance the JV witnesses, the HT targets (SelectHtTargetEdgeIds order), and per target the
+c,d task list (BuildCdScreenTasks) and its flags (ScreenCdTasksCpu) -- all exact. The
+one-launch-per-instance path and the chunked end-to-end call must give the same bytes."""
+import numpy as np
+import pytest
+
+from cudaedgeelimination_b200 import GraphSnapshot, synth
+from cudaedgeelimination_b200.api import BatchOptions
+
+pytestmark = pytest.mark.gpu
+
+
+class TinyBatch:
+    """A hand-built batch: instances of varied size including degenerate ones."""
+
+    def __init__(self, graphs):
+        nb = np.cumsum([0] + [g.n for g in graphs]).astype(np.int64)
+        eb = np.cumsum([0] + [g.m for g in graphs]).astype(np.int64)
+        self.node_begin, self.edge_begin, self.count = nb, eb, len(graphs)
+        self.graph = GraphSnapshot(int(nb[-1]), graphs[0].dist_type, np.concatenate([g.x for g in graphs]),
+                                   np.concatenate([g.y for g in graphs]),
+                                   np.concatenate([g.edge_u + nb[i] for i, g in enumerate(graphs)]),
+                                   np.concatenate([g.edge_v + nb[i] for i, g in enumerate(graphs)]),
+                                   np.concatenate([g.edge_w for g in graphs]), np.concatenate([g.active for g in graphs]))
+        self.graphs = graphs
+
+    def instance(self, i):
+        return self.graphs[i]
+
+
+def check_against_oracle(port, batch, res, opt, instances=None):
+    g = batch.graph
+    np.testing.assert_array_equal(res.witness, port.jv_screen(g))
+    T, NB = opt.targets, opt.max_neighborhood
+    for i in instances if instances is not None else range(batch.count):
+        inst = batch.instance(i)
+        n0, e0 = int(batch.node_begin[i]), int(batch.edge_begin[i])
+        expected = port.ht_targets(inst)[:T]
+        assert res.target_count[i] == expected.shape[0]
+        np.testing.assert_array_equal(res.target_ids[i, :expected.shape[0]], expected + e0)
+        assert (res.target_ids[i, expected.shape[0]:] == -1).all()
+        for t, local in enumerate(expected):
+            u, v = int(inst.edge_u[local]), int(inst.edge_v[local])
+            c, d, a = port.cd_tasks(inst, u, v, NB, opt.max_candidate_degree)
+            hood = res.nbhd[i, t]
+            size = int((hood >= 0).sum())
+            ii, jj = np.triu_indices(size, 1)
+            gc = np.minimum(hood[ii], hood[jj]) - n0
+            gd = np.maximum(hood[ii], hood[jj]) - n0
+            np.testing.assert_array_equal(gc, c)
+            np.testing.assert_array_equal(gd, d)
+            np.testing.assert_array_equal(res.pair_flags(i, t), port.cd_screen(inst, u, v, c, d, a, opt.cd_mode))
+        for t in range(expected.shape[0], T):
+            assert (res.nbhd[i, t] == -1).all() and (res.flags[i, t] == 0).all()
+
+
+@pytest.fixture(scope="module")
+def small_batch():
+    return synth.BatchUnion(48)
+
+
+@pytest.mark.parametrize("opt", [BatchOptions(), BatchOptions(10, 8, 0, 1), BatchOptions(40, 32, 50, 0)],
+                         ids=["defaults", "t10-nb8-nocap-missing", "t40-nb32"])
+def test_batch_graph_launch(ctx, port, small_batch, opt):
+    ctx.batch_prepare(small_batch, opt)
+    ctx.batch_launch()
+    res = ctx.batch_fetch()
+    check_against_oracle(port, small_batch, res, opt, instances=range(0, 48, 5))
+
+
+def test_plain_e2e_and_autotune_agree(ctx, small_batch):
+    opt = BatchOptions()
+    ctx.batch_prepare(small_batch, opt)
+    ctx.batch_launch()
+    graph_res = ctx.batch_fetch()
+    ctx.batch_launch_plain()
+    plain_res = ctx.batch_fetch()
+    for chunks in (1, 3, 8):
+        ctx.set_batch_tuning(64, 0, chunks)
+        e2e_res, stats = ctx.batch_screen(small_batch, opt)
+        assert stats.h2d_bytes > 0 and stats.d2h_bytes > 0
+        for a, b in ((graph_res, plain_res), (graph_res, e2e_res)):
+            for name in ("witness", "target_ids", "target_count", "nbhd", "flags"):
+                np.testing.assert_array_equal(getattr(a, name), getattr(b, name))
+    chosen = ctx.batch_autotune(reps=1)
+    assert chosen.jv_tile > 0
+    ctx.batch_launch()
+    tuned = ctx.batch_fetch()
+    np.testing.assert_array_equal(tuned.witness, graph_res.witness)
+    np.testing.assert_array_equal(tuned.flags, graph_res.flags)
+
+
+def test_degenerate_instances(ctx, port):
+    from helpers import complete_graph
+    graphs = [GraphSnapshot.from_edges([0, 5, 9, 20], [0, 3, 1, 4], [(0, 1), (1, 2), (2, 3)]),  # no eligible target
+              complete_graph([0, 10, 0, 10, 5], [0, 0, 10, 10, 5]),                             # 5 nodes < nb
+              synth.batch_instance(3), complete_graph(list(range(0, 90, 9)), [(7 * i) % 31 for i in range(10)])]
+    batch = TinyBatch(graphs)
+    for opt in (BatchOptions(), BatchOptions(64, 4, 0, 1)):
+        ctx.batch_prepare(batch, opt)
+        ctx.batch_launch()
+        check_against_oracle(port, batch, ctx.batch_fetch(), opt)
+        res, _ = ctx.batch_screen(batch, opt)
+        check_against_oracle(port, batch, res, opt)
+
+
+def test_unsorted_instance_rejected(ctx):
+    g = synth.batch_instance(0)
+    swapped = GraphSnapshot(g.n, 0, g.x, g.y, g.edge_u[::-1].copy(), g.edge_v[::-1].copy(), g.edge_w[::-1].copy(),
+                            g.active)
+    batch = TinyBatch([swapped])
+    from cudaedgeelimination_b200._native import NativeError
+    with pytest.raises(NativeError):
+        ctx.batch_prepare(batch, BatchOptions())
+    with pytest.raises(NativeError):
+        ctx.batch_screen(batch, BatchOptions())
