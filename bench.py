@@ -4,18 +4,23 @@
 
 Workload (default "batch"): the 4,096-instance batching mix (n log-uniform in [100, 5000],
 uniform / clustered 50/50, 10-NN, EUC_2D; seeded synthetic stand-ins for the reference's TSPLIB
-inputs), screened as one snapshot. A step is one JV screen of every active edge of the batch in
-one launch. metric = JV edges screened per second over the whole job.
+inputs). A step is the batched screen of every instance in one persistent, CUDA-graph-captured
+launch: the JV screen of every active edge plus the HT c,d root screen (neighbourhood 25,
+degree cap 50, active-incompatible) of the first 64 SelectHtTargetEdgeIds targets of every
+instance. metric = JV edges screened per second over the whole job (c,d tasks/s alongside).
 
-  value      resident inputs (uploaded once), K launches timed with CUDA events on the
+  value      resident inputs (uploaded once), K graph launches timed with CUDA events on the
              launching stream; inputs (~1.1 GB) exceed L2, so no flush is needed
-  e2e        the same step through the C ABI with pinned host buffers: cee_jv_screen per step
-             (static-key compare, H2D of active bits + CSR, launch, D2H of the witnesses)
-  roofline   jv_screen_kernel: algorithmic bytes per launch (12 n + 33 m) / launch time
+  plain      the same work as one synchronous launch per instance (cee_batch_launch_plain)
+  e2e        the same step through the C ABI from pinned host buffers: cee_batch_screen per
+             step (chunked H2D of the whole batch, screens, D2H of every result, overlapped)
+  roofline   batch_screen_kernel: compulsory bytes per launch (12 n + 33 m for the JV part plus
+             the c,d outputs) / launch time
   kopt       the 200,000-row k-opt leaf cost matrix (k = 3/4/5 in thirds, 15,000-node CEIL_2D
              instance): cells/s resident and end to end, with its own roofline
-  cpu_baseline  the reference's own CPU FindJvCandidatesCpu (oracle/_ref, compiled from the
-             reference sources) on a bounded sample of the same instances, threads over instances
+  cpu_baseline  the reference's own CPU code for the same step (oracle/_ref, compiled from the
+             reference sources): FindJvCandidatesCpu plus BuildCdScreenTasks + ScreenCdTasksCpu
+             for the same targets, on a bounded sample of the instances, threads over instances
 
 --impl reference times the reference's CPU implementation of the same step on the host cores.
 Multi-GPU: one process per GPU, independent replicas (the screen shards by instance with no
@@ -51,8 +56,8 @@ def parse():
     p.add_argument("--workload", default="batch", choices=["batch"])
     p.add_argument("--instances", type=int, default=4096)
     p.add_argument("--no-kopt", action="store_true")
-    p.add_argument("--part", default="all", choices=["all", "jv", "kopt"],
-                   help="profiling aid: run only the JV or only the k-opt part")
+    p.add_argument("--part", default="all", choices=["all", "batch", "kopt"],
+                   help="profiling aid: run only the batched screen or only the k-opt part")
     p.add_argument("--cpu-budget-s", type=float, default=12.0)
     return p.parse_args()
 
@@ -132,17 +137,32 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- CPU reference -----------
 
-def reference_jv_rate(batch, budget_s: float, threads: int):
-    """The reference's FindJvCandidatesCpu over instances in order until the time budget is
-    spent; instances run concurrently on `threads` host threads. Returns (edges/s, sample)."""
+def reference_step_rate(batch, budget_s: float, threads: int, targets: int = 64, nb: int = 25, max_deg: int = 50):
+    """The reference's CPU code for one instance of the step -- FindJvCandidatesCpu, then
+    SelectHtTargetEdgeIds and BuildCdScreenTasks + ScreenCdTasksCpu for the first `targets`
+    targets -- over instances in order until the budget is spent, `threads` instances at a time.
+    Returns (edges screened/s, kind, sample description)."""
     import oracle
     kind = "reference" if oracle.reference_available() else "port"
     if kind == "reference":
         ref = oracle.Reference()
-        screen = lambda g: ref.graph(g).jv_cpu()  # noqa: E731
+
+        def screen(g):
+            rg = ref.graph(g)
+            rg.jv_cpu()
+            for t in rg.ht_targets(1)[:targets]:
+                u, v = int(g.edge_u[t]), int(g.edge_v[t])
+                c, d, a = rg.cd_tasks(u, v, nb, max_deg)
+                rg.cd_screen(u, v, c, d, a, 0)
     else:
         port = oracle.Port()
-        screen = port.jv_screen
+
+        def screen(g):
+            port.jv_screen(g)
+            for t in port.ht_targets(g)[:targets]:
+                u, v = int(g.edge_u[t]), int(g.edge_v[t])
+                c, d, a = port.cd_tasks(g, u, v, nb, max_deg)
+                port.cd_screen(g, u, v, c, d, a, 0)
     edges = 0
     done = 0
     lock = threading.Lock()
@@ -162,11 +182,29 @@ def reference_jv_rate(batch, budget_s: float, threads: int):
     with concurrent.futures.ThreadPoolExecutor(max_workers=threads) as pool:
         list(pool.map(work, range(batch.count)))
     elapsed = time.perf_counter() - start
-    sample = f"{done} of {batch.count} instances ({edges} edges), {threads} threads, {elapsed:.1f} s"
+    sample = (f"{done} of {batch.count} instances ({edges} edges, JV screen + {targets} c,d root screens each), "
+              f"{threads} threads, {elapsed:.1f} s")
     return edges / elapsed, kind, sample
 
 
 # ---------------------------------------------------------------- our arm -----------------
+
+def spot_check(batch, res, opt):
+    """Cheap parity check of a few instances against the CPU oracle (the tests do the full one)."""
+    import oracle
+    port = oracle.Port()
+    for i in range(0, batch.count, max(1, batch.count // 6)):
+        inst = batch.instance(i)
+        e0, e1, n0 = int(batch.edge_begin[i]), int(batch.edge_begin[i + 1]), int(batch.node_begin[i])
+        w = port.jv_screen(inst)
+        assert (res.witness[e0:e1] == np.where(w >= 0, w + n0, -1)).all()
+        expected = port.ht_targets(inst)[:opt.targets]
+        assert (res.target_ids[i, :expected.shape[0]] == expected + e0).all()
+        local = int(expected[0])
+        u, v = int(inst.edge_u[local]), int(inst.edge_v[local])
+        c, d, a = port.cd_tasks(inst, u, v, opt.max_neighborhood, opt.max_candidate_degree)
+        assert (res.pair_flags(i, 0) == port.cd_screen(inst, u, v, c, d, a, opt.cd_mode)).all()
+
 
 def pinned_copy(arr: np.ndarray):
     """A page-locked copy of `arr` (any dtype) and a numpy view of it."""
@@ -186,26 +224,22 @@ def run_ours(args, rank: int, world: int, device: int):
         out = run_kopt(args, ctx, torch.cuda.ExternalStream(ctx.stream, device=device), device, world)
         ctx.close()
         return out
+    from cudaedgeelimination_b200.api import BatchOptions
     batch = synth.BatchUnion(args.instances)
     g = batch.graph
     ctx = Context(device)
     stream = torch.cuda.ExternalStream(ctx.stream, device=device)
-    n, m, adj = g.n, g.m, int(g.row_offsets[-1])
+    n, m = g.n, g.m
+    opt = BatchOptions()  # 64 targets, neighbourhood 25, degree cap 50, active-incompatible
 
-    # ---- resident timing of the screen kernel ----
-    ctx.jv_prepare(g)
+    # ---- resident timing of the batched launch ----
+    ctx.batch_prepare(batch, opt)
+    tuning = ctx.batch_autotune(reps=2)
     for _ in range(args.warmup):
-        ctx.jv_launch()
-    ctx.synchronize()
-    witness = ctx.jv_fetch(m)
+        ctx.batch_launch()
+    res = ctx.batch_fetch()
     if rank == 0:
-        import oracle
-        port = oracle.Port()
-        for i in range(0, batch.count, max(1, batch.count // 8)):  # spot parity check, cheap
-            e0, e1 = int(batch.edge_begin[i]), int(batch.edge_begin[i + 1])
-            inst = batch.instance(i)
-            assert (witness[e0:e1] == np.where(port.jv_screen(inst) >= 0,
-                                                port.jv_screen(inst) + int(batch.node_begin[i]), -1)).all()
+        spot_check(batch, res, opt)
     barrier(world)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -214,77 +248,92 @@ def run_ours(args, rank: int, world: int, device: int):
         barrier(world)
         ev0.record(stream)
         for _ in range(args.steps):
-            ctx.jv_launch()
+            ctx.batch_launch()
         ev1.record(stream)
         ev1.synchronize()
         torch.cuda.synchronize(device)
         barrier(world)
-    ms_total = ev0.elapsed_time(ev1)
-    ms_total = max_over_ranks(ms_total, world)
-    ms_step = ms_total / args.steps
+    ms_step = max_over_ranks(ev0.elapsed_time(ev1), world) / args.steps
     edges_step = int(g.active.sum())
+    targets = int(res.target_count.sum())
+    sizes = (res.nbhd >= 0).sum(axis=2)
+    pairs = int((sizes * (sizes - 1) // 2).sum())
     value = edges_step * world / (ms_step / 1e3)
 
-    # ---- end to end through the C ABI with pinned host buffers ----
+    # ---- the same work, one synchronous launch per instance ----
+    plain_steps = max(1, min(3, args.steps))
+    ctx.batch_launch_plain()
+    t0 = time.perf_counter()
+    for _ in range(plain_steps):
+        ctx.batch_launch_plain()
+    plain_ms = max_over_ranks((time.perf_counter() - t0) / plain_steps * 1e3, world)
+    plain = ctx.batch_fetch()
+    assert (plain.witness == res.witness).all() and (plain.flags == res.flags).all()
+
+    # ---- end to end through the C ABI from pinned host buffers ----
     keep = []
-    arrays = {}
+    host = GraphSnapshot.__new__(GraphSnapshot)
+    host.n, host.dist_type = g.n, g.dist_type
     for name in ("x", "y", "edge_u", "edge_v", "edge_w", "active", "row_offsets", "neighbors", "csr_edge_ids"):
         t, a = pinned_copy(getattr(g, name))
         keep.append(t)
-        arrays[name] = a
-    hg = GraphSnapshot.__new__(GraphSnapshot)
-    hg.n, hg.dist_type = g.n, g.dist_type
-    for name, a in arrays.items():
-        setattr(hg, name, a)
-    wt, wout = pinned_copy(np.empty(m, np.int32))
-    keep.append(wt)
-    import ctypes
-    from cudaedgeelimination_b200 import _native
-    view = hg.view()
-    stats = _native.JvStats()
-    L = _native.lib()
-
-    def e2e_step():
-        _native.check(ctx.handle, L.cee_jv_screen(ctx.handle, ctypes.byref(view),
-                                                   wout.ctypes.data_as(_native.c_i32p), ctypes.byref(stats)))
-
+        setattr(host, name, a)
+    hb = type("PinnedBatch", (), {})()
+    for name in ("node_begin", "edge_begin"):
+        t, a = pinned_copy(getattr(batch, name))
+        keep.append(t)
+        setattr(hb, name, a)
+    from cudaedgeelimination_b200.api import _batch_outputs
+    out = _batch_outputs(m, batch.count, opt)
+    for name in ("witness", "target_ids", "target_count", "nbhd", "flags"):
+        t, a = pinned_copy(getattr(out, name))
+        keep.append(t)
+        setattr(out, name, a)
     for _ in range(args.warmup):
-        e2e_step()
+        _, stats = ctx.batch_screen(hb, opt, graph=host, out=out)
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        e2e_step()
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
-    assert (wout == witness).all()
-    e2e_value = edges_step * world / (e2e_s / args.steps)
-    h2d_bytes = int(stats.h2d_bytes)
-    d2h_bytes = int(stats.d2h_bytes)
+        _, stats = ctx.batch_screen(hb, opt, graph=host, out=out)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world) / args.steps
+    assert (out.witness == res.witness).all() and (out.flags == res.flags).all()
+    e2e_value = edges_step * world / e2e_s
 
     # ---- roofline of the dominant kernel ----
     peak, peak_kind = load_peaks()
-    alg_bytes = 12 * n + 33 * m
+    out_bytes = 4 * m + targets * 4 + batch.count * 4 + res.nbhd.nbytes + res.flags.nbytes
+    alg_bytes = 12 * n + 33 * m + out_bytes - 4 * m  # the witness write is already in 33 m
     achieved = alg_bytes / (ms_step / 1e3) / 1e9
-    traffic = load_traffic().get("jv_screen_kernel")
 
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded; TSPLIB/ElimTSP inputs not shipped)",
-        "config": {"workload": f"batching mix: {batch.count} instances, n log-uniform [100,5000], "
-                               "uniform/clustered 50/50, 10-NN, EUC_2D; JV screen of every active edge "
-                               "in one launch", "instances": batch.count, "nodes": n, "edges": m,
+        "config": {"workload": f"batching mix: {batch.count} instances, n log-uniform [100,5000], uniform/clustered "
+                               "50/50, 10-NN, EUC_2D; per step the JV screen of every active edge plus the HT c,d "
+                               "root screen of 64 targets per instance (neighbourhood 25, degree cap 50), one "
+                               "persistent graph-captured launch",
+                   "instances": batch.count, "nodes": n, "edges": m, "targets": targets, "cd_tasks": pairs,
+                   "tuning": {"jv_tile": tuning.jv_tile, "blocks_per_sm": tuning.blocks_per_sm,
+                              "chunks": tuning.chunks},
                    "l2": "inputs (~1.1 GB) larger than L2, no flush", "parallelism": f"replicas x{world}"},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
-                "ms_per_step": e2e_s / args.steps * 1e3, "api": "cee_jv_screen (pinned host buffers)"},
-        "roofline": {"kernel": "jv_screen_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
+        "cd_tasks_per_s": pairs * world / (ms_step / 1e3),
+        "plain": {"ms_per_step": plain_ms, "value": edges_step * world / (plain_ms / 1e3), "unit": UNIT,
+                  "launches_per_step": batch.count, "batched_speedup": plain_ms / ms_step,
+                  "api": "cee_batch_launch_plain (one synchronous launch per instance)"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(stats.h2d_bytes),
+                "d2h_bytes_per_step": int(stats.d2h_bytes), "ms_per_step": e2e_s * 1e3,
+                "api": "cee_batch_screen (pinned host buffers, chunked copy/compute overlap)"},
+        "roofline": {"kernel": "batch_screen_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
-                     "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
-                     "note": "JV is ALU/latency bound; see distance_evals_per_s"},
+                     "traffic": load_traffic().get("batch_screen_kernel"), "algorithmic_bytes_per_launch": alg_bytes,
+                     "note": "the screen is ALU/latency bound (integer and FP64 exact-distance work); "
+                             "see distance_evals_per_s"},
         "clocks": clocks.summary(),
         "gpu_launches": args.steps,
     }
 
-    # algorithmic distance evaluations (sequential CPU count) on a sample, scaled per edge
+    # algorithmic exact-distance evaluations of the JV part (sequential CPU count) on a sample
     if rank == 0:
         import oracle
         port = oracle.Port()
@@ -295,14 +344,14 @@ def run_ours(args, rank: int, world: int, device: int):
             ev_total += int(ev.sum())
             ev_edges += inst.m
         per_edge = ev_total / max(1, ev_edges)
-        result["roofline"]["distance_evals_per_edge"] = per_edge
-        result["roofline"]["distance_evals_per_s"] = per_edge * edges_step / (ms_step / 1e3)
+        result["roofline"]["jv_distance_evals_per_edge"] = per_edge
+        result["roofline"]["distance_evals_per_s"] = (per_edge * edges_step + 351 * targets) / (ms_step / 1e3)
 
     if not args.no_kopt and args.part == "all":
         result["kopt"] = run_kopt(args, ctx, stream, device, world)
 
     if rank == 0:
-        rate, kind, sample = reference_jv_rate(batch, args.cpu_budget_s, os.cpu_count() or 1)
+        rate, kind, sample = reference_step_rate(batch, args.cpu_budget_s, os.cpu_count() or 1)
         result["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": kind,
                                   "sample": sample}
     ctx.close()
@@ -390,12 +439,12 @@ def run_reference(args, rank: int):
     # each step: the reference's CPU JV screen over a bounded sample of the batch
     budget = max(2.0, min(20.0, 120.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
-        reference_jv_rate(batch, budget / 4, threads)
+        reference_step_rate(batch, budget / 4, threads)
     rates = []
     sample = ""
     kind = "reference"
     for _ in range(args.steps):
-        rate, kind, sample = reference_jv_rate(batch, budget, threads)
+        rate, kind, sample = reference_step_rate(batch, budget, threads)
         rates.append(rate)
     value = float(np.median(rates))
     return {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
