@@ -56,8 +56,10 @@ def parse():
     p.add_argument("--workload", default="batch", choices=["batch"])
     p.add_argument("--instances", type=int, default=4096)
     p.add_argument("--no-kopt", action="store_true")
-    p.add_argument("--part", default="all", choices=["all", "batch", "kopt"],
-                   help="profiling aid: run only the batched screen or only the k-opt part")
+    p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--serve-jobs", type=int, default=10_000)
+    p.add_argument("--part", default="all", choices=["all", "batch", "kopt", "serve"],
+                   help="profiling aid: run only the batched screen, the k-opt part or the serving loop")
     p.add_argument("--cpu-budget-s", type=float, default=12.0)
     return p.parse_args()
 
@@ -224,6 +226,8 @@ def run_ours(args, rank: int, world: int, device: int):
         out = run_kopt(args, ctx, torch.cuda.ExternalStream(ctx.stream, device=device), device, world)
         ctx.close()
         return out
+    if args.part == "serve":
+        return run_serve(args, device, world)
     from cudaedgeelimination_b200.api import BatchOptions
     batch = synth.BatchUnion(args.instances)
     g = batch.graph
@@ -349,6 +353,8 @@ def run_ours(args, rank: int, world: int, device: int):
 
     if not args.no_kopt and args.part == "all":
         result["kopt"] = run_kopt(args, ctx, stream, device, world)
+    if not args.no_serve and args.part == "all":
+        result["serve"] = run_serve(args, device, world)
 
     if rank == 0:
         rate, kind, sample = reference_step_rate(batch, args.cpu_budget_s, os.cpu_count() or 1)
@@ -408,6 +414,153 @@ def run_kopt(args, ctx, stream, device, world):
             "roofline": {"kernel": "kopt_cost_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
                          "traffic": load_traffic().get("kopt_cost_kernel"), "algorithmic_bytes_per_launch": alg_bytes}}
+
+
+def _pinned_pool(count: int, nbytes: int):
+    """`count` page-locked host buffers of `nbytes` each (uint8 numpy views) and their owners."""
+    import torch
+    owners = [torch.empty(nbytes, dtype=torch.uint8).pin_memory() for _ in range(count)]
+    return owners, [t.numpy() for t in owners]
+
+
+def _job_outputs(wl, job, buf):
+    """Output arrays of `job` carved from one pinned buffer."""
+    if job[0] == "jv":
+        return buf[:4 * wl.jv[job[1]].m].view(np.int32)
+    outs, at = [], 0
+    for (c, _), t in zip(job[2], (4, 25, 208)):
+        outs.append(buf[at:at + 8 * c * t].view(np.int64).reshape(c, t))
+        at += 8 * c * t
+    return outs
+
+
+def _latency_summary(lat_s):
+    ms = np.asarray(lat_s) * 1e3
+    return {"p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
+            "mean_ms": float(ms.mean()), "max_ms": float(ms.max())}
+
+
+def serve_drive(ctx, wl, sids, ksids, arrivals, buffers, keep_every: int):
+    """Feeds the jobs into the serving loop at their arrival times (admitting while it accepts
+    them), polls completions, and returns (completion - arrival latencies, wall seconds, kept
+    sample outputs)."""
+    n = len(wl.jobs)
+    free = list(range(len(buffers)))
+    inflight = {}
+    latency = np.zeros(n)
+    kept = {}
+    task_cache = {}
+    nxt = done = 0
+    t0 = time.perf_counter()
+    while done < n:
+        now = time.perf_counter() - t0
+        while nxt < n and arrivals[nxt] <= now and free:
+            job = wl.jobs[nxt]
+            out = _job_outputs(wl, job, buffers[free[-1]])
+            if job[0] == "jv":
+                jid = ctx.serve_submit_jv(sids[job[1]], wl.jv[job[1]].m, nxt, out=out)
+            else:
+                tasks = task_cache.get(nxt) or wl.kopt_tasks(job)
+                jid = ctx.serve_submit_kopt(ksids[job[1]], [3, 4, 5], tasks, nxt, outs=out)
+            if jid is None:  # no slot or arena room: poll first
+                break
+            inflight[jid] = (nxt, free.pop())
+            nxt += 1
+        for jid, tag, res in ctx.serve_poll():
+            idx, b = inflight.pop(jid)
+            latency[idx] = time.perf_counter() - t0 - arrivals[idx]
+            if idx % keep_every == 0:
+                kept[idx] = np.array(res, copy=True) if not isinstance(res, list) else [r.copy() for r in res]
+            free.append(b)
+            done += 1
+    return latency, time.perf_counter() - t0, kept
+
+
+def plain_drive(ctx, wl, arrivals, buffer, keep_every: int):
+    """The same jobs one at a time through the regular entry points (cee_jv_screen,
+    cee_kopt_costs_multi), each started at max(arrival, previous completion)."""
+    n = len(wl.jobs)
+    latency = np.zeros(n)
+    service = np.zeros(n)
+    kept = {}
+    t0 = time.perf_counter()
+    for idx, job in enumerate(wl.jobs):
+        while time.perf_counter() - t0 < arrivals[idx]:
+            pass
+        s0 = time.perf_counter()
+        out = _job_outputs(wl, job, buffer)
+        if job[0] == "jv":
+            ctx.jv_screen(wl.jv[job[1]], out=out)
+        else:
+            ctx.kopt_costs_multi(wl.kopt[job[1]][0], [3, 4, 5], wl.kopt_tasks(job), outs=out)
+        end = time.perf_counter()
+        service[idx] = end - s0
+        latency[idx] = end - t0 - arrivals[idx]
+        if idx % keep_every == 0:
+            kept[idx] = np.array(out, copy=True) if not isinstance(out, list) else [r.copy() for r in out]
+    return latency, service, time.perf_counter() - t0, kept
+
+
+def run_serve(args, device, world):
+    """The serving stream (Poisson arrivals at 0.8 x the loop's measured capacity) through the
+    serving loop, and the same jobs run plain-sequentially through the regular entry points."""
+    from cudaedgeelimination_b200 import Context, synth
+    from cudaedgeelimination_b200.api import ServeConfig
+
+    wl = synth.ServeWorkload(jobs=args.serve_jobs)
+    slots = 32
+    max_bytes = max(wl.output_bytes(j) for j in wl.jobs)
+    owners, buffers = _pinned_pool(slots + 1, max_bytes)
+    ctx = Context(device)
+    ctx.serve_start(ServeConfig(hbm_budget_bytes=8 << 30, slots=slots, idle_ms=20))
+    sids = [ctx.serve_add_snapshot(g) for g in wl.jv]
+    ksids = [ctx.serve_add_snapshot(g) for g, _ in wl.kopt]
+    assert None not in sids and None not in ksids
+    keep_every = max(1, len(wl.jobs) // 100)
+    # warm-up on the first jobs, then capacity: every job queued at t = 0 (closed loop)
+    warm = synth.ServeWorkload.__new__(synth.ServeWorkload)
+    warm.__dict__.update(wl.__dict__)
+    warm.jobs = wl.jobs[:min(200, len(wl.jobs))]
+    serve_drive(ctx, warm, sids, ksids, np.zeros(len(warm.jobs)), buffers[:slots], keep_every)
+    _, cap_s, _ = serve_drive(ctx, wl, sids, ksids, np.zeros(len(wl.jobs)), buffers[:slots], keep_every)
+    capacity = len(wl.jobs) / cap_s
+    lam = 0.8 * capacity
+    arrivals = np.cumsum(wl.gaps) / lam
+    lat, wall, kept = serve_drive(ctx, wl, sids, ksids, arrivals, buffers[:slots], keep_every)
+    ctx.serve_stop()
+    ctx.close()
+
+    plain_ctx = Context(device)
+    _, service, plain_closed_s, _ = plain_drive(plain_ctx, warm, np.zeros(len(warm.jobs)), buffers[slots], keep_every)
+    _, service, plain_closed_s, _ = plain_drive(plain_ctx, wl, np.zeros(len(wl.jobs)), buffers[slots], keep_every)
+    plain_capacity = len(wl.jobs) / plain_closed_s
+    plain_lat, _, plain_wall, plain_kept = plain_drive(plain_ctx, wl, arrivals, buffers[slots], keep_every)
+    plain_ctx.close()
+    for idx, want in plain_kept.items():  # served results equal the regular entry points' results
+        got = kept[idx]
+        if isinstance(want, list):
+            assert all((a == b).all() for a, b in zip(got, want)), f"serve/plain mismatch on job {idx}"
+        else:
+            assert (got == want).all(), f"serve/plain mismatch on job {idx}"
+    del owners
+    jv_jobs = sum(1 for j in wl.jobs if j[0] == "jv")
+    return {
+        "metric": "served jobs/s and p50/p99 latency", "jobs": len(wl.jobs), "jv_jobs": jv_jobs,
+        "kopt_jobs": len(wl.jobs) - jv_jobs, "seed": wl.seed, "lambda_jobs_per_s": lam,
+        "capacity_jobs_per_s": capacity, "jobs_per_s": len(wl.jobs) / wall,
+        **_latency_summary(lat),
+        "plain": {"capacity_jobs_per_s": plain_capacity, "jobs_per_s": len(wl.jobs) / plain_wall,
+                  **_latency_summary(plain_lat), "service_p50_ms": float(np.percentile(service, 50) * 1e3),
+                  "service_p99_ms": float(np.percentile(service, 99) * 1e3),
+                  "api": "cee_jv_screen / cee_kopt_costs_multi, one job at a time"},
+        "capacity_speedup": capacity / plain_capacity,
+        "d2h_bytes": int(sum(wl.output_bytes(j) for j in wl.jobs)),
+        "config": f"{len(wl.jobs)} jobs, Poisson arrivals at 0.8 x measured serving capacity; 70% JV epochs on "
+                  f"{len(wl.jv)} resident instances of the batching mix (n log-uniform [200,20000]), 30% k-opt "
+                  f"batches of 1k-50k rows (k = 3/4/5 in thirds) on {len(wl.kopt)} resident CEIL_2D instances; "
+                  f"{slots} slots, results into pinned host buffers; latency = arrival to results on the host",
+        "checked_jobs": len(plain_kept),
+    }
 
 
 # ---------------------------------------------------------------- plumbing ----------------

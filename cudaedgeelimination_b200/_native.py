@@ -14,6 +14,7 @@ c_u8p = ctypes.POINTER(ctypes.c_uint8)
 c_u64p = ctypes.POINTER(ctypes.c_uint64)
 
 CEE_OK = 0
+CEE_BUSY = 1
 CEE_ERR_INVALID = -1
 CEE_ERR_RANGE = -2
 CEE_ERR_CUDA = -3
@@ -88,6 +89,15 @@ class BatchStats(ctypes.Structure):
                 ("total_ms", ctypes.c_double)]
 
 
+class ServeConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("slots", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
+                ("idle_ms", ctypes.c_int32)]
+
+
+class ServeEvent(ctypes.Structure):
+    _fields_ = [("job", ctypes.c_int32), ("status", ctypes.c_int32), ("tag", ctypes.c_uint64)]
+
+
 class NativeError(RuntimeError):
     """A non-zero status from libcee; `code` is the CEE_ERR_* value."""
 
@@ -149,6 +159,16 @@ def lib() -> ctypes.CDLL:
             "cee_batch_set_tuning": (ctypes.c_int, [vp, ctypes.POINTER(BatchTuning)]),
             "cee_batch_get_tuning": (ctypes.c_int, [vp, ctypes.POINTER(BatchTuning)]),
             "cee_batch_autotune": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.POINTER(BatchTuning)]),
+            "cee_serve_start": (ctypes.c_int, [vp, ctypes.POINTER(ServeConfig)]),
+            "cee_serve_add_snapshot": (ctypes.c_int, [vp, ctypes.POINTER(GraphView), c_i32p]),
+            "cee_serve_release_snapshot": (ctypes.c_int, [vp, ctypes.c_int32]),
+            "cee_serve_submit_jv": (ctypes.c_int, [vp, ctypes.c_int32, vp, ctypes.c_uint64, c_i32p]),
+            "cee_serve_submit_kopt": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint32),
+                                                     ctypes.POINTER(vp), c_i64p, ctypes.POINTER(vp), ctypes.c_uint64,
+                                                     c_i32p]),
+            "cee_serve_poll": (ctypes.c_int, [vp, ctypes.POINTER(ServeEvent), ctypes.c_int32, c_i32p]),
+            "cee_serve_pending": (ctypes.c_int, [vp, c_i32p, c_u64p]),
+            "cee_serve_stop": (ctypes.c_int, [vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

@@ -135,7 +135,101 @@ class BatchMixin:
 
 
 
-class Context(BatchMixin):
+# ---- serving loop ------------------------------------------------------------------------
+
+@dataclass
+class ServeConfig:
+    """cee_serve_config: the device arena (HBM budget), jobs in flight, kernel shape, idle exit."""
+    hbm_budget_bytes: int = 4 << 30
+    slots: int = 64
+    blocks_per_sm: int = 0
+    idle_ms: int = 20
+
+    def native(self) -> _native.ServeConfig:
+        return _native.ServeConfig(self.hbm_budget_bytes, self.slots, self.blocks_per_sm, self.idle_ms)
+
+
+class ServeMixin:
+    """Request loop: snapshots stay in device memory, jobs are admitted while an HBM budget and
+    a slot are free, one persistent kernel runs all admitted jobs item by item. Submission calls
+    return None when the loop is full (CEE_BUSY): poll, then retry."""
+
+    def serve_start(self, config: ServeConfig | None = None) -> None:
+        config = ServeConfig() if config is None else config
+        self._serve_jobs = {}
+        _native.check(self.handle, _native.lib().cee_serve_start(self.handle, ctypes.byref(config.native())))
+
+    def serve_add_snapshot(self, graph: GraphSnapshot) -> int | None:
+        sid = ctypes.c_int32(-1)
+        view = graph.view()
+        rc = _native.lib().cee_serve_add_snapshot(self.handle, ctypes.byref(view), ctypes.byref(sid))
+        if rc == _native.CEE_BUSY:
+            return None
+        _native.check(self.handle, rc)
+        return sid.value
+
+    def serve_release_snapshot(self, sid: int) -> None:
+        _native.check(self.handle, _native.lib().cee_serve_release_snapshot(self.handle, sid))
+
+    def serve_submit_jv(self, sid: int, m: int, tag: int = 0, out: np.ndarray | None = None) -> int | None:
+        """Screens every edge of snapshot `sid` (m edges); the witness array is returned by serve_poll."""
+        out = np.empty(m, np.int32) if out is None else out
+        assert out.dtype == np.int32 and out.flags.c_contiguous and out.shape[0] >= m
+        job = ctypes.c_int32(-1)
+        rc = _native.lib().cee_serve_submit_jv(self.handle, sid, ctypes.c_void_p(out.ctypes.data), tag,
+                                               ctypes.byref(job))
+        if rc == _native.CEE_BUSY:
+            return None
+        _native.check(self.handle, rc)
+        self._serve_jobs[job.value] = out
+        return job.value
+
+    def serve_submit_kopt(self, sid: int, ks, task_lists, tag: int = 0, outs=None) -> int | None:
+        """k-opt leaf costs of up to three segments on snapshot `sid`'s coordinates (the library's
+        proper templates); the list of cost matrices is returned by serve_poll."""
+        tasks = [np.ascontiguousarray(t, dtype=KOPT_TASK_DTYPE) for t in task_lists]
+        n = len(ks)
+        if outs is None:
+            outs = [np.empty((t.shape[0], KOPT_TEMPLATE_COUNTS.get(k, 0)), np.int64) for k, t in zip(ks, tasks)]
+        karr = (ctypes.c_uint32 * n)(*ks)
+        tptr = (ctypes.c_void_p * n)(*[t.ctypes.data for t in tasks])
+        rows = np.array([t.shape[0] for t in tasks], np.int64)
+        optr = (ctypes.c_void_p * n)(*[o.ctypes.data for o in outs])
+        job = ctypes.c_int32(-1)
+        rc = _native.lib().cee_serve_submit_kopt(self.handle, sid, n, karr, tptr, rows.ctypes.data_as(_native.c_i64p),
+                                                 optr, tag, ctypes.byref(job))
+        if rc == _native.CEE_BUSY:
+            return None
+        _native.check(self.handle, rc)
+        self._serve_jobs[job.value] = outs
+        return job.value
+
+    def serve_poll(self, capacity: int = 256):
+        """Completed jobs as (job, tag, outputs) tuples."""
+        events = getattr(self, "_serve_events", None)
+        if events is None or len(events) < capacity:
+            events = self._serve_events = (_native.ServeEvent * capacity)()
+        count = ctypes.c_int32(0)
+        _native.check(self.handle, _native.lib().cee_serve_poll(self.handle, events, capacity, ctypes.byref(count)))
+        done = []
+        for i in range(count.value):
+            ev = events[i]
+            _native.check(self.handle, ev.status)
+            done.append((ev.job, ev.tag, self._serve_jobs.pop(ev.job)))
+        return done
+
+    def serve_pending(self) -> tuple[int, int]:
+        jobs = ctypes.c_int32(0)
+        used = ctypes.c_uint64(0)
+        _native.check(self.handle, _native.lib().cee_serve_pending(self.handle, ctypes.byref(jobs), ctypes.byref(used)))
+        return jobs.value, used.value
+
+    def serve_stop(self) -> None:
+        self._serve_jobs = {}
+        _native.check(self.handle, _native.lib().cee_serve_stop(self.handle))
+
+
+class Context(BatchMixin, ServeMixin):
     """One cee_ctx: a device, a stream and the resident caches."""
 
     def __init__(self, device: int = -1):
@@ -174,8 +268,9 @@ class Context(BatchMixin):
         _native.check(self.handle, _native.lib().cee_ctx_clear(self.handle, what))
 
     # ---- JV -------------------------------------------------------------------------
-    def jv_screen(self, graph: GraphSnapshot) -> tuple[np.ndarray, _native.JvStats]:
-        witness = np.empty(graph.m, np.int32)
+    def jv_screen(self, graph: GraphSnapshot, out: np.ndarray | None = None) -> tuple[np.ndarray, _native.JvStats]:
+        witness = np.empty(graph.m, np.int32) if out is None else out
+        assert witness.dtype == np.int32 and witness.flags.c_contiguous and witness.shape[0] >= graph.m
         stats = _native.JvStats()
         view = graph.view()
         _native.check(self.handle, _native.lib().cee_jv_screen(
@@ -219,9 +314,10 @@ class Context(BatchMixin):
         rows = np.array([t.shape[0] for t in tasks], np.int64)
         return tasks, karr, tptr, rows
 
-    def kopt_costs_multi(self, graph: GraphSnapshot, ks, task_lists):
+    def kopt_costs_multi(self, graph: GraphSnapshot, ks, task_lists, outs=None):
         tasks, karr, tptr, rows = self._multi_args(ks, task_lists)
-        outs = [np.empty((int(r), KOPT_TEMPLATE_COUNTS[k]), np.int64) for k, r in zip(ks, rows)]
+        if outs is None:
+            outs = [np.empty((int(r), KOPT_TEMPLATE_COUNTS[k]), np.int64) for k, r in zip(ks, rows)]
         optr = (ctypes.c_void_p * len(ks))(*[o.ctypes.data for o in outs])
         stats = _native.KoptStats()
         _native.check(self.handle, _native.lib().cee_kopt_costs_multi(

@@ -267,7 +267,7 @@ __device__ void batch_cd_target(const BatchArgs& A, int32_t inst, int32_t t, con
 }
 
 template <bool kWide>
-static __global__ void __launch_bounds__(kBatchWarps * 32) batch_screen_kernel(BatchArgs A) {
+static __global__ void __launch_bounds__(kBatchWarps * 32, 5) batch_screen_kernel(BatchArgs A) {
   __shared__ BatchWarpScratch scratch[kBatchWarps];
   __shared__ uint8_t pair_i[kBatchMaxPairs], pair_j[kBatchMaxPairs];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

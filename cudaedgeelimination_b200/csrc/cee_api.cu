@@ -488,7 +488,7 @@ int KoptCoords(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x, con
 
 int KoptTemplatesFor(int k) { return k == 3 ? 4 : (k == 4 ? 25 : 208); }
 
-int DefaultRowsPerTile(uint32_t k) { return k == 3 ? 128 : (k == 4 ? 128 : 32); }
+int DefaultRowsPerTile(uint32_t k) { return k == 3 ? 208 : (k == 4 ? 128 : 32); }
 
 // Uploads the rows of every segment and records the launch description.
 int KoptPrepareSegments(cee_ctx* ctx, int32_t segments, const uint32_t* ks, const KoptTable* const* tables,
@@ -564,12 +564,15 @@ int KoptLaunchPrepared(cee_ctx* ctx) {
     smem = std::max(smem, kopt_tile_smem(s.launch.seg[i].k, s.launch.seg[i].rows_per_tile));
   }
   if (smem > kKoptSmemBytes) return Fail(ctx, CEE_ERR_INVALID, "k-opt tile exceeds shared memory");
+  cudaError_t status = cudaSuccess;
   if (s.narrow) {
-    kopt_cost_kernel<false><<<s.tiles, kKoptThreads, smem, ctx->stream>>>(s.launch, ctx->d_error);
+    if (smem > 48 * 1024) status = cudaFuncSetAttribute(kopt_cost_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (status == cudaSuccess) kopt_cost_kernel<false><<<s.tiles, kKoptThreads, smem, ctx->stream>>>(s.launch, ctx->d_error);
   } else {
-    kopt_cost_kernel<true><<<s.tiles, kKoptThreads, smem, ctx->stream>>>(s.launch, ctx->d_error);
+    if (smem > 48 * 1024) status = cudaFuncSetAttribute(kopt_cost_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (status == cudaSuccess) kopt_cost_kernel<true><<<s.tiles, kKoptThreads, smem, ctx->stream>>>(s.launch, ctx->d_error);
   }
-  const cudaError_t status = cudaGetLastError();
+  if (status == cudaSuccess) status = cudaGetLastError();
   if (status != cudaSuccess) return CudaFail(ctx, status, "kopt_cost_kernel launch");
   return CEE_OK;
 }
@@ -697,6 +700,7 @@ void cee_destroy(cee_ctx* ctx) {
   if (ctx == nullptr) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream != nullptr) cudaStreamSynchronize(ctx->stream);
+  ReleaseServe(ctx);
   ReleaseBatch(ctx);
   ctx->jv.Release();
   ctx->kopt.Release();
@@ -730,7 +734,7 @@ int cee_ctx_synchronize(cee_ctx* ctx) {
 uint64_t cee_ctx_resident_bytes(const cee_ctx* ctx) {
   if (ctx == nullptr) return 0;
   return JvResident(ctx->jv) + KoptResident(ctx->kopt) + ctx->cd.xy.capacity + ctx->cd.tasks.capacity +
-         ctx->cd.flags.capacity + BatchResident(ctx);
+         ctx->cd.flags.capacity + BatchResident(ctx) + ServeResident(ctx);
 }
 
 int cee_ctx_clear(cee_ctx* ctx, unsigned what) {
@@ -741,6 +745,7 @@ int cee_ctx_clear(cee_ctx* ctx, unsigned what) {
   if (what & 2u) ctx->kopt.Release();
   if (what & 4u) ctx->cd.Release();
   if (what & 8u) ReleaseBatch(ctx);
+  if (what & 16u) ReleaseServe(ctx);
   return CEE_OK;
 }
 

@@ -106,6 +106,7 @@ struct CdState {
 };
 
 struct BatchState;
+struct ServeState;
 
 }  // namespace cee
 
@@ -126,6 +127,7 @@ struct cee_ctx {
   cee::KoptState kopt;
   cee::CdState cd;
   cee::BatchState* batch = nullptr;
+  cee::ServeState* serve = nullptr;
 };
 
 namespace cee {
@@ -140,5 +142,7 @@ float EventMs(cudaEvent_t a, cudaEvent_t b);
 int CheckDeviceError(cee_ctx* ctx, const char* what);
 void ReleaseBatch(cee_ctx* ctx);
 uint64_t BatchResident(const cee_ctx* ctx);
+void ReleaseServe(cee_ctx* ctx, int32_t* error_word = nullptr);
+uint64_t ServeResident(const cee_ctx* ctx);
 
 }  // namespace cee

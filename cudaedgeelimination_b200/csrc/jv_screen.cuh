@@ -159,8 +159,8 @@ struct JvWarpScratch {
 template <bool kWide>
 __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t e, JvWarpScratch& s,
                                                        int lane, int32_t* __restrict__ error) {
-  if (g.active[e] == 0) return -1;
-  const int2 uv = g.edge_uv[e];
+  if (__ldg(g.active + e) == 0) return -1;
+  const int2 uv = __ldg(g.edge_uv + e);
   const int32_t a = uv.x, b = uv.y;
   const int32_t ra0 = __ldg(g.row_offsets + a), ra1 = __ldg(g.row_offsets + a + 1);
   const int32_t rb0 = __ldg(g.row_offsets + b), rb1 = __ldg(g.row_offsets + b + 1);
@@ -174,21 +174,30 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
   for (int base = 0; base < total; base += 32) {
     const int i = base + lane;
     uint64_t key = kEmptyKey;
+    const bool second = i >= da;
+    const int32_t slot = second ? rb0 + (i - da) : ra0 + i;
+    int32_t c = -1;
+    bool ok = false;
     if (i < total) {
-      const bool second = i >= da;
-      const int32_t slot = second ? rb0 + (i - da) : ra0 + i;
-      const int32_t c = __ldg(g.nbr + slot);
-      bool ok = c != a && c != b;
+      c = __ldg(g.nbr + slot);
+      ok = c != a && c != b;
       if (ok && static_cast<uint32_t>(c) >= static_cast<uint32_t>(g.n)) {
         atomicOr(error, 1);
         ok = false;
       }
-      if (ok && second) ok = !row_contains(g.nbr, ra0, ra1, c);
-      if (ok) {
-        const uint64_t score = static_cast<uint64_t>(static_cast<uint32_t>(__ldg(g.slot_w + slot))) +
-                               exact_distance<kWide>(__ldg(g.xy + c), second ? pa : pb, g.dist_type);
-        key = (score << 32) | static_cast<uint32_t>(c);
-      }
+    }
+    if (total <= 32) {
+      // one round: N(a) sits on lanes [0, da), so a node of N(b) already scored through N(a)
+      // is found by matching lane values (other lanes hold distinct negative placeholders)
+      const unsigned same = __match_any_sync(kFullMask, ok ? c : -1 - lane);
+      if (ok && second) ok = (same & ((1u << da) - 1u)) == 0;
+    } else if (ok && second) {
+      ok = !row_contains(g.nbr, ra0, ra1, c);
+    }
+    if (ok) {
+      const uint64_t score = static_cast<uint64_t>(static_cast<uint32_t>(__ldg(g.slot_w + slot))) +
+                             exact_distance<kWide>(__ldg(g.xy + c), second ? pa : pb, g.dist_type);
+      key = (score << 32) | static_cast<uint32_t>(c);
     }
     key = warp_sort_asc(key, lane);
     top = base == 0 ? key : warp_merge_smallest(top, key, lane);

@@ -6,28 +6,39 @@
 // deleted edges canon(port 2e, port 2e+1), repeats an earlier added edge, or the sum overflows
 // (impossible here: k <= 5 int32 distances). Otherwise it is the int64 sum.
 //
-// B200 mapping: a block owns a tile of consecutive rows of one segment (one k).
-//   1. the tile's ports are staged in shared memory;
-//   2. every port is mapped to the first port of the row holding the same node (its class);
-//      every port pair p < q gets its exact distance once (k(2k-1) pairs, at most 45, instead
-//      of k distances per cell); rows that repeat a node get a validity summary (KoptRowInfo);
-//   3. thread j owns template t = j mod T, keeps its k pair indices and its 64-bit pair mask in
-//      registers and walks rows j / T, j / T + 256 / T, ...; the threads of one step write
-//      256/T consecutive rows, i.e. one contiguous run of row-major cells, with streaming stores.
-// Rows with pairwise-distinct ports cannot produce an invalid cell (a template never pairs 2e
-// with 2e+1), so their cells are plain sums.
+// Validity in port-class space: every port is mapped to its class, the first port of the row
+// holding the same node, and every port pair p < q to the pair index of its class pair
+// (min, max), its code. Two added edges are the same node pair iff their codes are equal; an
+// added edge is a self loop iff its two classes are equal and re-adds a deleted edge iff its
+// code is a deleted edge's code. So each port pair gets a one-hot 64-bit mask (bit = code, or
+// bit 63 when the pair is a self loop or a deleted edge), and a template is valid iff the OR of
+// its k masks has bit 63 clear and exactly k bits set. Rows whose 2k ports are distinct nodes
+// need no masks: a proper template never pairs 2e with 2e+1, so all their cells are plain sums.
+//
+// B200 mapping: a block owns a tile of consecutive rows of one segment (one k; the tile
+// routine is compiled per k so the per-row work is fully unrolled).
+//   A. the tile's ports are staged in shared memory (one thread per port);
+//   B. one thread per row finds the port classes, whether the row repeats a node and the
+//      row's deleted-code set;
+//   C. one thread per (row, port pair) computes the pair's exact distance (k(2k-1) pairs, at
+//      most 45, instead of k distances per cell) and, for rows that repeat a node, its mask;
+//   D. thread j owns template t = j mod T with its k pair indices in registers and walks rows
+//      j / T, j / T + B / T, ... (B = 416 threads: 104 rows of k = 3, 16 rows of k = 4, two
+//      rows of k = 5 per step); the threads of a step write one contiguous run of row-major
+//      cells with streaming stores.
 #pragma once
 
 #include "device_common.cuh"
 
 namespace cee {
 
-constexpr int kKoptThreads = 256;
+constexpr int kKoptThreads = 416;          // 13 warps: 104 x 4 = 2 x 208 cells per step, 16 x 25 + 16
 constexpr int kKoptMaxPorts = 10;
 constexpr int kKoptMaxPairs = 45;          // k(2k-1) for k = 5
 constexpr int kKoptMaxTemplates = 208;     // proper 5-opt templates
-constexpr int kKoptSmemBytes = 48 * 1024;  // dynamic shared memory per block
+constexpr int kKoptSmemBytes = 96 * 1024;  // dynamic shared memory cap per block (opted in above 48 KB)
 constexpr int kKoptMaxSegments = 8;
+constexpr uint64_t kKoptBadPair = uint64_t{1} << 63;
 
 // pair index of ports p < q among 2k ports (row-major upper triangle)
 __host__ __device__ __forceinline__ int kopt_pair_index(int p, int q, int ports) {
@@ -53,54 +64,172 @@ struct KoptLaunch {
   const int2* __restrict__ xy;
 };
 
-// Per-row validity summary. A cell is invalid iff its template uses a pair marked in `bad`
-// (self loop or a re-added deleted edge) or uses two pairs adding the same node pair. Each
-// pair's code is the pair index of its node pair in port-class space; the port pairs sharing a
-// code form a duplicate set, and a template contains two of them iff the popcount of its pair
-// mask restricted to the set is >= 2. Only codes whose two classes both hold two or more ports
-// need a set (otherwise all members share the single port and no matching holds two), so a row
-// of 10 ports has at most C(5,2) = 10 sets.
-constexpr int kKoptMaxDupSets = 10;
-
-struct KoptRowInfo {
-  uint32_t bad_lo, bad_hi;  // 64-bit mask over pair indices
-  uint32_t dup_count;
-  uint32_t repeats;          // number of repeated nodes (0 = all ports distinct)
-  uint64_t dup[kKoptMaxDupSets];
-};
-
+// Shared-memory tile: 8-byte arrays first, then 4-byte, then bytes.
 struct KoptSmem {
+  uint64_t* mask;     // rows * npairs (rows that repeat a node)
+  uint64_t* delmask;  // rows: one-hot codes of the deleted edges
   int32_t* ports;     // rows * ports: node ids
   int32_t* dist;      // rows * npairs
-  uint8_t* cls;       // rows * ports: first port holding the same node
-  uint8_t* code;      // rows * npairs: class-pair index, 0xff when bad (rows with repeats only)
-  KoptRowInfo* info;  // rows
-  uint8_t* pp;        // npairs: first port of pair
-  uint8_t* pq;        // npairs: second port of pair
+  uint8_t* cls;       // rows * ports
+  uint8_t* repeats;   // rows: 1 when the row repeats a node
+  uint8_t* pp;        // npairs: first port of each pair
+  uint8_t* pq;        // npairs: second port
+  uint8_t* ctab;      // ports * ports: code of a class pair, 0xff on the diagonal
 };
 
-__host__ __device__ __forceinline__ int kopt_tile_smem(int k, int rows) {
+__host__ __device__ constexpr int kopt_tile_smem(int k, int rows) {
   const int ports = 2 * k, npairs = k * (ports - 1);
-  return rows * ports * 4 + rows * npairs * 4 + ((rows * ports + 15) & ~15) + ((rows * npairs + 15) & ~15) +
-         rows * static_cast<int>(sizeof(KoptRowInfo)) + 96;
+  const int bytes = rows * ports + rows + 2 * npairs + ports * ports;
+  return rows * npairs * 8 + rows * 8 + rows * ports * 4 + rows * npairs * 4 + ((bytes + 15) & ~15);
 }
 
 __device__ __forceinline__ KoptSmem kopt_carve(unsigned char* base, int k, int rows) {
   const int ports = 2 * k, npairs = k * (ports - 1);
   KoptSmem s;
-  s.ports = reinterpret_cast<int32_t*>(base);
+  s.mask = reinterpret_cast<uint64_t*>(base);
+  s.delmask = s.mask + rows * npairs;
+  s.ports = reinterpret_cast<int32_t*>(s.delmask + rows);
   s.dist = s.ports + rows * ports;
   s.cls = reinterpret_cast<uint8_t*>(s.dist + rows * npairs);
-  s.code = s.cls + ((rows * ports + 15) & ~15);
-  s.info = reinterpret_cast<KoptRowInfo*>(s.code + ((rows * npairs + 15) & ~15));
-  s.pp = reinterpret_cast<uint8_t*>(s.info + rows);
-  s.pq = s.pp + 48;
+  s.repeats = s.cls + rows * ports;
+  s.pp = s.repeats + rows;
+  s.pq = s.pp + npairs;
+  s.ctab = s.pq + npairs;
   return s;
 }
 
-// q = i / d for i * d < 2^32, with magic = ceil(2^32 / d).
-__device__ __forceinline__ int kopt_div(int i, uint32_t magic) {
-  return static_cast<int>(__umulhi(static_cast<uint32_t>(i), magic));
+// Pair decode and class-pair code tables for k (any group of threads; callers synchronise).
+template <int K>
+__device__ __forceinline__ void kopt_tables(uint8_t* pp, uint8_t* pq, uint8_t* ctab, int tid, int threads) {
+  constexpr int P = 2 * K, NP = K * (P - 1);
+  for (int i = tid; i < NP; i += threads) {
+    int p = 0, rest = i;
+    while (rest >= P - 1 - p) {
+      rest -= P - 1 - p;
+      ++p;
+    }
+    pp[i] = static_cast<uint8_t>(p);
+    pq[i] = static_cast<uint8_t>(p + 1 + rest);
+  }
+  for (int i = tid; i < P * P; i += threads) {
+    const int a = i / P, b = i - (i / P) * P;
+    ctab[i] = a == b ? 0xff : static_cast<uint8_t>(kopt_pair_index(min(a, b), max(a, b), P));
+  }
+}
+
+// Stage B for one row: port classes (first port with the same node), the repeat flag and the
+// one-hot codes of the deleted edges.
+template <int K>
+__device__ __forceinline__ void kopt_row_classes(const int32_t* nodes, const uint8_t* ctab, uint8_t* cls,
+                                                 uint8_t* repeats, uint64_t* delmask) {
+  constexpr int P = 2 * K;
+  int32_t nd[P];
+#pragma unroll
+  for (int p = 0; p < P; ++p) nd[p] = nodes[p];
+  int c[P];
+  bool rep = false;
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    int cp = p;
+#pragma unroll
+    for (int q = p - 1; q >= 0; --q) cp = nd[q] == nd[p] ? q : cp;
+    c[p] = cp;
+    rep = rep || cp != p;
+    cls[p] = static_cast<uint8_t>(cp);
+  }
+  uint64_t dm = 0;
+  if (rep) {
+#pragma unroll
+    for (int e = 0; e < K; ++e) {
+      const int code = ctab[c[2 * e] * P + c[2 * e + 1]];
+      if (code != 0xff) dm |= uint64_t{1} << code;
+    }
+  }
+  *repeats = rep ? 1 : 0;
+  *delmask = dm;
+}
+
+// Stage C for one (row, pair): the exact distance and, when the row repeats a node, the mask.
+template <int K, bool kWide>
+__device__ __forceinline__ void kopt_pair_entry(const KoptSmem& sm, int r, int pid, const int2* xy, int32_t dist_type) {
+  constexpr int P = 2 * K, NP = K * (P - 1);
+  const int p = sm.pp[pid], q = sm.pq[pid];
+  const int32_t* pr = sm.ports + r * P;
+  const int2 a = __ldg(xy + pr[p]);
+  const int2 b = __ldg(xy + pr[q]);
+  sm.dist[r * NP + pid] = static_cast<int32_t>(exact_distance<kWide>(a, b, dist_type));
+  if (sm.repeats[r] != 0) {
+    const uint8_t* cr = sm.cls + r * P;
+    const int code = sm.ctab[cr[p] * P + cr[q]];
+    const bool bad = code == 0xff || ((sm.delmask[r] >> code) & 1u) != 0;
+    sm.mask[r * NP + pid] = bad ? kKoptBadPair : uint64_t{1} << code;
+  }
+}
+
+// Stage D for one cell.
+template <int K, bool kWide>
+__device__ __forceinline__ int64_t kopt_cell(const KoptSmem& sm, int r, const int (&pid)[K]) {
+  constexpr int NP = K * (2 * K - 1);
+  const int32_t* dr = sm.dist + r * NP;
+  int64_t v;
+  if constexpr (kWide) {
+    v = 0;
+#pragma unroll
+    for (int i = 0; i < K; ++i) v += dr[pid[i]];
+  } else {  // coordinate span < 2^26: each distance < 2^26.5, so k <= 5 of them sum below 2^31
+    int32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < K; ++i) s += dr[pid[i]];
+    v = s;
+  }
+  if (sm.repeats[r] != 0) {
+    const uint64_t* mr = sm.mask + r * NP;
+    uint64_t m = 0;
+#pragma unroll
+    for (int i = 0; i < K; ++i) m |= mr[pid[i]];
+    if ((m & kKoptBadPair) != 0 || __popcll(m) != K) v = INT64_MAX;
+  }
+  return v;
+}
+
+template <int K, bool kWide>
+__device__ __forceinline__ void kopt_tile(const KoptLaunch& L, const KoptSegment& S, int64_t row0, int rows,
+                                          unsigned char* smem, int32_t* error) {
+  constexpr int P = 2 * K, NP = K * (P - 1);
+  const KoptSmem sm = kopt_carve(smem, K, S.rows_per_tile);
+  const int tid = threadIdx.x;
+  kopt_tables<K>(sm.pp, sm.pq, sm.ctab, tid, kKoptThreads);
+  for (int i = tid; i < rows * P; i += kKoptThreads) {
+    const int r = i / P, p = i - (i / P) * P;
+    int32_t node = __ldg(S.tasks + (row0 + r) * 12 + p);
+    if (static_cast<uint32_t>(node) >= static_cast<uint32_t>(L.n)) {
+      atomicOr(error, 1);
+      node = 0;
+    }
+    sm.ports[i] = node;
+  }
+  __syncthreads();
+  for (int r = tid; r < rows; r += kKoptThreads) {
+    kopt_row_classes<K>(sm.ports + r * P, sm.ctab, sm.cls + r * P, sm.repeats + r, sm.delmask + r);
+  }
+  __syncthreads();
+  for (int i = tid; i < rows * NP; i += kKoptThreads) {
+    const int r = i / NP;
+    kopt_pair_entry<K, kWide>(sm, r, i - r * NP, L.xy, L.dist_type);
+  }
+  __syncthreads();
+  const int T = S.templates;
+  const int per_step = kKoptThreads / T;
+  const int rr = tid / T, t = tid - rr * T;
+  if (rr >= per_step) return;
+  int pid[K];
+#pragma unroll
+  for (int i = 0; i < K; ++i) pid[i] = __ldg(S.pairs + t * K + i);
+  long long* out = reinterpret_cast<long long*>(S.costs + row0 * T) + static_cast<int64_t>(rr) * T + t;
+  const int64_t out_step = static_cast<int64_t>(per_step) * T;
+  for (int r = rr; r < rows; r += per_step, out += out_step) {
+    __stcs(out, static_cast<long long>(kopt_cell<K, kWide>(sm, r, pid)));
+  }
 }
 
 template <bool kWide>
@@ -110,130 +239,19 @@ static __global__ void __launch_bounds__(kKoptThreads) kopt_cost_kernel(KoptLaun
   int si = 0;
   while (si + 1 < L.segments && static_cast<int32_t>(blockIdx.x) >= L.seg[si + 1].tile_begin) ++si;
   const KoptSegment& S = L.seg[si];
-  const int k = S.k, ports = 2 * k, T = S.templates;
-  const int npairs = k * (ports - 1);
   const int64_t row0 = static_cast<int64_t>(blockIdx.x - S.tile_begin) * S.rows_per_tile;
   if (row0 >= S.rows) return;
   const int rows = static_cast<int>(min(static_cast<int64_t>(S.rows_per_tile), S.rows - row0));
-  const KoptSmem sm = kopt_carve(smem, k, S.rows_per_tile);
-  const int tid = threadIdx.x;
-  const uint32_t magic_ports = static_cast<uint32_t>((0x100000000ull + ports - 1) / ports);
-  const uint32_t magic_pairs = static_cast<uint32_t>((0x100000000ull + npairs - 1) / npairs);
-
-  if (tid < npairs) {  // invert the pair numbering p < q
-    int p = 0, idx = tid;
-    while (idx >= ports - 1 - p) {
-      idx -= ports - 1 - p;
-      ++p;
-    }
-    sm.pp[tid] = static_cast<uint8_t>(p);
-    sm.pq[tid] = static_cast<uint8_t>(p + 1 + idx);
-  }
-  for (int r = tid; r < rows; r += kKoptThreads) {
-    sm.info[r].bad_lo = sm.info[r].bad_hi = 0;
-    sm.info[r].dup_count = sm.info[r].repeats = 0;
-  }
-  for (int i = tid; i < rows * ports; i += kKoptThreads) {
-    const int r = kopt_div(i, magic_ports), p = i - r * ports;
-    int32_t node = __ldg(S.tasks + (row0 + r) * 12 + p);
-    if (static_cast<uint32_t>(node) >= static_cast<uint32_t>(L.n)) {
-      atomicOr(error, 1);
-      node = 0;
-    }
-    sm.ports[i] = node;
-  }
-  __syncthreads();
-  // port classes: the first port of the row holding the same node
-  for (int i = tid; i < rows * ports; i += kKoptThreads) {
-    const int r = kopt_div(i, magic_ports), p = i - r * ports;
-    const int32_t* pr = sm.ports + r * ports;
-    int c = p;
-    for (int q = p - 1; q >= 0; --q) c = pr[q] == pr[p] ? q : c;
-    sm.cls[i] = static_cast<uint8_t>(c);
-    if (c != p) atomicAdd(&sm.info[r].repeats, 1u);
-  }
-  __syncthreads();
-  // exact distance of every port pair; pairs that are self loops or re-add a deleted edge
-  // (compared in port-class space) are marked in the row's bad mask
-  for (int i = tid; i < rows * npairs; i += kKoptThreads) {
-    const int r = kopt_div(i, magic_pairs), pid = i - r * npairs;
-    const int p = sm.pp[pid], q = sm.pq[pid];
-    const int32_t* pr = sm.ports + r * ports;
-    sm.dist[i] = static_cast<int32_t>(exact_distance<kWide>(__ldg(L.xy + pr[p]), __ldg(L.xy + pr[q]), L.dist_type));
-    if (sm.info[r].repeats != 0) {
-      const uint8_t* cr = sm.cls + r * ports;
-      const int cp = cr[p], cq = cr[q];
-      bool bad = cp == cq;
-      const int code = kopt_pair_index(min(cp, cq), max(cp, cq), ports);
-      for (int e = 0; e < k && !bad; ++e) {
-        const int d0 = cr[2 * e], d1 = cr[2 * e + 1];
-        bad = d0 != d1 && code == kopt_pair_index(min(d0, d1), max(d0, d1), ports);
-      }
-      if (bad) atomicOr(pid < 32 ? &sm.info[r].bad_lo : &sm.info[r].bad_hi, 1u << (pid & 31));
-      sm.code[i] = bad ? 0xff : static_cast<uint8_t>(code);
-    }
-  }
-  __syncthreads();
-  // duplicate sets: the pairs sharing a class-pair code (the representative pair, whose code
-  // is its own index, plus every pair mapped onto it)
-  for (int r = tid; r < rows; r += kKoptThreads) {
-    if (sm.info[r].repeats == 0) continue;
-    const uint8_t* cr = sm.code + r * npairs;
-    const uint8_t* cl = sm.cls + r * ports;
-    uint32_t multi = 0;  // classes holding two or more ports
-    for (int p = 0; p < ports; ++p) {
-      if (cl[p] != p) multi |= 1u << cl[p];
-    }
-    uint32_t sets = 0;
-    for (int a = 0; a < npairs; ++a) {
-      const int c = cr[a];
-      if (c == 0xff || c == a) continue;
-      // pairs through a single-port class all share that port: never two in one template
-      if (((multi >> cl[sm.pp[a]]) & (multi >> cl[sm.pq[a]]) & 1u) == 0) continue;
-      const uint64_t rep = uint64_t{1} << c;
-      uint32_t j = 0;
-      while (j < sets && (sm.info[r].dup[j] & rep) == 0) ++j;
-      if (j == sets) {
-        if (sets == kKoptMaxDupSets) {  // cannot happen (see kKoptMaxDupSets); fail loudly
-          atomicOr(error, 4);
-          break;
-        }
-        sm.info[r].dup[sets++] = rep;
-      }
-      sm.info[r].dup[j] |= uint64_t{1} << a;
-    }
-    sm.info[r].dup_count = sets;
-  }
-  __syncthreads();
-
-  // cells: thread owns template t for rows rr, rr + per_step, ...
-  const int per_step = kKoptThreads / T;
-  const int rr = tid / T, t = tid - rr * T;
-  if (rr >= per_step) return;
-  int pid[5];
-  uint64_t tmask = 0;
-#pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    pid[i] = i < k ? __ldg(S.pairs + t * k + i) : 0;
-    if (i < k) tmask |= uint64_t{1} << pid[i];
-  }
-  long long* out = reinterpret_cast<long long*>(S.costs + row0 * T) + static_cast<int64_t>(rr) * T + t;
-  const int64_t out_step = static_cast<int64_t>(per_step) * T;
-  for (int r = rr; r < rows; r += per_step, out += out_step) {
-    const int32_t* dr = sm.dist + r * npairs;
-    int64_t v = 0;
-#pragma unroll
-    for (int i = 0; i < 5; ++i) {
-      if (i < k) v += dr[pid[i]];
-    }
-    const KoptRowInfo& info = sm.info[r];
-    if (info.repeats != 0) {
-      const uint64_t bad = (static_cast<uint64_t>(info.bad_hi) << 32) | info.bad_lo;
-      bool invalid = (bad & tmask) != 0;
-      for (uint32_t j = 0; j < info.dup_count; ++j) invalid = invalid || __popcll(info.dup[j] & tmask) >= 2;
-      if (invalid) v = INT64_MAX;
-    }
-    __stcs(out, static_cast<long long>(v));
+  switch (S.k) {
+    case 3:
+      kopt_tile<3, kWide>(L, S, row0, rows, smem, error);
+      break;
+    case 4:
+      kopt_tile<4, kWide>(L, S, row0, rows, smem, error);
+      break;
+    default:
+      kopt_tile<5, kWide>(L, S, row0, rows, smem, error);
+      break;
   }
 }
 

@@ -1,0 +1,271 @@
+// Device side of the serving loop: one persistent kernel runs every admitted job.
+//
+// The host publishes a job in a slot of a fixed table: it clears the slot's state word, writes the
+// job's descriptor, then sets the state word to the descriptor's generation, all with ordered
+// copies (a seqlock: see serve_read_job). A warp keeps claiming items of the job it holds while
+// that job has unclaimed items; otherwise it scans the slots for the oldest published job with
+// unclaimed items (jobs only get younger, so this keeps oldest-first order) and claims one item
+// with a compare-and-swap on the slot's cursor that never moves it past the job's end. A slot's
+// cursor and done counters only grow: the host places each new job of a slot at
+// [previous end, previous end + items), so a warp holding a stale descriptor can never claim an
+// item of a newer job. The warp that finishes a job's last item makes the job's outputs visible
+// and writes the loop's error word, then the generation, into the slot's words of a host-mapped
+// array; the host then copies the results back. Jobs that arrive while others run share the
+// warps item by item (continuous batching). Every wait is bounded: a warp that finds no work for
+// `idle_limit` scans, or sees the stop word, leaves after its current item; the host relaunches
+// the kernel when work arrives.
+//
+// Memory: snapshot arrays are read through the non-coherent L1 path (__ldg). That is safe
+// because the host never writes snapshot memory while a launch runs: a snapshot upload first
+// stops the kernel (stop word, wait for it to end) and the next launch starts with a clean L1.
+// Per-job inputs (k-opt rows) are written into reused arena memory while the kernel runs, so
+// they are read L2-coherently (__ldcg); the control table is read with volatile loads.
+#pragma once
+
+#include "jv_screen.cuh"
+#include "kopt_cost.cuh"
+
+namespace cee {
+
+constexpr int kServeWarps = 8;
+constexpr int kServeMaxSlots = 256;
+constexpr int kServeJv = 1;
+constexpr int kServeKopt = 2;
+constexpr int kServeJvTile = 32;          // JV edges per item
+constexpr int kServeKoptRowsPerItem = 64; // k-opt rows per item, processed in chunks
+
+struct ServeSegment {
+  const int32_t* tasks;  // 48-byte rows
+  int64_t* costs;        // rows x T
+  int64_t rows;
+  int64_t item_begin;    // first item (relative to the job) of this segment
+  int32_t k, T, pad0, pad1;
+};
+
+struct ServeJob {
+  uint32_t generation;
+  int32_t type;
+  int32_t narrow;
+  int32_t segments;
+  unsigned long long begin, end;  // the job's items on the slot's cursor
+  JvGraph g;                      // JV jobs; k-opt jobs use g.xy / g.n / g.dist_type
+  int32_t* witness;
+  ServeSegment seg[3];
+};
+
+struct ServeControl {
+  ServeJob jobs[kServeMaxSlots];
+  unsigned long long cursor[kServeMaxSlots];
+  unsigned long long done[kServeMaxSlots];
+  uint32_t state[kServeMaxSlots];
+  uint32_t stop;
+  int32_t error;  // sticky bounds-check word of every job
+};
+
+// k-opt rows per warp chunk: 8 rows of k = 3, 4 of k = 4, 2 of k = 5 (32..416 cells).
+__host__ __device__ constexpr int serve_rows_per_chunk(int k) { return k == 3 ? 8 : (k == 4 ? 4 : 2); }
+
+// One warp's k-opt tile (kopt_cost.cuh's layout), sized for the largest chunk of any k.
+constexpr int kServeKoptScratch = 1856;
+static_assert(kopt_tile_smem(3, serve_rows_per_chunk(3)) <= kServeKoptScratch, "k = 3 chunk tile");
+static_assert(kopt_tile_smem(4, serve_rows_per_chunk(4)) <= kServeKoptScratch, "k = 4 chunk tile");
+static_assert(kopt_tile_smem(5, serve_rows_per_chunk(5)) <= kServeKoptScratch, "k = 5 chunk tile");
+
+// The k-opt cells of rows [row_begin, row_end) of a segment, one warp, chunk by chunk
+// (kopt_cost_kernel's stages at warp size).
+template <int K, bool kWide>
+__device__ void kopt_rows_warp(const ServeSegment& S, int64_t row_begin, int64_t row_end, const uint8_t* tpairs,
+                               const int2* xy, int32_t n, int32_t dist_type, unsigned char* scratch, int lane,
+                               int32_t* error) {
+  constexpr int P = 2 * K, NP = K * (P - 1), C = serve_rows_per_chunk(K);
+  constexpr int T = K == 3 ? 4 : (K == 4 ? 25 : 208);
+  const KoptSmem sm = kopt_carve(scratch, K, C);
+  kopt_tables<K>(sm.pp, sm.pq, sm.ctab, lane, 32);
+  for (int64_t row0 = row_begin; row0 < row_end; row0 += C) {
+    const int rows = static_cast<int>(min(static_cast<int64_t>(C), row_end - row0));
+    __syncwarp();
+    for (int i = lane; i < rows * P; i += 32) {
+      const int r = i / P, p = i - (i / P) * P;
+      int32_t node = __ldcg(S.tasks + (row0 + r) * 12 + p);
+      if (static_cast<uint32_t>(node) >= static_cast<uint32_t>(n)) {
+        atomicOr(error, 1);
+        node = 0;
+      }
+      sm.ports[i] = node;
+    }
+    __syncwarp();
+    if (lane < rows) {
+      kopt_row_classes<K>(sm.ports + lane * P, sm.ctab, sm.cls + lane * P, sm.repeats + lane, sm.delmask + lane);
+    }
+    __syncwarp();
+    for (int i = lane; i < rows * NP; i += 32) {
+      const int r = i / NP;
+      kopt_pair_entry<K, kWide>(sm, r, i - r * NP, xy, dist_type);
+    }
+    __syncwarp();
+    long long* out = reinterpret_cast<long long*>(S.costs + row0 * T);
+    for (int j = lane; j < rows * T; j += 32) {
+      const int r = j / T, t = j - (j / T) * T;
+      int pid[K];
+#pragma unroll
+      for (int i = 0; i < K; ++i) pid[i] = tpairs[t * K + i];
+      __stcs(out + j, static_cast<long long>(kopt_cell<K, kWide>(sm, r, pid)));
+    }
+  }
+  __syncwarp();
+}
+
+// Canonical template pair tables for k = 3, 4, 5 packed back to back (4*3 + 25*4 + 208*5 bytes).
+constexpr int kServeTemplateBytes = 4 * 3 + 25 * 4 + 208 * 5;
+__host__ __device__ __forceinline__ int serve_template_offset(int k) { return k == 3 ? 0 : (k == 4 ? 12 : 112); }
+
+__device__ __forceinline__ uint32_t volatile_load(const uint32_t* p) { return *reinterpret_cast<const volatile uint32_t*>(p); }
+__device__ __forceinline__ unsigned long long volatile_load(const unsigned long long* p) {
+  return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+
+// Copies slot `slot`'s descriptor into `out` (all lanes) and returns true when it is the
+// published, complete descriptor: state read before and after the copy (with fences) equals the
+// copy's generation. The host unpublishes a slot (state = 0) before rewriting its descriptor and
+// republishes it after, all with ordered copies, so a torn copy always fails this check.
+__device__ __forceinline__ bool serve_read_job(const ServeControl* ctl, int slot, ServeJob& out, int lane) {
+  const uint32_t s1 = volatile_load(&ctl->state[slot]);
+  __threadfence();
+  constexpr int kWords = static_cast<int>(sizeof(ServeJob) / 4);
+  const volatile uint32_t* src = reinterpret_cast<const volatile uint32_t*>(&ctl->jobs[slot]);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(&out);
+  for (int i = lane; i < kWords; i += 32) dst[i] = src[i];
+  __threadfence();
+  const uint32_t s2 = volatile_load(&ctl->state[slot]);
+  __syncwarp();
+  return s1 != 0 && s1 == s2 && out.generation == s1;
+}
+
+// Lane 0 claims the next item of `job` on the slot's cursor, never past the job's end;
+// returns the claimed cursor value, or -1, on every lane.
+__device__ __forceinline__ long long serve_claim(ServeControl* ctl, int slot, const ServeJob& job, int lane) {
+  long long item = -1;
+  if (lane == 0) {
+    unsigned long long cur = volatile_load(&ctl->cursor[slot]);
+    while (cur >= job.begin && cur < job.end) {
+      const unsigned long long seen = atomicCAS(&ctl->cursor[slot], cur, cur + 1);
+      if (seen == cur) {
+        item = static_cast<long long>(cur);
+        break;
+      }
+      cur = seen;
+    }
+  }
+  return __shfl_sync(kFullMask, item, 0);
+}
+
+template <int K>
+__device__ __forceinline__ void serve_kopt_item(const ServeJob& job, const ServeSegment& S, int64_t r0, int64_t r1,
+                                                const uint8_t* tpairs, unsigned char* scratch, int lane,
+                                                int32_t* error) {
+  if (job.narrow) {
+    kopt_rows_warp<K, false>(S, r0, r1, tpairs, job.g.xy, job.g.n, job.g.dist_type, scratch, lane, error);
+  } else {
+    kopt_rows_warp<K, true>(S, r0, r1, tpairs, job.g.xy, job.g.n, job.g.dist_type, scratch, lane, error);
+  }
+}
+
+static __global__ void __launch_bounds__(kServeWarps * 32, 4)
+    serve_kernel(ServeControl* ctl, uint32_t* finished, const uint8_t* templates, int32_t slots,
+                 long long idle_limit) {
+  int32_t* error = &ctl->error;
+  __shared__ JvWarpScratch jv_scratch[kServeWarps];
+  __shared__ __align__(16) unsigned char kopt_scratch[kServeWarps][kServeKoptScratch];
+  __shared__ ServeJob job_copy[kServeWarps];
+  __shared__ uint8_t tpairs[kServeTemplateBytes];
+  for (int i = threadIdx.x; i < kServeTemplateBytes; i += blockDim.x) tpairs[i] = templates[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  ServeJob& job = job_copy[warp];
+  int held = -1;  // slot whose descriptor `job` holds
+  long long idle = 0;
+  while (idle < idle_limit) {
+    if (volatile_load(&ctl->stop) != 0) break;
+    long long item = -1;
+    int slot = held;
+    if (held >= 0) {  // keep working on the held job while it is published and has items
+      const uint32_t state = __shfl_sync(kFullMask, lane == 0 ? volatile_load(&ctl->state[held]) : 0u, 0);
+      if (state == job.generation) item = serve_claim(ctl, held, job, lane);
+      if (item < 0) held = -1;
+    }
+    if (item < 0) {
+      // the oldest published job that looks unfinished
+      uint32_t best_gen = 0xffffffffu;
+      int best_slot = -1;
+      for (int s = lane; s < slots; s += 32) {
+        const uint32_t gen = volatile_load(&ctl->state[s]);
+        if (gen == 0 || gen >= best_gen) continue;
+        if (volatile_load(&ctl->cursor[s]) < volatile_load(&ctl->jobs[s].end)) {
+          best_gen = gen;
+          best_slot = s;
+        }
+      }
+      const uint32_t oldest = __reduce_min_sync(kFullMask, best_gen);
+      const unsigned owner = __ballot_sync(kFullMask, best_slot >= 0 && best_gen == oldest);
+      if (owner == 0) {
+        ++idle;
+        __nanosleep(2000);
+        continue;
+      }
+      slot = __shfl_sync(kFullMask, best_slot, __ffs(owner) - 1);
+      if (!serve_read_job(ctl, slot, job, lane)) {  // torn by a concurrent publication: rescan
+        ++idle;
+        continue;
+      }
+      held = slot;
+      item = serve_claim(ctl, slot, job, lane);
+      if (item < 0) {  // another warp took the last item
+        held = -1;
+        ++idle;
+        continue;
+      }
+    }
+    idle = 0;
+    const long long local = item - static_cast<long long>(job.begin);
+    if (job.type == kServeJv) {
+      const int64_t e0 = local * kServeJvTile;
+      const int64_t e1 = min(e0 + kServeJvTile, job.g.m);
+      for (int64_t e = e0; e < e1; ++e) {
+        const int32_t wv = job.narrow ? jv_screen_edge_warp<false>(job.g, e, jv_scratch[warp], lane, error)
+                                      : jv_screen_edge_warp<true>(job.g, e, jv_scratch[warp], lane, error);
+        if (lane == 0) job.witness[e] = wv;
+        __syncwarp();
+      }
+    } else {
+      int si = 0;
+      while (si + 1 < job.segments && local >= job.seg[si + 1].item_begin) ++si;
+      const ServeSegment& S = job.seg[si];
+      const int64_t r0 = (local - S.item_begin) * kServeKoptRowsPerItem;
+      const int64_t r1 = min(r0 + kServeKoptRowsPerItem, S.rows);
+      const uint8_t* tp = tpairs + serve_template_offset(S.k);
+      unsigned char* ks = kopt_scratch[warp];
+      if (S.k == 3) {
+        serve_kopt_item<3>(job, S, r0, r1, tp, ks, lane, error);
+      } else if (S.k == 4) {
+        serve_kopt_item<4>(job, S, r0, r1, tp, ks, lane, error);
+      } else {
+        serve_kopt_item<5>(job, S, r0, r1, tp, ks, lane, error);
+      }
+    }
+    __threadfence();  // this warp's outputs before its done count
+    __syncwarp();
+    if (lane == 0) {
+      const unsigned long long finished_items = atomicAdd(&ctl->done[slot], 1ull) + 1;
+      if (finished_items == job.end) {  // finished[slot + kServeMaxSlots]: error word, then the generation
+        __threadfence_system();
+        reinterpret_cast<volatile uint32_t*>(finished)[kServeMaxSlots + slot] =
+            volatile_load(reinterpret_cast<uint32_t*>(error));
+        __threadfence_system();
+        reinterpret_cast<volatile uint32_t*>(finished)[slot] = job.generation;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace cee

@@ -8,6 +8,9 @@ instances of the same shapes stand in for them.
   kopt_instance()   15,000 nodes uniform in [0,10^6)^2, 10-NN, CEIL_2D, with 200,000 leaf rows
                     of k in {3,4,5} in thirds                                 (k-opt cost matrix)
   batch_instance(i) instance i of the 4,096-instance mix (n log-uniform in [100,5000])
+  ServeWorkload()   the serving stream: 10,000 jobs, 70% JV epochs on instances of the batching
+                    mix with n log-uniform in [200,20000], 30% k-opt leaf batches of 1k-50k rows
+                    (k = 3/4/5 in thirds) on CEIL_2D instances of the same n range
 """
 from __future__ import annotations
 
@@ -159,3 +162,49 @@ class BatchUnion:
         g = self.graph
         return GraphSnapshot(n1 - n0, g.dist_type, g.x[n0:n1], g.y[n0:n1], g.edge_u[e0:e1] - n0,
                              g.edge_v[e0:e1] - n0, g.edge_w[e0:e1], g.active[e0:e1])
+
+
+class ServeWorkload:
+    """The serving stream. Snapshots come from fixed pools that stay resident on the device
+    (`jv_pool` instances of the batching mix with n log-uniform in [n_lo, n_hi]; `kopt_pool`
+    uniform CEIL_2D 10-NN instances of the same n range, each with a pool of leaf rows per k);
+    job j is a JV epoch on a pool snapshot (probability 0.7) or a k-opt batch of
+    rows ~ floor(exp(U[ln rows_lo, ln rows_hi])) split over k = 3/4/5 in thirds, taken as
+    contiguous slices of a k-opt snapshot's row pools. `gaps` are unit-rate exponential
+    inter-arrival times (scale by 1/lambda for a Poisson stream of rate lambda)."""
+
+    def __init__(self, jobs: int = 10_000, jv_pool: int = 192, kopt_pool: int = 8, seed: int = SEED_BASE + 4,
+                 n_lo: float = 200.0, n_hi: float = 20_000.0, rows_lo: float = 1_000.0, rows_hi: float = 50_000.0):
+        rng = np.random.default_rng(seed)
+        self.seed = seed
+        self.jv = [batch_instance(i, seed, n_lo, n_hi) for i in range(jv_pool)]
+        self.per_k = int(rows_hi) // 3 + 1
+        self.kopt = []
+        for i in range(kopt_pool):
+            n = int(np.floor(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi)))))
+            h = _Handle(lib().cees_uniform_knn(n, 1_000_000, 10, CEIL_2D, seed + 1000 + i))
+            rows = h.kopt_rows(np.repeat(np.array([3, 4, 5], np.uint8), self.per_k), seed + 2000 + i)
+            self.kopt.append((h.snapshot(), {k: rows[j * self.per_k:(j + 1) * self.per_k] for j, k in enumerate((3, 4, 5))}))
+        is_jv = rng.random(jobs) < 0.7
+        self.jobs = []
+        for j in range(jobs):
+            if is_jv[j]:
+                self.jobs.append(("jv", int(rng.integers(jv_pool)), None))
+                continue
+            rows = int(np.floor(np.exp(rng.uniform(np.log(rows_lo), np.log(rows_hi)))))
+            third = -(-rows // 3)
+            counts = (third, third, rows - 2 * third)
+            offsets = tuple(int(rng.integers(0, self.per_k - c + 1)) for c in counts)
+            self.jobs.append(("kopt", int(rng.integers(kopt_pool)), tuple(zip(counts, offsets))))
+        self.gaps = rng.exponential(1.0, jobs)
+
+    def kopt_tasks(self, job):
+        """The three task slices (k = 3, 4, 5) of a k-opt job."""
+        _, s, parts = job
+        pools = self.kopt[s][1]
+        return [pools[k][off:off + c] for k, (c, off) in zip((3, 4, 5), parts)]
+
+    def output_bytes(self, job) -> int:
+        if job[0] == "jv":
+            return 4 * self.jv[job[1]].m
+        return sum(8 * c * t for (c, _), t in zip(job[2], (4, 25, 208)))

@@ -6,7 +6,8 @@
  * symbols onto these calls so that the reference's CPU code drives the B200 kernels.
  *
  * Conventions
- *   - Every int-returning function returns CEE_OK (0) or a negative CEE_ERR_* code; the text
+ *   - Every int-returning function returns CEE_OK (0) or a negative CEE_ERR_* code (the serving
+ *     loop's admission calls may also return CEE_BUSY, 1); the text
  *     of the last error is available from cee_last_error(ctx) (ctx may be NULL for errors
  *     raised before a context exists).
  *   - A cee_ctx belongs to one host thread and one device, owns a CUDA stream and all device
@@ -35,6 +36,7 @@ extern "C" {
 
 enum cee_status {
   CEE_OK = 0,
+  CEE_BUSY = 1,          /* serving loop: no slot or no HBM budget left now; poll, then retry */
   CEE_ERR_INVALID = -1,  /* malformed input (reference: std::invalid_argument / runtime_error) */
   CEE_ERR_RANGE = -2,    /* outside the exact-arithmetic range (reference: std::overflow_error) */
   CEE_ERR_CUDA = -3,     /* CUDA runtime or launch failure */
@@ -82,7 +84,8 @@ enum cee_option {
 };
 /* Sets a launch-shape option of this context; results never depend on it. */
 int cee_ctx_set_option(cee_ctx* ctx, int32_t option, int64_t value);
-/* Frees cached device state: bit 1 = JV, bit 2 = k-opt, bit 4 = c,d, bit 8 = batch.
+/* Frees cached device state: bit 1 = JV, bit 2 = k-opt, bit 4 = c,d, bit 8 = batch,
+ * bit 16 = serving loop (stops it; its jobs are dropped).
  * Replaces ClearJvCudaCache (include/cuda_edge_elimination/elimination.hpp:338) and
  * ClearKOptCostCudaCache (include/cuda_edge_elimination/local_search.hpp:242). */
 int cee_ctx_clear(cee_ctx* ctx, unsigned what);
@@ -308,6 +311,48 @@ int cee_batch_get_tuning(const cee_ctx* ctx, cee_batch_tuning* tuning);
 /* Times every candidate launch shape on the prepared batch (`reps` graph launches each, CUDA
  * events) and keeps the fastest; writes it to *chosen. */
 int cee_batch_autotune(cee_ctx* ctx, int32_t reps, cee_batch_tuning* chosen);
+
+/* ---- serving loop (device-resident snapshots, continuous batching) ----------------------- */
+/* No counterpart in the reference: a request loop for callers that screen many snapshots as
+ * they arrive. One persistent kernel runs every admitted job; a job's result is the same as
+ * cee_jv_screen's (witness per edge) or cee_kopt_costs_multi's (the library's proper templates)
+ * on the same snapshot, whatever else runs beside it. */
+typedef struct {
+  uint64_t hbm_budget_bytes; /* device arena for snapshots, k-opt rows and results */
+  int32_t slots;             /* jobs in flight at most (1..256) */
+  int32_t blocks_per_sm;     /* persistent kernel blocks per SM (0 = occupancy limit) */
+  int32_t idle_ms;           /* the kernel leaves after about this long without work */
+} cee_serve_config;
+
+typedef struct {
+  int32_t job;
+  int32_t status;
+  uint64_t tag;
+} cee_serve_event;
+
+int cee_serve_start(cee_ctx* ctx, const cee_serve_config* config);
+/* Uploads a snapshot into the arena (validated on the host; ids as for cee_jv_screen).
+ * CEE_BUSY when the arena has no room now. */
+int cee_serve_add_snapshot(cee_ctx* ctx, const cee_graph_view* graph, int32_t* snapshot);
+/* The snapshot's memory returns to the arena once its last job has completed. */
+int cee_serve_release_snapshot(cee_ctx* ctx, int32_t snapshot);
+/* Screens every edge of the snapshot; witness_out (m entries) is written before the job's
+ * completion event is returned by cee_serve_poll. CEE_BUSY: no slot or arena room now. */
+int cee_serve_submit_jv(cee_ctx* ctx, int32_t snapshot, int32_t* witness_out, uint64_t tag,
+                        int32_t* job);
+/* k-opt leaf costs of 1..3 segments (k = ks[s], rows[s] rows at tasks[s], output costs_out[s],
+ * rows x template_count(k) cells) on the snapshot's coordinates. Task rows are copied at
+ * submission. CEE_BUSY: no slot or arena room now. */
+int cee_serve_submit_kopt(cee_ctx* ctx, int32_t snapshot, int32_t segments, const uint32_t* ks,
+                          const cee_kopt_task* const* tasks, const int64_t* rows,
+                          int64_t* const* costs_out, uint64_t tag, int32_t* job);
+/* Returns up to `capacity` completed jobs (their host outputs are written) and relaunches the
+ * kernel if it went idle while jobs wait. */
+int cee_serve_poll(cee_ctx* ctx, cee_serve_event* events, int32_t capacity, int32_t* count);
+/* Jobs admitted and not yet returned by cee_serve_poll, and arena bytes in use. */
+int cee_serve_pending(const cee_ctx* ctx, int32_t* jobs, uint64_t* arena_used);
+/* Stops the kernel and frees the arena (outstanding jobs are dropped). */
+int cee_serve_stop(cee_ctx* ctx);
 
 #ifdef __cplusplus
 }

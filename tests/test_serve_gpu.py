@@ -1,0 +1,261 @@
+"""Serving loop on the B200: each job's result equals the regular entry point's on the same
+snapshot and the same job run alone, whatever other jobs share the persistent kernel; small
+cases are also checked against the CPU oracle. Covers slot reuse, the idle exit and relaunch,
+HBM-budget admission (CEE_BUSY) and malformed requests."""
+import time
+
+import numpy as np
+import pytest
+
+from cudaedgeelimination_b200 import KOPT_TASK_DTYPE, Context, synth
+from cudaedgeelimination_b200._native import CEE_ERR_INVALID, CEE_ERR_STATE, NativeError
+from cudaedgeelimination_b200.api import ServeConfig
+from helpers import knn_graph, random_graph
+
+pytestmark = pytest.mark.gpu
+
+
+def random_tasks(g, k, rows, seed, repeats=False):
+    """k-opt rows with random ports (repeated ports when `repeats`), any node ids in range."""
+    rng = np.random.default_rng(seed)
+    tasks = np.zeros(rows, KOPT_TASK_DTYPE)
+    pool = g.n if not repeats else min(g.n, 2 * k - 2)
+    base = rng.integers(0, g.n, pool)
+    tasks["port_nodes"][:, :2 * k] = base[rng.integers(0, pool, (rows, 2 * k))]
+    tasks["deleted_cost"] = rng.integers(0, 1 << 20, rows)
+    return tasks
+
+
+def drain(c, want, limit_s=60.0):
+    out = {}
+    t0 = time.time()
+    while len(out) < want:
+        for job, tag, res in c.serve_poll():
+            out[tag] = res
+        assert time.time() - t0 < limit_s, f"serving loop stalled ({len(out)} of {want} jobs back)"
+    return out
+
+
+def submit(c, fn, *args, **kwargs):
+    """Submits, polling the loop while it answers CEE_BUSY; returns the completions seen meanwhile."""
+    seen = {}
+    t0 = time.time()
+    while True:
+        job = fn(*args, **kwargs)
+        if job is not None:
+            return job, seen
+        for _, tag, res in c.serve_poll():
+            seen[tag] = res
+        assert time.time() - t0 < 60.0, "admission never succeeded"
+
+
+@pytest.fixture(scope="module")
+def snapshots():
+    wide = knn_graph(400, 8, seed=31, coord=1 << 28)      # coordinate span >= 2^26: wide distance path
+    sparse = random_graph(500, 1500, seed=32, active_frac=0.7)
+    ceil = knn_graph(300, 6, seed=33, dist_type=1)
+    kg, ktasks = synth.kopt_instance(rows=3000, n=2000)
+    return {"small": synth.jv_small(), "clustered": synth.jv_clustered(), "wide": wide, "sparse": sparse,
+            "ceil": ceil, "kopt": kg, "_ktasks": ktasks}
+
+
+def job_list(snaps):
+    """(tag, snapshot name, kind, payload): JV jobs on every snapshot and k-opt jobs of 1..3 segments."""
+    jobs = []
+    tag = 1
+    for name in ("small", "clustered", "wide", "sparse", "ceil", "kopt"):
+        jobs.append((tag, name, "jv", None))
+        tag += 1
+    kt = snaps["_ktasks"]
+    jobs.append((tag, "kopt", "kopt", ([3, 4, 5], [kt[3], kt[4], kt[5]])))
+    tag += 1
+    jobs.append((tag, "kopt", "kopt", ([5], [kt[5][:777]])))
+    tag += 1
+    for i, name in enumerate(("wide", "ceil", "small")):
+        for k in (3, 4, 5):
+            jobs.append((tag, name, "kopt", ([k], [random_tasks(snaps[name], k, 301 + 17 * k, 40 + i * 3 + k,
+                                                             repeats=(k + i) % 2 == 0)])))
+            tag += 1
+    jobs.append((tag, "ceil", "kopt", ([4, 3], [random_tasks(snaps["ceil"], 4, 50, 61, True),
+                                              random_tasks(snaps["ceil"], 3, 1, 62)])))
+    return jobs
+
+
+def run_jobs(c, snaps, ids, jobs):
+    results = {}
+    for tag, name, kind, payload in jobs:
+        if kind == "jv":
+            _, seen = submit(c, c.serve_submit_jv, ids[name], snaps[name].m, tag)
+        else:
+            _, seen = submit(c, c.serve_submit_kopt, ids[name], payload[0], payload[1], tag)
+        results.update(seen)
+    results.update(drain(c, len(jobs) - len(results)))
+    return results
+
+
+def expected(ctx, snaps, job):
+    tag, name, kind, payload = job
+    g = snaps[name]
+    if kind == "jv":
+        return ctx.jv_screen(g)[0]
+    outs, _ = ctx.kopt_costs_multi(g, payload[0], payload[1])
+    return outs
+
+
+def assert_same(kind, got, want):
+    if kind == "jv":
+        np.testing.assert_array_equal(got, want)
+    else:
+        assert len(got) == len(want)
+        for a, b in zip(got, want):
+            np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("slots", [64, 2], ids=["slots64", "slots2"])
+def test_mix_matches_regular_and_alone(ctx, snapshots, slots):
+    jobs = job_list(snapshots)
+    c = Context(0)
+    try:
+        c.serve_start(ServeConfig(hbm_budget_bytes=256 << 20, slots=slots, idle_ms=5))
+        ids = {name: c.serve_add_snapshot(g) for name, g in snapshots.items() if not name.startswith("_")}
+        assert all(v is not None for v in ids.values())
+        mixed = run_jobs(c, snapshots, ids, jobs)
+        assert sorted(mixed) == [j[0] for j in jobs]
+        for job in jobs:
+            assert_same(job[2], mixed[job[0]], expected(ctx, snapshots, job))
+        # the same jobs alone, one at a time, with the kernel idle in between
+        for job in jobs[::3]:
+            alone = run_jobs(c, snapshots, ids, [job])
+            assert_same(job[2], alone[job[0]], mixed[job[0]])
+        assert c.serve_pending()[0] == 0
+        for sid in ids.values():
+            c.serve_release_snapshot(sid)
+        assert c.serve_pending() == (0, 0)
+        c.serve_stop()
+    finally:
+        c.close()
+
+
+def test_oracle_small(port, snapshots):
+    g = snapshots["small"]
+    k_tasks = random_tasks(g, 4, 64, 7, repeats=True)
+    c = Context(0)
+    try:
+        c.serve_start(ServeConfig(hbm_budget_bytes=64 << 20, slots=4, idle_ms=5))
+        sid = c.serve_add_snapshot(g)
+        c.serve_submit_jv(sid, g.m, tag=1)
+        c.serve_submit_kopt(sid, [4], [k_tasks], tag=2)
+        res = drain(c, 2)
+        np.testing.assert_array_equal(res[1], port.jv_screen(g))
+        np.testing.assert_array_equal(res[2][0], port.kopt_costs(g, 4, k_tasks))
+        c.serve_stop()
+    finally:
+        c.close()
+
+
+def test_idle_exit_and_relaunch(ctx, snapshots):
+    g = snapshots["sparse"]
+    want = ctx.jv_screen(g)[0]
+    c = Context(0)
+    try:
+        c.serve_start(ServeConfig(hbm_budget_bytes=64 << 20, slots=2, idle_ms=1))
+        sid = c.serve_add_snapshot(g)
+        for i in range(6):
+            submit(c, c.serve_submit_jv, sid, g.m, i)
+            np.testing.assert_array_equal(drain(c, 1)[i], want)
+            time.sleep(0.02)  # the kernel leaves after about 1 ms without work
+        c.serve_stop()
+    finally:
+        c.close()
+
+
+def test_snapshot_upload_while_jobs_run(ctx, snapshots):
+    """Adding a snapshot stops the running kernel and resumes its jobs afterwards."""
+    big = synth.uniform_knn(20_000, 1_000_000, 10, 0, 78)
+    later = snapshots["ceil"]
+    c = Context(0)
+    try:
+        c.serve_start(ServeConfig(hbm_budget_bytes=256 << 20, slots=8, idle_ms=50))
+        sid = c.serve_add_snapshot(big)
+        for t in range(4):
+            c.serve_submit_jv(sid, big.m, tag=t)
+        lid = c.serve_add_snapshot(later)  # while the four jobs are on the GPU
+        c.serve_submit_jv(lid, later.m, tag=10)
+        res = drain(c, 5)
+        want = ctx.jv_screen(big)[0]
+        for t in range(4):
+            np.testing.assert_array_equal(res[t], want)
+        np.testing.assert_array_equal(res[10], ctx.jv_screen(later)[0])
+        c.serve_stop()
+    finally:
+        c.close()
+
+
+def test_admission_and_release(snapshots):
+    big, small = synth.uniform_knn(20_000, 1_000_000, 10, 0, 77), snapshots["small"]  # ~4 MB resident
+    c = Context(0)
+    try:
+        c.serve_start(ServeConfig(hbm_budget_bytes=1 << 20, slots=8, idle_ms=5))
+        assert c.serve_add_snapshot(big) is None          # over the budget: CEE_BUSY
+        sid = c.serve_add_snapshot(small)
+        assert sid is not None
+        used_snapshot = c.serve_pending()[1]
+        assert 0 < used_snapshot <= 1 << 20
+        jobs = [c.serve_submit_jv(sid, small.m, tag=t) for t in range(8)]
+        assert all(j is not None for j in jobs)
+        assert c.serve_submit_jv(sid, small.m, tag=99) is None  # every slot taken: CEE_BUSY
+        drain(c, 8)
+        assert c.serve_pending() == (0, used_snapshot)
+        c.serve_release_snapshot(sid)
+        assert c.serve_pending() == (0, 0)
+        assert c.serve_add_snapshot(big) is None
+        c.serve_stop()
+    finally:
+        c.close()
+
+
+def test_empty_jobs(snapshots):
+    g = snapshots["small"].copy()
+    g.active[:] = 0
+    g.rebuild_csr()
+    empty = random_graph(10, 0, seed=5)
+    c = Context(0)
+    try:
+        c.serve_start(ServeConfig(hbm_budget_bytes=16 << 20, slots=2, idle_ms=5))
+        sid = c.serve_add_snapshot(g)
+        eid = c.serve_add_snapshot(empty)
+        c.serve_submit_jv(sid, g.m, tag=1)
+        c.serve_submit_jv(eid, 0, tag=2)
+        c.serve_submit_kopt(sid, [3], [np.zeros(0, KOPT_TASK_DTYPE)], tag=3)
+        res = drain(c, 3)
+        assert (res[1] == -1).all() and res[2].shape == (0,) and res[3][0].shape == (0, 4)
+        c.serve_stop()
+    finally:
+        c.close()
+
+
+def test_malformed_requests(snapshots):
+    g = snapshots["small"]
+    c = Context(0)
+    try:
+        with pytest.raises(NativeError) as e:
+            c.serve_submit_jv(0, g.m)
+        assert e.value.code == CEE_ERR_STATE
+        c.serve_start(ServeConfig(hbm_budget_bytes=16 << 20, slots=2, idle_ms=5))
+        sid = c.serve_add_snapshot(g)
+        for bad in (lambda: c.serve_submit_jv(sid + 5, g.m),
+                    lambda: c.serve_submit_kopt(sid, [6], [np.zeros(1, KOPT_TASK_DTYPE)]),
+                    lambda: c.serve_submit_kopt(sid, [3, 3, 3, 3], [np.zeros(1, KOPT_TASK_DTYPE)] * 4),
+                    lambda: c.serve_release_snapshot(sid + 9)):
+            with pytest.raises(NativeError) as e:
+                bad()
+            assert e.value.code == CEE_ERR_INVALID
+        bad_ports = random_tasks(g, 3, 4, 1)
+        bad_ports["port_nodes"][2, 1] = g.n + 3  # out of range: rejected at submission
+        with pytest.raises(NativeError) as e:
+            c.serve_submit_kopt(sid, [3], [bad_ports], tag=1)
+        assert e.value.code == CEE_ERR_INVALID
+        assert c.serve_pending()[0] == 0
+        c.serve_stop()
+    finally:
+        c.close()
