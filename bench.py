@@ -449,7 +449,6 @@ def serve_drive(ctx, wl, sids, ksids, arrivals, buffers, keep_every: int):
     inflight = {}
     latency = np.zeros(n)
     kept = {}
-    task_cache = {}
     nxt = done = 0
     t0 = time.perf_counter()
     while done < n:
@@ -460,8 +459,7 @@ def serve_drive(ctx, wl, sids, ksids, arrivals, buffers, keep_every: int):
             if job[0] == "jv":
                 jid = ctx.serve_submit_jv(sids[job[1]], wl.jv[job[1]].m, nxt, out=out)
             else:
-                tasks = task_cache.get(nxt) or wl.kopt_tasks(job)
-                jid = ctx.serve_submit_kopt(ksids[job[1]], [3, 4, 5], tasks, nxt, outs=out)
+                jid = ctx.serve_submit_kopt(ksids[job[1]], [3, 4, 5], wl.kopt_tasks(job), nxt, outs=out)
             if jid is None:  # no slot or arena room: poll first
                 break
             inflight[jid] = (nxt, free.pop())
@@ -508,6 +506,14 @@ def run_serve(args, device, world):
     from cudaedgeelimination_b200.api import ServeConfig
 
     wl = synth.ServeWorkload(jobs=args.serve_jobs)
+    pinned_pools = []  # k-opt row pools in page-locked memory, as a serving caller would keep them
+    for i, (g, pools) in enumerate(wl.kopt):
+        pinned = {}
+        for k, rows in pools.items():
+            owner, view = pinned_copy(rows)
+            pinned_pools.append(owner)
+            pinned[k] = view
+        wl.kopt[i] = (g, pinned)
     slots = 32
     max_bytes = max(wl.output_bytes(j) for j in wl.jobs)
     owners, buffers = _pinned_pool(slots + 1, max_bytes)
@@ -542,7 +548,7 @@ def run_serve(args, device, world):
             assert all((a == b).all() for a, b in zip(got, want)), f"serve/plain mismatch on job {idx}"
         else:
             assert (got == want).all(), f"serve/plain mismatch on job {idx}"
-    del owners
+    del owners, pinned_pools
     jv_jobs = sum(1 for j in wl.jobs if j[0] == "jv")
     return {
         "metric": "served jobs/s and p50/p99 latency", "jobs": len(wl.jobs), "jv_jobs": jv_jobs,
@@ -558,7 +564,8 @@ def run_serve(args, device, world):
         "config": f"{len(wl.jobs)} jobs, Poisson arrivals at 0.8 x measured serving capacity; 70% JV epochs on "
                   f"{len(wl.jv)} resident instances of the batching mix (n log-uniform [200,20000]), 30% k-opt "
                   f"batches of 1k-50k rows (k = 3/4/5 in thirds) on {len(wl.kopt)} resident CEIL_2D instances; "
-                  f"{slots} slots, results into pinned host buffers; latency = arrival to results on the host",
+                  f"{slots} slots, k-opt rows and results in pinned host buffers; latency = arrival to results "
+                  "on the host",
         "checked_jobs": len(plain_kept),
     }
 

@@ -432,6 +432,10 @@ int PairTable(cee_ctx* ctx, uint32_t k, const uint8_t* mates, int32_t count, std
       }
       if (p < q) (*pairs)[static_cast<size_t>(t) * k + found++] = static_cast<uint8_t>(kopt_pair_index(p, q, ports));
     }
+    // a template that pairs 2e with 2e + 1 re-adds deleted edge e on every row
+    for (uint32_t e = 0; e < k; ++e) {
+      if (mate[2 * e] == 2 * e + 1) (*pairs)[static_cast<size_t>(t) * k] = kKoptReaddsDeleted;
+    }
   }
   return CEE_OK;
 }

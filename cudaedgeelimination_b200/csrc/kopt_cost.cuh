@@ -13,7 +13,8 @@
 // code is a deleted edge's code. So each port pair gets a one-hot 64-bit mask (bit = code, or
 // bit 63 when the pair is a self loop or a deleted edge), and a template is valid iff the OR of
 // its k masks has bit 63 clear and exactly k bits set. Rows whose 2k ports are distinct nodes
-// need no masks: a proper template never pairs 2e with 2e+1, so all their cells are plain sums.
+// need no masks: a proper template never pairs 2e with 2e+1, so all their cells are plain sums
+// (a caller template that does is marked in its pair table and yields invalid cells).
 //
 // B200 mapping: a block owns a tile of consecutive rows of one segment (one k; the tile
 // routine is compiled per k so the per-row work is fully unrolled).
@@ -39,6 +40,9 @@ constexpr int kKoptMaxTemplates = 208;     // proper 5-opt templates
 constexpr int kKoptSmemBytes = 96 * 1024;  // dynamic shared memory cap per block (opted in above 48 KB)
 constexpr int kKoptMaxSegments = 8;
 constexpr uint64_t kKoptBadPair = uint64_t{1} << 63;
+// First pair index of a template that pairs some port 2e with 2e + 1 (re-adds deleted edge e,
+// so every cell is invalid); proper templates never do.
+constexpr uint8_t kKoptReaddsDeleted = 0xff;
 
 // pair index of ports p < q among 2k ports (row-major upper triangle)
 __host__ __device__ __forceinline__ int kopt_pair_index(int p, int q, int ports) {
@@ -225,10 +229,13 @@ __device__ __forceinline__ void kopt_tile(const KoptLaunch& L, const KoptSegment
   int pid[K];
 #pragma unroll
   for (int i = 0; i < K; ++i) pid[i] = __ldg(S.pairs + t * K + i);
+  const bool readds_deleted = pid[0] == kKoptReaddsDeleted;
+  if (readds_deleted) pid[0] = 0;
   long long* out = reinterpret_cast<long long*>(S.costs + row0 * T) + static_cast<int64_t>(rr) * T + t;
   const int64_t out_step = static_cast<int64_t>(per_step) * T;
   for (int r = rr; r < rows; r += per_step, out += out_step) {
-    __stcs(out, static_cast<long long>(kopt_cell<K, kWide>(sm, r, pid)));
+    const int64_t v = kopt_cell<K, kWide>(sm, r, pid);
+    __stcs(out, static_cast<long long>(readds_deleted ? INT64_MAX : v));
   }
 }
 

@@ -104,10 +104,12 @@ struct ServeState {
   cee_serve_config cfg{};
   DevBuf arena_buf, control, templates;
   Arena arena;
-  uint32_t* finished_host = nullptr;  // mapped: [slot] generation done, [kServeMaxSlots + slot] error word
+  // mapped: [slot] generation done, [kServeMaxSlots + slot] error word, [kServeLostWord] lost item
+  uint32_t* finished_host = nullptr;
   uint32_t* finished_dev = nullptr;
   ServeJob* desc_host = nullptr;      // pinned staging, one descriptor per slot
   uint32_t* words_host = nullptr;     // pinned: [0] = 0, [1] = 1, [2 + s] = generation of slot s
+  uint64_t* tickets_host = nullptr;   // pinned: generation of slot s << 32 (ticket and done resets)
   uint8_t* pinned_stage = nullptr;    // snapshot packing
   size_t pinned_stage_bytes = 0;
   cudaStream_t server = nullptr, copy = nullptr, d2h = nullptr;
@@ -115,7 +117,6 @@ struct ServeState {
   bool launched = false;
   int grid = 1;
   long long idle_limit = 1;
-  uint64_t slot_end[kServeMaxSlots] = {};
   bool slot_busy[kServeMaxSlots] = {};
   int next_slot = 0;
   uint32_t next_generation = 1;
@@ -123,6 +124,7 @@ struct ServeState {
   std::vector<ServeJobHost> jobs;
   std::vector<int> finished_jobs;  // completed without device work, reported at the next poll
   int pending = 0;
+  bool broken = false;  // an item was lost (see cee_serve_poll)
 };
 
 namespace {
@@ -182,13 +184,18 @@ int FreeSlot(const ServeState& s) {
   return -1;
 }
 
-// Publishes `desc` in `slot`: state = 0, descriptor, state = generation (ordered copies).
+// Publishes `desc` in `slot` with ordered copies: state = 0, descriptor, ticket and done =
+// generation << 32, state = generation. The pinned sources of a slot are rewritten only after
+// its previous job finished, i.e. after the copies that read them ran.
 int Publish(cee_ctx* ctx, ServeState& s, int slot, const ServeJob& desc) {
   ServeControl* ctl = static_cast<ServeControl*>(s.control.ptr);
   s.desc_host[slot] = desc;
   s.words_host[2 + slot] = desc.generation;
+  s.tickets_host[slot] = static_cast<uint64_t>(desc.generation) << 32;
   cudaMemcpyAsync(&ctl->state[slot], &s.words_host[0], sizeof(uint32_t), cudaMemcpyHostToDevice, s.copy);
   cudaMemcpyAsync(&ctl->jobs[slot], &s.desc_host[slot], sizeof(ServeJob), cudaMemcpyHostToDevice, s.copy);
+  cudaMemcpyAsync(&ctl->ticket[slot], &s.tickets_host[slot], sizeof(uint64_t), cudaMemcpyHostToDevice, s.copy);
+  cudaMemcpyAsync(&ctl->done[slot], &s.tickets_host[slot], sizeof(uint64_t), cudaMemcpyHostToDevice, s.copy);
   cudaMemcpyAsync(&ctl->state[slot], &s.words_host[2 + slot], sizeof(uint32_t), cudaMemcpyHostToDevice, s.copy);
   const cudaError_t status = cudaGetLastError();
   if (status != cudaSuccess) return CudaFail(ctx, status, "serve publish");
@@ -252,6 +259,7 @@ void ReleaseServe(cee_ctx* ctx, int32_t* error_word) {
   if (s->finished_host != nullptr) cudaFreeHost(s->finished_host);
   if (s->desc_host != nullptr) cudaFreeHost(s->desc_host);
   if (s->words_host != nullptr) cudaFreeHost(s->words_host);
+  if (s->tickets_host != nullptr) cudaFreeHost(s->tickets_host);
   if (s->pinned_stage != nullptr) cudaFreeHost(s->pinned_stage);
   for (cudaStream_t st : {s->server, s->copy, s->d2h}) {
     if (st != nullptr) cudaStreamDestroy(st);
@@ -289,7 +297,7 @@ int cee_serve_start(cee_ctx* ctx, const cee_serve_config* config) {
   if (status == cudaSuccess) status = cudaMemset(s.control.ptr, 0, sizeof(ServeControl));
   if (status == cudaSuccess) status = s.templates.Reserve(kServeTemplateBytes, nullptr);
   if (status == cudaSuccess) {
-    status = cudaHostAlloc(reinterpret_cast<void**>(&s.finished_host), 2 * kServeMaxSlots * sizeof(uint32_t),
+    status = cudaHostAlloc(reinterpret_cast<void**>(&s.finished_host), (kServeLostWord + 1) * sizeof(uint32_t),
                            cudaHostAllocMapped);
   }
   if (status == cudaSuccess) status = cudaHostGetDevicePointer(reinterpret_cast<void**>(&s.finished_dev), s.finished_host, 0);
@@ -298,6 +306,10 @@ int cee_serve_start(cee_ctx* ctx, const cee_serve_config* config) {
   }
   if (status == cudaSuccess) {
     status = cudaHostAlloc(reinterpret_cast<void**>(&s.words_host), (kServeMaxSlots + 2) * sizeof(uint32_t),
+                           cudaHostAllocDefault);
+  }
+  if (status == cudaSuccess) {
+    status = cudaHostAlloc(reinterpret_cast<void**>(&s.tickets_host), kServeMaxSlots * sizeof(uint64_t),
                            cudaHostAllocDefault);
   }
   for (cudaStream_t* st : {&s.server, &s.copy, &s.d2h}) {
@@ -313,7 +325,7 @@ int cee_serve_start(cee_ctx* ctx, const cee_serve_config* config) {
     ReleaseServe(ctx);
     return code;
   }
-  std::memset(s.finished_host, 0, 2 * kServeMaxSlots * sizeof(uint32_t));
+  std::memset(s.finished_host, 0, (kServeLostWord + 1) * sizeof(uint32_t));
   s.words_host[0] = 0;
   s.words_host[1] = 1;
   per_sm = std::max(1, config->blocks_per_sm > 0 ? std::min(per_sm, config->blocks_per_sm) : per_sm);
@@ -481,6 +493,7 @@ int cee_serve_submit_jv(cee_ctx* ctx, int32_t snapshot, int32_t* witness_out, ui
   ServeState* sp = Serving(ctx);
   if (sp == nullptr) return ServeFail(ctx, CEE_ERR_STATE, "not started");
   ServeState& s = *sp;
+  if (s.broken) return ServeFail(ctx, CEE_ERR_TIMEOUT, "loop lost a work item; restart it");
   if (snapshot < 0 || snapshot >= static_cast<int>(s.snapshots.size()) || !s.snapshots[snapshot].live || job_out == nullptr ||
       (s.snapshots[snapshot].m > 0 && witness_out == nullptr)) {
     return ServeFail(ctx, CEE_ERR_INVALID, "bad JV job");
@@ -511,9 +524,7 @@ int cee_serve_submit_jv(cee_ctx* ctx, int32_t snapshot, int32_t* witness_out, ui
   desc.narrow = snap.narrow ? 1 : 0;
   desc.g = snap.g;
   desc.witness = reinterpret_cast<int32_t*>(static_cast<uint8_t*>(s.arena_buf.ptr) + out);
-  desc.begin = s.slot_end[slot];
-  desc.end = desc.begin + static_cast<unsigned long long>((snap.m + kServeJvTile - 1) / kServeJvTile);
-  s.slot_end[slot] = desc.end;
+  desc.items = static_cast<uint32_t>((snap.m + kServeJvTile - 1) / kServeJvTile);
   s.slot_busy[slot] = true;
   s.next_slot = (slot + 1) % s.cfg.slots;
   job.live = true;
@@ -536,6 +547,7 @@ int cee_serve_submit_kopt(cee_ctx* ctx, int32_t snapshot, int32_t segments, cons
   ServeState* sp = Serving(ctx);
   if (sp == nullptr) return ServeFail(ctx, CEE_ERR_STATE, "not started");
   ServeState& s = *sp;
+  if (s.broken) return ServeFail(ctx, CEE_ERR_TIMEOUT, "loop lost a work item; restart it");
   if (snapshot < 0 || snapshot >= static_cast<int>(s.snapshots.size()) || !s.snapshots[snapshot].live ||
       segments < 1 || segments > 3 || ks == nullptr || tasks == nullptr || rows == nullptr || costs_out == nullptr ||
       job_out == nullptr) {
@@ -606,9 +618,7 @@ int cee_serve_submit_kopt(cee_ctx* ctx, int32_t snapshot, int32_t segments, cons
     in_at += (static_cast<size_t>(rows[i]) * sizeof(cee_kopt_task) + 255) & ~size_t{255};
     out_at += (static_cast<size_t>(rows[i]) * seg.T * 8 + 255) & ~size_t{255};
   }
-  desc.begin = s.slot_end[slot];
-  desc.end = desc.begin + static_cast<unsigned long long>(items);
-  s.slot_end[slot] = desc.end;
+  desc.items = static_cast<uint32_t>(items);
   s.slot_busy[slot] = true;
   s.next_slot = (slot + 1) % s.cfg.slots;
   job.live = true;
@@ -646,10 +656,23 @@ int cee_serve_poll(cee_ctx* ctx, cee_serve_event* events, int32_t capacity, int3
     s.finished_jobs.pop_back();
     report(id, s.jobs[id]);
   }
+  if (!s.broken && reinterpret_cast<volatile uint32_t*>(s.finished_host)[kServeLostWord] != 0) {
+    // a claimed item's descriptor never became visible: that job cannot finish. Stop the kernel
+    // and fail every job still on the GPU; the loop must be restarted.
+    rc = QuiesceServer(ctx, s);
+    if (rc != CEE_OK) return rc;
+    s.broken = true;
+  }
   bool on_gpu = false;
   for (int id = 0; id < static_cast<int>(s.jobs.size()); ++id) {
     ServeJobHost& job = s.jobs[id];
     if (!job.live || job.phase == 2) continue;
+    if (job.phase == 0 && s.broken &&
+        *reinterpret_cast<volatile uint32_t*>(s.finished_host + job.slot) != job.generation) {
+      job.status = Fail(ctx, CEE_ERR_TIMEOUT, "serving loop lost a work item; restart it with cee_serve_start");
+      if (!report(id, job)) break;
+      continue;
+    }
     if (job.phase == 0) {
       if (*reinterpret_cast<volatile uint32_t*>(s.finished_host + job.slot) != job.generation) {
         on_gpu = true;
@@ -671,7 +694,7 @@ int cee_serve_poll(cee_ctx* ctx, cee_serve_event* events, int32_t capacity, int3
     if (q != cudaSuccess) return CudaFail(ctx, q, "serve download");
     if (!report(id, job)) break;
   }
-  if (on_gpu) {  // the kernel may have gone idle before a late publication: relaunch if it ended
+  if (on_gpu && !s.broken) {  // the kernel may have gone idle before a late publication: relaunch if it ended
     rc = LaunchServer(ctx, s);
     if (rc != CEE_OK) return rc;
   }

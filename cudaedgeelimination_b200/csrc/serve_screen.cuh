@@ -1,19 +1,21 @@
 // Device side of the serving loop: one persistent kernel runs every admitted job.
 //
-// The host publishes a job in a slot of a fixed table: it clears the slot's state word, writes the
-// job's descriptor, then sets the state word to the descriptor's generation, all with ordered
-// copies (a seqlock: see serve_read_job). A warp keeps claiming items of the job it holds while
-// that job has unclaimed items; otherwise it scans the slots for the oldest published job with
-// unclaimed items (jobs only get younger, so this keeps oldest-first order) and claims one item
-// with a compare-and-swap on the slot's cursor that never moves it past the job's end. A slot's
-// cursor and done counters only grow: the host places each new job of a slot at
-// [previous end, previous end + items), so a warp holding a stale descriptor can never claim an
-// item of a newer job. The warp that finishes a job's last item makes the job's outputs visible
-// and writes the loop's error word, then the generation, into the slot's words of a host-mapped
-// array; the host then copies the results back. Jobs that arrive while others run share the
-// warps item by item (continuous batching). Every wait is bounded: a warp that finds no work for
-// `idle_limit` scans, or sees the stop word, leaves after its current item; the host relaunches
-// the kernel when work arrives.
+// The host publishes a job in a slot of a fixed table with ordered copies: state word = 0, the
+// job's descriptor, the slot's ticket and done counters = generation << 32, state word =
+// generation (a seqlock: see serve_read_job). Work is claimed with one atomicAdd on the slot's
+// ticket, whose high half names the generation the item belongs to and whose low half the item
+// index, so claims never retry however many warps contend. A warp keeps claiming from the job it
+// holds while that job has items left; otherwise it scans the slots for the oldest published job
+// with items left (jobs only get younger, so this keeps oldest-first order). A claim may land on
+// a newer generation than the warp expected (the host republished the slot between the warp's
+// check and its atomicAdd): the warp then reads that generation's descriptor and runs the item,
+// so no item is ever lost; indices past a job's item count are simply dropped. The warp that
+// finishes a job's last item (done counter) makes the job's outputs visible and writes the
+// loop's error word, then the generation, into the slot's words of a host-mapped array; the host
+// then copies the results back. Jobs that arrive while others run share the warps item by item
+// (continuous batching). Every wait is bounded: a warp that finds no work for `idle_limit`
+// scans, or sees the stop word, leaves after its current item; the host relaunches the kernel
+// when work arrives.
 //
 // Memory: snapshot arrays are read through the non-coherent L1 path (__ldg). That is safe
 // because the host never writes snapshot memory while a launch runs: a snapshot upload first
@@ -47,20 +49,27 @@ struct ServeJob {
   int32_t type;
   int32_t narrow;
   int32_t segments;
-  unsigned long long begin, end;  // the job's items on the slot's cursor
-  JvGraph g;                      // JV jobs; k-opt jobs use g.xy / g.n / g.dist_type
+  uint32_t items;
+  uint32_t pad;
+  JvGraph g;  // JV jobs; k-opt jobs use g.xy / g.n / g.dist_type
   int32_t* witness;
   ServeSegment seg[3];
 };
 
 struct ServeControl {
   ServeJob jobs[kServeMaxSlots];
-  unsigned long long cursor[kServeMaxSlots];
-  unsigned long long done[kServeMaxSlots];
+  unsigned long long ticket[kServeMaxSlots];  // generation << 32 | next item
+  unsigned long long done[kServeMaxSlots];    // generation << 32 | items finished
   uint32_t state[kServeMaxSlots];
   uint32_t stop;
-  int32_t error;  // sticky bounds-check word of every job
+  int32_t error;  // sticky word: bounds checks (1), a descriptor that never appeared (8)
 };
+
+// Bounded wait (about a second) for the descriptor of a generation whose item a claim returned.
+constexpr int kServeDescriptorWaits = 1 << 22;
+// Word of the host-mapped `finished` array that mirrors a lost item (error bit 8), so the host
+// can fail the loop's pending jobs instead of waiting for them.
+constexpr int kServeLostWord = 2 * kServeMaxSlots;
 
 // k-opt rows per warp chunk: 8 rows of k = 3, 4 of k = 4, 2 of k = 5 (32..416 cells).
 __host__ __device__ constexpr int serve_rows_per_chunk(int k) { return k == 3 ? 8 : (k == 4 ? 4 : 2); }
@@ -141,22 +150,11 @@ __device__ __forceinline__ bool serve_read_job(const ServeControl* ctl, int slot
   return s1 != 0 && s1 == s2 && out.generation == s1;
 }
 
-// Lane 0 claims the next item of `job` on the slot's cursor, never past the job's end;
-// returns the claimed cursor value, or -1, on every lane.
-__device__ __forceinline__ long long serve_claim(ServeControl* ctl, int slot, const ServeJob& job, int lane) {
-  long long item = -1;
-  if (lane == 0) {
-    unsigned long long cur = volatile_load(&ctl->cursor[slot]);
-    while (cur >= job.begin && cur < job.end) {
-      const unsigned long long seen = atomicCAS(&ctl->cursor[slot], cur, cur + 1);
-      if (seen == cur) {
-        item = static_cast<long long>(cur);
-        break;
-      }
-      cur = seen;
-    }
-  }
-  return __shfl_sync(kFullMask, item, 0);
+// One atomicAdd on the slot's ticket (lane 0); returns the ticket value on every lane.
+__device__ __forceinline__ unsigned long long serve_take(ServeControl* ctl, int slot, int lane) {
+  unsigned long long t = 0;
+  if (lane == 0) t = atomicAdd(&ctl->ticket[slot], 1ull);
+  return __shfl_sync(kFullMask, t, 0);
 }
 
 template <int K>
@@ -186,21 +184,16 @@ static __global__ void __launch_bounds__(kServeWarps * 32, 4)
   long long idle = 0;
   while (idle < idle_limit) {
     if (volatile_load(&ctl->stop) != 0) break;
-    long long item = -1;
     int slot = held;
-    if (held >= 0) {  // keep working on the held job while it is published and has items
-      const uint32_t state = __shfl_sync(kFullMask, lane == 0 ? volatile_load(&ctl->state[held]) : 0u, 0);
-      if (state == job.generation) item = serve_claim(ctl, held, job, lane);
-      if (item < 0) held = -1;
-    }
-    if (item < 0) {
-      // the oldest published job that looks unfinished
+    if (held < 0) {
+      // the oldest published job with items left
       uint32_t best_gen = 0xffffffffu;
       int best_slot = -1;
       for (int s = lane; s < slots; s += 32) {
         const uint32_t gen = volatile_load(&ctl->state[s]);
         if (gen == 0 || gen >= best_gen) continue;
-        if (volatile_load(&ctl->cursor[s]) < volatile_load(&ctl->jobs[s].end)) {
+        const unsigned long long t = volatile_load(&ctl->ticket[s]);
+        if (static_cast<uint32_t>(t >> 32) == gen && static_cast<uint32_t>(t) < volatile_load(&ctl->jobs[s].items)) {
           best_gen = gen;
           best_slot = s;
         }
@@ -218,15 +211,43 @@ static __global__ void __launch_bounds__(kServeWarps * 32, 4)
         continue;
       }
       held = slot;
-      item = serve_claim(ctl, slot, job, lane);
-      if (item < 0) {  // another warp took the last item
+    }
+    const unsigned long long t = serve_take(ctl, slot, lane);
+    const uint32_t gen = static_cast<uint32_t>(t >> 32);
+    const uint32_t index = static_cast<uint32_t>(t);
+    if (gen != job.generation) {
+      // the slot was republished after this warp read it: the claimed item belongs to the newer
+      // job, whose descriptor was written before its ticket (ordered copies); read it, bounded
+      bool found = false;
+      for (int w = 0; w < kServeDescriptorWaits && !found; ++w) {
+        const uint32_t state = __shfl_sync(kFullMask, lane == 0 ? volatile_load(&ctl->state[slot]) : 0u, 0);
+        if (state == gen) {
+          found = serve_read_job(ctl, slot, job, lane) && job.generation == gen;
+        } else if (state != 0) {
+          break;  // an even newer job: generation `gen` already finished, so `index` was past its end
+        } else {
+          __nanosleep(256);
+        }
+      }
+      if (!found) {
+        if (lane == 0 && volatile_load(&ctl->state[slot]) == 0) {  // the publication never completed
+          atomicOr(error, 8);
+          __threadfence_system();
+          reinterpret_cast<volatile uint32_t*>(finished)[kServeLostWord] = 1u;
+        }
         held = -1;
         ++idle;
         continue;
       }
     }
+    if (index >= job.items) {  // every item of the held job is taken
+      held = -1;
+      ++idle;
+      continue;
+    }
+    held = slot;
     idle = 0;
-    const long long local = item - static_cast<long long>(job.begin);
+    const long long local = index;
     if (job.type == kServeJv) {
       const int64_t e0 = local * kServeJvTile;
       const int64_t e1 = min(e0 + kServeJvTile, job.g.m);
@@ -255,8 +276,9 @@ static __global__ void __launch_bounds__(kServeWarps * 32, 4)
     __threadfence();  // this warp's outputs before its done count
     __syncwarp();
     if (lane == 0) {
-      const unsigned long long finished_items = atomicAdd(&ctl->done[slot], 1ull) + 1;
-      if (finished_items == job.end) {  // finished[slot + kServeMaxSlots]: error word, then the generation
+      const unsigned long long d = atomicAdd(&ctl->done[slot], 1ull);
+      // the job's last item: finished[kServeMaxSlots + slot] = error word, then finished[slot] = generation
+      if (static_cast<uint32_t>(d >> 32) == job.generation && static_cast<uint32_t>(d) + 1 == job.items) {
         __threadfence_system();
         reinterpret_cast<volatile uint32_t*>(finished)[kServeMaxSlots + slot] =
             volatile_load(reinterpret_cast<uint32_t*>(error));

@@ -110,6 +110,28 @@ def test_bad_template_rejected(ctx):
         ctx.kopt_costs(g, table, make_tasks(g, 3, [list(range(6))]))
 
 
+def test_caller_templates_readding_deleted_edges(kc, port):
+    """A caller table may hold matchings that pair port 2e with 2e+1; every such cell re-adds a
+    deleted edge and is invalid, on rows with and without repeated nodes."""
+    g = coords_only(*seventeen())
+    rng = np.random.default_rng(5)
+    for k in (3, 4, 5):
+        P = 2 * k
+        mates = []
+        for _ in range(40):  # random perfect matchings, many of them improper
+            perm = rng.permutation(P)
+            m = np.full(14, 0xFF, np.uint8)
+            for a, b in zip(perm[0::2], perm[1::2]):
+                m[a], m[b] = b, a
+            mates.append(m)
+        table = BuildKOptReconnectTable(k)
+        table.templates = np.concatenate([table.templates[:8], np.array(mates, np.uint8)])
+        rows = [list(rng.integers(0, 17, P)) for _ in range(60)] + [list(range(P)), list(range(1, P + 1))]
+        tasks = make_tasks(g, k, rows)
+        gpu, _ = kc.kopt_costs(g, table, tasks)
+        np.testing.assert_array_equal(gpu, port.kopt_costs(g, k, tasks, table.templates))
+
+
 def test_heavily_repeated_ports(kc, port):
     """Nodes shared by several deleted edges: a node in three deleted edges (k=3), a closed
     5-cycle where every node repeats (k=5, the maximum number of duplicate sets), and runs."""
