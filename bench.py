@@ -330,7 +330,8 @@ def run_ours(args, rank: int, world: int, device: int):
                 "api": "cee_batch_screen (pinned host buffers, chunked copy/compute overlap)"},
         "roofline": {"kernel": "batch_screen_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
-                     "traffic": load_traffic().get("batch_screen_kernel"), "algorithmic_bytes_per_launch": alg_bytes,
+                     "traffic": load_traffic().get("batch_screen_kernel"), "traffic_unit": "DRAM bytes per launch (ncu)",
+                     "algorithmic_bytes_per_launch": alg_bytes,
                      "note": "the screen is ALU/latency bound (integer and FP64 exact-distance work); "
                              "see distance_evals_per_s"},
         "clocks": clocks.summary(),
@@ -413,7 +414,8 @@ def run_kopt(args, ctx, stream, device, world):
                     "api": "cee_kopt_costs_multi (host buffers)"},
             "roofline": {"kernel": "kopt_cost_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
-                         "traffic": load_traffic().get("kopt_cost_kernel"), "algorithmic_bytes_per_launch": alg_bytes}}
+                         "traffic": load_traffic().get("kopt_cost_kernel"), "traffic_unit": "DRAM bytes per launch (ncu)",
+                         "algorithmic_bytes_per_launch": alg_bytes}}
 
 
 def _pinned_pool(count: int, nbytes: int):

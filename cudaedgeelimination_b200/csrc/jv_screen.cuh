@@ -17,8 +17,10 @@
 //     compare-exchange chain; N(b) is filtered against N(a) by a merge walk over the two
 //     sorted rows; the witness scan is the sequential early-exit loop. Few instructions per
 //     edge; lanes of a warp diverge on loop lengths.
-//   * jv_screen_warp_kernel, one warp per edge: the lanes score up to 32 candidates at once and
-//     keep the top-10 as a warp-wide bitonic-sorted list; the witness search tests the first
+//   * jv_screen_warp_kernel, one warp per edge: the lanes score up to 32 candidates at once (when
+//     N(a) and N(b) fit one round, a node of N(b) already in N(a) is found by matching lane
+//     values, otherwise by a binary search of row a) and keep the top-10 as a warp-wide
+//     bitonic-sorted list; the witness search tests the first
 //     three neighbours of all ten candidates at once, then flattens the remaining pairs of the
 //     still-open candidates over the lanes, accepting a candidate only once all of its pairs
 //     are tested and every earlier candidate is closed (so the sequential choice is kept).

@@ -10,19 +10,29 @@
 // holding the same node, and every port pair p < q to the pair index of its class pair
 // (min, max), its code. Two added edges are the same node pair iff their codes are equal; an
 // added edge is a self loop iff its two classes are equal and re-adds a deleted edge iff its
-// code is a deleted edge's code. So each port pair gets a one-hot 64-bit mask (bit = code, or
-// bit 63 when the pair is a self loop or a deleted edge), and a template is valid iff the OR of
-// its k masks has bit 63 clear and exactly k bits set. Rows whose 2k ports are distinct nodes
-// need no masks: a proper template never pairs 2e with 2e+1, so all their cells are plain sums
-// (a caller template that does is marked in its pair table and yields invalid cells).
+// code is a deleted edge's code ("bad" pairs). Two pairs of one template can share a code only
+// if both classes of that code hold two or more ports (pairs through a one-port class share that
+// port, and a matching uses each port once): with 2k <= 10 ports there are at most C(5,2) = 10
+// such "multi" codes. Rows whose 2k ports are distinct nodes have no bad pair and no shared code
+// (a proper template never pairs 2e with 2e+1; a caller template that does is marked in its
+// pair table and yields invalid cells).
+//
+// Narrow coordinates (span < 2^26, each distance < 2^26.5): a pair's entry is one 64-bit word,
+// low half = its distance, or 2^29 when the pair is bad; high half = 1 << 3f when its code is
+// the f-th multi code of the row, else 0. A cell adds its k entries: the low half is the cost
+// (< 5 * 2^26.5 < 2^29 unless a bad pair is present; < 2^32 always), each 3-bit field of the
+// high half counts the template's pairs on one multi code (<= 5), and the cell is invalid iff
+// low >= 2^29 or some field is >= 2. Wide coordinates keep int32 distances and a one-hot 64-bit
+// mask per pair (bit = code, bit 63 = bad): invalid iff the OR of the k masks has bit 63 set or
+// fewer than k bits.
 //
 // B200 mapping: a block owns a tile of consecutive rows of one segment (one k; the tile
 // routine is compiled per k so the per-row work is fully unrolled).
 //   A. the tile's ports are staged in shared memory (one thread per port);
-//   B. one thread per row finds the port classes, whether the row repeats a node and the
-//      row's deleted-code set;
+//   B. one thread per row finds the port classes, whether the row repeats a node, the rank of
+//      each port's class among the multi classes and the row's deleted-code set;
 //   C. one thread per (row, port pair) computes the pair's exact distance (k(2k-1) pairs, at
-//      most 45, instead of k distances per cell) and, for rows that repeat a node, its mask;
+//      most 45, instead of k distances per cell) and its entry (narrow) or mask (wide);
 //   D. thread j owns template t = j mod T with its k pair indices in registers and walks rows
 //      j / T, j / T + B / T, ... (B = 416 threads: 104 rows of k = 3, 16 rows of k = 4, two
 //      rows of k = 5 per step); the threads of a step write one contiguous run of row-major
@@ -39,7 +49,9 @@ constexpr int kKoptMaxPairs = 45;          // k(2k-1) for k = 5
 constexpr int kKoptMaxTemplates = 208;     // proper 5-opt templates
 constexpr int kKoptSmemBytes = 96 * 1024;  // dynamic shared memory cap per block (opted in above 48 KB)
 constexpr int kKoptMaxSegments = 8;
-constexpr uint64_t kKoptBadPair = uint64_t{1} << 63;
+constexpr uint64_t kKoptBadPair = uint64_t{1} << 63;     // wide masks
+constexpr uint32_t kKoptBadCost = uint32_t{1} << 29;      // narrow entries: cost of a bad pair
+constexpr uint32_t kKoptSharedCode = 0x36DB6DB6u;         // bits 1 and 2 of ten 3-bit fields
 // First pair index of a template that pairs some port 2e with 2e + 1 (re-adds deleted edge e,
 // so every cell is invalid); proper templates never do.
 constexpr uint8_t kKoptReaddsDeleted = 0xff;
@@ -70,11 +82,12 @@ struct KoptLaunch {
 
 // Shared-memory tile: 8-byte arrays first, then 4-byte, then bytes.
 struct KoptSmem {
-  uint64_t* mask;     // rows * npairs (rows that repeat a node)
+  uint64_t* mask;     // rows * npairs: packed entries (narrow) or one-hot masks (wide, repeating rows)
   uint64_t* delmask;  // rows: one-hot codes of the deleted edges
   int32_t* ports;     // rows * ports: node ids
-  int32_t* dist;      // rows * npairs
+  int32_t* dist;      // rows * npairs (wide)
   uint8_t* cls;       // rows * ports
+  uint8_t* mrank;     // rows * ports: rank of the port's class among the multi classes, or 0xff
   uint8_t* repeats;   // rows: 1 when the row repeats a node
   uint8_t* pp;        // npairs: first port of each pair
   uint8_t* pq;        // npairs: second port
@@ -83,7 +96,7 @@ struct KoptSmem {
 
 __host__ __device__ constexpr int kopt_tile_smem(int k, int rows) {
   const int ports = 2 * k, npairs = k * (ports - 1);
-  const int bytes = rows * ports + rows + 2 * npairs + ports * ports;
+  const int bytes = 2 * rows * ports + rows + 2 * npairs + ports * ports;
   return rows * npairs * 8 + rows * 8 + rows * ports * 4 + rows * npairs * 4 + ((bytes + 15) & ~15);
 }
 
@@ -95,7 +108,8 @@ __device__ __forceinline__ KoptSmem kopt_carve(unsigned char* base, int k, int r
   s.ports = reinterpret_cast<int32_t*>(s.delmask + rows);
   s.dist = s.ports + rows * ports;
   s.cls = reinterpret_cast<uint8_t*>(s.dist + rows * npairs);
-  s.repeats = s.cls + rows * ports;
+  s.mrank = s.cls + rows * ports;
+  s.repeats = s.mrank + rows * ports;
   s.pp = s.repeats + rows;
   s.pq = s.pp + npairs;
   s.ctab = s.pq + npairs;
@@ -121,28 +135,44 @@ __device__ __forceinline__ void kopt_tables(uint8_t* pp, uint8_t* pq, uint8_t* c
   }
 }
 
-// Stage B for one row: port classes (first port with the same node), the repeat flag and the
-// one-hot codes of the deleted edges.
+// Stage B for one row: port classes (first port with the same node), the repeat flag, the rank
+// of each port's class among the multi classes (classes of two or more ports) and the one-hot
+// codes of the deleted edges.
 template <int K>
-__device__ __forceinline__ void kopt_row_classes(const int32_t* nodes, const uint8_t* ctab, uint8_t* cls,
+__device__ __forceinline__ void kopt_row_classes(const int32_t* nodes, const uint8_t* ctab, uint8_t* cls, uint8_t* mrank,
                                                  uint8_t* repeats, uint64_t* delmask) {
   constexpr int P = 2 * K;
   int32_t nd[P];
 #pragma unroll
   for (int p = 0; p < P; ++p) nd[p] = nodes[p];
   int c[P];
+  bool multi[P];
   bool rep = false;
 #pragma unroll
   for (int p = 0; p < P; ++p) {
     int cp = p;
+    bool shared = false;
 #pragma unroll
-    for (int q = p - 1; q >= 0; --q) cp = nd[q] == nd[p] ? q : cp;
+    for (int q = P - 1; q >= 0; --q) {
+      if (q != p && nd[q] == nd[p]) {
+        shared = true;
+        if (q < p) cp = q;
+      }
+    }
     c[p] = cp;
-    rep = rep || cp != p;
+    multi[p] = shared;
+    rep = rep || shared;
     cls[p] = static_cast<uint8_t>(cp);
   }
   uint64_t dm = 0;
   if (rep) {
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      int rank = 0;  // multi classes whose first port precedes this port's class
+#pragma unroll
+      for (int q = 0; q < P; ++q) rank += (q < c[p] && c[q] == q && multi[q]) ? 1 : 0;
+      mrank[p] = multi[p] ? static_cast<uint8_t>(rank) : 0xff;
+    }
 #pragma unroll
     for (int e = 0; e < K; ++e) {
       const int code = ctab[c[2 * e] * P + c[2 * e + 1]];
@@ -153,7 +183,7 @@ __device__ __forceinline__ void kopt_row_classes(const int32_t* nodes, const uin
   *delmask = dm;
 }
 
-// Stage C for one (row, pair): the exact distance and, when the row repeats a node, the mask.
+// Stage C for one (row, pair): the exact distance and the pair's entry (narrow) or mask (wide).
 template <int K, bool kWide>
 __device__ __forceinline__ void kopt_pair_entry(const KoptSmem& sm, int r, int pid, const int2* xy, int32_t dist_type) {
   constexpr int P = 2 * K, NP = K * (P - 1);
@@ -161,12 +191,28 @@ __device__ __forceinline__ void kopt_pair_entry(const KoptSmem& sm, int r, int p
   const int32_t* pr = sm.ports + r * P;
   const int2 a = __ldg(xy + pr[p]);
   const int2 b = __ldg(xy + pr[q]);
-  sm.dist[r * NP + pid] = static_cast<int32_t>(exact_distance<kWide>(a, b, dist_type));
-  if (sm.repeats[r] != 0) {
-    const uint8_t* cr = sm.cls + r * P;
-    const int code = sm.ctab[cr[p] * P + cr[q]];
-    const bool bad = code == 0xff || ((sm.delmask[r] >> code) & 1u) != 0;
-    sm.mask[r * NP + pid] = bad ? kKoptBadPair : uint64_t{1} << code;
+  const uint32_t d = exact_distance<kWide>(a, b, dist_type);
+  if constexpr (kWide) {
+    sm.dist[r * NP + pid] = static_cast<int32_t>(d);
+    if (sm.repeats[r] != 0) {
+      const uint8_t* cr = sm.cls + r * P;
+      const int code = sm.ctab[cr[p] * P + cr[q]];
+      const bool bad = code == 0xff || ((sm.delmask[r] >> code) & 1u) != 0;
+      sm.mask[r * NP + pid] = bad ? kKoptBadPair : uint64_t{1} << code;
+    }
+  } else {
+    uint32_t lo = d, hi = 0;
+    if (sm.repeats[r] != 0) {
+      const uint8_t* cr = sm.cls + r * P;
+      const int code = sm.ctab[cr[p] * P + cr[q]];
+      if (code == 0xff || ((sm.delmask[r] >> code) & 1u) != 0) {
+        lo = kKoptBadCost;
+      } else {
+        const int ra = sm.mrank[r * P + p], rb = sm.mrank[r * P + q];
+        if (ra != 0xff && rb != 0xff) hi = 1u << (3 * kopt_pair_index(min(ra, rb), max(ra, rb), 5));
+      }
+    }
+    sm.mask[r * NP + pid] = (static_cast<uint64_t>(hi) << 32) | lo;
   }
 }
 
@@ -174,26 +220,27 @@ __device__ __forceinline__ void kopt_pair_entry(const KoptSmem& sm, int r, int p
 template <int K, bool kWide>
 __device__ __forceinline__ int64_t kopt_cell(const KoptSmem& sm, int r, const int (&pid)[K]) {
   constexpr int NP = K * (2 * K - 1);
-  const int32_t* dr = sm.dist + r * NP;
-  int64_t v;
   if constexpr (kWide) {
-    v = 0;
+    const int32_t* dr = sm.dist + r * NP;
+    int64_t v = 0;
 #pragma unroll
     for (int i = 0; i < K; ++i) v += dr[pid[i]];
-  } else {  // coordinate span < 2^26: each distance < 2^26.5, so k <= 5 of them sum below 2^31
-    int32_t s = 0;
+    if (sm.repeats[r] != 0) {
+      const uint64_t* mr = sm.mask + r * NP;
+      uint64_t m = 0;
 #pragma unroll
-    for (int i = 0; i < K; ++i) s += dr[pid[i]];
-    v = s;
-  }
-  if (sm.repeats[r] != 0) {
-    const uint64_t* mr = sm.mask + r * NP;
-    uint64_t m = 0;
+      for (int i = 0; i < K; ++i) m |= mr[pid[i]];
+      if ((m & kKoptBadPair) != 0 || __popcll(m) != K) v = INT64_MAX;
+    }
+    return v;
+  } else {
+    const uint64_t* er = sm.mask + r * NP;
+    uint64_t acc = 0;
 #pragma unroll
-    for (int i = 0; i < K; ++i) m |= mr[pid[i]];
-    if ((m & kKoptBadPair) != 0 || __popcll(m) != K) v = INT64_MAX;
+    for (int i = 0; i < K; ++i) acc += er[pid[i]];
+    const uint32_t lo = static_cast<uint32_t>(acc), hi = static_cast<uint32_t>(acc >> 32);
+    return (lo >= kKoptBadCost || (hi & kKoptSharedCode) != 0) ? INT64_MAX : static_cast<int64_t>(lo);
   }
-  return v;
 }
 
 template <int K, bool kWide>
@@ -214,7 +261,7 @@ __device__ __forceinline__ void kopt_tile(const KoptLaunch& L, const KoptSegment
   }
   __syncthreads();
   for (int r = tid; r < rows; r += kKoptThreads) {
-    kopt_row_classes<K>(sm.ports + r * P, sm.ctab, sm.cls + r * P, sm.repeats + r, sm.delmask + r);
+    kopt_row_classes<K>(sm.ports + r * P, sm.ctab, sm.cls + r * P, sm.mrank + r * P, sm.repeats + r, sm.delmask + r);
   }
   __syncthreads();
   for (int i = tid; i < rows * NP; i += kKoptThreads) {
@@ -240,7 +287,7 @@ __device__ __forceinline__ void kopt_tile(const KoptLaunch& L, const KoptSegment
 }
 
 template <bool kWide>
-static __global__ void __launch_bounds__(kKoptThreads) kopt_cost_kernel(KoptLaunch L,
+static __global__ void __launch_bounds__(kKoptThreads, 4) kopt_cost_kernel(KoptLaunch L,
                                                                         int32_t* __restrict__ error) {
   extern __shared__ __align__(16) unsigned char smem[];
   int si = 0;

@@ -75,7 +75,7 @@ constexpr int kServeLostWord = 2 * kServeMaxSlots;
 __host__ __device__ constexpr int serve_rows_per_chunk(int k) { return k == 3 ? 8 : (k == 4 ? 4 : 2); }
 
 // One warp's k-opt tile (kopt_cost.cuh's layout), sized for the largest chunk of any k.
-constexpr int kServeKoptScratch = 1856;
+constexpr int kServeKoptScratch = 1936;
 static_assert(kopt_tile_smem(3, serve_rows_per_chunk(3)) <= kServeKoptScratch, "k = 3 chunk tile");
 static_assert(kopt_tile_smem(4, serve_rows_per_chunk(4)) <= kServeKoptScratch, "k = 4 chunk tile");
 static_assert(kopt_tile_smem(5, serve_rows_per_chunk(5)) <= kServeKoptScratch, "k = 5 chunk tile");
@@ -104,7 +104,8 @@ __device__ void kopt_rows_warp(const ServeSegment& S, int64_t row_begin, int64_t
     }
     __syncwarp();
     if (lane < rows) {
-      kopt_row_classes<K>(sm.ports + lane * P, sm.ctab, sm.cls + lane * P, sm.repeats + lane, sm.delmask + lane);
+      kopt_row_classes<K>(sm.ports + lane * P, sm.ctab, sm.cls + lane * P, sm.mrank + lane * P, sm.repeats + lane,
+                          sm.delmask + lane);
     }
     __syncwarp();
     for (int i = lane; i < rows * NP; i += 32) {
