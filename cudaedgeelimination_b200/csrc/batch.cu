@@ -25,7 +25,7 @@ struct BatchState {
   int32_t flag_words = 0;
   std::vector<int64_t> node_begin, edge_begin;
   // the union snapshot in the kernels' layout
-  DevBuf d_node_begin, d_edge_begin, xy, uv, w32, active, ro, nbr, ids, slotw;
+  DevBuf d_node_begin, d_edge_begin, xy, uv, w32, active, ro, nbr, ids, slot4;
   // raw uploads of the end-to-end call (converted on the device)
   DevBuf raw_x, raw_y, raw_u, raw_v, raw_w;
   // outputs and work-queue state
@@ -45,7 +45,7 @@ struct BatchState {
   }
   void Release() {
     ReleaseGraph();
-    for (DevBuf* b : {&d_node_begin, &d_edge_begin, &xy, &uv, &w32, &active, &ro, &nbr, &ids, &slotw, &raw_x, &raw_y,
+    for (DevBuf* b : {&d_node_begin, &d_edge_begin, &xy, &uv, &w32, &active, &ro, &nbr, &ids, &slot4, &raw_x, &raw_y,
                       &raw_u, &raw_v, &raw_w, &witness, &target_ids, &target_count, &nbhd, &flags, &counter, &ready}) {
       b->Release();
     }
@@ -74,7 +74,7 @@ uint64_t BatchResident(const cee_ctx* ctx) {
   if (s == nullptr) return 0;
   uint64_t bytes = 0;
   for (const DevBuf* b : {&s->d_node_begin, &s->d_edge_begin, &s->xy, &s->uv, &s->w32, &s->active, &s->ro, &s->nbr,
-                          &s->ids, &s->slotw, &s->raw_x, &s->raw_y, &s->raw_u, &s->raw_v, &s->raw_w, &s->witness,
+                          &s->ids, &s->slot4, &s->raw_x, &s->raw_y, &s->raw_u, &s->raw_v, &s->raw_w, &s->witness,
                           &s->target_ids, &s->target_count, &s->nbhd, &s->flags, &s->counter, &s->ready}) {
     bytes += b->capacity;
   }
@@ -147,7 +147,7 @@ int ReserveAll(cee_ctx* ctx, BatchState& s) {
   const std::pair<DevBuf*, size_t> wants[] = {
       {&s.d_node_begin, (I + 1) * 8}, {&s.d_edge_begin, (I + 1) * 8}, {&s.xy, n * 8}, {&s.uv, m * 8},
       {&s.w32, m * 4}, {&s.active, m}, {&s.ro, (n + 1) * 4}, {&s.nbr, adj * 4}, {&s.ids, adj * 4},
-      {&s.slotw, adj * 4}, {&s.witness, m * 4}, {&s.target_ids, I * T * 4}, {&s.target_count, I * 4},
+      {&s.slot4, adj * 16}, {&s.witness, m * 4}, {&s.target_ids, I * T * 4}, {&s.target_count, I * 4},
       {&s.nbhd, I * T * NB * 4}, {&s.flags, I * T * static_cast<size_t>(s.flag_words) * 4},
       {&s.counter, kMaxChunks * 8}, {&s.ready, I * 4}};
   for (const auto& [buf, bytes] : wants) {
@@ -181,7 +181,8 @@ BatchArgs MakeArgs(cee_ctx* ctx, BatchState& s, int32_t first, int32_t count, in
   A.g.active = static_cast<const uint8_t*>(s.active.ptr);
   A.g.row_offsets = static_cast<const int32_t*>(s.ro.ptr);
   A.g.nbr = static_cast<const int32_t*>(s.nbr.ptr);
-  A.g.slot_w = static_cast<const int32_t*>(s.slotw.ptr);
+  A.g.slot_w = nullptr;
+  A.g.slot4 = static_cast<const int4*>(s.slot4.ptr);
   A.node_begin = static_cast<const int64_t*>(s.d_node_begin.ptr);
   A.edge_begin = static_cast<const int64_t*>(s.d_edge_begin.ptr);
   A.first_instance = first;
@@ -243,18 +244,19 @@ int Capture(cee_ctx* ctx, BatchState& s) {
   return CEE_OK;
 }
 
-// slot_w[s] = edge_w[ids[s]] over slots [s0, s1); bad ids are recorded and read as 0.
-__global__ void batch_gather(const int32_t* __restrict__ ids, int64_t s0, int64_t s1, const int32_t* __restrict__ w32,
-                             int64_t m, int32_t* __restrict__ slotw, int32_t* __restrict__ error) {
+// slot4[s] = {nbr[s], edge_w[ids[s]], xy[nbr[s]]} over slots [s0, s1) (the JV screen's one-load
+// view of a CSR slot); bad ids or neighbours are recorded and read as zeros.
+__global__ void batch_gather(const int32_t* __restrict__ ids, const int32_t* __restrict__ nbr, const int2* __restrict__ xy,
+                             int64_t s0, int64_t s1, const int32_t* __restrict__ w32, int64_t m, int64_t n,
+                             int4* __restrict__ slot4, int32_t* __restrict__ error) {
   for (int64_t s = s0 + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; s < s1;
        s += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int32_t id = ids[s];
-    if (static_cast<uint64_t>(static_cast<uint32_t>(id)) >= static_cast<uint64_t>(m)) {
-      atomicOr(error, 2);
-      slotw[s] = 0;
-    } else {
-      slotw[s] = __ldg(w32 + id);
-    }
+    const int32_t id = ids[s], c = nbr[s];
+    const bool id_ok = static_cast<uint64_t>(static_cast<uint32_t>(id)) < static_cast<uint64_t>(m);
+    const bool c_ok = static_cast<uint64_t>(static_cast<uint32_t>(c)) < static_cast<uint64_t>(n);
+    if (!id_ok || !c_ok) atomicOr(error, 2);
+    const int2 p = c_ok ? xy[c] : make_int2(0, 0);
+    slot4[s] = make_int4(c_ok ? c : 0, id_ok ? __ldg(w32 + id) : 0, p.x, p.y);
   }
 }
 
@@ -354,8 +356,8 @@ int cee_batch_prepare(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opt
   cudaMemsetAsync(ctx->d_error, 0, sizeof(int32_t), st);
   if (g.adjacency > 0) {
     batch_gather<<<GridFor(g.adjacency, 256, ctx->sm_count * 8), 256, 0, st>>>(
-        static_cast<const int32_t*>(s.ids.ptr), 0, g.adjacency, static_cast<const int32_t*>(s.w32.ptr), g.m,
-        static_cast<int32_t*>(s.slotw.ptr), ctx->d_error);
+        static_cast<const int32_t*>(s.ids.ptr), static_cast<const int32_t*>(s.nbr.ptr), static_cast<const int2*>(s.xy.ptr),
+        0, g.adjacency, static_cast<const int32_t*>(s.w32.ptr), g.m, g.n, static_cast<int4*>(s.slot4.ptr), ctx->d_error);
   }
   cudaError_t status = cudaStreamSynchronize(st);  // host staging vectors die at return
   if (status != cudaSuccess) return CudaFail(ctx, status, "batch upload");
@@ -575,8 +577,8 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
         static_cast<int32_t*>(s.w32.ptr), ctx->d_error);
     if (s1 > s0) {
       batch_gather<<<GridFor(s1 - s0, 256, ctx->sm_count * 8), 256, 0, cs>>>(
-          static_cast<const int32_t*>(s.ids.ptr), s0, s1, static_cast<const int32_t*>(s.w32.ptr), g.m,
-          static_cast<int32_t*>(s.slotw.ptr), ctx->d_error);
+          static_cast<const int32_t*>(s.ids.ptr), static_cast<const int32_t*>(s.nbr.ptr), static_cast<const int2*>(s.xy.ptr),
+          s0, s1, static_cast<const int32_t*>(s.w32.ptr), g.m, g.n, static_cast<int4*>(s.slot4.ptr), ctx->d_error);
     }
     rc = LaunchRange(ctx, s, i0, i1 - i0, c, cs);
     if (rc != CEE_OK) return rc;

@@ -76,6 +76,21 @@ __device__ __forceinline__ uint64_t warp_sort_asc(uint64_t key, int lane) {
   return key;
 }
 
+// The same network on 32-bit keys.
+__device__ __forceinline__ uint32_t warp_sort_asc32(uint32_t key, int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const uint32_t other = __shfl_xor_sync(kFullMask, key, j);
+      const bool ascending = (lane & k) == 0;
+      const bool lower = (lane & j) == 0;
+      key = (lower == ascending) ? min(key, other) : max(key, other);
+    }
+  }
+  return key;
+}
+
 // Given two ascending warp-wide lists, returns the 32 smallest keys of their union,
 // ascending (min against the reversed second list yields a bitonic sequence holding them;
 // one bitonic merge pass sorts it).

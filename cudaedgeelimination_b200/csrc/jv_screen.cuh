@@ -46,6 +46,7 @@ struct JvGraph {
   const int32_t* __restrict__ row_offsets;  // [n + 1]
   const int32_t* __restrict__ nbr;          // [adjacency], rows ascending
   const int32_t* __restrict__ slot_w;       // [adjacency], weight of the CSR slot's edge
+  const int4* __restrict__ slot4;           // [adjacency] {neighbour, slot weight, x, y} (batched screen)
 };
 
 // ------------------------------------------------------------------ thread per edge -----
@@ -157,8 +158,9 @@ struct JvWarpScratch {
   uint32_t cbc[kJvMaxCandidates];   // C(b, c)
 };
 
-// Screens edge e with the calling (full) warp; returns the witness or -1 on every lane.
-template <bool kWide>
+// Screens edge e with the calling (full) warp; returns the witness or -1 on every lane. With
+// kSlot4 a CSR slot's neighbour, weight and neighbour coordinates come from one 16-byte load.
+template <bool kWide, bool kSlot4 = false>
 __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t e, JvWarpScratch& s,
                                                        int lane, int32_t* __restrict__ error) {
   if (__ldg(g.active + e) == 0) return -1;
@@ -178,10 +180,18 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
     uint64_t key = kEmptyKey;
     const bool second = i >= da;
     const int32_t slot = second ? rb0 + (i - da) : ra0 + i;
-    int32_t c = -1;
+    int32_t c = -1, sw = 0;
+    int2 pc = make_int2(0, 0);
     bool ok = false;
     if (i < total) {
-      c = __ldg(g.nbr + slot);
+      if constexpr (kSlot4) {
+        const int4 si = __ldg(g.slot4 + slot);
+        c = si.x;
+        sw = si.y;
+        pc = make_int2(si.z, si.w);
+      } else {
+        c = __ldg(g.nbr + slot);
+      }
       ok = c != a && c != b;
       if (ok && static_cast<uint32_t>(c) >= static_cast<uint32_t>(g.n)) {
         atomicOr(error, 1);
@@ -196,10 +206,32 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
     } else if (ok && second) {
       ok = !row_contains(g.nbr, ra0, ra1, c);
     }
+    uint64_t score = 0;
     if (ok) {
-      const uint64_t score = static_cast<uint64_t>(static_cast<uint32_t>(__ldg(g.slot_w + slot))) +
-                             exact_distance<kWide>(__ldg(g.xy + c), second ? pa : pb, g.dist_type);
+      if constexpr (!kSlot4) {
+        sw = __ldg(g.slot_w + slot);
+        pc = __ldg(g.xy + c);
+      }
+      score = static_cast<uint64_t>(static_cast<uint32_t>(sw)) + exact_distance<kWide>(pc, second ? pa : pb, g.dist_type);
       key = (score << 32) | static_cast<uint32_t>(c);
+    }
+    if (total <= 32) {
+      // compact keys: (score, node - min node) in 32 bits sort in half the shuffles; used when
+      // every score and the node spread fit (the order is the same as the 64-bit keys')
+      const uint32_t cmin = __reduce_min_sync(kFullMask, ok ? static_cast<uint32_t>(c) : 0xffffffffu);
+      const uint32_t cmax = __reduce_max_sync(kFullMask, ok ? static_cast<uint32_t>(c) : 0u);
+      const uint32_t smax = __reduce_max_sync(kFullMask, ok ? static_cast<uint32_t>(score) : 0u);
+      const bool narrow_scores = __all_sync(kFullMask, (score >> 32) == 0);
+      const uint32_t span = cmax >= cmin ? cmax - cmin : 0u;
+      const int node_bits = span == 0 ? 1 : 32 - __clz(span);
+      if (narrow_scores && node_bits < 31 && smax < (1u << (32 - node_bits)) - 1u) {
+        uint32_t k32 = ok ? (static_cast<uint32_t>(score) << node_bits) | (static_cast<uint32_t>(c) - cmin) : 0xffffffffu;
+        k32 = warp_sort_asc32(k32, lane);
+        top = k32 == 0xffffffffu ? kEmptyKey
+                                 : (static_cast<uint64_t>(k32 >> node_bits) << 32) |
+                                       (cmin + (k32 & ((1u << node_bits) - 1u)));
+        break;  // total <= 32: this was the only round
+      }
     }
     key = warp_sort_asc(key, lane);
     top = base == 0 ? key : warp_merge_smallest(top, key, lane);
@@ -226,14 +258,26 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
   __syncwarp();
 
   auto compatible_pair = [&](int ci, int32_t slot) -> bool {
-    const int32_t d = __ldg(g.nbr + slot);
+    int32_t d, dw;
+    int2 pd;
+    if constexpr (kSlot4) {
+      const int4 si = __ldg(g.slot4 + slot);
+      d = si.x;
+      dw = si.y;
+      pd = make_int2(si.z, si.w);
+    } else {
+      d = __ldg(g.nbr + slot);
+    }
     if (d == a || d == b) return false;
     if (static_cast<uint32_t>(d) >= static_cast<uint32_t>(g.n)) {
       atomicOr(error, 1);
       return false;
     }
-    const int2 pd = __ldg(g.xy + d);
-    const int64_t left = cab + __ldg(g.slot_w + slot);
+    if constexpr (!kSlot4) {
+      pd = __ldg(g.xy + d);
+      dw = __ldg(g.slot_w + slot);
+    }
+    const int64_t left = cab + dw;
     return left <= static_cast<int64_t>(s.cac[ci]) + exact_distance<kWide>(pd, pb, g.dist_type) ||
            left <= static_cast<int64_t>(exact_distance<kWide>(pa, pd, g.dist_type)) + s.cbc[ci];
   };
