@@ -89,6 +89,11 @@ class BatchStats(ctypes.Structure):
                 ("total_ms", ctypes.c_double)]
 
 
+class JvElimStats(ctypes.Structure):
+    _fields_ = [("epochs", ctypes.c_int32), ("committed", ctypes.c_int64), ("total_ms", ctypes.c_double),
+                ("resident_bytes", ctypes.c_uint64)]
+
+
 class ServeConfig(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("slots", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
                 ("idle_ms", ctypes.c_int32)]
@@ -134,6 +139,8 @@ def lib() -> ctypes.CDLL:
             "cee_jv_launch": (ctypes.c_int, [vp]),
             "cee_jv_fetch": (ctypes.c_int, [vp, c_i32p]),
             "cee_jv_screen_noalloc": (ctypes.c_int, [ctypes.POINTER(DeviceGraph), vp, vp]),
+            "cee_jv_eliminate": (ctypes.c_int, [vp, ctypes.POINTER(GraphView), ctypes.c_uint32, c_u8p, c_i32p, c_i32p,
+                                                c_i64p, c_i64p, ctypes.POINTER(JvElimStats)]),
             "cee_kopt_templates": (ctypes.c_int, [ctypes.c_uint32, c_u8p, c_u64p]),
             "cee_kopt_costs": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, c_i64p, c_i64p, ctypes.c_uint32,
                                               c_u8p, ctypes.c_int32, ctypes.c_uint64, vp, ctypes.c_int64, c_i64p,

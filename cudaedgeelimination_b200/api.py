@@ -291,6 +291,25 @@ class Context(BatchMixin, ServeMixin):
         _native.check(self.handle, _native.lib().cee_jv_fetch(self.handle, witness.ctypes.data_as(_native.c_i32p)))
         return witness
 
+    def jv_eliminate(self, graph: GraphSnapshot, max_rounds: int = 100):
+        """JV elimination to a fixed point on the device (cee_jv_eliminate). Returns (final active,
+        witness per eliminated edge or -1, epoch per eliminated edge or -1, active edges before each
+        epoch, edges committed per epoch, stats)."""
+        m = graph.m
+        active = np.empty(m, np.uint8)
+        witness = np.empty(m, np.int32)
+        epoch = np.empty(m, np.int32)
+        before = np.zeros(max_rounds, np.int64)
+        committed = np.zeros(max_rounds, np.int64)
+        stats = _native.JvElimStats()
+        view = graph.view()
+        _native.check(self.handle, _native.lib().cee_jv_eliminate(
+            self.handle, ctypes.byref(view), max_rounds, active.ctypes.data_as(_native.c_u8p),
+            witness.ctypes.data_as(_native.c_i32p), epoch.ctypes.data_as(_native.c_i32p),
+            before.ctypes.data_as(_native.c_i64p), committed.ctypes.data_as(_native.c_i64p), ctypes.byref(stats)))
+        e = stats.epochs
+        return active, witness, epoch, before[:e], committed[:e], stats
+
     # ---- k-opt ----------------------------------------------------------------------
     def kopt_costs(self, graph: GraphSnapshot, table: "KOptReconnectTable", tasks: np.ndarray):
         tasks = np.ascontiguousarray(tasks, dtype=KOPT_TASK_DTYPE)

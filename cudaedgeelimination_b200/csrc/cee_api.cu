@@ -706,6 +706,7 @@ void cee_destroy(cee_ctx* ctx) {
   if (ctx->stream != nullptr) cudaStreamSynchronize(ctx->stream);
   ReleaseServe(ctx);
   ReleaseBatch(ctx);
+  ReleaseEpoch(ctx);
   ctx->jv.Release();
   ctx->kopt.Release();
   ctx->cd.Release();
@@ -738,7 +739,7 @@ int cee_ctx_synchronize(cee_ctx* ctx) {
 uint64_t cee_ctx_resident_bytes(const cee_ctx* ctx) {
   if (ctx == nullptr) return 0;
   return JvResident(ctx->jv) + KoptResident(ctx->kopt) + ctx->cd.xy.capacity + ctx->cd.tasks.capacity +
-         ctx->cd.flags.capacity + BatchResident(ctx) + ServeResident(ctx);
+         ctx->cd.flags.capacity + BatchResident(ctx) + ServeResident(ctx) + EpochResident(ctx);
 }
 
 int cee_ctx_clear(cee_ctx* ctx, unsigned what) {
@@ -750,6 +751,7 @@ int cee_ctx_clear(cee_ctx* ctx, unsigned what) {
   if (what & 4u) ctx->cd.Release();
   if (what & 8u) ReleaseBatch(ctx);
   if (what & 16u) ReleaseServe(ctx);
+  if (what & 32u) ReleaseEpoch(ctx);
   return CEE_OK;
 }
 

@@ -107,6 +107,7 @@ struct CdState {
 
 struct BatchState;
 struct ServeState;
+struct EpochState;
 
 }  // namespace cee
 
@@ -128,6 +129,7 @@ struct cee_ctx {
   cee::CdState cd;
   cee::BatchState* batch = nullptr;
   cee::ServeState* serve = nullptr;
+  cee::EpochState* epoch = nullptr;
 };
 
 namespace cee {
@@ -144,5 +146,7 @@ void ReleaseBatch(cee_ctx* ctx);
 uint64_t BatchResident(const cee_ctx* ctx);
 void ReleaseServe(cee_ctx* ctx, int32_t* error_word = nullptr);
 uint64_t ServeResident(const cee_ctx* ctx);
+void ReleaseEpoch(cee_ctx* ctx);
+uint64_t EpochResident(const cee_ctx* ctx);
 
 }  // namespace cee

@@ -85,7 +85,7 @@ enum cee_option {
 /* Sets a launch-shape option of this context; results never depend on it. */
 int cee_ctx_set_option(cee_ctx* ctx, int32_t option, int64_t value);
 /* Frees cached device state: bit 1 = JV, bit 2 = k-opt, bit 4 = c,d, bit 8 = batch,
- * bit 16 = serving loop (stops it; its jobs are dropped).
+ * bit 16 = serving loop (stops it; its jobs are dropped), bit 32 = JV epoch loop workspace.
  * Replaces ClearJvCudaCache (include/cuda_edge_elimination/elimination.hpp:338) and
  * ClearKOptCostCudaCache (include/cuda_edge_elimination/local_search.hpp:242). */
 int cee_ctx_clear(cee_ctx* ctx, unsigned what);
@@ -178,6 +178,27 @@ typedef struct {
  * be serialised by the caller. The snapshot is validated on the device first (CEE_ERR_INVALID
  * on failure); errors are reported through cee_last_error(NULL). */
 int cee_jv_screen_noalloc(const cee_device_graph* graph, int32_t* witness_out, void* stream);
+
+/* ---- JV elimination to a fixed point, device resident ------------------------------------ */
+
+typedef struct {
+  int32_t epochs;          /* epochs run (the last one commits nothing unless max_rounds stopped it) */
+  int64_t committed;       /* edges eliminated in total */
+  double total_ms;         /* wall time of the call */
+  uint64_t resident_bytes; /* device workspace of the epoch loop */
+} cee_jv_elim_stats;
+
+/* RunJvElimination's epoch loop (src/cpu/jv_elimination.cpp:250-322) without the host in the
+ * loop: screen, commit gate (CommitVerifiedCandidates, src/cpu/elimination_commit.cpp:13-76) and CSR
+ * rebuild (GraphSnapshot::RebuildCsr, src/common/graph.cpp:230-282) all on the device, until an
+ * epoch commits nothing or max_rounds epochs ran. Edges must be unique canonical pairs (u < v), as
+ * the reference's edge files are. Outputs per edge: active_out (final flag), epoch_out (epoch that
+ * eliminated it or -1), witness_out (its witness or -1); per epoch (capacity max_rounds): active
+ * edges before the epoch and edges committed. The reference's CPU re-verification and proof log
+ * stay with the caller (the outputs give every record: epoch, edge, witness). */
+int cee_jv_eliminate(cee_ctx* ctx, const cee_graph_view* graph, uint32_t max_rounds, uint8_t* active_out,
+                     int32_t* witness_out, int32_t* epoch_out, int64_t* epoch_edges_before,
+                     int64_t* epoch_committed, cee_jv_elim_stats* stats);
 
 /* ---- k-opt leaf cost matrix ----------------------------------------------------------- */
 
