@@ -58,7 +58,8 @@ def parse():
     p.add_argument("--no-kopt", action="store_true")
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--serve-jobs", type=int, default=10_000)
-    p.add_argument("--part", default="all", choices=["all", "batch", "kopt", "serve"],
+    p.add_argument("--no-epochs", action="store_true")
+    p.add_argument("--part", default="all", choices=["all", "batch", "kopt", "serve", "epochs"],
                    help="profiling aid: run only the batched screen, the k-opt part or the serving loop")
     p.add_argument("--cpu-budget-s", type=float, default=12.0)
     return p.parse_args()
@@ -228,6 +229,8 @@ def run_ours(args, rank: int, world: int, device: int):
         return out
     if args.part == "serve":
         return run_serve(args, device, world)
+    if args.part == "epochs":
+        return run_fixed_point(args, device)
     from cudaedgeelimination_b200.api import BatchOptions
     batch = synth.BatchUnion(args.instances)
     g = batch.graph
@@ -356,6 +359,8 @@ def run_ours(args, rank: int, world: int, device: int):
         result["kopt"] = run_kopt(args, ctx, stream, device, world)
     if not args.no_serve and args.part == "all":
         result["serve"] = run_serve(args, device, world)
+    if not args.no_epochs and args.part == "all" and rank == 0:
+        result["jv_fixed_point"] = run_fixed_point(args, device)
 
     if rank == 0:
         rate, kind, sample = reference_step_rate(batch, args.cpu_budget_s, os.cpu_count() or 1)
@@ -570,6 +575,39 @@ def run_serve(args, device, world):
                   "on the host",
         "checked_jobs": len(plain_kept),
     }
+
+
+def run_fixed_point(args, device):
+    """JV elimination to a fixed point with every epoch on the device (cee_jv_eliminate), against
+    the reference's own RunJvElimination(kCpu) loop (oracle/_ref) on the same instance."""
+    import oracle
+    from cudaedgeelimination_b200 import Context, synth
+    cases = [("3,000-node clustered (8-NN + quadrant neighbours), EUC_2D", synth.jv_clustered()),
+             ("50,000-node uniform in [0,10^7)^2, 10-NN, EUC_2D", synth.uniform_knn(50_000, 10_000_000, 10, 0, 7))]
+    ctx = Context(device)
+    ref = oracle.Reference() if oracle.reference_available() else None
+    out = []
+    for name, g in cases:
+        ctx.jv_eliminate(g)  # warm-up (allocations, module load)
+        t0 = time.perf_counter()
+        active, witness, epoch, before, committed, stats = ctx.jv_eliminate(g)
+        wall = time.perf_counter() - t0
+        screened = int(before.sum())
+        row = {"workload": name, "nodes": g.n, "edges": g.m, "epochs": int(stats.epochs),
+               "eliminated": int(stats.committed), "ms": wall * 1e3, "edges_screened_per_s": screened / wall,
+               "api": "cee_jv_eliminate (upload, every epoch on the device, download)"}
+        if ref is not None:
+            rg = ref.graph(g)
+            t0 = time.perf_counter()
+            rstats, records, _, _ = rg.run_jv(1)
+            rwall = time.perf_counter() - t0
+            assert np.array_equal(rg.active(), active) and np.array_equal(rstats[:, 2], committed)
+            row["reference_cpu"] = {"ms": rwall * 1e3, "edges_screened_per_s": screened / rwall, "cores": 1,
+                                    "api": "RunJvElimination(kCpu): screen, CPU verify, commit, hash per epoch"}
+            row["speedup_vs_reference"] = rwall / wall
+        out.append(row)
+    ctx.close()
+    return out
 
 
 # ---------------------------------------------------------------- plumbing ----------------
