@@ -149,6 +149,10 @@ def lib() -> ctypes.CDLL:
                                                     ctypes.c_int32, ctypes.POINTER(ctypes.c_uint32),
                                                     ctypes.POINTER(vp), c_i64p, ctypes.POINTER(vp),
                                                     ctypes.POINTER(KoptStats)]),
+            "cee_kopt_improving_multi": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, c_i64p, c_i64p,
+                                                        ctypes.c_int32, ctypes.POINTER(ctypes.c_uint32),
+                                                        ctypes.POINTER(vp), c_i64p, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                                        ctypes.POINTER(vp), ctypes.POINTER(KoptStats)]),
             "cee_kopt_prepare_multi": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, c_i64p, c_i64p,
                                                       ctypes.c_int32, ctypes.POINTER(ctypes.c_uint32),
                                                       ctypes.POINTER(vp), c_i64p, ctypes.POINTER(KoptStats)]),

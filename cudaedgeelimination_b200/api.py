@@ -345,6 +345,26 @@ class Context(BatchMixin, ServeMixin):
             optr, ctypes.byref(stats)))
         return outs, stats
 
+    def kopt_improving_multi(self, graph: GraphSnapshot, ks, task_lists, with_costs: bool = False):
+        """Fused leaf consume (cee_kopt_improving_multi): per segment the improving-template bit
+        masks [rows, ceil(T/32)] uint32, the first improving template per row (-1: none) and, with
+        with_costs, the full cost matrix."""
+        tasks, karr, tptr, rows = self._multi_args(ks, task_lists)
+        words = [(KOPT_TEMPLATE_COUNTS[k] + 31) // 32 for k in ks]
+        masks = [np.empty((int(r), w), np.uint32) for r, w in zip(rows, words)]
+        firsts = [np.empty(int(r), np.int32) for r in rows]
+        costs = [np.empty((int(r), KOPT_TEMPLATE_COUNTS[k]), np.int64) for k, r in zip(ks, rows)] if with_costs else None
+        n = len(ks)
+        mptr = (ctypes.c_void_p * n)(*[a.ctypes.data for a in masks])
+        fptr = (ctypes.c_void_p * n)(*[a.ctypes.data for a in firsts])
+        cptr = (ctypes.c_void_p * n)(*[a.ctypes.data for a in costs]) if with_costs else None
+        stats = _native.KoptStats()
+        _native.check(self.handle, _native.lib().cee_kopt_improving_multi(
+            self.handle, graph.n, graph.dist_type, graph.x.ctypes.data_as(_native.c_i64p),
+            graph.y.ctypes.data_as(_native.c_i64p), n, karr, tptr, rows.ctypes.data_as(_native.c_i64p),
+            mptr, fptr, cptr, ctypes.byref(stats)))
+        return masks, firsts, costs, stats
+
     def kopt_prepare_multi(self, graph: GraphSnapshot, ks, task_lists) -> _native.KoptStats:
         tasks, karr, tptr, rows = self._multi_args(ks, task_lists)
         stats = _native.KoptStats()

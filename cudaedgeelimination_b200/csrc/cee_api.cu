@@ -161,7 +161,7 @@ uint64_t JvResident(const JvState& s) {
 }
 
 uint64_t KoptResident(const KoptState& s) {
-  uint64_t bytes = s.xy.capacity + s.tasks.capacity + s.costs.capacity;
+  uint64_t bytes = s.xy.capacity + s.tasks.capacity + s.costs.capacity + s.masks.capacity + s.firsts.capacity;
   for (const KoptTable& t : s.user) bytes += t.pairs.capacity;
   for (const KoptTable& t : s.canon) bytes += t.pairs.capacity;
   return bytes;
@@ -536,6 +536,7 @@ int KoptPrepareSegments(cee_ctx* ctx, int32_t segments, const uint32_t* ks, cons
     seg.pairs = static_cast<const uint8_t*>(tables[i]->pairs.ptr);
     seg.k = static_cast<int32_t>(ks[i]);
     seg.templates = tables[i]->T;
+    seg.write_costs = 1;
     seg.rows_per_tile = ctx->kopt_rows_per_tile[ks[i] - 3] > 0 ? ctx->kopt_rows_per_tile[ks[i] - 3]
                                                                 : DefaultRowsPerTile(ks[i]);
     seg.tile_begin = tile;
@@ -565,7 +566,7 @@ int KoptLaunchPrepared(cee_ctx* ctx) {
   if (s.tiles == 0) return CEE_OK;
   int smem = 0;
   for (int32_t i = 0; i < s.segments; ++i) {
-    smem = std::max(smem, kopt_tile_smem(s.launch.seg[i].k, s.launch.seg[i].rows_per_tile));
+    smem = std::max(smem, kopt_tile_smem(s.launch.seg[i].k, s.launch.seg[i].rows_per_tile, s.launch.seg[i].mask_words));
   }
   if (smem > kKoptSmemBytes) return Fail(ctx, CEE_ERR_INVALID, "k-opt tile exceeds shared memory");
   cudaError_t status = cudaSuccess;
@@ -908,6 +909,66 @@ int cee_kopt_fetch(cee_ctx* ctx, int64_t* const* costs_out) {
   if (rc != CEE_OK) return rc;
   if (costs_out == nullptr) return Fail(ctx, CEE_ERR_INVALID, "null k-opt outputs");
   return KoptFetch(ctx, costs_out);
+}
+
+int cee_kopt_improving_multi(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x, const int64_t* y,
+                             int32_t segments, const uint32_t* ks, const cee_kopt_task* const* tasks,
+                             const int64_t* rows, uint32_t* const* masks_out, int32_t* const* first_out,
+                             int64_t* const* costs_out, cee_kopt_stats* stats) {
+  cee_kopt_stats local{};
+  if (masks_out == nullptr || first_out == nullptr) return Fail(ctx, CEE_ERR_INVALID, "null improving-set outputs");
+  int rc = cee_kopt_prepare_multi(ctx, n, dist_type, x, y, segments, ks, tasks, rows, &local);
+  if (rc != CEE_OK) return rc;
+  KoptState& s = ctx->kopt;
+  int64_t words = 0, total_rows = 0;
+  for (int32_t i = 0; i < segments; ++i) {
+    words += rows[i] * ((s.launch.seg[i].templates + 31) / 32);
+    total_rows += rows[i];
+  }
+  cudaError_t status = s.masks.Reserve(static_cast<size_t>(words) * 4 + 16, nullptr);
+  if (status == cudaSuccess) status = s.firsts.Reserve(static_cast<size_t>(total_rows) * 4 + 16, nullptr);
+  if (status != cudaSuccess) return CudaFail(ctx, status, "k-opt improving-set allocation");
+  int64_t word_at = 0, row_at = 0;
+  for (int32_t i = 0; i < segments; ++i) {
+    KoptSegment& seg = s.launch.seg[i];
+    seg.mask_words = (seg.templates + 31) / 32;
+    seg.improving = static_cast<uint32_t*>(s.masks.ptr) + word_at;
+    seg.first = static_cast<int32_t*>(s.firsts.ptr) + row_at;
+    seg.write_costs = costs_out != nullptr && costs_out[i] != nullptr ? 1 : 0;
+    word_at += rows[i] * seg.mask_words;
+    row_at += rows[i];
+  }
+  cudaEventRecord(ctx->ev[2], ctx->stream);
+  rc = KoptLaunchPrepared(ctx);
+  if (rc != CEE_OK) return rc;
+  cudaEventRecord(ctx->ev[3], ctx->stream);
+  int64_t d2h = 0;
+  for (int32_t i = 0; i < segments; ++i) {
+    const KoptSegment& seg = s.launch.seg[i];
+    if (rows[i] == 0) continue;
+    if (masks_out[i] == nullptr || first_out[i] == nullptr) return Fail(ctx, CEE_ERR_INVALID, "null improving-set output");
+    const size_t mb = static_cast<size_t>(rows[i]) * seg.mask_words * 4;
+    cudaMemcpyAsync(masks_out[i], seg.improving, mb, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaMemcpyAsync(first_out[i], seg.first, static_cast<size_t>(rows[i]) * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    d2h += static_cast<int64_t>(mb) + rows[i] * 4;
+    if (seg.write_costs != 0) {
+      const size_t cb = static_cast<size_t>(rows[i]) * seg.templates * 8;
+      cudaMemcpyAsync(costs_out[i], seg.costs, cb, cudaMemcpyDeviceToHost, ctx->stream);
+      d2h += static_cast<int64_t>(cb);
+    }
+  }
+  cudaMemcpyAsync(ctx->h_error, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaEventRecord(ctx->ev[4], ctx->stream);
+  status = cudaEventSynchronize(ctx->ev[4]);
+  if (status != cudaSuccess) return CudaFail(ctx, status, "k-opt improving sets");
+  rc = CheckDeviceError(ctx, "k-opt improving sets");
+  if (rc != CEE_OK) return rc;
+  local.h2d_ms = EventMs(ctx->ev[0], ctx->ev[1]);
+  local.kernel_ms = EventMs(ctx->ev[2], ctx->ev[3]);
+  local.d2h_ms = EventMs(ctx->ev[3], ctx->ev[4]);
+  local.d2h_bytes = d2h;
+  if (stats != nullptr) *stats = local;
+  return CEE_OK;
 }
 
 int cee_kopt_costs_multi(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x, const int64_t* y,

@@ -70,6 +70,7 @@ struct KoptState {
   KoptTable user[3];   // caller templates per k (the reference's template cache)
   KoptTable canon[3];  // this library's proper templates per k
   DevBuf tasks, costs;
+  DevBuf masks, firsts;  // improving-template sets of the fused leaf consume
   KoptLaunch launch{};
   int32_t segments = 0, tiles = 0;
   int64_t seg_rows[kKoptMaxSegments] = {};
@@ -80,6 +81,8 @@ struct KoptState {
     xy.Release();
     tasks.Release();
     costs.Release();
+    masks.Release();
+    firsts.Release();
     for (KoptTable& t : user) t.Release();
     for (KoptTable& t : canon) t.Release();
     has_coords = false;

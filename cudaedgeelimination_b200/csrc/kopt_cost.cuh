@@ -37,6 +37,10 @@
 //      j / T, j / T + B / T, ... (B = 416 threads: 104 rows of k = 3, 16 rows of k = 4, two
 //      rows of k = 5 per step); the threads of a step write one contiguous run of row-major
 //      cells with streaming stores.
+// Fused leaf consume (mask_words > 0): stage D also marks, per row, the templates whose cost is
+// below the row's deleted cost — the templates the reference's leaf consumer tries, in order — in a
+// shared bit mask; the tile then writes the masks and each row's first improving template, and the
+// cost matrix itself becomes optional (write_costs).
 #pragma once
 
 #include "device_common.cuh"
@@ -66,10 +70,14 @@ struct KoptSegment {
   int64_t* __restrict__ costs;        // rows x T
   int64_t rows;
   const uint8_t* __restrict__ pairs;  // T x k pair indices (device)
+  uint32_t* __restrict__ improving;   // rows x mask_words: bit t = template t improves the row
+  int32_t* __restrict__ first;        // rows: first improving template, or -1
   int32_t k;
   int32_t templates;
   int32_t rows_per_tile;
   int32_t tile_begin;                 // first block index of this segment
+  int32_t mask_words;                 // 0: no improving sets (the plain cost matrix)
+  int32_t write_costs;                // 0: improving sets only
 };
 
 struct KoptLaunch {
@@ -92,15 +100,18 @@ struct KoptSmem {
   uint8_t* pp;        // npairs: first port of each pair
   uint8_t* pq;        // npairs: second port
   uint8_t* ctab;      // ports * ports: code of a class pair, 0xff on the diagonal
+  int64_t* deleted;   // rows: deleted cost (improving sets only)
+  uint32_t* imask;    // rows * mask words: improving templates (improving sets only)
 };
 
-__host__ __device__ constexpr int kopt_tile_smem(int k, int rows) {
+__host__ __device__ constexpr int kopt_tile_smem(int k, int rows, int mask_words = 0) {
   const int ports = 2 * k, npairs = k * (ports - 1);
   const int bytes = 2 * rows * ports + rows + 2 * npairs + ports * ports;
-  return rows * npairs * 8 + rows * 8 + rows * ports * 4 + rows * npairs * 4 + ((bytes + 15) & ~15);
+  return rows * npairs * 8 + rows * 8 + rows * ports * 4 + rows * npairs * 4 + ((bytes + 15) & ~15) +
+         (mask_words > 0 ? rows * 8 + rows * mask_words * 4 : 0);
 }
 
-__device__ __forceinline__ KoptSmem kopt_carve(unsigned char* base, int k, int rows) {
+__device__ __forceinline__ KoptSmem kopt_carve(unsigned char* base, int k, int rows, int mask_words = 0) {
   const int ports = 2 * k, npairs = k * (ports - 1);
   KoptSmem s;
   s.mask = reinterpret_cast<uint64_t*>(base);
@@ -113,6 +124,9 @@ __device__ __forceinline__ KoptSmem kopt_carve(unsigned char* base, int k, int r
   s.pp = s.repeats + rows;
   s.pq = s.pp + npairs;
   s.ctab = s.pq + npairs;
+  const int bytes = 2 * rows * ports + rows + 2 * npairs + ports * ports;
+  s.deleted = reinterpret_cast<int64_t*>(reinterpret_cast<unsigned char*>(s.cls) + ((bytes + 15) & ~15));
+  s.imask = reinterpret_cast<uint32_t*>(s.deleted + (mask_words > 0 ? rows : 0));
   return s;
 }
 
@@ -247,9 +261,16 @@ template <int K, bool kWide>
 __device__ __forceinline__ void kopt_tile(const KoptLaunch& L, const KoptSegment& S, int64_t row0, int rows,
                                           unsigned char* smem, int32_t* error) {
   constexpr int P = 2 * K, NP = K * (P - 1);
-  const KoptSmem sm = kopt_carve(smem, K, S.rows_per_tile);
+  const KoptSmem sm = kopt_carve(smem, K, S.rows_per_tile, S.mask_words);
   const int tid = threadIdx.x;
+  const int W = S.mask_words;
   kopt_tables<K>(sm.pp, sm.pq, sm.ctab, tid, kKoptThreads);
+  if (W > 0) {
+    for (int r = tid; r < rows; r += kKoptThreads) {
+      sm.deleted[r] = __ldg(reinterpret_cast<const long long*>(S.tasks + (row0 + r) * 12 + 10));
+    }
+    for (int i = tid; i < rows * W; i += kKoptThreads) sm.imask[i] = 0;
+  }
   for (int i = tid; i < rows * P; i += kKoptThreads) {
     const int r = i / P, p = i - (i / P) * P;
     int32_t node = __ldg(S.tasks + (row0 + r) * 12 + p);
@@ -272,17 +293,31 @@ __device__ __forceinline__ void kopt_tile(const KoptLaunch& L, const KoptSegment
   const int T = S.templates;
   const int per_step = kKoptThreads / T;
   const int rr = tid / T, t = tid - rr * T;
-  if (rr >= per_step) return;
-  int pid[K];
+  if (rr < per_step) {
+    int pid[K];
 #pragma unroll
-  for (int i = 0; i < K; ++i) pid[i] = __ldg(S.pairs + t * K + i);
-  const bool readds_deleted = pid[0] == kKoptReaddsDeleted;
-  if (readds_deleted) pid[0] = 0;
-  long long* out = reinterpret_cast<long long*>(S.costs + row0 * T) + static_cast<int64_t>(rr) * T + t;
-  const int64_t out_step = static_cast<int64_t>(per_step) * T;
-  for (int r = rr; r < rows; r += per_step, out += out_step) {
-    const int64_t v = kopt_cell<K, kWide>(sm, r, pid);
-    __stcs(out, static_cast<long long>(readds_deleted ? INT64_MAX : v));
+    for (int i = 0; i < K; ++i) pid[i] = __ldg(S.pairs + t * K + i);
+    const bool readds_deleted = pid[0] == kKoptReaddsDeleted;
+    if (readds_deleted) pid[0] = 0;
+    long long* out = reinterpret_cast<long long*>(S.costs + row0 * T) + static_cast<int64_t>(rr) * T + t;
+    const int64_t out_step = static_cast<int64_t>(per_step) * T;
+    for (int r = rr; r < rows; r += per_step, out += out_step) {
+      const int64_t v = readds_deleted ? INT64_MAX : kopt_cell<K, kWide>(sm, r, pid);
+      if (S.write_costs != 0) __stcs(out, static_cast<long long>(v));
+      // the leaf consumer tries templates with added cost < deleted cost (src/cpu/kopt_search.cpp:697)
+      if (W > 0 && v < sm.deleted[r]) atomicOr(sm.imask + r * W + (t >> 5), 1u << (t & 31));
+    }
+  }
+  if (W == 0) return;
+  __syncthreads();
+  for (int i = tid; i < rows * W; i += kKoptThreads) S.improving[row0 * W + i] = sm.imask[i];
+  for (int r = tid; r < rows; r += kKoptThreads) {
+    int f = -1;
+    for (int w = W - 1; w >= 0; --w) {
+      const uint32_t bits = sm.imask[r * W + w];
+      if (bits != 0) f = w * 32 + __ffs(bits) - 1;
+    }
+    S.first[row0 + r] = f;
   }
 }
 

@@ -243,6 +243,17 @@ int cee_kopt_costs_multi(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64
                          const int64_t* y, int32_t segments, const uint32_t* ks,
                          const cee_kopt_task* const* tasks, const int64_t* rows,
                          int64_t* const* costs_out, cee_kopt_stats* stats);
+/* Fused leaf consume: for every row the set of templates whose added cost is below the row's
+ * deleted_cost — the templates the reference's leaf consumer tries, in order
+ * (src/cpu/kopt_search.cpp:694-715) — as a bit mask of ceil(T/32) uint32 words per row (bit t of word
+ * t / 32 = template t, the library's proper templates) and the first such template (-1 if none).
+ * costs_out may be NULL (or hold NULL segments): the full matrix is then not written, and only the
+ * masks cross PCIe. */
+int cee_kopt_improving_multi(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x,
+                             const int64_t* y, int32_t segments, const uint32_t* ks,
+                             const cee_kopt_task* const* tasks, const int64_t* rows,
+                             uint32_t* const* masks_out, int32_t* const* first_out,
+                             int64_t* const* costs_out, cee_kopt_stats* stats);
 /* Phases of cee_kopt_costs_multi (prepare = upload, launch = enqueue, fetch = copy back). */
 int cee_kopt_prepare_multi(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x,
                            const int64_t* y, int32_t segments, const uint32_t* ks,

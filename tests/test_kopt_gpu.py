@@ -144,3 +144,36 @@ def test_heavily_repeated_ports(kc, port):
         table = BuildKOptReconnectTable(k)
         gpu, _ = kc.kopt_costs(g, table, tasks)
         np.testing.assert_array_equal(gpu, port.kopt_costs(g, k, tasks))
+
+
+def expected_improving(costs, deleted):
+    """Bit masks and first index of the templates with cost < deleted cost, row by row."""
+    better = costs < deleted[:, None]
+    words = (costs.shape[1] + 31) // 32
+    masks = np.zeros((costs.shape[0], words), np.uint32)
+    for t in range(costs.shape[1]):
+        masks[:, t // 32] |= (better[:, t].astype(np.uint32) << np.uint32(t % 32))
+    first = np.where(better.any(axis=1), better.argmax(axis=1), -1).astype(np.int32)
+    return masks, first
+
+
+@pytest.mark.parametrize("with_costs", [False, True], ids=["masks-only", "with-costs"])
+def test_improving_sets(kc, with_costs):
+    """Fused leaf consume: improving-template masks and first improving template per row equal the
+    ones derived from the full cost matrix (walk rows and rows with shifted deleted costs)."""
+    g, rows = synth.kopt_instance(rows=6000, n=3000)
+    lists = []
+    rng = np.random.default_rng(3)
+    for k in (3, 4, 5):
+        t = rows[k].copy()
+        t["deleted_cost"] += rng.integers(-2000, 2000, t.shape[0])  # a spread of improving and not
+        lists.append(t)
+    full, _ = kc.kopt_costs_multi(g, [3, 4, 5], lists)
+    masks, firsts, costs, stats = kc.kopt_improving_multi(g, [3, 4, 5], lists, with_costs=with_costs)
+    for seg in range(3):
+        want_m, want_f = expected_improving(full[seg], lists[seg]["deleted_cost"])
+        np.testing.assert_array_equal(masks[seg], want_m)
+        np.testing.assert_array_equal(firsts[seg], want_f)
+        if with_costs:
+            np.testing.assert_array_equal(costs[seg], full[seg])
+    assert any((f >= 0).any() for f in firsts) and any((f < 0).any() for f in firsts)
