@@ -407,6 +407,13 @@ def run_kopt(args, ctx, stream, device, world):
     e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps, world)
     for a, b in zip(out_arrays, outs):
         assert (a == b).all()
+    # fused leaf consume: improving-template masks only (the 126 MB matrix never crosses PCIe)
+    masks, firsts, _, lstats = ctx.kopt_improving_multi(g, ks, ptasks)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        masks, firsts, _, lstats = ctx.kopt_improving_multi(g, ks, ptasks)
+    leaf_s = max_over_ranks((time.perf_counter() - t0) / args.steps, world)
+    improving_rows = int(sum(int((f >= 0).sum()) for f in firsts))
     peak, peak_kind = load_peaks()
     alg_bytes = rows * 48 + cells * 8 + 8 * g.n
     achieved = alg_bytes / (ms / 1e3) / 1e9
@@ -417,6 +424,10 @@ def run_kopt(args, ctx, stream, device, world):
             "e2e": {"value": cells * world / e2e_s, "unit": "cells/s", "ms_per_step": e2e_s * 1e3,
                     "h2d_bytes_per_step": int(stats.h2d_bytes), "d2h_bytes_per_step": int(stats.d2h_bytes),
                     "api": "cee_kopt_costs_multi (host buffers)"},
+            "leaf_consume": {"value": cells * world / leaf_s, "unit": "cells/s", "ms_per_step": leaf_s * 1e3,
+                             "kernel_ms": lstats.kernel_ms, "d2h_bytes_per_step": int(lstats.d2h_bytes),
+                             "rows_with_improving_template": improving_rows,
+                             "api": "cee_kopt_improving_multi (host rows in, improving-template masks out)"},
             "roofline": {"kernel": "kopt_cost_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
                          "traffic": load_traffic().get("kopt_cost_kernel"), "traffic_unit": "DRAM bytes per launch (ncu)",
