@@ -79,6 +79,11 @@ class Port:
                                     ctypes.c_int32, u8p]
         L.ceo_ht_targets.restype = ctypes.c_int64
         L.ceo_ht_targets.argtypes = [G, ctypes.c_int32, i32p]
+        L.ceo_ht_reply_count.restype = ctypes.c_int64
+        L.ceo_ht_reply_count.argtypes = [G, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
+        L.ceo_cd_finalize.restype = ctypes.c_int64
+        L.ceo_cd_finalize.argtypes = [G, ctypes.c_int32, ctypes.c_int32, i32p, i32p, u8p, ctypes.c_int64,
+                                      ctypes.c_uint32, i32p, i32p, u64p]
         self.L = L
 
     def graph(self, g) -> CeoGraph:
@@ -192,6 +197,26 @@ class Port:
         out = np.empty(max(1, g.edge_u.shape[0]), np.int32)
         count = self.L.ceo_ht_targets(self.graph(g), order, _p(out, ctypes.c_int32))
         return out[:count].copy()
+
+    def cd_finalize(self, g, u: int, v: int, c, d, flags, max_cd: int = 5) -> np.ndarray:
+        """FinalizeCdCandidates: the flagged (c, d) ranked by (reply product, c, d), first max_cd
+        kept; rows (c, d, product)."""
+        c = np.ascontiguousarray(c, np.int32)
+        d = np.ascontiguousarray(d, np.int32)
+        flags = np.ascontiguousarray(flags, np.uint8)
+        cap = max(1, int(flags.sum()))
+        oc, od = np.empty(cap, np.int32), np.empty(cap, np.int32)
+        op = np.empty(cap, np.uint64)
+        count = self.L.ceo_cd_finalize(self.graph(g), u, v, _p(c, ctypes.c_int32), _p(d, ctypes.c_int32),
+                                       _p(flags, ctypes.c_uint8), c.shape[0], max_cd, _p(oc, ctypes.c_int32),
+                                       _p(od, ctypes.c_int32), _p(op, ctypes.c_uint64))
+        out = np.empty((count, 3), np.int64)
+        out[:, 0], out[:, 1] = oc[:count], od[:count]
+        out[:, 2] = np.minimum(op[:count], np.uint64(np.iinfo(np.int64).max)).astype(np.int64)
+        return out
+
+    def ht_reply_count(self, g, u: int, v: int, center: int) -> int:
+        return int(self.L.ceo_ht_reply_count(self.graph(g), min(u, v), max(u, v), center))
 
 
 def reference_available(dropin: bool = False) -> bool:

@@ -601,6 +601,93 @@ void ceo_cd_screen(const ceo_graph* g, int32_t u, int32_t v, const int32_t* c, c
   }
 }
 
+/* ---- FinalizeCdCandidates: src/cpu/hamilton_tutte.cpp:283-327 ---- */
+
+/* AppendHtHamiltonRepliesUnchecked (:230-269), counted: pairs of neighbours (first < second in
+ * CSR order) of `center` whose edges to the center both survive 2-opt against the target, whose
+ * node pair is not the target, and for which the target plus the two center edges cost no more
+ * than the pair's edge plus the center's two target edges. */
+int64_t ceo_ht_reply_count(const ceo_graph* g, int32_t tu, int32_t tv, int32_t center) {
+  const int32_t begin = g->row_offsets[center], end = g->row_offsets[center + 1];
+  const int32_t deg = end - begin;
+  if (deg < 2) return 0;
+  int64_t* cost = malloc(sizeof(int64_t) * (size_t)deg);
+  int* survives = malloc(sizeof(int) * (size_t)deg);
+  int64_t count = 0;
+  if (cost != NULL && survives != NULL) {
+    for (int32_t i = 0; i < deg; ++i) {
+      const int32_t node = g->neighbors[begin + i];
+      cost[i] = dist_nodes(g, center, node);
+      const int32_t ou = center < node ? center : node, ov = center < node ? node : center;
+      survives[i] = survives_two_opt(g, tu, tv, ou, ov);
+    }
+    const __int128 target_cost = dist_nodes(g, tu, tv);
+    const __int128 center_target = (__int128)dist_nodes(g, tu, center) + dist_nodes(g, tv, center);
+    for (int32_t a = 0; a < deg; ++a) {
+      for (int32_t b = a + 1; b < deg; ++b) {
+        const int32_t na = g->neighbors[begin + a], nb = g->neighbors[begin + b];
+        const int32_t lo = na < nb ? na : nb, hi = na < nb ? nb : na;
+        if ((lo == tu && hi == tv) || !survives[a] || !survives[b]) continue;
+        const __int128 original = target_cost + cost[a] + cost[b];
+        const __int128 replacement = (__int128)dist_nodes(g, na, nb) + center_target;
+        if (original <= replacement) ++count;
+      }
+    }
+  }
+  free(cost);
+  free(survives);
+  return count;
+}
+
+typedef struct {
+  uint64_t product;
+  int32_t c, d;
+} cd_candidate;
+
+static int cmp_cd_candidate(const void* lhs, const void* rhs) {
+  const cd_candidate* a = lhs;
+  const cd_candidate* b = rhs;
+  if (a->product != b->product) return a->product < b->product ? -1 : 1;
+  if (a->c != b->c) return a->c < b->c ? -1 : 1;
+  if (a->d != b->d) return a->d < b->d ? -1 : 1;
+  return 0;
+}
+
+/* The flagged tasks ranked by (reply product, c, d), saturating the product at 2^64 - 1, first
+ * max_cd kept (0 = all). Writes (c, d, product) triples; returns the count or -1. */
+int64_t ceo_cd_finalize(const ceo_graph* g, int32_t u, int32_t v, const int32_t* c, const int32_t* d,
+                        const uint8_t* flags, int64_t count, uint32_t max_cd, int32_t* out_c, int32_t* out_d,
+                        uint64_t* out_product) {
+  const int32_t tu = u < v ? u : v, tv = u < v ? v : u;
+  cd_candidate* list = malloc(sizeof(cd_candidate) * (size_t)(count > 0 ? count : 1));
+  if (list == NULL) return -1;
+  int64_t kept = 0;
+  for (int64_t i = 0; i < count; ++i) {
+    if (flags[i] == 0) continue;
+    const uint64_t rc = (uint64_t)ceo_ht_reply_count(g, tu, tv, c[i]);
+    const uint64_t rd = (uint64_t)ceo_ht_reply_count(g, tu, tv, d[i]);
+    uint64_t product = 0;
+    if (rc != 0 && rd > UINT64_MAX / rc) {
+      product = UINT64_MAX;
+    } else {
+      product = rc * rd;
+    }
+    list[kept].product = product;
+    list[kept].c = c[i];
+    list[kept].d = d[i];
+    ++kept;
+  }
+  qsort(list, (size_t)kept, sizeof(cd_candidate), cmp_cd_candidate);
+  if (max_cd != 0 && kept > (int64_t)max_cd) kept = max_cd;
+  for (int64_t i = 0; i < kept; ++i) {
+    out_c[i] = list[i].c;
+    out_d[i] = list[i].d;
+    out_product[i] = list[i].product;
+  }
+  free(list);
+  return kept;
+}
+
 /* ---- SelectHtTargetEdgeIds: src/cpu/ht_scan.cpp:316-345 ---- */
 
 static const ceo_graph* g_target_graph;

@@ -92,6 +92,11 @@ int64_t ceo_cd_tasks(const ceo_graph* g, int32_t u, int32_t v, uint32_t max_neig
                      uint32_t max_candidate_degree, int32_t* c, int32_t* d, uint8_t* active);
 void ceo_cd_screen(const ceo_graph* g, int32_t u, int32_t v, const int32_t* c, const int32_t* d,
                    const uint8_t* active, int64_t count, int32_t mode, uint8_t* flags);
+/* FinalizeCdCandidates (hamilton_tutte.cpp:283-327) and its Hamilton reply count (:230-269). */
+int64_t ceo_ht_reply_count(const ceo_graph* g, int32_t tu, int32_t tv, int32_t center);
+int64_t ceo_cd_finalize(const ceo_graph* g, int32_t u, int32_t v, const int32_t* c, const int32_t* d,
+                        const uint8_t* flags, int64_t count, uint32_t max_cd, int32_t* out_c, int32_t* out_d,
+                        uint64_t* out_product);
 /* HT scan target order (weight descending when order == 1, else canonical). */
 int64_t ceo_ht_targets(const ceo_graph* g, int32_t order, int32_t* out);
 

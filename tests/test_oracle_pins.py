@@ -88,7 +88,10 @@ def test_cd_golden(port):
         np.testing.assert_array_equal(dd, d[f"d_{t}"])
         np.testing.assert_array_equal(a, d[f"active_{t}"])
         for mode in (0, 1):
-            np.testing.assert_array_equal(port.cd_screen(g, 0, 1, c, dd, a, mode), d[f"flags_{t}_{mode}"])
+            flags = port.cd_screen(g, 0, 1, c, dd, a, mode)
+            np.testing.assert_array_equal(flags, d[f"flags_{t}_{mode}"])
+            # FinalizeCdCandidates: ranked by Hamilton reply product (all kept)
+            np.testing.assert_array_equal(port.cd_finalize(g, 0, 1, c, dd, flags, 0), d[f"candidates_{t}_{mode}"])
 
 
 def test_verifier_rejects_tampered_witness(port):
@@ -127,4 +130,7 @@ def test_kopt_and_cd_match_reference_live(port, ref):
         rc, rd, ra = rg.cd_tasks(u, v)
         np.testing.assert_array_equal(c, rc)
         for mode in (0, 1):
-            np.testing.assert_array_equal(port.cd_screen(g, u, v, c, d, a, mode), rg.cd_screen(u, v, c, d, a, mode))
+            flags = port.cd_screen(g, u, v, c, d, a, mode)
+            np.testing.assert_array_equal(flags, rg.cd_screen(u, v, c, d, a, mode))
+            np.testing.assert_array_equal(port.cd_finalize(g, u, v, c, d, flags, 5),
+                                          rg.cd_candidates(u, v, 25, 5, 50, mode, backend=1))
