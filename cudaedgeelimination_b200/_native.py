@@ -74,7 +74,8 @@ class BatchView(ctypes.Structure):
 
 class BatchOptions(ctypes.Structure):
     _fields_ = [("targets", ctypes.c_int32), ("max_neighborhood", ctypes.c_int32),
-                ("max_candidate_degree", ctypes.c_int32), ("cd_mode", ctypes.c_int32)]
+                ("max_candidate_degree", ctypes.c_int32), ("cd_mode", ctypes.c_int32),
+                ("max_cd_candidates", ctypes.c_int32)]
 
 
 class BatchTuning(ctypes.Structure):
@@ -167,6 +168,7 @@ def lib() -> ctypes.CDLL:
             "cee_batch_fetch": (ctypes.c_int, [vp, vp, vp, vp, vp, vp]),
             "cee_batch_screen": (ctypes.c_int, [vp, ctypes.POINTER(BatchView), ctypes.POINTER(BatchOptions),
                                                 vp, vp, vp, vp, vp, ctypes.POINTER(BatchStats)]),
+            "cee_batch_fetch_candidates": (ctypes.c_int, [vp, vp, vp, vp, vp]),
             "cee_batch_set_tuning": (ctypes.c_int, [vp, ctypes.POINTER(BatchTuning)]),
             "cee_batch_get_tuning": (ctypes.c_int, [vp, ctypes.POINTER(BatchTuning)]),
             "cee_batch_autotune": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.POINTER(BatchTuning)]),

@@ -40,9 +40,11 @@ class BatchOptions:
     max_neighborhood: int = 25
     max_candidate_degree: int = 50
     cd_mode: int = 0
+    max_cd_candidates: int = 0  # 0: flags only; else FinalizeCdCandidates' ranked list (reference default 5)
 
     def native(self) -> _native.BatchOptions:
-        return _native.BatchOptions(self.targets, self.max_neighborhood, self.max_candidate_degree, self.cd_mode)
+        return _native.BatchOptions(self.targets, self.max_neighborhood, self.max_candidate_degree, self.cd_mode,
+                                    self.max_cd_candidates)
 
     @property
     def flag_words(self) -> int:
@@ -118,6 +120,19 @@ class BatchMixin:
                                                                   ctypes.byref(opt.native()), *_ptrs(out),
                                                                   ctypes.byref(stats)))
         return out, stats
+
+    def batch_fetch_candidates(self):
+        """The finalised c,d candidates of the last launch: (c, d, product) arrays [I, T, K] and the
+        count per (instance, target) [I, T]."""
+        batch, graph, opt = self._batch
+        I, T, K = int(batch.node_begin.shape[0] - 1), opt.targets, opt.max_cd_candidates
+        c = np.empty((I, T, K), np.int32)
+        d = np.empty((I, T, K), np.int32)
+        product = np.empty((I, T, K), np.int64)
+        count = np.empty((I, T), np.int32)
+        _native.check(self.handle, _native.lib().cee_batch_fetch_candidates(
+            self.handle, c.ctypes.data, d.ctypes.data, product.ctypes.data, count.ctypes.data))
+        return c, d, product, count
 
     def batch_tuning(self) -> _native.BatchTuning:
         t = _native.BatchTuning()

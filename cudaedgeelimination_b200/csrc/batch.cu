@@ -30,6 +30,7 @@ struct BatchState {
   DevBuf raw_x, raw_y, raw_u, raw_v, raw_w;
   // outputs and work-queue state
   DevBuf witness, target_ids, target_count, nbhd, flags, counter, ready;
+  DevBuf cand_c, cand_d, cand_product, cand_count;  // finalised c,d candidates (max_cd_candidates > 0)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaStream_t h2d = nullptr, d2h = nullptr;
@@ -46,7 +47,8 @@ struct BatchState {
   void Release() {
     ReleaseGraph();
     for (DevBuf* b : {&d_node_begin, &d_edge_begin, &xy, &uv, &w32, &active, &ro, &nbr, &ids, &slot4, &raw_x, &raw_y,
-                      &raw_u, &raw_v, &raw_w, &witness, &target_ids, &target_count, &nbhd, &flags, &counter, &ready}) {
+                      &raw_u, &raw_v, &raw_w, &witness, &target_ids, &target_count, &nbhd, &flags, &counter, &ready,
+                      &cand_c, &cand_d, &cand_product, &cand_count}) {
       b->Release();
     }
     for (int i = 0; i < kMaxChunks; ++i) {
@@ -97,6 +99,9 @@ int ValidateOptions(cee_ctx* ctx, const cee_batch_options* o) {
   if (o->max_candidate_degree < 0) return Fail(ctx, CEE_ERR_INVALID, "negative degree cap");
   if (o->cd_mode != CEE_CD_ACTIVE_INCOMPATIBLE && o->cd_mode != CEE_CD_MISSING_OR_INCOMPATIBLE) {
     return Fail(ctx, CEE_ERR_INVALID, "unknown c,d mode");
+  }
+  if (o->max_cd_candidates < 0 || o->max_cd_candidates > kBatchMaxCd) {
+    return Fail(ctx, CEE_ERR_INVALID, "max_cd_candidates must lie in [0,32]");
   }
   return CEE_OK;
 }
@@ -150,11 +155,30 @@ int ReserveAll(cee_ctx* ctx, BatchState& s) {
       {&s.slot4, adj * 16}, {&s.witness, m * 4}, {&s.target_ids, I * T * 4}, {&s.target_count, I * 4},
       {&s.nbhd, I * T * NB * 4}, {&s.flags, I * T * static_cast<size_t>(s.flag_words) * 4},
       {&s.counter, kMaxChunks * 8}, {&s.ready, I * 4}};
+  const size_t K = static_cast<size_t>(s.opt.max_cd_candidates);
   for (const auto& [buf, bytes] : wants) {
     rc = Reserve(ctx, *buf, bytes);
     if (rc != CEE_OK) return rc;
   }
+  if (K > 0) {
+    const std::pair<DevBuf*, size_t> cands[] = {
+        {&s.cand_c, I * T * K * 4}, {&s.cand_d, I * T * K * 4}, {&s.cand_product, I * T * K * 8}, {&s.cand_count, I * T * 4}};
+    for (const auto& [buf, bytes] : cands) {
+      rc = Reserve(ctx, *buf, bytes);
+      if (rc != CEE_OK) return rc;
+    }
+  }
   return CEE_OK;
+}
+
+// Device error word of the batched screen: bounds checks and the bounded wait are malformed-input
+// or scheduling errors, the finalisation's range limits are CEE_ERR_RANGE.
+int BatchCheck(cee_ctx* ctx) {
+  if ((*ctx->h_error & kBatchRangeError) != 0) {
+    return Fail(ctx, CEE_ERR_RANGE, "batched c,d finalisation: an instance has more than 65536 nodes or a reply "
+                                    "product reached 2^32 - 2");
+  }
+  return CheckDeviceError(ctx, "batched screen");
 }
 
 void SetShape(BatchState& s, const cee_batch_view* b, const cee_batch_options* o) {
@@ -201,6 +225,11 @@ BatchArgs MakeArgs(cee_ctx* ctx, BatchState& s, int32_t first, int32_t count, in
   A.target_count = static_cast<int32_t*>(s.target_count.ptr);
   A.nbhd = static_cast<int32_t*>(s.nbhd.ptr);
   A.flags = static_cast<uint32_t*>(s.flags.ptr);
+  A.max_cd = s.opt.max_cd_candidates;
+  A.cand_c = static_cast<int32_t*>(s.cand_c.ptr);
+  A.cand_d = static_cast<int32_t*>(s.cand_d.ptr);
+  A.cand_product = static_cast<int64_t*>(s.cand_product.ptr);
+  A.cand_count = static_cast<int32_t*>(s.cand_count.ptr);
   A.counter = static_cast<unsigned long long*>(s.counter.ptr) + chunk;
   A.ready = static_cast<int32_t*>(s.ready.ptr);
   A.error = ctx->d_error;
@@ -225,6 +254,14 @@ int LaunchRange(cee_ctx* ctx, BatchState& s, int32_t first, int32_t count, int c
     batch_screen_kernel<false><<<blocks, kBatchWarps * 32, 0, stream>>>(A);
   } else {
     batch_screen_kernel<true><<<blocks, kBatchWarps * 32, 0, stream>>>(A);
+  }
+  if (A.max_cd > 0) {  // FinalizeCdCandidates for every target of the range
+    const int fin_blocks = GridFor(static_cast<int64_t>(count) * s.opt.targets, kBatchWarps, ctx->sm_count * 8);
+    if (s.narrow) {
+      batch_finalize_kernel<false><<<fin_blocks, kBatchWarps * 32, 0, stream>>>(A);
+    } else {
+      batch_finalize_kernel<true><<<fin_blocks, kBatchWarps * 32, 0, stream>>>(A);
+    }
   }
   const cudaError_t status = cudaGetLastError();
   if (status != cudaSuccess) return CudaFail(ctx, status, "batch_screen_kernel launch");
@@ -430,7 +467,26 @@ int cee_batch_fetch(cee_ctx* ctx, int32_t* witness, int32_t* target_ids, int32_t
   cudaMemcpyAsync(ctx->h_error, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
   const cudaError_t status = cudaStreamSynchronize(st);
   if (status != cudaSuccess) return CudaFail(ctx, status, "batch fetch");
-  return CheckDeviceError(ctx, "batched screen");
+  return BatchCheck(ctx);
+}
+
+int cee_batch_fetch_candidates(cee_ctx* ctx, int32_t* c, int32_t* d, int64_t* product, int32_t* count) {
+  int rc = Activate(ctx);
+  if (rc != CEE_OK) return rc;
+  BatchState* s = ctx->batch;
+  if (s == nullptr || !s->prepared) return Fail(ctx, CEE_ERR_STATE, "batch not prepared");
+  if (s->opt.max_cd_candidates == 0) return Fail(ctx, CEE_ERR_STATE, "the batch was prepared without c,d finalisation");
+  const size_t IT = static_cast<size_t>(s->instances) * s->opt.targets;
+  const size_t K = static_cast<size_t>(s->opt.max_cd_candidates);
+  cudaStream_t st = ctx->stream;
+  if (c != nullptr) cudaMemcpyAsync(c, s->cand_c.ptr, IT * K * 4, cudaMemcpyDeviceToHost, st);
+  if (d != nullptr) cudaMemcpyAsync(d, s->cand_d.ptr, IT * K * 4, cudaMemcpyDeviceToHost, st);
+  if (product != nullptr) cudaMemcpyAsync(product, s->cand_product.ptr, IT * K * 8, cudaMemcpyDeviceToHost, st);
+  if (count != nullptr) cudaMemcpyAsync(count, s->cand_count.ptr, IT * 4, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(ctx->h_error, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+  const cudaError_t status = cudaStreamSynchronize(st);
+  if (status != cudaSuccess) return CudaFail(ctx, status, "batch candidate fetch");
+  return BatchCheck(ctx);
 }
 
 int cee_batch_set_tuning(cee_ctx* ctx, const cee_batch_tuning* t) {
@@ -617,7 +673,7 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
   cudaEventRecord(ctx->ev[5], cs);
   status = cudaStreamSynchronize(cs);
   if (status != cudaSuccess) return CudaFail(ctx, status, "batched screen");
-  rc = CheckDeviceError(ctx, "batched screen");
+  rc = BatchCheck(ctx);
   if (rc != CEE_OK) return rc;
   s.prepared = true;  // the resident copy now holds this batch
   rc = Capture(ctx, s);

@@ -11,7 +11,11 @@
 //                     other than u, v with degree <= max_degree (0 = no cap) nearest to the
 //                     doubled midpoint 2p - p_u - p_v, ties by node -- then every pair i < j of
 //                     that neighbourhood as (c, d) = (min, max) screened as ScreenHtCdKernel
-//                     (src/cuda/ht_cd.cu:157-178).
+//                     (src/cuda/ht_cd.cu:157-178); with max_cd > 0 the item then ranks the
+//                     flagged pairs as FinalizeCdCandidates (src/cpu/hamilton_tutte.cpp:283-327):
+//                     Hamilton reply count of every neighbourhood node (pairs of its CSR
+//                     neighbours, AppendHtHamiltonRepliesUnchecked :230-269), product per pair,
+//                     the max_cd smallest (product, c, d).
 //
 // The c,d items of an instance wait (bounded, with an error on timeout) for that instance's
 // target-selection item; those items come first in the queue and take a few microseconds, so
@@ -30,6 +34,8 @@ constexpr int kBatchMaxNeighborhood = 32;
 constexpr int kBatchMaxPairs = kBatchMaxNeighborhood * (kBatchMaxNeighborhood - 1) / 2;  // 496
 constexpr int kBatchFlagWords = (kBatchMaxPairs + 31) / 32;                              // 16
 constexpr int32_t kBatchWaitError = 8;
+constexpr int32_t kBatchRangeError = 128;  // finalisation: instance > 65536 nodes or a product too large
+constexpr int kBatchMaxCd = 32;
 
 struct BatchArgs {
   JvGraph g;                          // the union snapshot (global node and edge ids)
@@ -49,6 +55,11 @@ struct BatchArgs {
   int32_t* __restrict__ target_count; // [I]
   int32_t* __restrict__ nbhd;         // [I * T * nb] global node ids, -1 padding
   uint32_t* __restrict__ flags;       // [I * T * flag_words] bit p = flag of pair p
+  int32_t max_cd;                     // 0: flags only; else finalised candidates per target
+  int32_t* __restrict__ cand_c;       // [I * T * max_cd] global node ids
+  int32_t* __restrict__ cand_d;
+  int64_t* __restrict__ cand_product; // reply products
+  int32_t* __restrict__ cand_count;   // [I * T]
   unsigned long long* __restrict__ counter;  // work counter, zero at launch
   int32_t* __restrict__ ready;        // [I] set when the instance's targets are written, zero at launch
   int32_t* __restrict__ error;
@@ -155,6 +166,77 @@ __device__ void batch_select_targets(const BatchArgs& A, int32_t inst, int lane)
     __threadfence();
     atomicExch(A.ready + inst, 1);
   }
+}
+
+// Number of Hamilton replies at `center` for target (u, v) (AppendHtHamiltonRepliesUnchecked,
+// src/cpu/hamilton_tutte.cpp:230-269): pairs first < second of the center's CSR neighbours whose
+// edges to the center both survive 2-opt against the target, whose node pair is not the target,
+// and with C(u,v) + C(c,first) + C(c,second) <= C(first,second) + C(u,c) + C(v,c). Whole warp; rows
+// of up to 32 neighbours keep them one per lane, longer rows re-read both neighbours per pair.
+template <bool kWide>
+__device__ int32_t ht_reply_count(const JvGraph& g, int32_t u, int32_t v, int2 pu, int2 pv, uint32_t cuv,
+                                  int32_t center, int2 pc, uint32_t cuc, uint32_t cvc, int lane) {
+  const int32_t r0 = __ldg(g.row_offsets + center), deg = __ldg(g.row_offsets + center + 1) - r0;
+  if (deg < 2) return 0;
+  const uint64_t center_target = static_cast<uint64_t>(cuc) + cvc;
+  // neighbour j: node, C(center, j), 2-opt survival of edge (center, j) against the target
+  auto neighbour = [&](int j, int32_t& node, int2& p, uint32_t& cost, bool& survives) {
+    node = __ldg(g.nbr + r0 + j);
+    p = __ldg(g.xy + node);
+    cost = exact_distance<kWide>(pc, p, g.dist_type);
+    const bool center_low = center < node;  // canonical edge (ou, ov)
+    const uint32_t cu_o = exact_distance<kWide>(pu, p, g.dist_type), cv_o = exact_distance<kWide>(pv, p, g.dist_type);
+    const uint64_t original = static_cast<uint64_t>(cuv) + cost;
+    // first = C(u, ov) + C(v, ou), second = C(u, ou) + C(v, ov)
+    const uint64_t first = center_low ? static_cast<uint64_t>(cu_o) + cvc : static_cast<uint64_t>(cuc) + cv_o;
+    const uint64_t second = center_low ? static_cast<uint64_t>(cuc) + cv_o : static_cast<uint64_t>(cu_o) + cvc;
+    survives = first >= original || second >= original;
+  };
+  int32_t my_node = -1;
+  int2 my_p = make_int2(0, 0);
+  uint32_t my_cost = 0;
+  bool my_survives = false;
+  if (deg <= 32 && lane < deg) neighbour(lane, my_node, my_p, my_cost, my_survives);
+  const int64_t pairs = static_cast<int64_t>(deg) * (deg - 1) / 2;
+  const int tu = min(u, v), tv = max(u, v);
+  int32_t count = 0;
+  for (int64_t base = 0; base < pairs; base += 32) {
+    const int64_t p = base + lane;
+    int a = 0, b = 1;
+    if (p < pairs) {  // invert p = a (2 deg - a - 1) / 2 + (b - a - 1)
+      const float twod = 2.0f * deg - 1.0f;
+      a = static_cast<int>((twod - sqrtf(twod * twod - 8.0f * static_cast<float>(p))) * 0.5f);
+      a = max(0, min(a, deg - 2));
+      while (a > 0 && static_cast<int64_t>(a) * (2 * deg - a - 1) / 2 > p) --a;
+      while (static_cast<int64_t>(a + 1) * (2 * deg - a - 2) / 2 <= p) ++a;
+      b = static_cast<int>(p - static_cast<int64_t>(a) * (2 * deg - a - 1) / 2) + a + 1;
+    }
+    int32_t na = -1, nb = -1;
+    int2 qa = make_int2(0, 0), qb = make_int2(0, 0);
+    uint32_t ca = 0, cb = 0;
+    bool sa = false, sb = false;
+    if (deg <= 32) {
+      na = __shfl_sync(kFullMask, my_node, a);
+      nb = __shfl_sync(kFullMask, my_node, b);
+      qa = make_int2(__shfl_sync(kFullMask, my_p.x, a), __shfl_sync(kFullMask, my_p.y, a));
+      qb = make_int2(__shfl_sync(kFullMask, my_p.x, b), __shfl_sync(kFullMask, my_p.y, b));
+      ca = __shfl_sync(kFullMask, my_cost, a);
+      cb = __shfl_sync(kFullMask, my_cost, b);
+      sa = __shfl_sync(kFullMask, my_survives, a);
+      sb = __shfl_sync(kFullMask, my_survives, b);
+    } else if (p < pairs) {
+      neighbour(a, na, qa, ca, sa);
+      neighbour(b, nb, qb, cb, sb);
+    }
+    bool reply = false;
+    if (p < pairs && sa && sb && !(min(na, nb) == tu && max(na, nb) == tv)) {
+      const uint64_t original = static_cast<uint64_t>(cuv) + ca + cb;
+      const uint64_t replacement = static_cast<uint64_t>(exact_distance<kWide>(qa, qb, g.dist_type)) + center_target;
+      reply = original <= replacement;
+    }
+    count += __popc(__ballot_sync(kFullMask, reply));
+  }
+  return count;
 }
 
 template <bool kWide>
@@ -306,6 +388,121 @@ static __global__ void __launch_bounds__(kBatchWarps * 32, 5) batch_screen_kerne
       batch_cd_target<kWide>(A, A.first_instance + static_cast<int32_t>(s / A.targets),
                              static_cast<int32_t>(s % A.targets), pair_i, pair_j, lane);
     }
+    __syncwarp();
+  }
+}
+
+// FinalizeCdCandidates (src/cpu/hamilton_tutte.cpp:283-327) for one (instance, target) slot, after
+// the screen: the Hamilton reply count of every neighbourhood node, the reply product of every
+// flagged pair, and the max_cd smallest (product, c, d) as 64-bit keys
+// product << 32 | (c - n0) << 16 | (d - n0). A separate launch, so that the screen keeps its
+// registers.
+template <bool kWide>
+__device__ void batch_finalize_target(const BatchArgs& A, int32_t inst, int32_t t, const uint8_t* pair_i,
+                                      const uint8_t* pair_j, int lane) {
+  const JvGraph& g = A.g;
+  const int64_t slot = static_cast<int64_t>(inst) * A.targets + t;
+  const int32_t count = A.target_count[inst];
+  if (t >= count) {
+    if (lane == 0) A.cand_count[slot] = 0;
+    return;
+  }
+  const int2 uv = g.edge_uv[A.target_ids[slot]];
+  const int32_t u = uv.x, v = uv.y;
+  const int2 pu = __ldg(g.xy + u), pv = __ldg(g.xy + v);
+  const int64_t n0 = A.node_begin[inst], n1 = A.node_begin[inst + 1];
+  const int NB = A.nb;
+  const int32_t ln = lane < NB ? A.nbhd[slot * NB + lane] : -1;
+  const bool have = ln >= 0;
+  const int size = __popc(__ballot_sync(kFullMask, have));
+  const int pairs = size * (size - 1) / 2;
+  uint32_t cu = 0, cv = 0;
+  int2 px = make_int2(0, 0);
+  if (have) {
+    px = __ldg(g.xy + ln);
+    cu = exact_distance<kWide>(pu, px, g.dist_type);
+    cv = exact_distance<kWide>(pv, px, g.dist_type);
+  }
+  const uint32_t cuv = exact_distance<kWide>(pu, pv, g.dist_type);
+  const uint32_t my_word = lane < A.flag_words ? A.flags[slot * A.flag_words + lane] : 0u;  // lane w: word w
+  const bool any_flag = __any_sync(kFullMask, my_word != 0);
+  int32_t* cc_out = A.cand_c + slot * A.max_cd;
+  int32_t* cd_out = A.cand_d + slot * A.max_cd;
+  int64_t* cp_out = A.cand_product + slot * A.max_cd;
+  // FinalizeCdCandidates: reply count of every neighbourhood node (lane k keeps node k's)
+  int32_t my_replies = 0;
+  if (any_flag) {
+    for (int k = 0; k < size; ++k) {
+      const int32_t x = __shfl_sync(kFullMask, ln, k);
+      const int2 pxk = make_int2(__shfl_sync(kFullMask, px.x, k), __shfl_sync(kFullMask, px.y, k));
+      const uint32_t cuk = __shfl_sync(kFullMask, cu, k), cvk = __shfl_sync(kFullMask, cv, k);
+      const int32_t r = ht_reply_count<kWide>(g, u, v, pu, pv, cuv, x, pxk, cuk, cvk, lane);
+      if (lane == k) my_replies = r;
+    }
+  }
+  // the max_cd smallest (product, c, d) among the flagged pairs, as 64-bit keys
+  // product << 32 | (c - n0) << 16 | (d - n0)
+  uint64_t top = kEmptyKey;
+  for (int base = 0; base < A.flag_words * 32 && any_flag; base += 32) {
+    const int p = base + lane;
+    const uint32_t word = __shfl_sync(kFullMask, my_word, base >> 5);
+    const bool flagged = p < pairs && ((word >> lane) & 1u) != 0;
+    int i = 0, j = 1;
+    if (flagged) {
+      if (size == NB) {
+        i = pair_i[p];
+        j = pair_j[p];
+      } else {
+        int rest = p;
+        while (rest >= size - 1 - i) {
+          rest -= size - 1 - i;
+          ++i;
+        }
+        j = i + 1 + rest;
+      }
+    }
+    const int32_t ni = __shfl_sync(kFullMask, ln, i), nj = __shfl_sync(kFullMask, ln, j);
+    const int32_t ri = __shfl_sync(kFullMask, my_replies, i), rj = __shfl_sync(kFullMask, my_replies, j);
+    uint64_t key = kEmptyKey;
+    if (flagged) {
+      const int32_t c = min(ni, nj), d = max(ni, nj);
+      const uint64_t product = static_cast<uint64_t>(ri) * static_cast<uint64_t>(rj);
+      if (n1 - n0 > 65536 || product >= 0xfffffffeull) atomicOr(A.error, kBatchRangeError);
+      key = (min(product, static_cast<uint64_t>(0xfffffffeull)) << 32) |
+            (static_cast<uint64_t>(c - n0) << 16) | static_cast<uint64_t>((d - n0) & 0xffff);
+    }
+    if (!__any_sync(kFullMask, key != kEmptyKey)) continue;
+    key = warp_sort_asc(key, lane);
+    top = warp_merge_smallest(top, key, lane);
+  }
+  const int kept = min(A.max_cd, __popc(__ballot_sync(kFullMask, top != kEmptyKey)));
+  if (lane < kept) {
+    cc_out[lane] = static_cast<int32_t>(n0 + ((top >> 16) & 0xffff));
+    cd_out[lane] = static_cast<int32_t>(n0 + (top & 0xffff));
+    cp_out[lane] = static_cast<int64_t>(top >> 32);
+  }
+  if (lane == 0) A.cand_count[slot] = kept;
+}
+
+template <bool kWide>
+static __global__ void __launch_bounds__(kBatchWarps * 32) batch_finalize_kernel(BatchArgs A) {
+  __shared__ uint8_t pair_i[kBatchMaxPairs], pair_j[kBatchMaxPairs];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int p = threadIdx.x; p < A.nb * (A.nb - 1) / 2; p += blockDim.x) {
+    int i = 0, rest = p;
+    while (rest >= A.nb - 1 - i) {
+      rest -= A.nb - 1 - i;
+      ++i;
+    }
+    pair_i[p] = static_cast<uint8_t>(i);
+    pair_j[p] = static_cast<uint8_t>(i + 1 + rest);
+  }
+  __syncthreads();
+  const int64_t slots = static_cast<int64_t>(A.instances) * A.targets;
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * kBatchWarps;
+  for (int64_t q = static_cast<int64_t>(blockIdx.x) * kBatchWarps + warp; q < slots; q += warps) {
+    batch_finalize_target<kWide>(A, A.first_instance + static_cast<int32_t>(q / A.targets),
+                                 static_cast<int32_t>(q % A.targets), pair_i, pair_j, lane);
     __syncwarp();
   }
 }

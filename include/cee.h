@@ -300,6 +300,9 @@ typedef struct {
   int32_t max_neighborhood;     /* 2..32 */
   int32_t max_candidate_degree; /* 0 = no cap */
   int32_t cd_mode;              /* cee_cd_mode */
+  int32_t max_cd_candidates;    /* 0: flags only; 1..32: also FinalizeCdCandidates' ranked list
+                                   (hamilton_tutte.cpp:283-327, reference default 5), read with
+                                   cee_batch_fetch_candidates; needs instances of <= 65536 nodes */
 } cee_batch_options;
 
 /* Launch shape of the batch kernel (chosen by cee_batch_autotune; results never depend on it). */
@@ -338,6 +341,11 @@ int cee_batch_fetch(cee_ctx* ctx, int32_t* witness, int32_t* target_ids, int32_t
 int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* batch, const cee_batch_options* options,
                      int32_t* witness, int32_t* target_ids, int32_t* target_count, int32_t* nbhd,
                      uint32_t* flags, cee_batch_stats* stats);
+/* The finalised c,d candidates of the last launch (max_cd_candidates > 0): per (instance, target)
+ * slot, `count` entries of (c, d, reply product) ranked by (product, c, d), global node ids;
+ * arrays of instances x targets x max_cd_candidates (products saturate at 2^32 - 2; a product that
+ * reaches it fails the launch with CEE_ERR_RANGE). */
+int cee_batch_fetch_candidates(cee_ctx* ctx, int32_t* c, int32_t* d, int64_t* product, int32_t* count);
 int cee_batch_set_tuning(cee_ctx* ctx, const cee_batch_tuning* tuning);
 int cee_batch_get_tuning(const cee_ctx* ctx, cee_batch_tuning* tuning);
 /* Times every candidate launch shape on the prepared batch (`reps` graph launches each, CUDA

@@ -115,3 +115,54 @@ def test_unsorted_instance_rejected(ctx):
         ctx.batch_prepare(batch, BatchOptions())
     with pytest.raises(NativeError):
         ctx.batch_screen(batch, BatchOptions())
+
+
+def check_candidates(port, batch, opt, cand, instances):
+    """Finalised c,d candidates equal FinalizeCdCandidates over the oracle's tasks and flags."""
+    c, d, product, count = cand
+    K = opt.max_cd_candidates
+    for i in instances:
+        inst = batch.instance(i)
+        n0 = int(batch.node_begin[i])
+        for t, local in enumerate(port.ht_targets(inst)[:opt.targets]):
+            u, v = int(inst.edge_u[local]), int(inst.edge_v[local])
+            tc, td, ta = port.cd_tasks(inst, u, v, opt.max_neighborhood, opt.max_candidate_degree)
+            flags = port.cd_screen(inst, u, v, tc, td, ta, opt.cd_mode)
+            want = port.cd_finalize(inst, u, v, tc, td, flags, K)
+            k = int(count[i, t])
+            assert k == want.shape[0]
+            np.testing.assert_array_equal(c[i, t, :k] - n0, want[:, 0])
+            np.testing.assert_array_equal(d[i, t, :k] - n0, want[:, 1])
+            np.testing.assert_array_equal(product[i, t, :k], want[:, 2])
+
+
+@pytest.mark.parametrize("opt", [BatchOptions(max_cd_candidates=5), BatchOptions(targets=8, cd_mode=1, max_cd_candidates=32),
+                                 BatchOptions(targets=16, max_neighborhood=32, max_candidate_degree=0, max_cd_candidates=3)],
+                         ids=["default-5", "missing-or-incompatible-32", "nb32-nocap-3"])
+def test_finalised_candidates(ctx, port, small_batch, opt):
+    ctx.batch_prepare(small_batch, opt)
+    ctx.batch_launch()
+    res = ctx.batch_fetch()
+    check_against_oracle(port, small_batch, res, opt, instances=range(0, small_batch.count, 6))
+    cand = ctx.batch_fetch_candidates()
+    check_candidates(port, small_batch, opt, cand, range(small_batch.count))
+    assert (cand[3] > 0).any()
+
+
+def test_finalised_candidates_match_reference(ctx, ref, small_batch):
+    opt = BatchOptions(max_cd_candidates=5)
+    ctx.batch_prepare(small_batch, opt)
+    ctx.batch_launch()
+    res = ctx.batch_fetch()
+    c, d, product, count = ctx.batch_fetch_candidates()
+    for i in range(0, small_batch.count, 8):
+        inst = small_batch.instance(i)
+        rg = ref.graph(inst)
+        n0 = int(small_batch.node_begin[i])
+        for t in range(int(res.target_count[i])):
+            local = int(res.target_ids[i, t] - small_batch.edge_begin[i])
+            u, v = int(inst.edge_u[local]), int(inst.edge_v[local])
+            want = rg.cd_candidates(u, v, 25, 5, 50, 0, backend=1)
+            k = int(count[i, t])
+            got = np.stack([c[i, t, :k] - n0, d[i, t, :k] - n0, product[i, t, :k]], 1)
+            np.testing.assert_array_equal(got, want)
