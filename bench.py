@@ -267,6 +267,25 @@ def run_ours(args, rank: int, world: int, device: int):
     pairs = int((sizes * (sizes - 1) // 2).sum())
     value = edges_step * world / (ms_step / 1e3)
 
+    # ---- the same step with the c,d candidates finalised (FinalizeCdCandidates, 5 per target) ----
+    fin_opt = BatchOptions(max_cd_candidates=5)
+    ctx.batch_prepare(batch, fin_opt)
+    ctx.set_batch_tuning(tuning.jv_tile, tuning.blocks_per_sm, tuning.chunks)
+    for _ in range(args.warmup):
+        ctx.batch_launch()
+    torch.cuda.synchronize(device)
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        ctx.batch_launch()
+    f1.record(stream)
+    f1.synchronize()
+    fin_ms = max_over_ranks(f0.elapsed_time(f1), world) / args.steps
+    fin_counts = ctx.batch_fetch_candidates()[3]
+    ctx.batch_prepare(batch, opt)
+    ctx.set_batch_tuning(tuning.jv_tile, tuning.blocks_per_sm, tuning.chunks)
+
     # ---- the same work, one synchronous launch per instance ----
     plain_steps = max(1, min(3, args.steps))
     ctx.batch_launch_plain()
@@ -325,6 +344,9 @@ def run_ours(args, rank: int, world: int, device: int):
                               "chunks": tuning.chunks},
                    "l2": "inputs (~1.1 GB) larger than L2, no flush", "parallelism": f"replicas x{world}"},
         "cd_tasks_per_s": pairs * world / (ms_step / 1e3),
+        "with_cd_finalisation": {"ms_per_step": fin_ms, "value": edges_step * world / (fin_ms / 1e3), "unit": UNIT,
+                                 "candidates": int(fin_counts.sum()),
+                                 "note": "same step plus FinalizeCdCandidates (reply counts, ranking, 5 per target)"},
         "plain": {"ms_per_step": plain_ms, "value": edges_step * world / (plain_ms / 1e3), "unit": UNIT,
                   "launches_per_step": batch.count, "batched_speedup": plain_ms / ms_step,
                   "api": "cee_batch_launch_plain (one synchronous launch per instance)"},
