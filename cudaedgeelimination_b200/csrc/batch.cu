@@ -9,9 +9,28 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace cee {
+
+// Runs body(begin, end) over [0, count) split across host threads (one range when small).
+template <typename Body>
+void ParallelRanges(int64_t count, Body body) {
+  const int64_t kMinPerThread = int64_t{1} << 18;
+  const int threads = static_cast<int>(std::min<int64_t>(
+      std::max(1u, std::min(16u, std::thread::hardware_concurrency())), std::max<int64_t>(1, count / kMinPerThread)));
+  if (threads <= 1) {
+    body(0, count, 0);
+    return;
+  }
+  std::vector<std::thread> pool;
+  pool.reserve(static_cast<size_t>(threads));
+  for (int t = 0; t < threads; ++t) {
+    pool.emplace_back([=] { body(count * t / threads, count * (t + 1) / threads, t); });
+  }
+  for (std::thread& th : pool) th.join();
+}
 
 constexpr int kMaxChunks = 64;
 
@@ -128,8 +147,14 @@ int ValidateShape(cee_ctx* ctx, const cee_batch_view* b) {
       g.row_offsets[g.n] != g.adjacency) {
     return Fail(ctx, CEE_ERR_INVALID, "bad union CSR");
   }
-  for (int64_t v = 0; v < g.n; ++v) {
-    if (g.row_offsets[v + 1] < g.row_offsets[v]) return Fail(ctx, CEE_ERR_INVALID, "row_offsets not non-decreasing");
+  std::vector<uint8_t> bad(16, 0);
+  ParallelRanges(g.n, [&](int64_t v0, int64_t v1, int t) {
+    for (int64_t v = v0; v < v1; ++v) {
+      if (g.row_offsets[v + 1] < g.row_offsets[v]) bad[t] = 1;
+    }
+  });
+  if (std::any_of(bad.begin(), bad.end(), [](uint8_t b) { return b != 0; })) {
+    return Fail(ctx, CEE_ERR_INVALID, "row_offsets not non-decreasing");
   }
   if (g.m > 0 && (g.x == nullptr || g.y == nullptr || g.edge_u == nullptr || g.edge_v == nullptr ||
                   g.edge_w == nullptr || g.active == nullptr)) {
@@ -561,11 +586,33 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
   s.prepared = false;
   s.ReleaseGraph();
   int64_t min_x = 0, min_y = 0, max_x = 0, max_y = 0;
-  for (int64_t i = 0; i < g.n; ++i) {
-    min_x = i == 0 ? g.x[i] : std::min(min_x, g.x[i]);
-    max_x = i == 0 ? g.x[i] : std::max(max_x, g.x[i]);
-    min_y = i == 0 ? g.y[i] : std::min(min_y, g.y[i]);
-    max_y = i == 0 ? g.y[i] : std::max(max_y, g.y[i]);
+  if (g.n > 0) {
+    std::vector<int64_t> part(16 * 4);
+    for (int t = 0; t < 16; ++t) {
+      part[4 * t] = part[4 * t + 2] = INT64_MAX;
+      part[4 * t + 1] = part[4 * t + 3] = INT64_MIN;
+    }
+    ParallelRanges(g.n, [&](int64_t i0, int64_t i1, int t) {
+      int64_t lx = INT64_MAX, hx = INT64_MIN, ly = INT64_MAX, hy = INT64_MIN;
+      for (int64_t i = i0; i < i1; ++i) {
+        lx = std::min(lx, g.x[i]);
+        hx = std::max(hx, g.x[i]);
+        ly = std::min(ly, g.y[i]);
+        hy = std::max(hy, g.y[i]);
+      }
+      part[4 * t] = lx;
+      part[4 * t + 1] = hx;
+      part[4 * t + 2] = ly;
+      part[4 * t + 3] = hy;
+    });
+    min_x = min_y = INT64_MAX;
+    max_x = max_y = INT64_MIN;
+    for (int t = 0; t < 16; ++t) {
+      min_x = std::min(min_x, part[4 * t]);
+      max_x = std::max(max_x, part[4 * t + 1]);
+      min_y = std::min(min_y, part[4 * t + 2]);
+      max_y = std::max(max_y, part[4 * t + 3]);
+    }
   }
   if (static_cast<__int128>(max_x) - min_x >= (__int128{1} << 30) ||
       static_cast<__int128>(max_y) - min_y >= (__int128{1} << 30)) {
