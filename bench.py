@@ -99,6 +99,9 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.reader = threading.Thread(target=self._read, daemon=True)
             self.reader.start()
+            deadline = time.time() + 3.0  # nvidia-smi takes a moment to start: sample before timing
+            while not self.lines and time.time() < deadline and self.proc.poll() is None:
+                time.sleep(0.02)
         except OSError:
             self.proc = None
         return self
