@@ -408,6 +408,22 @@ class Context(BatchMixin, ServeMixin):
         return flags
 
 
+    def exact_distances(self, x, y, dist_type: int, pair_i, pair_j):
+        """Exact TSPLIB distances of point pairs, evaluated on the device by the routine the screens
+        use for this point set's span class; returns (distances int32, span class)."""
+        x = np.ascontiguousarray(x, dtype=np.int64)
+        y = np.ascontiguousarray(y, dtype=np.int64)
+        pi = np.ascontiguousarray(pair_i, dtype=np.int32)
+        pj = np.ascontiguousarray(pair_j, dtype=np.int32)
+        out = np.empty(pi.shape[0], np.int32)
+        span = ctypes.c_int32(-1)
+        _native.check(self.handle, _native.lib().cee_exact_distances(
+            self.handle, int(x.shape[0]), x.ctypes.data_as(ctypes.c_void_p), y.ctypes.data_as(ctypes.c_void_p),
+            int(dist_type), int(pi.shape[0]), pi.ctypes.data_as(ctypes.c_void_p), pj.ctypes.data_as(ctypes.c_void_p),
+            out.ctypes.data_as(ctypes.c_void_p), ctypes.byref(span)))
+        return out, int(span.value)
+
+
 # ---- the reference seam, one context per (thread, device) ------------------------------
 
 _tls = threading.local()

@@ -40,7 +40,7 @@ struct BatchState {
   int32_t instances = 0;
   int64_t n = 0, m = 0, adj = 0;
   int32_t dist_type = 0;
-  bool narrow = true;
+  int span = kSpanSmall;  // span class of the union's coordinates
   int32_t flag_words = 0;
   std::vector<int64_t> node_begin, edge_begin;
   // the union snapshot in the kernels' layout
@@ -54,7 +54,7 @@ struct BatchState {
   cudaGraphExec_t exec = nullptr;
   cudaStream_t h2d = nullptr, d2h = nullptr;
   cudaEvent_t up[kMaxChunks] = {}, done[kMaxChunks] = {};
-  int occupancy[2] = {1, 1};
+  int occupancy[kSpanClasses] = {1, 1, 1};  // resident screen blocks per SM, per span class
   bool prepared = false;
 
   void ReleaseGraph() {
@@ -262,9 +262,21 @@ BatchArgs MakeArgs(cee_ctx* ctx, BatchState& s, int32_t first, int32_t count, in
   return A;
 }
 
+cudaError_t QueryBatchOccupancy(BatchState& s) {
+  cudaError_t status = cudaSuccess;
+  for (int span = 0; span < kSpanClasses && status == cudaSuccess; ++span) {
+    WithSpan(span, [&](auto S) {
+      int blocks = 0;
+      status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, batch_screen_kernel<S.value>, kBatchWarps * 32, 0);
+      s.occupancy[span] = std::max(1, blocks);
+    });
+  }
+  return status;
+}
+
 int Grid(cee_ctx* ctx, const BatchState& s, int64_t items) {
   const int per_sm = std::max(1, std::min(s.tune.blocks_per_sm > 0 ? s.tune.blocks_per_sm : 64,
-                                          s.occupancy[s.narrow ? 0 : 1]));
+                                          s.occupancy[s.span]));
   const int64_t want = (items + kBatchWarps - 1) / kBatchWarps;
   return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(want, static_cast<int64_t>(ctx->sm_count) * per_sm)));
 }
@@ -275,18 +287,10 @@ int LaunchRange(cee_ctx* ctx, BatchState& s, int32_t first, int32_t count, int c
   cudaMemsetAsync(A.counter, 0, sizeof(unsigned long long), stream);
   cudaMemsetAsync(A.ready + first, 0, static_cast<size_t>(count) * 4, stream);
   const int blocks = Grid(ctx, s, items);
-  if (s.narrow) {
-    batch_screen_kernel<false><<<blocks, kBatchWarps * 32, 0, stream>>>(A);
-  } else {
-    batch_screen_kernel<true><<<blocks, kBatchWarps * 32, 0, stream>>>(A);
-  }
+  WithSpan(s.span, [&](auto S) { batch_screen_kernel<S.value><<<blocks, kBatchWarps * 32, 0, stream>>>(A); });
   if (A.max_cd > 0) {  // FinalizeCdCandidates for every target of the range
     const int fin_blocks = GridFor(static_cast<int64_t>(count) * s.opt.targets, kBatchWarps, ctx->sm_count * 8);
-    if (s.narrow) {
-      batch_finalize_kernel<false><<<fin_blocks, kBatchWarps * 32, 0, stream>>>(A);
-    } else {
-      batch_finalize_kernel<true><<<fin_blocks, kBatchWarps * 32, 0, stream>>>(A);
-    }
+    WithSpan(s.span, [&](auto S) { batch_finalize_kernel<S.value><<<fin_blocks, kBatchWarps * 32, 0, stream>>>(A); });
   }
   const cudaError_t status = cudaGetLastError();
   if (status != cudaSuccess) return CudaFail(ctx, status, "batch_screen_kernel launch");
@@ -391,7 +395,7 @@ int cee_batch_prepare(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opt
   BatchState& s = *State(ctx);
   s.prepared = false;
   std::vector<int2> xy;
-  rc = PackCoordinates(ctx, g.n, g.x, g.y, &xy, &s.narrow);
+  rc = PackCoordinates(ctx, g.n, g.x, g.y, &xy, &s.span);
   if (rc != CEE_OK) return rc;
   SetShape(s, b, options);
   rc = ReserveAll(ctx, s);
@@ -424,13 +428,8 @@ int cee_batch_prepare(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opt
   cudaError_t status = cudaStreamSynchronize(st);  // host staging vectors die at return
   if (status != cudaSuccess) return CudaFail(ctx, status, "batch upload");
   cudaEventRecord(ctx->ev[1], st);
-  for (int wide = 0; wide < 2; ++wide) {
-    int blocks = 0;
-    status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &blocks, wide ? batch_screen_kernel<true> : batch_screen_kernel<false>, kBatchWarps * 32, 0);
-    if (status != cudaSuccess) return CudaFail(ctx, status, "batch occupancy");
-    s.occupancy[wide] = std::max(1, blocks);
-  }
+  status = QueryBatchOccupancy(s);
+  if (status != cudaSuccess) return CudaFail(ctx, status, "batch occupancy");
   rc = Capture(ctx, s);
   if (rc != CEE_OK) return rc;
   s.prepared = true;
@@ -542,7 +541,7 @@ int cee_batch_autotune(cee_ctx* ctx, int32_t reps, cee_batch_tuning* chosen) {
   const cee_batch_tuning start = s->tune;
   cee_batch_tuning best = start;
   float best_ms = 1e30f;
-  const int occ = s->occupancy[s->narrow ? 0 : 1];
+  const int occ = s->occupancy[s->span];
   for (const int tile : {16, 32, 64, 128, 256}) {
     for (const int per_sm : {occ, std::max(1, occ / 2)}) {
       cee_batch_tuning t = start;
@@ -618,7 +617,7 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
       static_cast<__int128>(max_y) - min_y >= (__int128{1} << 30)) {
     return Fail(ctx, CEE_ERR_RANGE, "coordinate span >= 2^30: outside the exact int32 distance range of the kernels");
   }
-  s.narrow = max_x - min_x < kNarrowSpan && max_y - min_y < kNarrowSpan;
+  s.span = span_class(max_x - min_x, max_y - min_y);
   SetShape(s, b, options);
   rc = ReserveAll(ctx, s);
   for (const auto& [buf, bytes] : {std::pair<DevBuf*, size_t>{&s.raw_x, g.n * 8ull}, {&s.raw_y, g.n * 8ull},
@@ -634,13 +633,8 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
     if (status == cudaSuccess && s.done[i] == nullptr) status = cudaEventCreateWithFlags(&s.done[i], cudaEventDisableTiming);
   }
   if (status != cudaSuccess) return CudaFail(ctx, status, "batch streams");
-  for (int wide = 0; wide < 2; ++wide) {
-    int blocks = 0;
-    status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &blocks, wide ? batch_screen_kernel<true> : batch_screen_kernel<false>, kBatchWarps * 32, 0);
-    if (status != cudaSuccess) return CudaFail(ctx, status, "batch occupancy");
-    s.occupancy[wide] = std::max(1, blocks);
-  }
+  status = QueryBatchOccupancy(s);
+  if (status != cudaSuccess) return CudaFail(ctx, status, "batch occupancy");
   const int chunks = std::max(1, std::min<int>(s.tune.chunks, b->instances));
   cudaStream_t cs = ctx->stream;
   cudaEventRecord(ctx->ev[0], cs);

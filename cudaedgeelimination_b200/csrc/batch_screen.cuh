@@ -126,7 +126,7 @@ __device__ __forceinline__ void warp_merge_pairs(uint64_t& score, int32_t& node,
 
 // ---- work items ----------------------------------------------------------------------
 
-template <bool kWide>
+template <int kSpan>
 __device__ void batch_select_targets(const BatchArgs& A, int32_t inst, int lane) {
   const JvGraph& g = A.g;
   const int64_t e0 = A.edge_begin[inst], e1 = A.edge_begin[inst + 1];
@@ -173,7 +173,7 @@ __device__ void batch_select_targets(const BatchArgs& A, int32_t inst, int lane)
 // edges to the center both survive 2-opt against the target, whose node pair is not the target,
 // and with C(u,v) + C(c,first) + C(c,second) <= C(first,second) + C(u,c) + C(v,c). Whole warp; rows
 // of up to 32 neighbours keep them one per lane, longer rows re-read both neighbours per pair.
-template <bool kWide>
+template <int kSpan>
 __device__ int32_t ht_reply_count(const JvGraph& g, int32_t u, int32_t v, int2 pu, int2 pv, uint32_t cuv,
                                   int32_t center, int2 pc, uint32_t cuc, uint32_t cvc, int lane) {
   const int32_t r0 = __ldg(g.row_offsets + center), deg = __ldg(g.row_offsets + center + 1) - r0;
@@ -183,9 +183,9 @@ __device__ int32_t ht_reply_count(const JvGraph& g, int32_t u, int32_t v, int2 p
   auto neighbour = [&](int j, int32_t& node, int2& p, uint32_t& cost, bool& survives) {
     node = __ldg(g.nbr + r0 + j);
     p = __ldg(g.xy + node);
-    cost = exact_distance<kWide>(pc, p, g.dist_type);
+    cost = exact_distance<kSpan>(pc, p, g.dist_type);
     const bool center_low = center < node;  // canonical edge (ou, ov)
-    const uint32_t cu_o = exact_distance<kWide>(pu, p, g.dist_type), cv_o = exact_distance<kWide>(pv, p, g.dist_type);
+    const uint32_t cu_o = exact_distance<kSpan>(pu, p, g.dist_type), cv_o = exact_distance<kSpan>(pv, p, g.dist_type);
     const uint64_t original = static_cast<uint64_t>(cuv) + cost;
     // first = C(u, ov) + C(v, ou), second = C(u, ou) + C(v, ov)
     const uint64_t first = center_low ? static_cast<uint64_t>(cu_o) + cvc : static_cast<uint64_t>(cuc) + cv_o;
@@ -231,7 +231,7 @@ __device__ int32_t ht_reply_count(const JvGraph& g, int32_t u, int32_t v, int2 p
     bool reply = false;
     if (p < pairs && sa && sb && !(min(na, nb) == tu && max(na, nb) == tv)) {
       const uint64_t original = static_cast<uint64_t>(cuv) + ca + cb;
-      const uint64_t replacement = static_cast<uint64_t>(exact_distance<kWide>(qa, qb, g.dist_type)) + center_target;
+      const uint64_t replacement = static_cast<uint64_t>(exact_distance<kSpan>(qa, qb, g.dist_type)) + center_target;
       reply = original <= replacement;
     }
     count += __popc(__ballot_sync(kFullMask, reply));
@@ -239,7 +239,7 @@ __device__ int32_t ht_reply_count(const JvGraph& g, int32_t u, int32_t v, int2 p
   return count;
 }
 
-template <bool kWide>
+template <int kSpan>
 __device__ void batch_cd_target(const BatchArgs& A, int32_t inst, int32_t t, const uint8_t* pair_i,
                                  const uint8_t* pair_j, int lane) {
   const JvGraph& g = A.g;
@@ -300,10 +300,10 @@ __device__ void batch_cd_target(const BatchArgs& A, int32_t inst, int32_t t, con
   int2 px = make_int2(0, 0);
   if (have) {
     px = __ldg(g.xy + ln);
-    cu = exact_distance<kWide>(pu, px, g.dist_type);
-    cv = exact_distance<kWide>(pv, px, g.dist_type);
+    cu = exact_distance<kSpan>(pu, px, g.dist_type);
+    cv = exact_distance<kSpan>(pv, px, g.dist_type);
   }
-  const uint32_t cuv = exact_distance<kWide>(pu, pv, g.dist_type);
+  const uint32_t cuv = exact_distance<kSpan>(pu, pv, g.dist_type);
   const int pairs = size * (size - 1) / 2;
   // pair p of the neighbourhood is (i, j), i < j, in the reference's order (i major); the smem
   // table holds that order for the full size NB, a smaller neighbourhood (a small instance)
@@ -337,7 +337,7 @@ __device__ void batch_cd_target(const BatchArgs& A, int32_t inst, int32_t t, con
       const uint32_t cuc = i_is_c ? cui : cuj, cud = i_is_c ? cuj : cui;
       const uint32_t cvc = i_is_c ? cvi : cvj, cvd = i_is_c ? cvj : cvi;
       const bool active = row_contains(g.nbr, __ldg(g.row_offsets + c), __ldg(g.row_offsets + c + 1), d);
-      const uint64_t original = static_cast<uint64_t>(cuv) + exact_distance<kWide>(pi, pj, g.dist_type);
+      const uint64_t original = static_cast<uint64_t>(cuv) + exact_distance<kSpan>(pi, pj, g.dist_type);
       const uint64_t orient0 = static_cast<uint64_t>(cud) + cvc;
       const uint64_t orient1 = static_cast<uint64_t>(cuc) + cvd;
       const bool incompatible = orient0 < original && orient1 < original;
@@ -348,7 +348,7 @@ __device__ void batch_cd_target(const BatchArgs& A, int32_t inst, int32_t t, con
   }
 }
 
-template <bool kWide>
+template <int kSpan>
 static __global__ void __launch_bounds__(kBatchWarps * 32, 5) batch_screen_kernel(BatchArgs A) {
   __shared__ BatchWarpScratch scratch[kBatchWarps];
   __shared__ uint8_t pair_i[kBatchMaxPairs], pair_j[kBatchMaxPairs];
@@ -374,18 +374,18 @@ static __global__ void __launch_bounds__(kBatchWarps * 32, 5) batch_screen_kerne
     if (static_cast<int64_t>(item) >= total) break;
     const int64_t q = static_cast<int64_t>(item);
     if (q < n_select) {
-      batch_select_targets<kWide>(A, A.first_instance + static_cast<int32_t>(q), lane);
+      batch_select_targets<kSpan>(A, A.first_instance + static_cast<int32_t>(q), lane);
     } else if (q < n_select + n_jv) {
       const int64_t e0 = A.jv_first + (q - n_select) * A.jv_tile;
       const int64_t e1 = min(e0 + A.jv_tile, A.jv_last);
       for (int64_t e = e0; e < e1; ++e) {
-        const int32_t w = jv_screen_edge_warp<kWide, true>(A.g, e, scratch[warp].jv, lane, A.error);
+        const int32_t w = jv_screen_edge_warp<kSpan, true>(A.g, e, scratch[warp].jv, lane, A.error);
         if (lane == 0) A.witness[e] = w;
         __syncwarp();
       }
     } else {
       const int64_t s = q - n_select - n_jv;
-      batch_cd_target<kWide>(A, A.first_instance + static_cast<int32_t>(s / A.targets),
+      batch_cd_target<kSpan>(A, A.first_instance + static_cast<int32_t>(s / A.targets),
                              static_cast<int32_t>(s % A.targets), pair_i, pair_j, lane);
     }
     __syncwarp();
@@ -397,7 +397,7 @@ static __global__ void __launch_bounds__(kBatchWarps * 32, 5) batch_screen_kerne
 // flagged pair, and the max_cd smallest (product, c, d) as 64-bit keys
 // product << 32 | (c - n0) << 16 | (d - n0). A separate launch, so that the screen keeps its
 // registers.
-template <bool kWide>
+template <int kSpan>
 __device__ void batch_finalize_target(const BatchArgs& A, int32_t inst, int32_t t, const uint8_t* pair_i,
                                       const uint8_t* pair_j, int lane) {
   const JvGraph& g = A.g;
@@ -420,10 +420,10 @@ __device__ void batch_finalize_target(const BatchArgs& A, int32_t inst, int32_t 
   int2 px = make_int2(0, 0);
   if (have) {
     px = __ldg(g.xy + ln);
-    cu = exact_distance<kWide>(pu, px, g.dist_type);
-    cv = exact_distance<kWide>(pv, px, g.dist_type);
+    cu = exact_distance<kSpan>(pu, px, g.dist_type);
+    cv = exact_distance<kSpan>(pv, px, g.dist_type);
   }
-  const uint32_t cuv = exact_distance<kWide>(pu, pv, g.dist_type);
+  const uint32_t cuv = exact_distance<kSpan>(pu, pv, g.dist_type);
   const uint32_t my_word = lane < A.flag_words ? A.flags[slot * A.flag_words + lane] : 0u;  // lane w: word w
   const bool any_flag = __any_sync(kFullMask, my_word != 0);
   int32_t* cc_out = A.cand_c + slot * A.max_cd;
@@ -436,7 +436,7 @@ __device__ void batch_finalize_target(const BatchArgs& A, int32_t inst, int32_t 
       const int32_t x = __shfl_sync(kFullMask, ln, k);
       const int2 pxk = make_int2(__shfl_sync(kFullMask, px.x, k), __shfl_sync(kFullMask, px.y, k));
       const uint32_t cuk = __shfl_sync(kFullMask, cu, k), cvk = __shfl_sync(kFullMask, cv, k);
-      const int32_t r = ht_reply_count<kWide>(g, u, v, pu, pv, cuv, x, pxk, cuk, cvk, lane);
+      const int32_t r = ht_reply_count<kSpan>(g, u, v, pu, pv, cuv, x, pxk, cuk, cvk, lane);
       if (lane == k) my_replies = r;
     }
   }
@@ -484,7 +484,7 @@ __device__ void batch_finalize_target(const BatchArgs& A, int32_t inst, int32_t 
   if (lane == 0) A.cand_count[slot] = kept;
 }
 
-template <bool kWide>
+template <int kSpan>
 static __global__ void __launch_bounds__(kBatchWarps * 32) batch_finalize_kernel(BatchArgs A) {
   __shared__ uint8_t pair_i[kBatchMaxPairs], pair_j[kBatchMaxPairs];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -501,7 +501,7 @@ static __global__ void __launch_bounds__(kBatchWarps * 32) batch_finalize_kernel
   const int64_t slots = static_cast<int64_t>(A.instances) * A.targets;
   const int64_t warps = static_cast<int64_t>(gridDim.x) * kBatchWarps;
   for (int64_t q = static_cast<int64_t>(blockIdx.x) * kBatchWarps + warp; q < slots; q += warps) {
-    batch_finalize_target<kWide>(A, A.first_instance + static_cast<int32_t>(q / A.targets),
+    batch_finalize_target<kSpan>(A, A.first_instance + static_cast<int32_t>(q / A.targets),
                                  static_cast<int32_t>(q % A.targets), pair_i, pair_j, lane);
     __syncwarp();
   }

@@ -17,19 +17,19 @@ struct CdTask {
   uint32_t active_word;  // low byte = active
 };
 
-template <bool kWide>
+template <int kSpan>
 __device__ __forceinline__ uint8_t cd_flag(int2 pu, int2 pv, uint32_t cuv, int2 pc, int2 pd,
                                            bool active, int mode, int dist_type) {
-  const uint64_t original = static_cast<uint64_t>(cuv) + exact_distance<kWide>(pc, pd, dist_type);
+  const uint64_t original = static_cast<uint64_t>(cuv) + exact_distance<kSpan>(pc, pd, dist_type);
   const uint64_t orient0 =
-      static_cast<uint64_t>(exact_distance<kWide>(pu, pd, dist_type)) + exact_distance<kWide>(pv, pc, dist_type);
+      static_cast<uint64_t>(exact_distance<kSpan>(pu, pd, dist_type)) + exact_distance<kSpan>(pv, pc, dist_type);
   const uint64_t orient1 =
-      static_cast<uint64_t>(exact_distance<kWide>(pu, pc, dist_type)) + exact_distance<kWide>(pv, pd, dist_type);
+      static_cast<uint64_t>(exact_distance<kSpan>(pu, pc, dist_type)) + exact_distance<kSpan>(pv, pd, dist_type);
   const bool incompatible = orient0 < original && orient1 < original;
   return static_cast<uint8_t>(mode == 0 ? (active && incompatible) : (!active || incompatible));
 }
 
-template <bool kWide>
+template <int kSpan>
 static __global__ void cd_screen_kernel(int32_t u, int32_t v, const CdTask* __restrict__ tasks,
                                  int64_t count, const int2* __restrict__ xy, int32_t n,
                                  int32_t dist_type, int32_t mode, uint8_t* __restrict__ flags,
@@ -44,7 +44,7 @@ static __global__ void cd_screen_kernel(int32_t u, int32_t v, const CdTask* __re
     return;
   }
   const int2 pu = __ldg(xy + u), pv = __ldg(xy + v);
-  flags[i] = cd_flag<kWide>(pu, pv, exact_distance<kWide>(pu, pv, dist_type), __ldg(xy + t.c), __ldg(xy + t.d),
+  flags[i] = cd_flag<kSpan>(pu, pv, exact_distance<kSpan>(pu, pv, dist_type), __ldg(xy + t.c), __ldg(xy + t.d),
                      (t.active_word & 0xffu) != 0, mode, dist_type);
 }
 

@@ -68,8 +68,8 @@ int Activate(cee_ctx* ctx) {
 
 // Coordinates as int32 offsets from the bounding-box corner; rejects spans >= 2^30.
 int PackCoordinates(cee_ctx* ctx, int32_t n, const int64_t* x, const int64_t* y,
-                    std::vector<int2>* out, bool* narrow) {
-  *narrow = true;
+                    std::vector<int2>* out, int* span) {
+  *span = kSpanSmall;
   if (n <= 0) {
     out->clear();
     return CEE_OK;
@@ -88,7 +88,7 @@ int PackCoordinates(cee_ctx* ctx, int32_t n, const int64_t* x, const int64_t* y,
     return Fail(ctx, CEE_ERR_RANGE,
                 "coordinate span >= 2^30: outside the exact int32 distance range of the kernels");
   }
-  *narrow = span_x < kNarrowSpan && span_y < kNarrowSpan;
+  *span = span_class(static_cast<int64_t>(span_x), static_cast<int64_t>(span_y));
   out->resize(static_cast<size_t>(n));
   for (int32_t i = 0; i < n; ++i) {
     (*out)[i] = make_int2(static_cast<int32_t>(x[i] - min_x), static_cast<int32_t>(y[i] - min_y));
@@ -186,11 +186,27 @@ int QueryOccupancyOne(const void* kernel, int threads, int smem, int* out) {
 
 cudaError_t QueryOccupancy(cee_ctx* ctx) {
   int bad = 0;
-  bad |= QueryOccupancyOne(reinterpret_cast<const void*>(jv_screen_thread_kernel<false>), kJvThreadBlock, 0, &ctx->occ_jv_thread[0]);
-  bad |= QueryOccupancyOne(reinterpret_cast<const void*>(jv_screen_thread_kernel<true>), kJvThreadBlock, 0, &ctx->occ_jv_thread[1]);
-  bad |= QueryOccupancyOne(reinterpret_cast<const void*>(jv_screen_warp_kernel<false>), kJvWarpsPerBlock * 32, 0, &ctx->occ_jv_warp[0]);
-  bad |= QueryOccupancyOne(reinterpret_cast<const void*>(jv_screen_warp_kernel<true>), kJvWarpsPerBlock * 32, 0, &ctx->occ_jv_warp[1]);
+  for (int span = 0; span < kSpanClasses; ++span) {
+    WithSpan(span, [&](auto S) {
+      bad |= QueryOccupancyOne(reinterpret_cast<const void*>(jv_screen_thread_kernel<S.value>), kJvThreadBlock, 0,
+                               &ctx->occ_jv_thread[span]);
+      bad |= QueryOccupancyOne(reinterpret_cast<const void*>(jv_screen_warp_kernel<S.value>), kJvWarpsPerBlock * 32,
+                               0, &ctx->occ_jv_warp[span]);
+    });
+  }
   return bad ? cudaErrorInvalidValue : cudaSuccess;
+}
+
+// ---------------------------------------------------------------- exact distance --------
+
+template <int kSpan>
+static __global__ void distance_pairs_kernel(const int2* __restrict__ xy, const int2* __restrict__ pairs, int64_t count,
+                                             int32_t dist_type, int32_t* __restrict__ out) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < count; k += stride) {
+    const int2 p = __ldg(pairs + k);
+    out[k] = static_cast<int32_t>(exact_distance<kSpan>(__ldg(xy + p.x), __ldg(xy + p.y), dist_type));
+  }
 }
 
 // ---------------------------------------------------------------- JV --------------------
@@ -210,7 +226,7 @@ int JvPrepare(cee_ctx* ctx, const cee_graph_view* g, cee_jv_stats* stats) {
   if (!static_hit) {
     s.has_static = false;
     std::vector<int2> xy;
-    rc = PackCoordinates(ctx, g->n, g->x, g->y, &xy, &s.narrow);
+    rc = PackCoordinates(ctx, g->n, g->x, g->y, &xy, &s.span);
     if (rc != CEE_OK) return rc;
     std::vector<int2> uv(static_cast<size_t>(g->m));
     std::vector<int32_t> w32(static_cast<size_t>(g->m));
@@ -304,21 +320,17 @@ int JvLaunch(cee_ctx* ctx) {
   graph.slot_w = static_cast<const int32_t*>(s.slotw.ptr);
   int32_t* witness = static_cast<int32_t*>(s.witness.ptr);
   if (ctx->jv_kernel == 1) {
-    const int per_sm = s.narrow ? ctx->occ_jv_warp[0] : ctx->occ_jv_warp[1];
-    const int blocks = GridFor(s.m, kJvWarpsPerBlock, ctx->sm_count * per_sm);
-    if (s.narrow) {
-      jv_screen_warp_kernel<false><<<blocks, kJvWarpsPerBlock * 32, 0, ctx->stream>>>(graph, 0, s.m, witness, ctx->d_error);
-    } else {
-      jv_screen_warp_kernel<true><<<blocks, kJvWarpsPerBlock * 32, 0, ctx->stream>>>(graph, 0, s.m, witness, ctx->d_error);
-    }
+    const int blocks = GridFor(s.m, kJvWarpsPerBlock, ctx->sm_count * ctx->occ_jv_warp[s.span]);
+    WithSpan(s.span, [&](auto S) {
+      jv_screen_warp_kernel<S.value><<<blocks, kJvWarpsPerBlock * 32, 0, ctx->stream>>>(graph, 0, s.m, witness,
+                                                                                         ctx->d_error);
+    });
   } else {
-    const int per_sm = s.narrow ? ctx->occ_jv_thread[0] : ctx->occ_jv_thread[1];
-    const int blocks = GridFor(s.m, kJvThreadBlock, ctx->sm_count * per_sm * ctx->jv_waves);
-    if (s.narrow) {
-      jv_screen_thread_kernel<false><<<blocks, kJvThreadBlock, 0, ctx->stream>>>(graph, 0, s.m, witness, ctx->d_error);
-    } else {
-      jv_screen_thread_kernel<true><<<blocks, kJvThreadBlock, 0, ctx->stream>>>(graph, 0, s.m, witness, ctx->d_error);
-    }
+    const int blocks = GridFor(s.m, kJvThreadBlock, ctx->sm_count * ctx->occ_jv_thread[s.span] * ctx->jv_waves);
+    WithSpan(s.span, [&](auto S) {
+      jv_screen_thread_kernel<S.value><<<blocks, kJvThreadBlock, 0, ctx->stream>>>(graph, 0, s.m, witness,
+                                                                                   ctx->d_error);
+    });
   }
   const cudaError_t status = cudaGetLastError();
   if (status != cudaSuccess) return CudaFail(ctx, status, "jv_screen_kernel launch");
@@ -476,7 +488,7 @@ int KoptCoords(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x, con
   *hit = false;
   s.has_coords = false;
   std::vector<int2> xy;
-  int rc = PackCoordinates(ctx, n, x, y, &xy, &s.narrow);
+  int rc = PackCoordinates(ctx, n, x, y, &xy, &s.span);
   if (rc != CEE_OK) return rc;
   cudaError_t status = s.xy.Reserve(xy.size() * sizeof(int2) + 16, nullptr);
   if (status != cudaSuccess) return CudaFail(ctx, status, "k-opt coordinate allocation");
@@ -570,13 +582,12 @@ int KoptLaunchPrepared(cee_ctx* ctx) {
   }
   if (smem > kKoptSmemBytes) return Fail(ctx, CEE_ERR_INVALID, "k-opt tile exceeds shared memory");
   cudaError_t status = cudaSuccess;
-  if (s.narrow) {
-    if (smem > 48 * 1024) status = cudaFuncSetAttribute(kopt_cost_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (status == cudaSuccess) kopt_cost_kernel<false><<<s.tiles, kKoptThreads, smem, ctx->stream>>>(s.launch, ctx->d_error);
-  } else {
-    if (smem > 48 * 1024) status = cudaFuncSetAttribute(kopt_cost_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (status == cudaSuccess) kopt_cost_kernel<true><<<s.tiles, kKoptThreads, smem, ctx->stream>>>(s.launch, ctx->d_error);
-  }
+  WithSpan(s.span, [&](auto S) {
+    if (smem > 48 * 1024) {
+      status = cudaFuncSetAttribute(kopt_cost_kernel<S.value>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    }
+    if (status == cudaSuccess) kopt_cost_kernel<S.value><<<s.tiles, kKoptThreads, smem, ctx->stream>>>(s.launch, ctx->d_error);
+  });
   if (status == cudaSuccess) status = cudaGetLastError();
   if (status != cudaSuccess) return CudaFail(ctx, status, "kopt_cost_kernel launch");
   return CEE_OK;
@@ -1021,7 +1032,7 @@ int cee_cd_screen(cee_ctx* ctx, const cee_graph_view* graph, int32_t u, int32_t 
         SameArray(s.hy, graph->y, graph->n))) {
     s.has_coords = false;
     std::vector<int2> xy;
-    rc = PackCoordinates(ctx, graph->n, graph->x, graph->y, &xy, &s.narrow);
+    rc = PackCoordinates(ctx, graph->n, graph->x, graph->y, &xy, &s.span);
     if (rc != CEE_OK) return rc;
     cudaError_t status = s.xy.Reserve(xy.size() * sizeof(int2) + 16, nullptr);
     if (status == cudaSuccess) status = cudaMemcpy(s.xy.ptr, xy.data(), xy.size() * sizeof(int2), cudaMemcpyHostToDevice);
@@ -1038,15 +1049,11 @@ int cee_cd_screen(cee_ctx* ctx, const cee_graph_view* graph, int32_t u, int32_t 
   cudaStream_t st = ctx->stream;
   cudaMemsetAsync(ctx->d_error, 0, sizeof(int32_t), st);
   cudaMemcpyAsync(s.tasks.ptr, tasks, static_cast<size_t>(count) * sizeof(cee_cd_task), cudaMemcpyHostToDevice, st);
-  if (s.narrow) {
-    cd_screen_kernel<false><<<GridFor(count, 256, 1 << 30), 256, 0, st>>>(
+  WithSpan(s.span, [&](auto S) {
+    cd_screen_kernel<S.value><<<GridFor(count, 256, 1 << 30), 256, 0, st>>>(
         u, v, static_cast<const CdTask*>(s.tasks.ptr), count, static_cast<const int2*>(s.xy.ptr), s.n,
         s.dist_type, mode, static_cast<uint8_t*>(s.flags.ptr), ctx->d_error);
-  } else {
-    cd_screen_kernel<true><<<GridFor(count, 256, 1 << 30), 256, 0, st>>>(
-        u, v, static_cast<const CdTask*>(s.tasks.ptr), count, static_cast<const int2*>(s.xy.ptr), s.n,
-        s.dist_type, mode, static_cast<uint8_t*>(s.flags.ptr), ctx->d_error);
-  }
+  });
   status = cudaGetLastError();
   if (status != cudaSuccess) return CudaFail(ctx, status, "cd_screen_kernel launch");
   cudaMemcpyAsync(flags_out, s.flags.ptr, static_cast<size_t>(count), cudaMemcpyDeviceToHost, st);
@@ -1054,6 +1061,55 @@ int cee_cd_screen(cee_ctx* ctx, const cee_graph_view* graph, int32_t u, int32_t 
   status = cudaStreamSynchronize(st);
   if (status != cudaSuccess) return CudaFail(ctx, status, "c,d screen");
   return CheckDeviceError(ctx, "c,d screen");
+}
+
+int cee_exact_distances(cee_ctx* ctx, int32_t n, const int64_t* x, const int64_t* y, int32_t dist_type,
+                        int64_t count, const int32_t* pair_i, const int32_t* pair_j, int32_t* out,
+                        int32_t* span_class) {
+  if (ctx == nullptr) return Fail(nullptr, CEE_ERR_INVALID, "null context");
+  int rc = Activate(ctx);
+  if (rc != CEE_OK) return rc;
+  if (n < 0 || count < 0 || (dist_type != CEE_EUC_2D && dist_type != CEE_CEIL_2D) ||
+      (count > 0 && (pair_i == nullptr || pair_j == nullptr || out == nullptr))) {
+    return Fail(ctx, CEE_ERR_INVALID, "exact distances: bad arguments");
+  }
+  std::vector<int2> pairs(static_cast<size_t>(count));
+  for (int64_t k = 0; k < count; ++k) {
+    if (pair_i[k] < 0 || pair_i[k] >= n || pair_j[k] < 0 || pair_j[k] >= n) {
+      return Fail(ctx, CEE_ERR_INVALID, "exact distances: point index out of range");
+    }
+    pairs[static_cast<size_t>(k)] = make_int2(pair_i[k], pair_j[k]);
+  }
+  std::vector<int2> xy;
+  int span = kSpanSmall;
+  rc = PackCoordinates(ctx, n, x, y, &xy, &span);
+  if (rc != CEE_OK) return rc;
+  if (span_class != nullptr) *span_class = span;
+  if (count == 0) return CEE_OK;
+  DevBuf d_xy, d_pairs, d_out;
+  cudaError_t status = d_xy.Reserve(xy.size() * sizeof(int2), nullptr);
+  if (status == cudaSuccess) status = d_pairs.Reserve(pairs.size() * sizeof(int2), nullptr);
+  if (status == cudaSuccess) status = d_out.Reserve(static_cast<size_t>(count) * sizeof(int32_t), nullptr);
+  cudaStream_t st = ctx->stream;
+  if (status == cudaSuccess) {
+    cudaMemcpyAsync(d_xy.ptr, xy.data(), xy.size() * sizeof(int2), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_pairs.ptr, pairs.data(), pairs.size() * sizeof(int2), cudaMemcpyHostToDevice, st);
+    WithSpan(span, [&](auto S) {
+      distance_pairs_kernel<S.value><<<GridFor(count, 256, ctx->sm_count * 8), 256, 0, st>>>(
+          static_cast<const int2*>(d_xy.ptr), static_cast<const int2*>(d_pairs.ptr), count, dist_type,
+          static_cast<int32_t*>(d_out.ptr));
+    });
+    status = cudaGetLastError();
+  }
+  if (status == cudaSuccess) {
+    cudaMemcpyAsync(out, d_out.ptr, static_cast<size_t>(count) * sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+    status = cudaStreamSynchronize(st);
+  }
+  d_xy.Release();
+  d_pairs.Release();
+  d_out.Release();
+  if (status != cudaSuccess) return CudaFail(ctx, status, "exact distances");
+  return CEE_OK;
 }
 
 }  // extern "C"

@@ -8,6 +8,7 @@
 
 #include <cstdint>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 namespace cee {
@@ -28,7 +29,7 @@ struct JvState {
   std::vector<int64_t> hx, hy, hw;
   std::vector<int32_t> heu, hev;
   DevBuf xy, uv, w32;
-  bool narrow = true;  // coordinate span < 2^26: FP64 distance path
+  int span = kSpanSmall;  // span class of the coordinates (exact-distance routine)
   // dynamic workspace, refreshed every call
   DevBuf active, ro, nbr, ids, slotw, witness;
   int64_t adjacency = 0;
@@ -66,7 +67,7 @@ struct KoptState {
   int32_t n = 0, dist_type = 0;
   std::vector<int64_t> hx, hy;
   DevBuf xy;
-  bool narrow = true;
+  int span = kSpanSmall;
   KoptTable user[3];   // caller templates per k (the reference's template cache)
   KoptTable canon[3];  // this library's proper templates per k
   DevBuf tasks, costs;
@@ -97,7 +98,7 @@ struct CdState {
   int32_t n = 0, dist_type = 0;
   std::vector<int64_t> hx, hy;
   DevBuf xy, tasks, flags;
-  bool narrow = true;
+  int span = kSpanSmall;
   void Release() {
     xy.Release();
     tasks.Release();
@@ -119,8 +120,8 @@ struct cee_ctx {
   int sm_count = 148;
   int jv_kernel = 1;                  // 0 = thread per edge, 1 = warp per edge (default)
   int jv_waves = 4;                   // grid = SMs x resident blocks x waves (thread kernel)
-  int occ_jv_thread[2] = {1, 1};      // resident blocks per SM, [narrow, wide]
-  int occ_jv_warp[2] = {1, 1};
+  int occ_jv_thread[cee::kSpanClasses] = {1, 1, 1};  // resident blocks per SM, per span class
+  int occ_jv_warp[cee::kSpanClasses] = {1, 1, 1};
   int kopt_rows_per_tile[3] = {0, 0, 0};  // 0 = default tile for k = 3, 4, 5
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[6] = {};
@@ -137,11 +138,25 @@ struct cee_ctx {
 
 namespace cee {
 
+// Calls f(std::integral_constant<int, S>{}) with S the span class `span`, so that one call site
+// launches the kernel instantiation for that class.
+template <typename F>
+decltype(auto) WithSpan(int span, F&& f) {
+  switch (span) {
+    case kSpanSmall:
+      return f(std::integral_constant<int, kSpanSmall>{});
+    case kSpanNarrow:
+      return f(std::integral_constant<int, kSpanNarrow>{});
+    default:
+      return f(std::integral_constant<int, kSpanWide>{});
+  }
+}
+
 int Fail(cee_ctx* ctx, int code, const std::string& message);
 int CudaFail(cee_ctx* ctx, cudaError_t status, const char* what);
 int Activate(cee_ctx* ctx);
 int PackCoordinates(cee_ctx* ctx, int32_t n, const int64_t* x, const int64_t* y, std::vector<int2>* out,
-                    bool* narrow);
+                    int* span);
 int GridFor(int64_t work, int per_block, int max_blocks);
 float EventMs(cudaEvent_t a, cudaEvent_t b);
 int CheckDeviceError(cee_ctx* ctx, const char* what);

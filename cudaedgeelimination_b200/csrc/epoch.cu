@@ -90,14 +90,14 @@ static __global__ void scan_add(int32_t* __restrict__ out, int64_t count, const 
 // ---- epoch kernels ---------------------------------------------------------------------------
 
 // JV screen of every edge with one 16-byte load per CSR slot.
-template <bool kWide>
+template <int kSpan>
 static __global__ void __launch_bounds__(kJvWarpsPerBlock * 32)
     epoch_screen(JvGraph g, int32_t* __restrict__ witness, int32_t* __restrict__ error) {
   __shared__ JvWarpScratch scratch[kJvWarpsPerBlock];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t warps = static_cast<int64_t>(gridDim.x) * kJvWarpsPerBlock;
   for (int64_t e = static_cast<int64_t>(blockIdx.x) * kJvWarpsPerBlock + warp; e < g.m; e += warps) {
-    const int32_t w = jv_screen_edge_warp<kWide, true>(g, e, scratch[warp], lane, error);
+    const int32_t w = jv_screen_edge_warp<kSpan, true>(g, e, scratch[warp], lane, error);
     if (lane == 0) witness[e] = w;
     __syncwarp();
   }
@@ -322,8 +322,8 @@ extern "C" int cee_jv_eliminate(cee_ctx* ctx, const cee_graph_view* g, uint32_t 
     }
   }
   std::vector<int2> xy;
-  bool narrow = true;
-  rc = PackCoordinates(ctx, n, g->x, g->y, &xy, &narrow);
+  int span = kSpanSmall;
+  rc = PackCoordinates(ctx, n, g->x, g->y, &xy, &span);
   if (rc != CEE_OK) return rc;
   std::vector<int2> uv(static_cast<size_t>(m));
   std::vector<int32_t> w32(static_cast<size_t>(m)), degree(static_cast<size_t>(n));
@@ -380,8 +380,9 @@ extern "C" int cee_jv_eliminate(cee_ctx* ctx, const cee_graph_view* g, uint32_t 
         static_cast<int4*>(s.slot4[0].ptr), ctx->d_error);
   }
   int occ = 1;
-  status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &occ, narrow ? epoch_screen<false> : epoch_screen<true>, kJvWarpsPerBlock * 32, 0);
+  WithSpan(span, [&](auto S) {
+    status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, epoch_screen<S.value>, kJvWarpsPerBlock * 32, 0);
+  });
   if (status != cudaSuccess) return CudaFail(ctx, status, "epoch occupancy");
   const int screen_blocks = GridFor(m, kJvWarpsPerBlock, ctx->sm_count * std::max(1, occ));
   int32_t* counters = static_cast<int32_t*>(s.counters.ptr);  // [0] committed, [1] undecided
@@ -407,11 +408,9 @@ extern "C" int cee_jv_eliminate(cee_ctx* ctx, const cee_graph_view* g, uint32_t 
     jg.nbr = static_cast<const int32_t*>(s.nbr[cur].ptr);
     jg.slot4 = static_cast<const int4*>(s.slot4[cur].ptr);
     int32_t* witness = static_cast<int32_t*>(s.witness.ptr);
-    if (narrow) {
-      epoch_screen<false><<<screen_blocks, kJvWarpsPerBlock * 32, 0, st>>>(jg, witness, ctx->d_error);
-    } else {
-      epoch_screen<true><<<screen_blocks, kJvWarpsPerBlock * 32, 0, st>>>(jg, witness, ctx->d_error);
-    }
+    WithSpan(span, [&](auto S) {
+      epoch_screen<S.value><<<screen_blocks, kJvWarpsPerBlock * 32, 0, st>>>(jg, witness, ctx->d_error);
+    });
     // candidates in (u, v) order
     epoch_flags<<<GridFor(m, 256, grid), 256, 0, st>>>(static_cast<const int32_t*>(s.order.ptr), m, witness,
                                                           static_cast<int32_t*>(s.flag.ptr));

@@ -62,7 +62,7 @@ __device__ __forceinline__ void top10_insert(uint64_t (&list)[kJvMaxCandidates],
   }
 }
 
-template <bool kWide>
+template <int kSpan>
 __device__ __forceinline__ int32_t jv_screen_edge_thread(const JvGraph& g, int64_t e,
                                                          int32_t* __restrict__ error) {
   if (g.active[e] == 0) return -1;
@@ -86,7 +86,7 @@ __device__ __forceinline__ int32_t jv_screen_edge_thread(const JvGraph& g, int64
       continue;
     }
     const uint64_t score = static_cast<uint64_t>(static_cast<uint32_t>(__ldg(g.slot_w + off))) +
-                           exact_distance<kWide>(__ldg(g.xy + c), pb, g.dist_type);
+                           exact_distance<kSpan>(__ldg(g.xy + c), pb, g.dist_type);
     top10_insert(top, (score << 32) | static_cast<uint32_t>(c));
   }
   // N(b) ascending, skipping nodes already reached through N(a) (merge walk over N(a))
@@ -104,7 +104,7 @@ __device__ __forceinline__ int32_t jv_screen_edge_thread(const JvGraph& g, int64
       continue;
     }
     const uint64_t score = static_cast<uint64_t>(static_cast<uint32_t>(__ldg(g.slot_w + off))) +
-                           exact_distance<kWide>(__ldg(g.xy + c), pa, g.dist_type);
+                           exact_distance<kSpan>(__ldg(g.xy + c), pa, g.dist_type);
     top10_insert(top, (score << 32) | static_cast<uint32_t>(c));
   }
 
@@ -113,8 +113,8 @@ __device__ __forceinline__ int32_t jv_screen_edge_thread(const JvGraph& g, int64
     if (top[i] == kEmptyKey) return -1;
     const int32_t c = static_cast<int32_t>(top[i] & 0xffffffffu);
     const int2 pc = __ldg(g.xy + c);
-    const int64_t cac = exact_distance<kWide>(pa, pc, g.dist_type);
-    const int64_t cbc = exact_distance<kWide>(pb, pc, g.dist_type);
+    const int64_t cac = exact_distance<kSpan>(pa, pc, g.dist_type);
+    const int64_t cbc = exact_distance<kSpan>(pb, pc, g.dist_type);
     const int32_t rc1 = __ldg(g.row_offsets + c + 1);
     bool witness = true;
     for (int32_t off = __ldg(g.row_offsets + c); off < rc1; ++off) {
@@ -126,8 +126,8 @@ __device__ __forceinline__ int32_t jv_screen_edge_thread(const JvGraph& g, int64
       }
       const int2 pd = __ldg(g.xy + d);
       const int64_t left = cab + __ldg(g.slot_w + off);
-      if (left <= cac + exact_distance<kWide>(pd, pb, g.dist_type) ||
-          left <= exact_distance<kWide>(pa, pd, g.dist_type) + cbc) {
+      if (left <= cac + exact_distance<kSpan>(pd, pb, g.dist_type) ||
+          left <= exact_distance<kSpan>(pa, pd, g.dist_type) + cbc) {
         witness = false;  // d is compatible with (a,b)
         break;
       }
@@ -137,13 +137,13 @@ __device__ __forceinline__ int32_t jv_screen_edge_thread(const JvGraph& g, int64
   return -1;
 }
 
-template <bool kWide>
+template <int kSpan>
 static __global__ void __launch_bounds__(kJvThreadBlock)
     jv_screen_thread_kernel(JvGraph g, int64_t first, int64_t last, int32_t* __restrict__ witness,
                             int32_t* __restrict__ error) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t e = first + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < last; e += stride) {
-    witness[e] = jv_screen_edge_thread<kWide>(g, e, error);
+    witness[e] = jv_screen_edge_thread<kSpan>(g, e, error);
   }
 }
 
@@ -160,7 +160,7 @@ struct JvWarpScratch {
 
 // Screens edge e with the calling (full) warp; returns the witness or -1 on every lane. With
 // kSlot4 a CSR slot's neighbour, weight and neighbour coordinates come from one 16-byte load.
-template <bool kWide, bool kSlot4 = false>
+template <int kSpan, bool kSlot4 = false>
 __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t e, JvWarpScratch& s,
                                                        int lane, int32_t* __restrict__ error) {
   if (__ldg(g.active + e) == 0) return -1;
@@ -212,7 +212,7 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
         sw = __ldg(g.slot_w + slot);
         pc = __ldg(g.xy + c);
       }
-      score = static_cast<uint64_t>(static_cast<uint32_t>(sw)) + exact_distance<kWide>(pc, second ? pa : pb, g.dist_type);
+      score = static_cast<uint64_t>(static_cast<uint32_t>(sw)) + exact_distance<kSpan>(pc, second ? pa : pb, g.dist_type);
       key = (score << 32) | static_cast<uint32_t>(c);
     }
     if (total <= 32) {
@@ -244,7 +244,7 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
     const uint64_t key = __shfl_sync(kFullMask, top, ci);
     if (lane < 2 * kJvMaxCandidates && ci < nc) {
       const int32_t c = static_cast<int32_t>(key & 0xffffffffu);
-      const uint32_t dist = exact_distance<kWide>(lane < kJvMaxCandidates ? pa : pb, __ldg(g.xy + c), g.dist_type);
+      const uint32_t dist = exact_distance<kSpan>(lane < kJvMaxCandidates ? pa : pb, __ldg(g.xy + c), g.dist_type);
       if (lane < kJvMaxCandidates) {
         s.c[ci] = c;
         s.row[ci] = __ldg(g.row_offsets + c);
@@ -278,8 +278,8 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
       dw = __ldg(g.slot_w + slot);
     }
     const int64_t left = cab + dw;
-    return left <= static_cast<int64_t>(s.cac[ci]) + exact_distance<kWide>(pd, pb, g.dist_type) ||
-           left <= static_cast<int64_t>(exact_distance<kWide>(pa, pd, g.dist_type)) + s.cbc[ci];
+    return left <= static_cast<int64_t>(s.cac[ci]) + exact_distance<kSpan>(pd, pb, g.dist_type) ||
+           left <= static_cast<int64_t>(exact_distance<kSpan>(pa, pd, g.dist_type)) + s.cbc[ci];
   };
 
   constexpr int kHead = 3;
@@ -331,7 +331,7 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
   }
 }
 
-template <bool kWide>
+template <int kSpan>
 static __global__ void __launch_bounds__(kJvWarpsPerBlock * 32)
     jv_screen_warp_kernel(JvGraph g, int64_t first, int64_t last, int32_t* __restrict__ witness,
                           int32_t* __restrict__ error) {
@@ -340,7 +340,7 @@ static __global__ void __launch_bounds__(kJvWarpsPerBlock * 32)
   const int warp = threadIdx.x >> 5;
   const int64_t warps = static_cast<int64_t>(gridDim.x) * kJvWarpsPerBlock;
   for (int64_t e = first + static_cast<int64_t>(blockIdx.x) * kJvWarpsPerBlock + warp; e < last; e += warps) {
-    const int32_t w = jv_screen_edge_warp<kWide>(g, e, scratch[warp], lane, error);
+    const int32_t w = jv_screen_edge_warp<kSpan>(g, e, scratch[warp], lane, error);
     if (lane == 0) witness[e] = w;
     __syncwarp();
   }

@@ -17,12 +17,12 @@
 // (a proper template never pairs 2e with 2e+1; a caller template that does is marked in its
 // pair table and yields invalid cells).
 //
-// Narrow coordinates (span < 2^26, each distance < 2^26.5): a pair's entry is one 64-bit word,
+// Small and narrow span classes (span < 2^26, each distance < 2^26.5): a pair's entry is one 64-bit word,
 // low half = its distance, or 2^29 when the pair is bad; high half = 1 << 3f when its code is
 // the f-th multi code of the row, else 0. A cell adds its k entries: the low half is the cost
 // (< 5 * 2^26.5 < 2^29 unless a bad pair is present; < 2^32 always), each 3-bit field of the
 // high half counts the template's pairs on one multi code (<= 5), and the cell is invalid iff
-// low >= 2^29 or some field is >= 2. Wide coordinates keep int32 distances and a one-hot 64-bit
+// low >= 2^29 or some field is >= 2. The wide span class keeps int32 distances and a one-hot 64-bit
 // mask per pair (bit = code, bit 63 = bad): invalid iff the OR of the k masks has bit 63 set or
 // fewer than k bits.
 //
@@ -198,15 +198,15 @@ __device__ __forceinline__ void kopt_row_classes(const int32_t* nodes, const uin
 }
 
 // Stage C for one (row, pair): the exact distance and the pair's entry (narrow) or mask (wide).
-template <int K, bool kWide>
+template <int K, int kSpan>
 __device__ __forceinline__ void kopt_pair_entry(const KoptSmem& sm, int r, int pid, const int2* xy, int32_t dist_type) {
   constexpr int P = 2 * K, NP = K * (P - 1);
   const int p = sm.pp[pid], q = sm.pq[pid];
   const int32_t* pr = sm.ports + r * P;
   const int2 a = __ldg(xy + pr[p]);
   const int2 b = __ldg(xy + pr[q]);
-  const uint32_t d = exact_distance<kWide>(a, b, dist_type);
-  if constexpr (kWide) {
+  const uint32_t d = exact_distance<kSpan>(a, b, dist_type);
+  if constexpr (kSpan == kSpanWide) {
     sm.dist[r * NP + pid] = static_cast<int32_t>(d);
     if (sm.repeats[r] != 0) {
       const uint8_t* cr = sm.cls + r * P;
@@ -231,10 +231,10 @@ __device__ __forceinline__ void kopt_pair_entry(const KoptSmem& sm, int r, int p
 }
 
 // Stage D for one cell.
-template <int K, bool kWide>
+template <int K, int kSpan>
 __device__ __forceinline__ int64_t kopt_cell(const KoptSmem& sm, int r, const int (&pid)[K]) {
   constexpr int NP = K * (2 * K - 1);
-  if constexpr (kWide) {
+  if constexpr (kSpan == kSpanWide) {
     const int32_t* dr = sm.dist + r * NP;
     int64_t v = 0;
 #pragma unroll
@@ -257,7 +257,7 @@ __device__ __forceinline__ int64_t kopt_cell(const KoptSmem& sm, int r, const in
   }
 }
 
-template <int K, bool kWide>
+template <int K, int kSpan>
 __device__ __forceinline__ void kopt_tile(const KoptLaunch& L, const KoptSegment& S, int64_t row0, int rows,
                                           unsigned char* smem, int32_t* error) {
   constexpr int P = 2 * K, NP = K * (P - 1);
@@ -287,7 +287,7 @@ __device__ __forceinline__ void kopt_tile(const KoptLaunch& L, const KoptSegment
   __syncthreads();
   for (int i = tid; i < rows * NP; i += kKoptThreads) {
     const int r = i / NP;
-    kopt_pair_entry<K, kWide>(sm, r, i - r * NP, L.xy, L.dist_type);
+    kopt_pair_entry<K, kSpan>(sm, r, i - r * NP, L.xy, L.dist_type);
   }
   __syncthreads();
   const int T = S.templates;
@@ -302,7 +302,7 @@ __device__ __forceinline__ void kopt_tile(const KoptLaunch& L, const KoptSegment
     long long* out = reinterpret_cast<long long*>(S.costs + row0 * T) + static_cast<int64_t>(rr) * T + t;
     const int64_t out_step = static_cast<int64_t>(per_step) * T;
     for (int r = rr; r < rows; r += per_step, out += out_step) {
-      const int64_t v = readds_deleted ? INT64_MAX : kopt_cell<K, kWide>(sm, r, pid);
+      const int64_t v = readds_deleted ? INT64_MAX : kopt_cell<K, kSpan>(sm, r, pid);
       if (S.write_costs != 0) __stcs(out, static_cast<long long>(v));
       // the leaf consumer tries templates with added cost < deleted cost (src/cpu/kopt_search.cpp:697)
       if (W > 0 && v < sm.deleted[r]) atomicOr(sm.imask + r * W + (t >> 5), 1u << (t & 31));
@@ -321,7 +321,7 @@ __device__ __forceinline__ void kopt_tile(const KoptLaunch& L, const KoptSegment
   }
 }
 
-template <bool kWide>
+template <int kSpan>
 static __global__ void __launch_bounds__(kKoptThreads, 4) kopt_cost_kernel(KoptLaunch L,
                                                                         int32_t* __restrict__ error) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -333,13 +333,13 @@ static __global__ void __launch_bounds__(kKoptThreads, 4) kopt_cost_kernel(KoptL
   const int rows = static_cast<int>(min(static_cast<int64_t>(S.rows_per_tile), S.rows - row0));
   switch (S.k) {
     case 3:
-      kopt_tile<3, kWide>(L, S, row0, rows, smem, error);
+      kopt_tile<3, kSpan>(L, S, row0, rows, smem, error);
       break;
     case 4:
-      kopt_tile<4, kWide>(L, S, row0, rows, smem, error);
+      kopt_tile<4, kSpan>(L, S, row0, rows, smem, error);
       break;
     default:
-      kopt_tile<5, kWide>(L, S, row0, rows, smem, error);
+      kopt_tile<5, kSpan>(L, S, row0, rows, smem, error);
       break;
   }
 }

@@ -12,7 +12,7 @@
 // kNoAllocMaxSlots) and a status word. Every GPU that loads the library holds these arrays
 // (16 MiB + 256 B) until the process exits. Every call shares them and they keep the last
 // call's contents: the slot weights are rewritten in full for [0, adjacency) and the status
-// word is cleared at the start of each call. Calls whose work overlaps on the GPU (different
+// words are cleared at the start of each call. Calls whose work overlaps on the GPU (different
 // streams, or different host threads on the same device) race on these arrays and must be
 // serialised by the caller.
 #include "cee.h"
@@ -52,15 +52,28 @@ enum : int32_t {
   kBadEdgeId = 16,
 };
 
-// Validates the caller's device snapshot and builds the slot weights in the scratch array.
+// Validates the caller's device snapshot and builds the slot weights in the scratch array;
+// status[1], status[2] receive the largest x and y (the coordinates are >= 0, so these bound the
+// spans and select the exact-distance routine).
 __global__ void noalloc_prepare(cee_device_graph g, int32_t* __restrict__ slot_w, int32_t* __restrict__ status) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   const int64_t first = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const uint32_t limit = 1u << 30;
+  uint32_t max_x = 0, max_y = 0;
   for (int64_t i = first; i < g.n; i += stride) {
-    if (static_cast<uint32_t>(g.xy[2 * i]) >= limit || static_cast<uint32_t>(g.xy[2 * i + 1]) >= limit) {
+    const uint32_t x = static_cast<uint32_t>(g.xy[2 * i]), y = static_cast<uint32_t>(g.xy[2 * i + 1]);
+    if (x >= limit || y >= limit) {
       atomicOr(status, kBadCoordinate);
+    } else {
+      max_x = max(max_x, x);
+      max_y = max(max_y, y);
     }
+  }
+  max_x = __reduce_max_sync(kFullMask, max_x);
+  max_y = __reduce_max_sync(kFullMask, max_y);
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(status + 1, static_cast<int32_t>(max_x));
+    atomicMax(status + 2, static_cast<int32_t>(max_y));
   }
   for (int64_t i = first; i <= g.n; i += stride) {
     const int32_t here = g.row_offsets[i];
@@ -102,8 +115,16 @@ int NoAllocSetup(int device, NoAllocDevice** out) {
     if (rc == cudaSuccess) rc = cudaGetSymbolAddress(&status, g_noalloc_status);
     if (rc == cudaSuccess) rc = cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device);
     if (rc == cudaSuccess) {
-      rc = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.warp_blocks_per_sm, jv_screen_warp_kernel<true>,
-                                                         kJvWarpsPerBlock * 32, 0);
+      // the smallest occupancy of the three span classes' instantiations sizes every launch
+      d.warp_blocks_per_sm = 1 << 20;
+      for (int span = 0; span < kSpanClasses && rc == cudaSuccess; ++span) {
+        WithSpan(span, [&](auto S) {
+          int blocks = 0;
+          rc = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, jv_screen_warp_kernel<S.value>,
+                                                             kJvWarpsPerBlock * 32, 0);
+          d.warp_blocks_per_sm = std::min(d.warp_blocks_per_sm, blocks);
+        });
+      }
     }
     if (rc != cudaSuccess) {
       cudaGetLastError();
@@ -118,9 +139,12 @@ int NoAllocSetup(int device, NoAllocDevice** out) {
   return CEE_OK;
 }
 
-int ReadStatus(const NoAllocDevice& d, cudaStream_t stream, const char* stage) {
-  int32_t status = 0;
-  cudaError_t rc = cudaMemcpyAsync(&status, d.status, sizeof(int32_t), cudaMemcpyDeviceToHost, stream);
+// Reads the status word (and, with `bounds`, the two coordinate maxima after it).
+int ReadStatus(const NoAllocDevice& d, cudaStream_t stream, const char* stage, int32_t* bounds = nullptr) {
+  int32_t words[3] = {0, 0, 0};
+  cudaError_t rc = cudaMemcpyAsync(words, d.status, (bounds != nullptr ? 3 : 1) * sizeof(int32_t),
+                                   cudaMemcpyDeviceToHost, stream);
+  const int32_t& status = words[0];
   if (rc == cudaSuccess) rc = cudaStreamSynchronize(stream);
   if (rc != cudaSuccess) {
     cudaGetLastError();
@@ -129,6 +153,10 @@ int ReadStatus(const NoAllocDevice& d, cudaStream_t stream, const char* stage) {
   if (status != 0) {
     return NoAllocFail(CEE_ERR_INVALID, std::string(stage) + ": the device snapshot failed validation (status bits " +
                                             std::to_string(status) + ")");
+  }
+  if (bounds != nullptr) {
+    bounds[0] = words[1];
+    bounds[1] = words[2];
   }
   return CEE_OK;
 }
@@ -166,7 +194,7 @@ extern "C" int cee_jv_screen_noalloc(const cee_device_graph* graph, int32_t* wit
   if (rc != CEE_OK) return rc;
   cudaStream_t stream = static_cast<cudaStream_t>(stream_handle);
 
-  cudaError_t status = cudaMemsetAsync(d->status, 0, sizeof(int32_t), stream);
+  cudaError_t status = cudaMemsetAsync(d->status, 0, 3 * sizeof(int32_t), stream);
   if (status == cudaSuccess) {
     const int64_t work = g.adjacency > g.m ? g.adjacency : (g.m > g.n ? g.m : g.n + 1);
     const int blocks = static_cast<int>(std::min<int64_t>((work + 255) / 256, static_cast<int64_t>(d->sms) * 8));
@@ -177,8 +205,10 @@ extern "C" int cee_jv_screen_noalloc(const cee_device_graph* graph, int32_t* wit
     cudaGetLastError();
     return NoAllocFail(CEE_ERR_CUDA, std::string("validation launch: ") + cudaGetErrorString(status));
   }
-  rc = ReadStatus(*d, stream, "validation");
+  int32_t bounds[2] = {0, 0};
+  rc = ReadStatus(*d, stream, "validation", bounds);
   if (rc != CEE_OK) return rc;
+  const int span = span_class(bounds[0], bounds[1]);
 
   JvGraph jg{};
   jg.n = g.n;
@@ -193,7 +223,9 @@ extern "C" int cee_jv_screen_noalloc(const cee_device_graph* graph, int32_t* wit
   jg.slot_w = d->slot_w;
   const int64_t max_blocks = static_cast<int64_t>(d->sms) * d->warp_blocks_per_sm;
   const int blocks = static_cast<int>(std::min<int64_t>((g.m + kJvWarpsPerBlock - 1) / kJvWarpsPerBlock, max_blocks));
-  jv_screen_warp_kernel<true><<<blocks, kJvWarpsPerBlock * 32, 0, stream>>>(jg, 0, g.m, witness_out, d->status);
+  WithSpan(span, [&](auto S) {
+    jv_screen_warp_kernel<S.value><<<blocks, kJvWarpsPerBlock * 32, 0, stream>>>(jg, 0, g.m, witness_out, d->status);
+  });
   status = cudaGetLastError();
   if (status != cudaSuccess) return NoAllocFail(CEE_ERR_CUDA, std::string("screen launch: ") + cudaGetErrorString(status));
   return ReadStatus(*d, stream, "screen");

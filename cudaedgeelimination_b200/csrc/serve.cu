@@ -74,7 +74,7 @@ struct ServeSnapshotHost {
   size_t offset = 0, bytes = 0;
   int32_t n = 0, dist_type = 0;
   int64_t m = 0, adj = 0;
-  bool narrow = true;
+  int span = kSpanSmall;
   JvGraph g{};
   int refs = 0;
 };
@@ -379,8 +379,8 @@ int cee_serve_add_snapshot(cee_ctx* ctx, const cee_graph_view* g, int32_t* snaps
     }
   }
   std::vector<int2> xy;
-  bool narrow = true;
-  rc = PackCoordinates(ctx, g->n, g->x, g->y, &xy, &narrow);
+  int span = kSpanSmall;
+  rc = PackCoordinates(ctx, g->n, g->x, g->y, &xy, &span);
   if (rc != CEE_OK) return rc;
   const size_t n = static_cast<size_t>(g->n), m = static_cast<size_t>(g->m);
   const size_t adj = g->m > 0 ? static_cast<size_t>(g->adjacency) : 0;
@@ -455,7 +455,7 @@ int cee_serve_add_snapshot(cee_ctx* ctx, const cee_graph_view* g, int32_t* snaps
   snap.m = g->m;
   snap.adj = static_cast<int64_t>(adj);
   snap.dist_type = g->dist_type;
-  snap.narrow = narrow;
+  snap.span = span;
   snap.g.n = g->n;
   snap.g.dist_type = g->dist_type;
   snap.g.m = g->m;
@@ -521,7 +521,7 @@ int cee_serve_submit_jv(cee_ctx* ctx, int32_t snapshot, int32_t* witness_out, ui
   ServeJob desc{};
   desc.generation = s.next_generation++;
   desc.type = kServeJv;
-  desc.narrow = snap.narrow ? 1 : 0;
+  desc.span = snap.span;
   desc.g = snap.g;
   desc.witness = reinterpret_cast<int32_t*>(static_cast<uint8_t*>(s.arena_buf.ptr) + out);
   desc.items = static_cast<uint32_t>((snap.m + kServeJvTile - 1) / kServeJvTile);
@@ -595,7 +595,7 @@ int cee_serve_submit_kopt(cee_ctx* ctx, int32_t snapshot, int32_t segments, cons
   ServeJob desc{};
   desc.generation = s.next_generation++;
   desc.type = kServeKopt;
-  desc.narrow = snap.narrow ? 1 : 0;
+  desc.span = snap.span;
   desc.g = snap.g;
   desc.segments = segments;
   uint8_t* arena = static_cast<uint8_t*>(s.arena_buf.ptr);

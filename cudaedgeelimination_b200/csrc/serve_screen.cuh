@@ -47,7 +47,7 @@ struct ServeSegment {
 struct ServeJob {
   uint32_t generation;
   int32_t type;
-  int32_t narrow;
+  int32_t span;  // span class of the snapshot's coordinates (kSpanSmall / kSpanNarrow / kSpanWide)
   int32_t segments;
   uint32_t items;
   uint32_t pad;
@@ -82,7 +82,7 @@ static_assert(kopt_tile_smem(5, serve_rows_per_chunk(5)) <= kServeKoptScratch, "
 
 // The k-opt cells of rows [row_begin, row_end) of a segment, one warp, chunk by chunk
 // (kopt_cost_kernel's stages at warp size).
-template <int K, bool kWide>
+template <int K, int kSpan>
 __device__ void kopt_rows_warp(const ServeSegment& S, int64_t row_begin, int64_t row_end, const uint8_t* tpairs,
                                const int2* xy, int32_t n, int32_t dist_type, unsigned char* scratch, int lane,
                                int32_t* error) {
@@ -110,7 +110,7 @@ __device__ void kopt_rows_warp(const ServeSegment& S, int64_t row_begin, int64_t
     __syncwarp();
     for (int i = lane; i < rows * NP; i += 32) {
       const int r = i / NP;
-      kopt_pair_entry<K, kWide>(sm, r, i - r * NP, xy, dist_type);
+      kopt_pair_entry<K, kSpan>(sm, r, i - r * NP, xy, dist_type);
     }
     __syncwarp();
     long long* out = reinterpret_cast<long long*>(S.costs + row0 * T);
@@ -119,7 +119,7 @@ __device__ void kopt_rows_warp(const ServeSegment& S, int64_t row_begin, int64_t
       int pid[K];
 #pragma unroll
       for (int i = 0; i < K; ++i) pid[i] = tpairs[t * K + i];
-      __stcs(out + j, static_cast<long long>(kopt_cell<K, kWide>(sm, r, pid)));
+      __stcs(out + j, static_cast<long long>(kopt_cell<K, kSpan>(sm, r, pid)));
     }
   }
   __syncwarp();
@@ -162,10 +162,12 @@ template <int K>
 __device__ __forceinline__ void serve_kopt_item(const ServeJob& job, const ServeSegment& S, int64_t r0, int64_t r1,
                                                 const uint8_t* tpairs, unsigned char* scratch, int lane,
                                                 int32_t* error) {
-  if (job.narrow) {
-    kopt_rows_warp<K, false>(S, r0, r1, tpairs, job.g.xy, job.g.n, job.g.dist_type, scratch, lane, error);
+  if (job.span == kSpanSmall) {
+    kopt_rows_warp<K, kSpanSmall>(S, r0, r1, tpairs, job.g.xy, job.g.n, job.g.dist_type, scratch, lane, error);
+  } else if (job.span == kSpanNarrow) {
+    kopt_rows_warp<K, kSpanNarrow>(S, r0, r1, tpairs, job.g.xy, job.g.n, job.g.dist_type, scratch, lane, error);
   } else {
-    kopt_rows_warp<K, true>(S, r0, r1, tpairs, job.g.xy, job.g.n, job.g.dist_type, scratch, lane, error);
+    kopt_rows_warp<K, kSpanWide>(S, r0, r1, tpairs, job.g.xy, job.g.n, job.g.dist_type, scratch, lane, error);
   }
 }
 
@@ -253,8 +255,10 @@ static __global__ void __launch_bounds__(kServeWarps * 32, 4)
       const int64_t e0 = local * kServeJvTile;
       const int64_t e1 = min(e0 + kServeJvTile, job.g.m);
       for (int64_t e = e0; e < e1; ++e) {
-        const int32_t wv = job.narrow ? jv_screen_edge_warp<false>(job.g, e, jv_scratch[warp], lane, error)
-                                      : jv_screen_edge_warp<true>(job.g, e, jv_scratch[warp], lane, error);
+        const int32_t wv =
+            job.span == kSpanSmall    ? jv_screen_edge_warp<kSpanSmall>(job.g, e, jv_scratch[warp], lane, error)
+            : job.span == kSpanNarrow ? jv_screen_edge_warp<kSpanNarrow>(job.g, e, jv_scratch[warp], lane, error)
+                                      : jv_screen_edge_warp<kSpanWide>(job.g, e, jv_scratch[warp], lane, error);
         if (lane == 0) job.witness[e] = wv;
         __syncwarp();
       }

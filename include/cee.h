@@ -112,6 +112,22 @@ typedef struct {
   const int32_t* csr_edge_ids;/* [adjacency] */
 } cee_graph_view;
 
+/* ---- exact distance ------------------------------------------------------------------ */
+
+/* Span classes of a point set: the larger of its x and y spans (max - min) selects the device
+ * routine for the exact distance (FP32 root, FP64 root or int64 residual; each followed by an
+ * exact integer fix-up, so all three return the same integer). */
+enum cee_span_class { CEE_SPAN_SMALL = 0 /* < 2^22 */, CEE_SPAN_NARROW = 1 /* < 2^26 */, CEE_SPAN_WIDE = 2 /* < 2^30 */ };
+
+/* The reference's exact TSPLIB distance (src/common/distance.cpp:29-52: integer square root,
+ * EUC_2D rounds to nearest, CEIL_2D rounds up) of `count` point pairs (pair_i[k], pair_j[k]) of
+ * the point set (x, y), evaluated on the device by the routine every screen uses for that point
+ * set, out[k] = the distance. *span_class (may be null) receives the cee_span_class used. A
+ * checking aid for the distance routines. */
+int cee_exact_distances(cee_ctx* ctx, int32_t n, const int64_t* x, const int64_t* y, int32_t dist_type,
+                        int64_t count, const int32_t* pair_i, const int32_t* pair_j, int32_t* out,
+                        int32_t* span_class);
+
 /* ---- JV fast-elimination screen ------------------------------------------------------ */
 
 /* JvCudaCacheUsage (include/cuda_edge_elimination/elimination.hpp:41-49) plus byte counts. */

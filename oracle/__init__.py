@@ -56,6 +56,8 @@ class Port:
         L.ceo_isqrt.argtypes = [ctypes.c_uint64]
         L.ceo_distance.restype = ctypes.c_int64
         L.ceo_distance.argtypes = [ctypes.c_int64] * 4 + [ctypes.c_int32]
+        L.ceo_distance_pairs.restype = None
+        L.ceo_distance_pairs.argtypes = [i64p, i64p, ctypes.c_int32, ctypes.c_int64, i32p, i32p, i64p]
         L.ceo_rebuild_csr.argtypes = [ctypes.c_int32, ctypes.c_int64, i32p, i32p, i64p, u8p, i32p, i32p, i32p, i64p]
         L.ceo_jv_screen.restype = ctypes.c_int64
         L.ceo_jv_screen.argtypes = [G, i32p, i64p]
@@ -107,6 +109,16 @@ class Port:
 
     def distance(self, x1, y1, x2, y2, t) -> int:
         return int(self.L.ceo_distance(x1, y1, x2, y2, t))
+
+    def distance_pairs(self, x, y, t, pair_i, pair_j) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.int64)
+        y = np.ascontiguousarray(y, np.int64)
+        pi = np.ascontiguousarray(pair_i, np.int32)
+        pj = np.ascontiguousarray(pair_j, np.int32)
+        out = np.empty(pi.shape[0], np.int64)
+        self.L.ceo_distance_pairs(_p(x, ctypes.c_int64), _p(y, ctypes.c_int64), int(t), int(pi.shape[0]),
+                                  _p(pi, ctypes.c_int32), _p(pj, ctypes.c_int32), _p(out, ctypes.c_int64))
+        return out
 
     def csr(self, n, edge_u, edge_v, edge_w, active):
         m = edge_u.shape[0]

@@ -42,6 +42,11 @@ int64_t ceo_distance(int64_t x1, int64_t y1, int64_t x2, int64_t y2, int32_t typ
   return (int64_t)rounded;
 }
 
+void ceo_distance_pairs(const int64_t* x, const int64_t* y, int32_t type, int64_t count, const int32_t* pi,
+                        const int32_t* pj, int64_t* out) {
+  for (int64_t k = 0; k < count; ++k) out[k] = ceo_distance(x[pi[k]], y[pi[k]], x[pj[k]], y[pj[k]], type);
+}
+
 static int64_t dist_nodes(const ceo_graph* g, int32_t a, int32_t b) {
   return ceo_distance(g->x[a], g->y[a], g->x[b], g->y[b], g->dist_type);
 }

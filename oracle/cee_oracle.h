@@ -49,6 +49,9 @@ typedef struct {
 uint64_t ceo_isqrt(uint64_t value);
 /* Exact TSPLIB distance; returns -1 when the squared distance overflows uint64. */
 int64_t ceo_distance(int64_t x1, int64_t y1, int64_t x2, int64_t y2, int32_t type);
+/* ceo_distance of points (pi[k], pj[k]) of (x, y), k < count. */
+void ceo_distance_pairs(const int64_t* x, const int64_t* y, int32_t type, int64_t count, const int32_t* pi,
+                        const int32_t* pj, int64_t* out);
 
 /* Active-only CSR, rows ascending by neighbour (sort fallback for unsorted edge lists). */
 int ceo_rebuild_csr(int32_t n, int64_t m, const int32_t* edge_u, const int32_t* edge_v,
