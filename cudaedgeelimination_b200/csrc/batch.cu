@@ -125,7 +125,7 @@ int ValidateOptions(cee_ctx* ctx, const cee_batch_options* o) {
   return CEE_OK;
 }
 
-// Structural checks: offsets, CSR row offsets (both O(n + instances)).
+// Structural checks in O(instances): sizes, instance offsets, the CSR's end points, null arrays.
 int ValidateShape(cee_ctx* ctx, const cee_batch_view* b) {
   if (b == nullptr || b->instances < 1 || b->node_begin == nullptr || b->edge_begin == nullptr) {
     return Fail(ctx, CEE_ERR_INVALID, "bad batch description");
@@ -147,18 +147,56 @@ int ValidateShape(cee_ctx* ctx, const cee_batch_view* b) {
       g.row_offsets[g.n] != g.adjacency) {
     return Fail(ctx, CEE_ERR_INVALID, "bad union CSR");
   }
+  if (g.n > 0 && (g.x == nullptr || g.y == nullptr)) return Fail(ctx, CEE_ERR_INVALID, "null union coordinates");
+  if (g.m > 0 && (g.edge_u == nullptr || g.edge_v == nullptr || g.edge_w == nullptr || g.active == nullptr)) {
+    return Fail(ctx, CEE_ERR_INVALID, "null union arrays");
+  }
+  if (g.adjacency > 0 && (g.neighbors == nullptr || g.csr_edge_ids == nullptr)) {
+    return Fail(ctx, CEE_ERR_INVALID, "null union CSR arrays");
+  }
+  return CEE_OK;
+}
+
+// The O(n) checks, one pass on host threads: row offsets non-decreasing (so that every row lies
+// inside [0, adjacency)) and the coordinate bounding box (box = {min x, max x, min y, max y}).
+int ScanNodes(cee_ctx* ctx, const cee_graph_view& g, int64_t box[4]) {
+  std::vector<int64_t> part(16 * 4);
   std::vector<uint8_t> bad(16, 0);
-  ParallelRanges(g.n, [&](int64_t v0, int64_t v1, int t) {
-    for (int64_t v = v0; v < v1; ++v) {
-      if (g.row_offsets[v + 1] < g.row_offsets[v]) bad[t] = 1;
+  for (int t = 0; t < 16; ++t) {
+    part[4 * t] = part[4 * t + 2] = INT64_MAX;
+    part[4 * t + 1] = part[4 * t + 3] = INT64_MIN;
+  }
+  ParallelRanges(g.n, [&](int64_t i0, int64_t i1, int t) {
+    int64_t lx = INT64_MAX, hx = INT64_MIN, ly = INT64_MAX, hy = INT64_MIN;
+    bool decreasing = false;
+    for (int64_t i = i0; i < i1; ++i) {
+      decreasing |= g.row_offsets[i + 1] < g.row_offsets[i];
+      lx = std::min(lx, g.x[i]);
+      hx = std::max(hx, g.x[i]);
+      ly = std::min(ly, g.y[i]);
+      hy = std::max(hy, g.y[i]);
     }
+    bad[t] = decreasing ? 1 : 0;
+    part[4 * t] = lx;
+    part[4 * t + 1] = hx;
+    part[4 * t + 2] = ly;
+    part[4 * t + 3] = hy;
   });
   if (std::any_of(bad.begin(), bad.end(), [](uint8_t b) { return b != 0; })) {
     return Fail(ctx, CEE_ERR_INVALID, "row_offsets not non-decreasing");
   }
-  if (g.m > 0 && (g.x == nullptr || g.y == nullptr || g.edge_u == nullptr || g.edge_v == nullptr ||
-                  g.edge_w == nullptr || g.active == nullptr)) {
-    return Fail(ctx, CEE_ERR_INVALID, "null union arrays");
+  box[0] = box[2] = INT64_MAX;
+  box[1] = box[3] = INT64_MIN;
+  for (int t = 0; t < 16; ++t) {
+    box[0] = std::min(box[0], part[4 * t]);
+    box[1] = std::max(box[1], part[4 * t + 1]);
+    box[2] = std::min(box[2], part[4 * t + 2]);
+    box[3] = std::max(box[3], part[4 * t + 3]);
+  }
+  if (g.n == 0) box[0] = box[1] = box[2] = box[3] = 0;
+  if (static_cast<__int128>(box[1]) - box[0] >= (__int128{1} << 30) ||
+      static_cast<__int128>(box[3]) - box[2] >= (__int128{1} << 30)) {
+    return Fail(ctx, CEE_ERR_RANGE, "coordinate span >= 2^30: outside the exact int32 distance range of the kernels");
   }
   return CEE_OK;
 }
@@ -378,6 +416,8 @@ int cee_batch_prepare(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opt
   if (rc != CEE_OK) return rc;
   rc = ValidateOptions(ctx, options);
   if (rc == CEE_OK) rc = ValidateShape(ctx, b);
+  int64_t box[4];
+  if (rc == CEE_OK) rc = ScanNodes(ctx, b->graph, box);
   if (rc != CEE_OK) return rc;
   const cee_graph_view& g = b->graph;
   // every edge canonical, inside its own instance, instance-sorted by (u, v)
@@ -451,7 +491,11 @@ int cee_batch_launch(cee_ctx* ctx) {
   int rc = Activate(ctx);
   if (rc != CEE_OK) return rc;
   BatchState* s = ctx->batch;
-  if (s == nullptr || !s->prepared || s->exec == nullptr) return Fail(ctx, CEE_ERR_STATE, "batch not prepared");
+  if (s == nullptr || !s->prepared) return Fail(ctx, CEE_ERR_STATE, "batch not prepared");
+  if (s->exec == nullptr) {  // first resident launch after cee_batch_screen
+    rc = Capture(ctx, *s);
+    if (rc != CEE_OK) return rc;
+  }
   const cudaError_t status = cudaGraphLaunch(s->exec, ctx->stream);
   if (status != cudaSuccess) return CudaFail(ctx, status, "batch graph launch");
   return CEE_OK;
@@ -584,40 +628,6 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
   BatchState& s = *State(ctx);
   s.prepared = false;
   s.ReleaseGraph();
-  int64_t min_x = 0, min_y = 0, max_x = 0, max_y = 0;
-  if (g.n > 0) {
-    std::vector<int64_t> part(16 * 4);
-    for (int t = 0; t < 16; ++t) {
-      part[4 * t] = part[4 * t + 2] = INT64_MAX;
-      part[4 * t + 1] = part[4 * t + 3] = INT64_MIN;
-    }
-    ParallelRanges(g.n, [&](int64_t i0, int64_t i1, int t) {
-      int64_t lx = INT64_MAX, hx = INT64_MIN, ly = INT64_MAX, hy = INT64_MIN;
-      for (int64_t i = i0; i < i1; ++i) {
-        lx = std::min(lx, g.x[i]);
-        hx = std::max(hx, g.x[i]);
-        ly = std::min(ly, g.y[i]);
-        hy = std::max(hy, g.y[i]);
-      }
-      part[4 * t] = lx;
-      part[4 * t + 1] = hx;
-      part[4 * t + 2] = ly;
-      part[4 * t + 3] = hy;
-    });
-    min_x = min_y = INT64_MAX;
-    max_x = max_y = INT64_MIN;
-    for (int t = 0; t < 16; ++t) {
-      min_x = std::min(min_x, part[4 * t]);
-      max_x = std::max(max_x, part[4 * t + 1]);
-      min_y = std::min(min_y, part[4 * t + 2]);
-      max_y = std::max(max_y, part[4 * t + 3]);
-    }
-  }
-  if (static_cast<__int128>(max_x) - min_x >= (__int128{1} << 30) ||
-      static_cast<__int128>(max_y) - min_y >= (__int128{1} << 30)) {
-    return Fail(ctx, CEE_ERR_RANGE, "coordinate span >= 2^30: outside the exact int32 distance range of the kernels");
-  }
-  s.span = span_class(max_x - min_x, max_y - min_y);
   SetShape(s, b, options);
   rc = ReserveAll(ctx, s);
   for (const auto& [buf, bytes] : {std::pair<DevBuf*, size_t>{&s.raw_x, g.n * 8ull}, {&s.raw_y, g.n * 8ull},
@@ -645,13 +655,21 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
   const size_t T = static_cast<size_t>(s.opt.targets), NB = static_cast<size_t>(s.opt.max_neighborhood);
   const size_t FW = static_cast<size_t>(s.flag_words);
   int64_t h2d_bytes = (b->instances + 1) * 16, d2h_bytes = 0;
+  // 1. every chunk's upload on the copy stream, so the copies start before the host checks
+  std::vector<int32_t> bounds(static_cast<size_t>(chunks) + 1, 0);
+  for (int c = 0; c <= chunks; ++c) {
+    bounds[static_cast<size_t>(c)] = static_cast<int32_t>(static_cast<int64_t>(b->instances) * c / chunks);
+    // the chunks' CSR slices are copied before the full row-offset check: their end points first
+    const int32_t slot = g.row_offsets[b->node_begin[bounds[static_cast<size_t>(c)]]];
+    if (slot < 0 || slot > g.adjacency || (c > 0 && slot < g.row_offsets[b->node_begin[bounds[c - 1]]])) {
+      return Fail(ctx, CEE_ERR_INVALID, "row_offsets not non-decreasing");
+    }
+  }
   for (int c = 0; c < chunks; ++c) {
-    const int32_t i0 = static_cast<int32_t>(static_cast<int64_t>(b->instances) * c / chunks);
-    const int32_t i1 = static_cast<int32_t>(static_cast<int64_t>(b->instances) * (c + 1) / chunks);
+    const int32_t i0 = bounds[c], i1 = bounds[c + 1];
     if (i1 == i0) continue;
     const int64_t n0 = b->node_begin[i0], n1 = b->node_begin[i1], e0 = b->edge_begin[i0], e1 = b->edge_begin[i1];
     const int64_t s0 = g.row_offsets[n0], s1 = g.row_offsets[n1];
-    // upload the chunk (copy engine stream)
     cudaMemcpyAsync(static_cast<int64_t*>(s.raw_x.ptr) + n0, g.x + n0, (n1 - n0) * 8, cudaMemcpyHostToDevice, s.h2d);
     cudaMemcpyAsync(static_cast<int64_t*>(s.raw_y.ptr) + n0, g.y + n0, (n1 - n0) * 8, cudaMemcpyHostToDevice, s.h2d);
     cudaMemcpyAsync(static_cast<int32_t*>(s.ro.ptr) + n0, g.row_offsets + n0, (n1 - n0 + 1) * 4, cudaMemcpyHostToDevice, s.h2d);
@@ -665,7 +683,23 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
     }
     h2d_bytes += (n1 - n0) * 20 + 4 + (e1 - e0) * 17 + (s1 - s0) * 8;
     cudaEventRecord(s.up[c], s.h2d);
-    // convert and screen (compute stream)
+  }
+  // 2. while they run: row offsets and the bounding box on host threads (nothing reads the
+  //    uploads on the device before these pass)
+  int64_t box[4];
+  rc = ScanNodes(ctx, g, box);
+  if (rc != CEE_OK) {
+    cudaStreamSynchronize(s.h2d);  // the caller's buffers stay borrowed until the copies end
+    return rc;
+  }
+  const int64_t min_x = box[0], min_y = box[2];
+  s.span = span_class(box[1] - box[0], box[3] - box[2]);
+  // 3. per chunk: convert and screen (compute stream), download (second copy stream)
+  for (int c = 0; c < chunks; ++c) {
+    const int32_t i0 = bounds[c], i1 = bounds[c + 1];
+    if (i1 == i0) continue;
+    const int64_t n0 = b->node_begin[i0], n1 = b->node_begin[i1], e0 = b->edge_begin[i0], e1 = b->edge_begin[i1];
+    const int64_t s0 = g.row_offsets[n0], s1 = g.row_offsets[n1];
     cudaStreamWaitEvent(cs, s.up[c], 0);
     batch_pack<<<GridFor(std::max(n1 - n0, e1 - e0), 256, ctx->sm_count * 8), 256, 0, cs>>>(
         static_cast<const int64_t*>(s.raw_x.ptr), static_cast<const int64_t*>(s.raw_y.ptr), n0, n1, min_x, min_y,
@@ -716,9 +750,7 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
   if (status != cudaSuccess) return CudaFail(ctx, status, "batched screen");
   rc = BatchCheck(ctx);
   if (rc != CEE_OK) return rc;
-  s.prepared = true;  // the resident copy now holds this batch
-  rc = Capture(ctx, s);
-  if (rc != CEE_OK) return rc;
+  s.prepared = true;  // the resident copy now holds this batch; its graph is captured by the next cee_batch_launch
   if (stats != nullptr) {
     *stats = cee_batch_stats{};
     stats->nodes = s.n;
