@@ -163,6 +163,7 @@ def lib() -> ctypes.CDLL:
                                              ctypes.c_int64, ctypes.c_int32, c_u8p]),
             "cee_exact_distances": (ctypes.c_int, [vp, ctypes.c_int32, vp, vp, ctypes.c_int32, ctypes.c_int64, vp,
                                                    vp, vp, ctypes.POINTER(ctypes.c_int32)]),
+            "cee_sqrt_estimate_error": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_double)]),
             "cee_batch_prepare": (ctypes.c_int, [vp, ctypes.POINTER(BatchView), ctypes.POINTER(BatchOptions),
                                                  ctypes.POINTER(BatchStats)]),
             "cee_batch_launch": (ctypes.c_int, [vp]),

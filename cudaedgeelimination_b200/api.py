@@ -408,6 +408,13 @@ class Context(BatchMixin, ServeMixin):
         return flags
 
 
+    def sqrt_estimate_error(self) -> float:
+        """Largest relative error of the device's FP32 square-root estimate over every float in
+        [1, 2^44) (the small span class is exact while it stays below 2^-21.6)."""
+        out = ctypes.c_double(0.0)
+        _native.check(self.handle, _native.lib().cee_sqrt_estimate_error(self.handle, ctypes.byref(out)))
+        return out.value
+
     def exact_distances(self, x, y, dist_type: int, pair_i, pair_j):
         """Exact TSPLIB distances of point pairs, evaluated on the device by the routine the screens
         use for this point set's span class; returns (distances int32, span class)."""

@@ -209,6 +209,19 @@ static __global__ void distance_pairs_kernel(const int2* __restrict__ xy, const 
   }
 }
 
+// Largest relative error of sqrt_estimate over the float bit patterns [lo, hi), as the bits of
+// a non-negative double (ordered like the value).
+static __global__ void root_error_kernel(uint32_t lo, uint32_t hi, unsigned long long* __restrict__ out) {
+  double worst = 0.0;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t b = lo + static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; b < hi; b += stride) {
+    const float x = __uint_as_float(static_cast<uint32_t>(b));
+    const double root = sqrt(static_cast<double>(x));
+    worst = fmax(worst, fabs(static_cast<double>(sqrt_estimate(x)) - root) / root);
+  }
+  atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(worst)));
+}
+
 // ---------------------------------------------------------------- JV --------------------
 
 int JvPrepare(cee_ctx* ctx, const cee_graph_view* g, cee_jv_stats* stats) {
@@ -1061,6 +1074,29 @@ int cee_cd_screen(cee_ctx* ctx, const cee_graph_view* graph, int32_t u, int32_t 
   status = cudaStreamSynchronize(st);
   if (status != cudaSuccess) return CudaFail(ctx, status, "c,d screen");
   return CheckDeviceError(ctx, "c,d screen");
+}
+
+int cee_sqrt_estimate_error(cee_ctx* ctx, double* max_relative_error) {
+  if (ctx == nullptr || max_relative_error == nullptr) return Fail(ctx, CEE_ERR_INVALID, "null argument");
+  int rc = Activate(ctx);
+  if (rc != CEE_OK) return rc;
+  DevBuf word;
+  cudaError_t status = word.Reserve(sizeof(unsigned long long), nullptr);
+  unsigned long long bits = 0;
+  if (status == cudaSuccess) status = cudaMemsetAsync(word.ptr, 0, sizeof(unsigned long long), ctx->stream);
+  if (status == cudaSuccess) {
+    const uint32_t lo = 0x3f800000u, hi = 0x55800000u;  // the floats in [1, 2^44)
+    root_error_kernel<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(lo, hi, static_cast<unsigned long long*>(word.ptr));
+    status = cudaGetLastError();
+  }
+  if (status == cudaSuccess) {
+    status = cudaMemcpyAsync(&bits, word.ptr, sizeof(bits), cudaMemcpyDeviceToHost, ctx->stream);
+  }
+  if (status == cudaSuccess) status = cudaStreamSynchronize(ctx->stream);
+  word.Release();
+  if (status != cudaSuccess) return CudaFail(ctx, status, "square-root estimate check");
+  std::memcpy(max_relative_error, &bits, sizeof(double));
+  return CEE_OK;
 }
 
 int cee_exact_distances(cee_ctx* ctx, int32_t n, const int64_t* x, const int64_t* y, int32_t dist_type,

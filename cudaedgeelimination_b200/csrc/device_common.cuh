@@ -11,11 +11,11 @@ constexpr uint64_t kEmptyKey = ~uint64_t{0};
 
 // Coordinate span classes: the larger of a snapshot's x and y spans selects the exact-distance
 // routine (a template parameter of every kernel that evaluates distances).
-constexpr int kSpanSmall = 0;   // span < 2^22: FP32 root, int32 residual
+constexpr int kSpanSmall = 0;   // span < 2^21: FP32 root estimate, int32 residual
 constexpr int kSpanNarrow = 1;  // span < 2^26: FP64
 constexpr int kSpanWide = 2;    // span < 2^30: int64 residual
 constexpr int kSpanClasses = 3;
-constexpr int64_t kSmallSpan = int64_t{1} << 22;
+constexpr int64_t kSmallSpan = int64_t{1} << 21;
 constexpr int64_t kNarrowSpan = int64_t{1} << 26;
 
 // The span class of coordinate spans sx, sy (both < 2^30).
@@ -25,22 +25,33 @@ __host__ __device__ constexpr int span_class(int64_t sx, int64_t sy) {
                                                   : kSpanWide;
 }
 
+// sqrt.approx.f32: the SM's one-instruction square-root approximation.
+__device__ __forceinline__ float sqrt_estimate(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // Exact TSPLIB distance between two points whose coordinates are stored relative to the
 // snapshot's bounding-box corner (0 <= x, y < 2^30, so the result fits int32).
 //
 // The reference computes q = floor(sqrt(s)) of the squared distance s with an integer
 // restoring square root (src/common/distance.cpp:9-27) and rounds: EUC_2D adds 1 when
-// s - q^2 > q (nearest integer; s is an integer so there are no ties), CEIL_2D adds 1 when
-// q^2 != s (:44-52). All three variants return exactly that value; they differ only in how
-// they find q.
+// s - q^2 > q, i.e. returns the nearest integer to sqrt(s) (s is an integer, so there are no
+// ties), CEIL_2D adds 1 when q^2 != s, i.e. returns ceil(sqrt(s)) (:44-52). All three variants
+// return exactly that value; they differ only in how they reach it.
 //
-// kSpanSmall (|dx|, |dy| < 2^22, s < 2^45): r = trunc of the correctly rounded FP32 root of
-// the FP32 sum of squares. dx and dy are exact in FP32; the sum carries a relative error of at
-// most 2u + u^2 (u = 2^-24: one rounded square, one rounded fma), the root halves it and adds
-// one rounding, so |r_f - sqrt(s)| <= sqrt(s) * 2^-23 * (1 + 2^-23) < 2^22.5 * 2^-23 < 0.71.
-// Hence r is q - 1, q or q + 1. The residual s - r^2 lies in (-(2q + 1), 4q], well inside
-// int32, so it is exact when computed modulo 2^32 from the wrapped 32-bit squares; one step
-// in either direction makes 0 <= s - r^2 <= 2r, i.e. r = q.
+// kSpanSmall (|dx|, |dy| < 2^21, s < 2^43): an FP32 estimate f of sqrt(s), rounded to the
+// candidate answer r (nearest for EUC_2D, up for CEIL_2D), then checked and corrected with the
+// exact residual t = s - r^2. dx and dy are exact in FP32; the FP32 sum of squares carries a
+// relative error of at most 2u + u^2 (u = 2^-24), which the root halves; sqrt.approx.f32 adds
+// at most 2^-23.25 (its largest relative error over every float in [1, 2^46), measured
+// exhaustively on the B200). So |f - sqrt(s)| <= sqrt(s) * 2^-22.58 <
+// 2^21.5 * 2^-22.58 < 0.48, the candidate is within one of the answer, and t lies well inside
+// int32, so it is exact when computed modulo 2^32 from wrapped 32-bit products. The answer is r
+// iff -r < t <= r (EUC_2D: (r - 1/2)^2 < s < (r + 1/2)^2) or -(2r - 1) < t <= 0 (CEIL_2D:
+// (r - 1)^2 < s <= r^2), for r > 0 (r = 0 iff s = 0); one step up or down fixes r otherwise.
+// The fix-up makes the routine exact for any estimate within one of sqrt(s), twice the bound.
 // kSpanNarrow (span < 2^26, so s < 2^53): everything in FP64. dx, dy, s and q^2 - s are exact
 // in double below 2^53; q = trunc(sqrt(s)) with the correctly rounded FP64 square root; the
 // two fma residuals then move q by one step if the root landed on the wrong side of an
@@ -53,18 +64,28 @@ __device__ __forceinline__ uint32_t exact_distance(int2 p, int2 q, int dist_type
   if constexpr (kSpan == kSpanSmall) {
     const int32_t dx = p.x - q.x, dy = p.y - q.y;
     const float fx = static_cast<float>(dx), fy = static_cast<float>(dy);
-    uint32_t r = static_cast<uint32_t>(__fsqrt_rn(__fmaf_rn(fx, fx, __fmul_rn(fy, fy))));
+    const float f = sqrt_estimate(__fmaf_rn(fx, fx, __fmul_rn(fy, fy)));
     const uint32_t ux = static_cast<uint32_t>(dx), uy = static_cast<uint32_t>(dy);
-    int32_t rem = static_cast<int32_t>(ux * ux + uy * uy - r * r);  // s - r^2, exact (see above)
-    if (rem < 0) {
-      r -= 1;
-      rem += static_cast<int32_t>(2 * r + 1);
-    } else if (rem > static_cast<int32_t>(2 * r)) {
-      rem -= static_cast<int32_t>(2 * r + 1);
-      r += 1;
+    const uint32_t s_lo = ux * ux + uy * uy;  // s modulo 2^32
+    if (dist_type == 0) {
+      uint32_t r = __float2uint_rn(f);
+      const int32_t t = static_cast<int32_t>(s_lo - r * r);
+      if (t > static_cast<int32_t>(r)) {
+        ++r;
+      } else if (t <= -static_cast<int32_t>(r) && r > 0) {
+        --r;
+      }
+      return r;
+    } else {
+      uint32_t r = __float2uint_ru(f);
+      const int32_t t = static_cast<int32_t>(s_lo - r * r);
+      if (t > 0) {
+        ++r;
+      } else if (t <= 1 - 2 * static_cast<int32_t>(r) && r > 0) {
+        --r;
+      }
+      return r;
     }
-    const bool up = dist_type == 0 ? rem > static_cast<int32_t>(r) : rem != 0;
-    return r + (up ? 1u : 0u);
   } else if constexpr (kSpan == kSpanWide) {
     const int64_t dx = static_cast<int64_t>(p.x) - q.x;
     const int64_t dy = static_cast<int64_t>(p.y) - q.y;

@@ -117,7 +117,7 @@ typedef struct {
 /* Span classes of a point set: the larger of its x and y spans (max - min) selects the device
  * routine for the exact distance (FP32 root, FP64 root or int64 residual; each followed by an
  * exact integer fix-up, so all three return the same integer). */
-enum cee_span_class { CEE_SPAN_SMALL = 0 /* < 2^22 */, CEE_SPAN_NARROW = 1 /* < 2^26 */, CEE_SPAN_WIDE = 2 /* < 2^30 */ };
+enum cee_span_class { CEE_SPAN_SMALL = 0 /* < 2^21 */, CEE_SPAN_NARROW = 1 /* < 2^26 */, CEE_SPAN_WIDE = 2 /* < 2^30 */ };
 
 /* The reference's exact TSPLIB distance (src/common/distance.cpp:29-52: integer square root,
  * EUC_2D rounds to nearest, CEIL_2D rounds up) of `count` point pairs (pair_i[k], pair_j[k]) of
@@ -127,6 +127,12 @@ enum cee_span_class { CEE_SPAN_SMALL = 0 /* < 2^22 */, CEE_SPAN_NARROW = 1 /* < 
 int cee_exact_distances(cee_ctx* ctx, int32_t n, const int64_t* x, const int64_t* y, int32_t dist_type,
                         int64_t count, const int32_t* pair_i, const int32_t* pair_j, int32_t* out,
                         int32_t* span_class);
+
+/* The largest relative error of the device's one-instruction FP32 square-root estimate (the
+ * estimate the CEE_SPAN_SMALL routine rounds and then corrects with an exact integer residual)
+ * over every float in [1, 2^44), i.e. every FP32 sum of squares that class produces. The routine
+ * is exact whenever this is below 2^-21.6; *max_relative_error receives it. A checking aid. */
+int cee_sqrt_estimate_error(cee_ctx* ctx, double* max_relative_error);
 
 /* ---- JV fast-elimination screen ------------------------------------------------------ */
 

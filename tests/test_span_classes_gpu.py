@@ -1,4 +1,4 @@
-"""The three exact-distance routines (span classes small < 2^22 <= narrow < 2^26 <= wide < 2^30)
+"""The three exact-distance routines (span classes small < 2^21 <= narrow < 2^26 <= wide < 2^30)
 against the oracle's integer-square-root distance (src/common/distance.cpp:9-52): directly, on
 pairs chosen at the rounding and fix-up boundaries up to each class's largest squared distance,
 and through the JV, k-opt and c,d screens on instances of each class."""
@@ -44,7 +44,7 @@ def boundary_pairs(span, count, seed):
     return xs, ys, np.where(swap, pj, pi), np.where(swap, pi, pj)
 
 
-@pytest.mark.parametrize("span,cls", [((1 << 22) - 1, SMALL), (1 << 22, NARROW), ((1 << 26) - 1, NARROW),
+@pytest.mark.parametrize("span,cls", [((1 << 21) - 1, SMALL), (1 << 21, NARROW), ((1 << 26) - 1, NARROW),
                                       (1 << 26, WIDE), ((1 << 30) - 1, WIDE), (1000, SMALL)])
 @pytest.mark.parametrize("dist_type", [0, 1])
 def test_exact_distances_at_boundaries(ctx, port, span, cls, dist_type):
@@ -53,6 +53,14 @@ def test_exact_distances_at_boundaries(ctx, port, span, cls, dist_type):
     gpu, got = ctx.exact_distances(xs + offset, ys - offset, dist_type, pi, pj)
     assert got == cls
     np.testing.assert_array_equal(gpu.astype(np.int64), port.distance_pairs(xs, ys, dist_type, pi, pj))
+
+
+def test_sqrt_estimate_error_bound(ctx):
+    # the small class rounds an FP32 root estimate and corrects it by one step with an exact
+    # residual: exact while the estimate's relative error stays below 2^-21.6 on every float the
+    # class can produce; the B200 measures 2^-23.25
+    err = ctx.sqrt_estimate_error()
+    assert 0.0 < err <= 2.0 ** -22, err
 
 
 def test_small_span_all_short_vectors(ctx, port):
@@ -79,7 +87,7 @@ def random_kopt_rows(g, k, rows, seed):
     return tasks
 
 
-@pytest.mark.parametrize("coord,cls", [(1 << 22, SMALL), (1 << 24, NARROW), (1 << 28, WIDE)])
+@pytest.mark.parametrize("coord,cls", [(1 << 21, SMALL), (1 << 24, NARROW), (1 << 28, WIDE)])
 @pytest.mark.parametrize("dist_type", [0, 1])
 def test_screens_per_class(ctx, port, coord, cls, dist_type):
     g = knn_graph(400, 8, seed=coord % 977 + dist_type, coord=coord, dist_type=dist_type)
