@@ -80,6 +80,22 @@ def load_traffic():
     return {}
 
 
+def issue_roofline(kernel: str, ms_per_launch: float, sm_mhz, device):
+    """The instruction-issue ceiling of an ALU-bound kernel: its warp instructions per launch (one ncu
+    capture, profiles/ncu_traffic.json) over the live launch time, against SMs x 4 schedulers x the
+    SM clock sampled during the timed region (one warp instruction per scheduler per cycle)."""
+    import torch
+    count = load_traffic().get("warp_instructions", {}).get(kernel)
+    if count is None or not sm_mhz:
+        return None
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    peak = sms * 4 * float(sm_mhz) * 1e6
+    achieved = count / (ms_per_launch / 1e3)
+    return {"unit": "warp instructions/s", "warp_instructions_per_launch": count, "achieved": achieved,
+            "peak": peak, "frac": achieved / peak,
+            "peak_source": f"{sms} SMs x 4 schedulers x {float(sm_mhz):.0f} MHz sampled"}
+
+
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
 
@@ -264,6 +280,7 @@ def run_ours(args, rank: int, world: int, device: int):
         torch.cuda.synchronize(device)
         barrier(world)
     ms_step = max_over_ranks(ev0.elapsed_time(ev1), world) / args.steps
+    clock_summary = clocks.summary()
     edges_step = int(g.active.sum())
     targets = int(res.target_count.sum())
     sizes = (res.nbhd >= 0).sum(axis=2)
@@ -360,9 +377,10 @@ def run_ours(args, rank: int, world: int, device: int):
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
                      "traffic": load_traffic().get("batch_screen_kernel"), "traffic_unit": "DRAM bytes per launch (ncu)",
                      "algorithmic_bytes_per_launch": alg_bytes,
-                     "note": "the screen is ALU/latency bound (integer and FP64 exact-distance work); "
-                             "see distance_evals_per_s"},
-        "clocks": clocks.summary(),
+                     "issue": issue_roofline("batch_screen_kernel", ms_step, clock_summary.get("sm_mhz"), device),
+                     "note": "the screen is instruction-issue bound (integer and FP32 exact-distance work, warp "
+                             "sorts and shuffles), not memory bound: see issue and distance_evals_per_s"},
+        "clocks": clock_summary,
         "gpu_launches": args.steps,
     }
 
@@ -410,7 +428,7 @@ def run_kopt(args, ctx, stream, device, world):
         ctx.kopt_launch()
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)
     total = 0.0
-    with torch.cuda.stream(stream):
+    with ClockSampler(device) as clocks, torch.cuda.stream(stream):
         for _ in range(args.steps):
             flush.zero_()  # evict L2 (126 MB) between timed launches
             e0 = torch.cuda.Event(enable_timing=True)
@@ -421,6 +439,7 @@ def run_kopt(args, ctx, stream, device, world):
             e1.synchronize()
             total += e0.elapsed_time(e1)
     ms = max_over_ranks(total / args.steps, world)
+    clock_summary = clocks.summary()
     outs = [np.empty((t.shape[0], KOPT_TEMPLATE_COUNTS[k]), np.int64) for k, t in zip(ks, lists)]
     ctx.kopt_fetch(outs)
     # end to end: H2D of the rows, launch, D2H of the full matrices into pinned buffers
@@ -456,7 +475,9 @@ def run_kopt(args, ctx, stream, device, world):
             "roofline": {"kernel": "kopt_cost_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
                          "traffic": load_traffic().get("kopt_cost_kernel"), "traffic_unit": "DRAM bytes per launch (ncu)",
-                         "algorithmic_bytes_per_launch": alg_bytes}}
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "issue": issue_roofline("kopt_cost_kernel", ms, clock_summary.get("sm_mhz"), device)},
+            "clocks": clock_summary}
 
 
 def _pinned_pool(count: int, nbytes: int):
