@@ -517,7 +517,7 @@ int KoptCoords(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x, con
 
 int KoptTemplatesFor(int k) { return k == 3 ? 4 : (k == 4 ? 25 : 208); }
 
-int DefaultRowsPerTile(uint32_t k) { return k == 3 ? 208 : (k == 4 ? 128 : 32); }
+int DefaultRowsPerTile(uint32_t k) { return k == 3 ? 96 : (k == 4 ? 56 : 32); }  // ~22 KB tiles: nine blocks per SM
 
 // Uploads the rows of every segment and records the launch description.
 int KoptPrepareSegments(cee_ctx* ctx, int32_t segments, const uint32_t* ks, const KoptTable* const* tables,

@@ -34,9 +34,10 @@
 //   C. one thread per (row, port pair) computes the pair's exact distance (k(2k-1) pairs, at
 //      most 45, instead of k distances per cell) and its entry (narrow) or mask (wide);
 //   D. thread j owns template t = j mod T with its k pair indices in registers and walks rows
-//      j / T, j / T + B / T, ... (B = 416 threads: 104 rows of k = 3, 16 rows of k = 4, two
-//      rows of k = 5 per step); the threads of a step write one contiguous run of row-major
-//      cells with streaming stores.
+//      j / T, j / T + B / T, ... (B = 224 threads: 56 rows of k = 3, 8 rows of k = 4, one
+//      row of k = 5 per step); the threads of a step write one contiguous run of row-major
+//      cells with streaming stores. Small blocks (7 warps, nine per SM) keep the stages'
+//      barriers and load latencies of one tile overlapped with other tiles' work.
 // Fused leaf consume (mask_words > 0): stage D also marks, per row, the templates whose cost is
 // below the row's deleted cost — the templates the reference's leaf consumer tries, in order — in a
 // shared bit mask; the tile then writes the masks and each row's first improving template, and the
@@ -47,7 +48,7 @@
 
 namespace cee {
 
-constexpr int kKoptThreads = 416;          // 13 warps: 104 x 4 = 2 x 208 cells per step, 16 x 25 + 16
+constexpr int kKoptThreads = 224;          // 7 warps: 56 x 4 cells per step, 8 x 25 + 24, 208 + 16
 constexpr int kKoptMaxPorts = 10;
 constexpr int kKoptMaxPairs = 45;          // k(2k-1) for k = 5
 constexpr int kKoptMaxTemplates = 208;     // proper 5-opt templates
@@ -322,7 +323,7 @@ __device__ __forceinline__ void kopt_tile(const KoptLaunch& L, const KoptSegment
 }
 
 template <int kSpan>
-static __global__ void __launch_bounds__(kKoptThreads, 4) kopt_cost_kernel(KoptLaunch L,
+static __global__ void __launch_bounds__(kKoptThreads, 9) kopt_cost_kernel(KoptLaunch L,
                                                                         int32_t* __restrict__ error) {
   extern __shared__ __align__(16) unsigned char smem[];
   int si = 0;
