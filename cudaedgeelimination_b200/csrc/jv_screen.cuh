@@ -314,9 +314,11 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
     const int p = base + lane;
     uint32_t bit = 0;
     if (p < pairs) {
-      int ci = 0;
+      int ci = 0;  // last candidate whose run starts at or before p (begin[] is non-decreasing)
 #pragma unroll
-      for (int i = 1; i < kJvMaxCandidates; ++i) ci += (i < nc && s.begin[i] <= p) ? 1 : 0;
+      for (int step = 8; step > 0; step >>= 1) {
+        if (ci + step < nc && s.begin[ci + step] <= p) ci += step;
+      }
       if (((compatible >> ci) & 1u) == 0 && compatible_pair(ci, s.row[ci] + kHead + (p - s.begin[ci]))) {
         bit = 1u << ci;
       }
