@@ -142,6 +142,13 @@ def lib() -> ctypes.CDLL:
             "cee_jv_screen_noalloc": (ctypes.c_int, [ctypes.POINTER(DeviceGraph), vp, vp]),
             "cee_jv_eliminate": (ctypes.c_int, [vp, ctypes.POINTER(GraphView), ctypes.c_uint32, c_u8p, c_i32p, c_i32p,
                                                 c_i64p, c_i64p, ctypes.POINTER(JvElimStats)]),
+            "cee_jv_eliminate_metrics": (ctypes.c_int, [vp, c_i64p, ctypes.POINTER(ctypes.c_double), ctypes.c_int32]),
+            "cee_content_hash": (ctypes.c_int, [ctypes.POINTER(GraphView), c_u64p]),
+            "cee_jv_proof": (ctypes.c_int, [ctypes.POINTER(GraphView), ctypes.c_uint32, c_i32p, c_i32p, vp,
+                                            ctypes.c_int64, c_i64p, c_u64p]),
+            "cee_write_active_edges": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(GraphView), c_u8p]),
+            "cee_jv_write_proof": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint64,
+                                                  vp, ctypes.c_int64, vp, ctypes.c_int32]),
             "cee_kopt_templates": (ctypes.c_int, [ctypes.c_uint32, c_u8p, c_u64p]),
             "cee_kopt_costs": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, c_i64p, c_i64p, ctypes.c_uint32,
                                               c_u8p, ctypes.c_int32, ctypes.c_uint64, vp, ctypes.c_int64, c_i64p,

@@ -24,6 +24,57 @@ from .snapshot import GraphSnapshot
 
 KOPT_TASK_DTYPE = np.dtype([("port_nodes", np.int32, (10,)), ("deleted_cost", np.int64)])
 CD_TASK_DTYPE = np.dtype([("c", np.int32), ("d", np.int32), ("active", np.uint8), ("pad", np.uint8, (3,))])
+# cee_jv_proof_record / cee_jv_epoch_metrics (include/cee.h)
+JV_PROOF_RECORD_DTYPE = np.dtype([("epoch", np.uint32), ("edge_id", np.int32), ("u", np.int32), ("v", np.int32),
+                                  ("witness", np.int32), ("reserved", np.int32), ("snapshot_hash", np.uint64)])
+JV_EPOCH_METRICS_DTYPE = np.dtype([("epoch", np.uint32), ("reserved", np.uint32), ("edges_before", np.int64),
+                                   ("proposed", np.int64), ("verified", np.int64), ("rejected", np.int64),
+                                   ("committed", np.int64), ("propose_ms", np.float64), ("verify_ms", np.float64)])
+
+
+def content_hash(graph: GraphSnapshot) -> int:
+    """GraphSnapshot::ContentHash of the snapshot (host FNV-1a, cee_content_hash)."""
+    view = graph.view()
+    out = ctypes.c_uint64(0)
+    _native.check(None, _native.lib().cee_content_hash(ctypes.byref(view), ctypes.byref(out)))
+    return int(out.value)
+
+
+def jv_proof(graph: GraphSnapshot, epochs: int, edge_epoch: np.ndarray, witness: np.ndarray):
+    """Proof records of an elimination that started from `graph` (cee_jv_proof): returns
+    (records as JV_PROOF_RECORD_DTYPE, hashes[epochs + 1]: before every epoch, then the final hash)."""
+    edge_epoch = np.ascontiguousarray(edge_epoch, np.int32)
+    witness = np.ascontiguousarray(witness, np.int32)
+    view = graph.view()
+    count = ctypes.c_int64(0)
+    hashes = np.zeros(epochs + 1, np.uint64)
+    cap = int((edge_epoch >= 0).sum())
+    records = np.zeros(cap, JV_PROOF_RECORD_DTYPE)
+    _native.check(None, _native.lib().cee_jv_proof(
+        ctypes.byref(view), epochs, edge_epoch.ctypes.data_as(_native.c_i32p), witness.ctypes.data_as(_native.c_i32p),
+        records.ctypes.data_as(ctypes.c_void_p), cap, ctypes.byref(count), hashes.ctypes.data_as(_native.c_u64p)))
+    return records[:count.value], hashes
+
+
+def write_active_edges(path, graph: GraphSnapshot, active: np.ndarray | None = None) -> None:
+    """The Concorde .edg file of the snapshot's active edges (cee_write_active_edges); `active` overrides
+    the snapshot's flags (e.g. the final flags of jv_eliminate)."""
+    view = graph.view()
+    flags = None
+    if active is not None:
+        active = np.ascontiguousarray(active, np.uint8)
+        assert active.shape == (graph.m,)
+        flags = active.ctypes.data_as(_native.c_u8p)
+    _native.check(None, _native.lib().cee_write_active_edges(str(path).encode(), ctypes.byref(view), flags))
+
+
+def write_jv_proof(path, backend: str, records: np.ndarray, hashes: np.ndarray, metrics: np.ndarray) -> None:
+    """CUDAEE_PROOF_V1 file (cee_jv_write_proof): initial hash hashes[0], final hash hashes[-1]."""
+    records = np.ascontiguousarray(records, JV_PROOF_RECORD_DTYPE)
+    metrics = np.ascontiguousarray(metrics, JV_EPOCH_METRICS_DTYPE)
+    _native.check(None, _native.lib().cee_jv_write_proof(
+        str(path).encode(), backend.encode(), int(hashes[0]), int(hashes[-1]), records.ctypes.data_as(ctypes.c_void_p),
+        int(records.shape[0]), metrics.ctypes.data_as(ctypes.c_void_p), int(metrics.shape[0])))
 assert KOPT_TASK_DTYPE.itemsize == 48 and CD_TASK_DTYPE.itemsize == 12
 
 INVALID_KOPT_COST = np.iinfo(np.int64).max
@@ -324,6 +375,29 @@ class Context(BatchMixin, ServeMixin):
             before.ctypes.data_as(_native.c_i64p), committed.ctypes.data_as(_native.c_i64p), ctypes.byref(stats)))
         e = stats.epochs
         return active, witness, epoch, before[:e], committed[:e], stats
+
+    def jv_eliminate_metrics(self, epochs: int):
+        """(candidates proposed, screen + commit-gate ms) per epoch of the last jv_eliminate."""
+        proposed = np.zeros(epochs, np.int64)
+        ms = np.zeros(epochs, np.float64)
+        _native.check(self.handle, _native.lib().cee_jv_eliminate_metrics(
+            self.handle, proposed.ctypes.data_as(_native.c_i64p), ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+            epochs))
+        return proposed, ms
+
+    def jv_eliminate_with_proof(self, graph: GraphSnapshot, path, max_rounds: int = 100):
+        """jv_eliminate, then the run's CUDAEE_PROOF_V1 file at `path` (records with the snapshot hash of
+        every epoch, one metrics line per epoch; the device path has no CPU re-verification, so
+        verified = proposed and rejected = 0). Returns jv_eliminate's tuple plus the proof records."""
+        active, witness, epoch, before, committed, stats = self.jv_eliminate(graph, max_rounds)
+        records, hashes = jv_proof(graph, stats.epochs, epoch, witness)
+        proposed, ms = self.jv_eliminate_metrics(stats.epochs)
+        metrics = np.zeros(stats.epochs, JV_EPOCH_METRICS_DTYPE)
+        metrics["epoch"] = np.arange(stats.epochs)
+        metrics["edges_before"], metrics["proposed"], metrics["verified"] = before, proposed, proposed
+        metrics["committed"], metrics["propose_ms"] = committed, ms
+        write_jv_proof(path, "cuda", records, hashes, metrics)
+        return active, witness, epoch, before, committed, stats, records
 
     # ---- k-opt ----------------------------------------------------------------------
     def kopt_costs(self, graph: GraphSnapshot, table: "KOptReconnectTable", tasks: np.ndarray):

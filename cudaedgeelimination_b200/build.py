@@ -27,7 +27,7 @@ REFERENCE = pathlib.Path(os.environ.get("CEE_REFERENCE_DIR", "/root/reference"))
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-Wall", f"-I{INCLUDE}", f"-I{CSRC}"]
-CUDA_SOURCES = ["cee_api.cu", "batch.cu", "noalloc.cu", "serve.cu", "epoch.cu"]
+CUDA_SOURCES = ["cee_api.cu", "batch.cu", "noalloc.cu", "serve.cu", "epoch.cu", "proof.cu"]
 
 
 def _host_cxx() -> str:

@@ -234,6 +234,10 @@ static __global__ void csr_fill(const int32_t* __restrict__ ro, int32_t n, const
 struct EpochState {
   DevBuf xy, uv, w32, active, ro[2], nbr[2], ids[2], slot4[2], order, witness, flag, pos, sums, cand, decided, commit,
       node_min, degree, epoch_of, witness_of, counters;
+  // per epoch of the last call: candidates found, wall time of the screen and commit gate
+  std::vector<int64_t> proposed;
+  std::vector<double> screen_ms;
+  bool ran = false;
   void Release() {
     for (DevBuf* b : {&xy, &uv, &w32, &active, &order, &witness, &flag, &pos, &sums, &cand, &decided, &commit, &node_min,
                       &degree, &epoch_of, &witness_of, &counters}) {
@@ -338,6 +342,9 @@ extern "C" int cee_jv_eliminate(cee_ctx* ctx, const cee_graph_view* g, uint32_t 
 
   if (ctx->epoch == nullptr) ctx->epoch = new EpochState();
   EpochState& s = *ctx->epoch;
+  s.ran = false;
+  s.proposed.clear();
+  s.screen_ms.clear();
   const size_t mm = static_cast<size_t>(std::max<int64_t>(m, 1)), nn = static_cast<size_t>(std::max<int32_t>(n, 1));
   const size_t aa = static_cast<size_t>(std::max<int64_t>(adj, 1));
   const size_t scan_blocks_max = (std::max(mm, nn + 1) + kScanBlock - 1) / kScanBlock + 2;
@@ -394,8 +401,11 @@ extern "C" int cee_jv_eliminate(cee_ctx* ctx, const cee_graph_view* g, uint32_t 
     if (epoch_edges_before != nullptr) epoch_edges_before[0] = 0;
     if (epoch_committed != nullptr) epoch_committed[0] = 0;
     epochs = 1;
+    s.proposed.push_back(0);
+    s.screen_ms.push_back(0.0);
   }
   for (uint32_t epoch = 0; epoch < max_rounds && m > 0; ++epoch) {
+    const auto epoch_start = std::chrono::steady_clock::now();
     JvGraph jg{};
     jg.n = n;
     jg.dist_type = g->dist_type;
@@ -462,6 +472,8 @@ extern "C" int cee_jv_eliminate(cee_ctx* ctx, const cee_graph_view* g, uint32_t 
       committed = host[0];
     }
     if (epoch_committed != nullptr) epoch_committed[epoch] = committed;
+    s.proposed.push_back(candidates);
+    s.screen_ms.push_back(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - epoch_start).count());
     total_committed += committed;
     active_edges -= committed;
     if (committed == 0) break;
@@ -498,6 +510,21 @@ extern "C" int cee_jv_eliminate(cee_ctx* ctx, const cee_graph_view* g, uint32_t 
     stats->committed = total_committed;
     stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
     stats->resident_bytes = EpochResident(ctx);
+  }
+  s.ran = true;
+  return CEE_OK;
+}
+
+extern "C" int cee_jv_eliminate_metrics(const cee_ctx* ctx, int64_t* proposed, double* screen_ms, int32_t capacity) {
+  using namespace cee;
+  if (ctx == nullptr) return Fail(nullptr, CEE_ERR_INVALID, "null context");
+  const EpochState* s = ctx->epoch;
+  if (s == nullptr || !s->ran) return Fail(nullptr, CEE_ERR_STATE, "cee_jv_eliminate_metrics before cee_jv_eliminate");
+  const int32_t epochs = static_cast<int32_t>(s->proposed.size());
+  if (capacity < epochs) return Fail(nullptr, CEE_ERR_INVALID, "capacity below the epoch count");
+  for (int32_t e = 0; e < epochs; ++e) {
+    if (proposed != nullptr) proposed[e] = s->proposed[static_cast<size_t>(e)];
+    if (screen_ms != nullptr) screen_ms[e] = s->screen_ms[static_cast<size_t>(e)];
   }
   return CEE_OK;
 }

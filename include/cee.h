@@ -222,6 +222,68 @@ int cee_jv_eliminate(cee_ctx* ctx, const cee_graph_view* graph, uint32_t max_rou
                      int32_t* witness_out, int32_t* epoch_out, int64_t* epoch_edges_before,
                      int64_t* epoch_committed, cee_jv_elim_stats* stats);
 
+/* Per-epoch figures of the context's last cee_jv_eliminate call, for the proof log's metrics lines
+ * (EpochMetrics, include/cuda_edge_elimination/elimination.hpp:21-39): proposed[e] = candidates the
+ * epoch's screen found, screen_ms[e] = device time of its screen and commit gate (CUDA events).
+ * capacity >= the call's epoch count; CEE_ERR_STATE before any call. */
+int cee_jv_eliminate_metrics(const cee_ctx* ctx, int64_t* proposed, double* screen_ms, int32_t capacity);
+
+/* ---- JV proof log --------------------------------------------------------------------------- */
+
+/* ProofRecord (include/cuda_edge_elimination/types.hpp:40-50) of a JV elimination. */
+typedef struct {
+  uint32_t epoch;
+  int32_t edge_id;
+  int32_t u;
+  int32_t v;
+  int32_t witness;
+  int32_t reserved;
+  uint64_t snapshot_hash; /* content hash of the snapshot the epoch screened */
+} cee_jv_proof_record;
+
+/* EpochMetrics' serialised fields (the proof's "metrics" lines). */
+typedef struct {
+  uint32_t epoch;
+  uint32_t reserved;
+  int64_t edges_before;
+  int64_t proposed;
+  int64_t verified;
+  int64_t rejected;
+  int64_t committed;
+  double propose_ms;
+  double verify_ms;
+} cee_jv_epoch_metrics;
+
+/* GraphSnapshot::ContentHash (src/common/graph.cpp:323-346) of an integer-coordinate snapshot:
+ * 64-bit FNV-1a over its dimension (int32), distance type (uint8), integer-coordinate flag (1), every
+ * point's (x, y) (int64 each) and every edge's (u, v, weight, active) (int32, int32, int64, bool), in
+ * the snapshot's edge order. Host computation; needs no context or device. */
+int cee_content_hash(const cee_graph_view* graph, uint64_t* hash);
+
+/* The proof records of a device elimination, from cee_jv_eliminate's per-edge epoch_out and
+ * witness_out (graph = the snapshot the elimination started from): the records RunJvElimination
+ * appends (src/cpu/jv_elimination.cpp:304-312), epoch by epoch, each epoch in commit order
+ * (src/cpu/elimination_commit.cpp:33-41: (u, v), then edge id), each carrying the content hash of the
+ * snapshot its epoch screened. hashes[0..epochs] (may be null) receives the hash before every epoch
+ * and, last, the final hash (hashes[0] is the proof's initial_hash, hashes[epochs] its final_hash);
+ * `epochs` = cee_jv_elim_stats.epochs. The epochs' hashes are computed on parallel host threads.
+ * *count = the number of records (at most capacity are written). CEE_ERR_INVALID when an eliminated
+ * edge was not active, its epoch is outside [0, epochs) or its witness is not a node. */
+int cee_jv_proof(const cee_graph_view* graph, uint32_t epochs, const int32_t* edge_epoch, const int32_t* witness,
+                 cee_jv_proof_record* records, int64_t capacity, int64_t* count, uint64_t* hashes);
+
+/* Writes the snapshot's active edges in GraphSnapshot::WriteActiveEdges' format (src/common/graph.cpp:284-298,
+ * the Concorde .edg file): "n count", then "u v weight" per active edge in edge order. active = the
+ * flags to write (e.g. cee_jv_eliminate's active_out), or null for graph->active. */
+int cee_write_active_edges(const char* path, const cee_graph_view* graph, const uint8_t* active);
+
+/* Writes a CUDAEE_PROOF_V1 file in WriteProof's format (src/cpu/jv_elimination.cpp:324-368): backend,
+ * initial_hash, the records, one metrics line per epoch, final_hash, END. The reference's ReadProof
+ * and ReplayProof accept it. */
+int cee_jv_write_proof(const char* path, const char* backend, uint64_t initial_hash, uint64_t final_hash,
+                       const cee_jv_proof_record* records, int64_t count, const cee_jv_epoch_metrics* metrics,
+                       int32_t epochs);
+
 /* ---- k-opt leaf cost matrix ----------------------------------------------------------- */
 
 /* KOptCostTask, include/cuda_edge_elimination/local_search.hpp:54-57 (48 bytes). */

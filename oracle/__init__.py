@@ -262,6 +262,9 @@ class Reference:
         L.ref_jv_verify.argtypes = [vp, ctypes.c_int32, ctypes.c_int32]
         L.ref_run_jv.argtypes = [vp, ctypes.c_int, ctypes.c_uint32, i64p, ctypes.c_int32, i32p, ctypes.c_int64, i64p,
                                  u64p, u64p]
+        L.ref_write_proof_cpu.argtypes = [vp, ctypes.c_uint32, ctypes.c_char_p]
+        L.ref_replay_proof_file.argtypes = [vp, ctypes.c_char_p]
+        L.ref_write_active_edges.argtypes = [vp, ctypes.c_char_p]
         L.ref_kopt_table.argtypes = [ctypes.c_uint32, u8p, u64p]
         L.ref_kopt_costs.argtypes = [vp, ctypes.c_uint32, vp, ctypes.c_int64, ctypes.c_int, i64p, i64p]
         L.ref_cd_candidates.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32,
@@ -342,6 +345,18 @@ class RefGraph:
 
     def content_hash(self) -> int:
         return int(self.ref.L.ref_graph_hash(self.handle))
+
+    def write_proof_cpu(self, path, max_rounds: int = 100) -> int:
+        """RunJvElimination(kCpu) in place and WriteProof of the run; returns the epoch count."""
+        return self.ref._check(self.ref.L.ref_write_proof_cpu(self.handle, max_rounds, str(path).encode()))
+
+    def write_active_edges(self, path) -> None:
+        """GraphSnapshot::WriteActiveEdges of the snapshot as it stands."""
+        self.ref._check(self.ref.L.ref_write_active_edges(self.handle, str(path).encode()))
+
+    def replay_proof_file(self, path) -> int:
+        """ReadProof + ReplayProof on a copy of this snapshot; the records replayed (raises when rejected)."""
+        return self.ref._check(self.ref.L.ref_replay_proof_file(self.handle, str(path).encode()))
 
     def jv_cpu(self) -> np.ndarray:
         w = np.empty(self.m, np.int32)

@@ -218,6 +218,36 @@ int ref_run_jv(void* handle, int backend, uint32_t max_rounds, int64_t* epoch_st
   });
 }
 
+// RunJvElimination(kCpu) on the snapshot in place, then WriteProof (src/cpu/jv_elimination.cpp:324-368)
+// of the run to `path`. Returns the epoch count.
+int ref_write_proof_cpu(void* handle, uint32_t max_rounds, const char* path) {
+  return Guard([&] {
+    const cudaee::EliminationResult result =
+        cudaee::RunJvElimination(AsGraph(handle), cudaee::Backend::kCpu, max_rounds);
+    cudaee::WriteProof(path, result);
+    return static_cast<int>(result.epochs.size());
+  });
+}
+
+// GraphSnapshot::WriteActiveEdges (src/common/graph.cpp:284-298) of the snapshot as it stands.
+int ref_write_active_edges(void* handle, const char* path) {
+  return Guard([&] {
+    AsGraph(handle)->WriteActiveEdges(path);
+    return 0;
+  });
+}
+
+// ReadProof(path), then ReplayProof (src/cpu/jv_elimination.cpp:525-600) on a copy of the snapshot:
+// the number of records replayed, or -1 with the reference's reason when it rejects the proof.
+int ref_replay_proof_file(void* handle, const char* path) {
+  return Guard([&] {
+    cudaee::GraphSnapshot working = *AsGraph(handle);
+    const cudaee::EliminationResult expected = cudaee::ReadProof(path);
+    const cudaee::EliminationResult replayed = cudaee::ReplayProof(&working, expected);
+    return static_cast<int>(replayed.proof.size());
+  });
+}
+
 // BuildKOptReconnectTable (src/cpu/kopt_search.cpp:1143-1193): mates[t*14 + p].
 int ref_kopt_table(uint32_t k, uint8_t* mates, uint64_t* hash) {
   return Guard([&] {

@@ -4,7 +4,7 @@ final active sets, per-epoch edges and commits, and every (epoch, edge, witness)
 import numpy as np
 import pytest
 
-from cudaedgeelimination_b200 import GraphSnapshot, synth
+from cudaedgeelimination_b200 import GraphSnapshot, synth, write_active_edges
 from cudaedgeelimination_b200._native import CEE_ERR_INVALID, NativeError
 from helpers import knn_graph, random_graph
 
@@ -86,3 +86,35 @@ def test_no_edges_and_errors(ctx):
     assert e.value.code == CEE_ERR_INVALID
     with pytest.raises(NativeError):
         ctx.jv_eliminate(g, 0)
+
+
+@pytest.mark.parametrize("which", ["clustered", "batch3"])
+def test_device_proof_replays_in_the_reference(ctx, ref, tmp_path, which):
+    """The proof file of a device elimination (records with every epoch's snapshot hash) is accepted
+    by the reference's ReadProof + ReplayProof, and its records, hashes and per-epoch counts equal
+    the reference's own RunJvElimination(kCpu) proof."""
+    g = synth.jv_clustered() if which == "clustered" else synth.batch_instance(3, n_lo=4000, n_hi=5000)
+    path, ref_path = tmp_path / "device.proof", tmp_path / "reference.proof"
+    _, _, _, _, committed, _, records = ctx.jv_eliminate_with_proof(g, path)
+    assert ref.graph(g).replay_proof_file(path) == len(records) == int(committed.sum())
+    ref.graph(g).write_proof_cpu(ref_path)
+
+    def fields(p):
+        lines = open(p).read().splitlines()
+        kept = [ln for ln in lines if ln.startswith(("record ", "initial_hash ", "final_hash "))]
+        counts = [ln.split()[1:7] for ln in lines if ln.startswith("metrics ")]  # epoch .. committed
+        return kept, counts
+
+    assert fields(path) == fields(ref_path)
+
+
+def test_device_final_edge_file_matches_reference(ctx, ref, tmp_path):
+    """The .edg file of the device elimination's final active edges equals the one the reference writes
+    after its own RunJvElimination(kCpu)."""
+    g = synth.jv_clustered()
+    active, *_ = ctx.jv_eliminate(g)
+    write_active_edges(tmp_path / "device.edg", g, active)
+    rg = ref.graph(g)
+    rg.write_proof_cpu(tmp_path / "reference.proof")
+    rg.write_active_edges(tmp_path / "reference.edg")
+    assert open(tmp_path / "device.edg").read() == open(tmp_path / "reference.edg").read()
