@@ -162,8 +162,8 @@ uint64_t JvResident(const JvState& s) {
 
 uint64_t KoptResident(const KoptState& s) {
   uint64_t bytes = s.xy.capacity + s.tasks.capacity + s.costs.capacity + s.masks.capacity + s.firsts.capacity;
-  for (const KoptTable& t : s.user) bytes += t.pairs.capacity;
-  for (const KoptTable& t : s.canon) bytes += t.pairs.capacity;
+  for (const KoptTable& t : s.user) bytes += t.pairs.capacity + t.patterns.capacity;
+  for (const KoptTable& t : s.canon) bytes += t.pairs.capacity + t.patterns.capacity;
   return bytes;
 }
 
@@ -465,6 +465,54 @@ int PairTable(cee_ctx* ctx, uint32_t k, const uint8_t* mates, int32_t count, std
   return CEE_OK;
 }
 
+// For each template (k pair indices, or the re-adds-deleted marker): bit g is set when the template's
+// cell is invalid on every gap-pattern row of pattern g (kopt_cost.cuh). Such a row's ports fall into
+// classes that merge port 2e+1 with port (2e+2) mod 2k for each closed gap e; a cell is invalid when
+// an added edge joins two ports of one class (a self loop), equals a deleted edge's class pair, or
+// repeats another added edge's class pair (src/cpu/kopt_search.cpp:962-1042).
+std::vector<uint32_t> GapPatternMasks(uint32_t k, const std::vector<uint8_t>& pairs, int32_t count) {
+  const int P = static_cast<int>(2 * k);
+  std::vector<int> pp, pq;
+  for (int p = 0; p < P; ++p) {
+    for (int q = p + 1; q < P; ++q) {
+      pp.push_back(p);
+      pq.push_back(q);
+    }
+  }
+  std::vector<uint32_t> masks(static_cast<size_t>(count), 0);
+  for (uint32_t g = 0; g < (1u << k); ++g) {
+    int cls[kKoptMaxPorts];
+    for (int p = 0; p < P; ++p) cls[p] = p;
+    for (uint32_t e = 0; e < k; ++e) {
+      if ((g >> e) & 1u) {  // the two ports share a node; the class is its lower port
+        const int a = static_cast<int>(2 * e + 1), b = static_cast<int>((2 * e + 2) % P);
+        const int lo = std::min(cls[a], cls[b]), hi = std::max(cls[a], cls[b]);
+        for (int p = 0; p < P; ++p) {
+          if (cls[p] == hi) cls[p] = lo;
+        }
+      }
+    }
+    std::vector<std::pair<int, int>> deleted;
+    for (uint32_t e = 0; e < k; ++e) {
+      deleted.emplace_back(std::min(cls[2 * e], cls[2 * e + 1]), std::max(cls[2 * e], cls[2 * e + 1]));
+    }
+    for (int32_t t = 0; t < count; ++t) {
+      const uint8_t* tp = pairs.data() + static_cast<size_t>(t) * k;
+      bool invalid = tp[0] == kKoptReaddsDeleted;
+      std::vector<std::pair<int, int>> added;
+      for (uint32_t i = 0; i < k && !invalid; ++i) {
+        const int a = cls[pp[tp[i]]], b = cls[pq[tp[i]]];
+        const std::pair<int, int> code{std::min(a, b), std::max(a, b)};
+        invalid = a == b || std::find(deleted.begin(), deleted.end(), code) != deleted.end() ||
+                  std::find(added.begin(), added.end(), code) != added.end();
+        added.push_back(code);
+      }
+      if (invalid) masks[static_cast<size_t>(t)] |= 1u << g;
+    }
+  }
+  return masks;
+}
+
 int EnsureTable(cee_ctx* ctx, KoptTable* table, uint32_t k, const uint8_t* mates, int32_t count,
                 uint64_t hash, bool* hit) {
   const size_t bytes = static_cast<size_t>(count) * 14;
@@ -481,6 +529,12 @@ int EnsureTable(cee_ctx* ctx, KoptTable* table, uint32_t k, const uint8_t* mates
   if (status != cudaSuccess) return CudaFail(ctx, status, "k-opt template allocation");
   status = cudaMemcpy(table->pairs.ptr, pairs.data(), pairs.size(), cudaMemcpyHostToDevice);
   if (status != cudaSuccess) return CudaFail(ctx, status, "k-opt template upload");
+  const std::vector<uint32_t> masks = GapPatternMasks(k, pairs, count);
+  status = table->patterns.Reserve(masks.size() * sizeof(uint32_t) + 16, nullptr);
+  if (status == cudaSuccess) {
+    status = cudaMemcpy(table->patterns.ptr, masks.data(), masks.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+  }
+  if (status != cudaSuccess) return CudaFail(ctx, status, "k-opt template pattern upload");
   table->k = k;
   table->hash = hash;
   table->T = count;
@@ -559,6 +613,7 @@ int KoptPrepareSegments(cee_ctx* ctx, int32_t segments, const uint32_t* ks, cons
     seg.costs = static_cast<int64_t*>(s.costs.ptr) + cost_offset[i];
     seg.rows = rows[i];
     seg.pairs = static_cast<const uint8_t*>(tables[i]->pairs.ptr);
+    seg.patterns = static_cast<const uint32_t*>(tables[i]->patterns.ptr);
     seg.k = static_cast<int32_t>(ks[i]);
     seg.templates = tables[i]->T;
     seg.write_costs = 1;

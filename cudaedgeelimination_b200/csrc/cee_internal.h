@@ -53,9 +53,11 @@ struct KoptTable {
   uint64_t hash = 0;
   int32_t T = 0;
   std::vector<uint8_t> mates;
-  DevBuf pairs;  // T x k pair indices
+  DevBuf pairs;     // T x k pair indices
+  DevBuf patterns;  // T: gap patterns on which the template is invalid (kopt_cost.cuh)
   void Release() {
     pairs.Release();
+    patterns.Release();
     k = 0;
     T = 0;
     mates.clear();

@@ -38,6 +38,15 @@
 //      row of k = 5 per step); the threads of a step write one contiguous run of row-major
 //      cells with streaming stores. Small blocks (7 warps, nine per SM) keep the stages'
 //      barriers and load latencies of one tile overlapped with other tiles' work.
+// Gap-pattern rows. Rows built from a tour (the reference's leaf rows, BuildKOptCostTask,
+// src/cpu/kopt_search.cpp:561-584) repeat a node only where two deleted edges are adjacent in the
+// tour: port 2e+1 and port (2e+2) mod 2k hold the same node ("gap" e closed), and all other ports
+// are distinct. Such a row's class structure is fixed by its gap pattern g (bit e = gap e closed,
+// < 2^k <= 32 patterns), so whether a template is invalid on it depends on (template, g) only: the
+// host precomputes per template a 32-bit mask over the patterns (KoptSegment::patterns). Stage B
+// recognises these rows (the equal port pairs are exactly the closed gaps), stage C then stores only
+// the pair distances, and stage D sums k int32 distances and tests one bit; every other row keeps
+// the general class-code path above.
 // Fused leaf consume (mask_words > 0): stage D also marks, per row, the templates whose cost is
 // below the row's deleted cost — the templates the reference's leaf consumer tries, in order — in a
 // shared bit mask; the tile then writes the masks and each row's first improving template, and the
@@ -60,6 +69,7 @@ constexpr uint32_t kKoptSharedCode = 0x36DB6DB6u;         // bits 1 and 2 of ten
 // First pair index of a template that pairs some port 2e with 2e + 1 (re-adds deleted edge e,
 // so every cell is invalid); proper templates never do.
 constexpr uint8_t kKoptReaddsDeleted = 0xff;
+constexpr uint8_t kKoptGeneralRow = 0xff;  // fastpat of a row that is not a gap-pattern row
 
 // pair index of ports p < q among 2k ports (row-major upper triangle)
 __host__ __device__ __forceinline__ int kopt_pair_index(int p, int q, int ports) {
@@ -71,6 +81,7 @@ struct KoptSegment {
   int64_t* __restrict__ costs;        // rows x T
   int64_t rows;
   const uint8_t* __restrict__ pairs;  // T x k pair indices (device)
+  const uint32_t* __restrict__ patterns;  // T: bit g = the template is invalid on rows of gap pattern g
   uint32_t* __restrict__ improving;   // rows x mask_words: bit t = template t improves the row
   int32_t* __restrict__ first;        // rows: first improving template, or -1
   int32_t k;
@@ -98,6 +109,7 @@ struct KoptSmem {
   uint8_t* cls;       // rows * ports
   uint8_t* mrank;     // rows * ports: rank of the port's class among the multi classes, or 0xff
   uint8_t* repeats;   // rows: 1 when the row repeats a node
+  uint8_t* fastpat;   // rows: gap pattern of a gap-pattern row, else kKoptGeneralRow
   uint8_t* pp;        // npairs: first port of each pair
   uint8_t* pq;        // npairs: second port
   uint8_t* ctab;      // ports * ports: code of a class pair, 0xff on the diagonal
@@ -107,7 +119,7 @@ struct KoptSmem {
 
 __host__ __device__ constexpr int kopt_tile_smem(int k, int rows, int mask_words = 0) {
   const int ports = 2 * k, npairs = k * (ports - 1);
-  const int bytes = 2 * rows * ports + rows + 2 * npairs + ports * ports;
+  const int bytes = 2 * rows * ports + 2 * rows + 2 * npairs + ports * ports;
   return rows * npairs * 8 + rows * 8 + rows * ports * 4 + rows * npairs * 4 + ((bytes + 15) & ~15) +
          (mask_words > 0 ? rows * 8 + rows * mask_words * 4 : 0);
 }
@@ -122,10 +134,11 @@ __device__ __forceinline__ KoptSmem kopt_carve(unsigned char* base, int k, int r
   s.cls = reinterpret_cast<uint8_t*>(s.dist + rows * npairs);
   s.mrank = s.cls + rows * ports;
   s.repeats = s.mrank + rows * ports;
-  s.pp = s.repeats + rows;
+  s.fastpat = s.repeats + rows;
+  s.pp = s.fastpat + rows;
   s.pq = s.pp + npairs;
   s.ctab = s.pq + npairs;
-  const int bytes = 2 * rows * ports + rows + 2 * npairs + ports * ports;
+  const int bytes = 2 * rows * ports + 2 * rows + 2 * npairs + ports * ports;
   s.deleted = reinterpret_cast<int64_t*>(reinterpret_cast<unsigned char*>(s.cls) + ((bytes + 15) & ~15));
   s.imask = reinterpret_cast<uint32_t*>(s.deleted + (mask_words > 0 ? rows : 0));
   return s;
@@ -196,6 +209,26 @@ __device__ __forceinline__ void kopt_row_classes(const int32_t* nodes, const uin
   }
   *repeats = rep ? 1 : 0;
   *delmask = dm;
+}
+
+// Stage B's test for a gap-pattern row: its gap pattern, or kKoptGeneralRow when some equal port
+// pair is not a closed gap.
+template <int K>
+__device__ __forceinline__ uint8_t kopt_gap_pattern(const int32_t* nodes) {
+  constexpr int P = 2 * K;
+  int32_t nd[P];
+#pragma unroll
+  for (int p = 0; p < P; ++p) nd[p] = nodes[p];
+  int equal = 0;
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+#pragma unroll
+    for (int q = p + 1; q < P; ++q) equal += nd[p] == nd[q] ? 1 : 0;
+  }
+  uint32_t g = 0;
+#pragma unroll
+  for (int e = 0; e < K; ++e) g |= (nd[2 * e + 1] == nd[(2 * e + 2) % P] ? 1u : 0u) << e;
+  return equal == __popc(g) ? static_cast<uint8_t>(g) : kKoptGeneralRow;
 }
 
 // Stage C for one (row, pair): the exact distance and the pair's entry (narrow) or mask (wide).
@@ -283,12 +316,22 @@ __device__ __forceinline__ void kopt_tile(const KoptLaunch& L, const KoptSegment
   }
   __syncthreads();
   for (int r = tid; r < rows; r += kKoptThreads) {
-    kopt_row_classes<K>(sm.ports + r * P, sm.ctab, sm.cls + r * P, sm.mrank + r * P, sm.repeats + r, sm.delmask + r);
+    const uint8_t g = kopt_gap_pattern<K>(sm.ports + r * P);
+    sm.fastpat[r] = g;
+    if (g == kKoptGeneralRow) {
+      kopt_row_classes<K>(sm.ports + r * P, sm.ctab, sm.cls + r * P, sm.mrank + r * P, sm.repeats + r, sm.delmask + r);
+    }
   }
   __syncthreads();
   for (int i = tid; i < rows * NP; i += kKoptThreads) {
-    const int r = i / NP;
-    kopt_pair_entry<K, kSpan>(sm, r, i - r * NP, L.xy, L.dist_type);
+    const int r = i / NP, pid = i - r * NP;
+    if (sm.fastpat[r] != kKoptGeneralRow) {  // gap-pattern row: the distance alone
+      const int32_t* pr = sm.ports + r * P;
+      sm.dist[i] = static_cast<int32_t>(
+          exact_distance<kSpan>(__ldg(L.xy + pr[sm.pp[pid]]), __ldg(L.xy + pr[sm.pq[pid]]), L.dist_type));
+    } else {
+      kopt_pair_entry<K, kSpan>(sm, r, pid, L.xy, L.dist_type);
+    }
   }
   __syncthreads();
   const int T = S.templates;
@@ -300,10 +343,29 @@ __device__ __forceinline__ void kopt_tile(const KoptLaunch& L, const KoptSegment
     for (int i = 0; i < K; ++i) pid[i] = __ldg(S.pairs + t * K + i);
     const bool readds_deleted = pid[0] == kKoptReaddsDeleted;
     if (readds_deleted) pid[0] = 0;
+    const uint32_t invalid_on = __ldg(S.patterns + t);
     long long* out = reinterpret_cast<long long*>(S.costs + row0 * T) + static_cast<int64_t>(rr) * T + t;
     const int64_t out_step = static_cast<int64_t>(per_step) * T;
     for (int r = rr; r < rows; r += per_step, out += out_step) {
-      const int64_t v = readds_deleted ? INT64_MAX : kopt_cell<K, kSpan>(sm, r, pid);
+      const uint32_t g = sm.fastpat[r];
+      int64_t v;
+      if (g != kKoptGeneralRow) {
+        const int32_t* dr = sm.dist + r * NP;
+        if constexpr (kSpan == kSpanWide) {
+          int64_t sum = 0;
+#pragma unroll
+          for (int i = 0; i < K; ++i) sum += dr[pid[i]];
+          v = sum;
+        } else {  // k distances < 2^26.5 each: the sum fits 32 bits
+          uint32_t sum = 0;
+#pragma unroll
+          for (int i = 0; i < K; ++i) sum += static_cast<uint32_t>(dr[pid[i]]);
+          v = sum;
+        }
+        if (((invalid_on >> g) & 1u) != 0 || readds_deleted) v = INT64_MAX;
+      } else {
+        v = readds_deleted ? INT64_MAX : kopt_cell<K, kSpan>(sm, r, pid);
+      }
       if (S.write_costs != 0) __stcs(out, static_cast<long long>(v));
       // the leaf consumer tries templates with added cost < deleted cost (src/cpu/kopt_search.cpp:697)
       if (W > 0 && v < sm.deleted[r]) atomicOr(sm.imask + r * W + (t >> 5), 1u << (t & 31));

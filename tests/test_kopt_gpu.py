@@ -146,6 +146,39 @@ def test_heavily_repeated_ports(kc, port):
         np.testing.assert_array_equal(gpu, port.kopt_costs(g, k, tasks))
 
 
+def tour_rows(k, rng, n, per_pattern=3):
+    """Rows cut from tours: for every gap pattern g (bit e: deleted edges e and e+1 adjacent in the tour,
+    bit k-1: the last and the first), `per_pattern` rows of random distinct tour nodes."""
+    rows = []
+    for g in range(1 << k):
+        for _ in range(per_pattern):
+            pos, p = [], 0
+            for e in range(k):
+                pos.append(p)
+                p += 1 if (g >> e) & 1 and e < k - 1 else 2 + int(rng.integers(0, 3))
+            length = pos[-1] + 1 if (g >> (k - 1)) & 1 else pos[-1] + 2 + int(rng.integers(0, 3))
+            tour = rng.choice(n, length, replace=False)
+            rows.append([int(tour[q]) for e in range(k) for q in (pos[e], (pos[e] + 1) % length)])
+    return rows
+
+
+@pytest.mark.parametrize("dist_type", [0, 1])
+def test_every_gap_pattern(kc, port, dist_type):
+    """Tour rows of every gap pattern (the recognised rows whose validity comes from the per-template
+    pattern masks), interleaved with rows of other repeats (the class-code path), in the same tiles."""
+    rng = np.random.default_rng(17 + dist_type)
+    xs, ys = rng.integers(0, 50_000, 400), rng.integers(0, 50_000, 400)
+    g = coords_only(xs, ys, dist_type)
+    for k in (3, 4, 5):
+        rows = tour_rows(k, rng, 400)
+        other = [list(rng.integers(0, 12, 2 * k)) for _ in range(len(rows) // 2)]  # arbitrary repeats
+        mixed = [r for pair in zip(rows, other + rows[len(other):]) for r in pair]
+        tasks = make_tasks(g, k, mixed)
+        table = BuildKOptReconnectTable(k)
+        gpu, _ = kc.kopt_costs(g, table, tasks)
+        np.testing.assert_array_equal(gpu, port.kopt_costs(g, k, tasks))
+
+
 def expected_improving(costs, deleted):
     """Bit masks and first index of the templates with cost < deleted cost, row by row."""
     better = costs < deleted[:, None]
