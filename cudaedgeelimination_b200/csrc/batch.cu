@@ -43,12 +43,15 @@ struct BatchState {
   int span = kSpanSmall;  // span class of the union's coordinates
   int32_t flag_words = 0;
   std::vector<int64_t> node_begin, edge_begin;
+  std::vector<int64_t> chunk_begin;  // spatial chunks per instance (batch_screen.cuh)
+  int spatial_keys = 0;               // padded key count of the largest chunked instance
   // the union snapshot in the kernels' layout
   DevBuf d_node_begin, d_edge_begin, xy, uv, w32, active, ro, nbr, ids, slot4;
   // raw uploads of the end-to-end call (converted on the device)
   DevBuf raw_x, raw_y, raw_u, raw_v, raw_w;
   // outputs and work-queue state
   DevBuf witness, target_ids, target_count, nbhd, flags, counter, ready;
+  DevBuf perm, chunk_box, d_chunk_begin;  // spatial chunks of the instances
   DevBuf cand_c, cand_d, cand_product, cand_count;  // finalised c,d candidates (max_cd_candidates > 0)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -67,7 +70,7 @@ struct BatchState {
     ReleaseGraph();
     for (DevBuf* b : {&d_node_begin, &d_edge_begin, &xy, &uv, &w32, &active, &ro, &nbr, &ids, &slot4, &raw_x, &raw_y,
                       &raw_u, &raw_v, &raw_w, &witness, &target_ids, &target_count, &nbhd, &flags, &counter, &ready,
-                      &cand_c, &cand_d, &cand_product, &cand_count}) {
+                      &cand_c, &cand_d, &cand_product, &cand_count, &perm, &chunk_box, &d_chunk_begin}) {
       b->Release();
     }
     for (int i = 0; i < kMaxChunks; ++i) {
@@ -96,7 +99,8 @@ uint64_t BatchResident(const cee_ctx* ctx) {
   uint64_t bytes = 0;
   for (const DevBuf* b : {&s->d_node_begin, &s->d_edge_begin, &s->xy, &s->uv, &s->w32, &s->active, &s->ro, &s->nbr,
                           &s->ids, &s->slot4, &s->raw_x, &s->raw_y, &s->raw_u, &s->raw_v, &s->raw_w, &s->witness,
-                          &s->target_ids, &s->target_count, &s->nbhd, &s->flags, &s->counter, &s->ready}) {
+                          &s->target_ids, &s->target_count, &s->nbhd, &s->flags, &s->counter, &s->ready, &s->perm,
+                          &s->chunk_box, &s->d_chunk_begin}) {
     bytes += b->capacity;
   }
   return bytes;
@@ -217,7 +221,8 @@ int ReserveAll(cee_ctx* ctx, BatchState& s) {
       {&s.w32, m * 4}, {&s.active, m}, {&s.ro, (n + 1) * 4}, {&s.nbr, adj * 4}, {&s.ids, adj * 4},
       {&s.slot4, adj * 16}, {&s.witness, m * 4}, {&s.target_ids, I * T * 4}, {&s.target_count, I * 4},
       {&s.nbhd, I * T * NB * 4}, {&s.flags, I * T * static_cast<size_t>(s.flag_words) * 4},
-      {&s.counter, kMaxChunks * 8}, {&s.ready, I * 4}};
+      {&s.counter, kMaxChunks * 8}, {&s.ready, I * 4}, {&s.perm, n * 4},
+      {&s.chunk_box, static_cast<size_t>(s.chunk_begin.back()) * 16}, {&s.d_chunk_begin, (I + 1) * 8}};
   const size_t K = static_cast<size_t>(s.opt.max_cd_candidates);
   for (const auto& [buf, bytes] : wants) {
     rc = Reserve(ctx, *buf, bytes);
@@ -255,6 +260,18 @@ void SetShape(BatchState& s, const cee_batch_view* b, const cee_batch_options* o
   s.flag_words = (pairs + 31) / 32;
   s.node_begin.assign(b->node_begin, b->node_begin + b->instances + 1);
   s.edge_begin.assign(b->edge_begin, b->edge_begin + b->instances + 1);
+  s.chunk_begin.assign(static_cast<size_t>(b->instances) + 1, 0);
+  s.spatial_keys = 0;
+  for (int32_t i = 0; i < b->instances; ++i) {
+    const int64_t n = b->node_begin[i + 1] - b->node_begin[i];
+    const int64_t chunks = n <= kSpatialMaxNodes ? (n + kSpatialChunk - 1) / kSpatialChunk : 0;
+    s.chunk_begin[i + 1] = s.chunk_begin[i] + chunks;
+    if (chunks > 0) {
+      int keys = 1;
+      while (keys < n) keys <<= 1;
+      s.spatial_keys = std::max(s.spatial_keys, keys);
+    }
+  }
 }
 
 BatchArgs MakeArgs(cee_ctx* ctx, BatchState& s, int32_t first, int32_t count, int chunk) {
@@ -297,7 +314,25 @@ BatchArgs MakeArgs(cee_ctx* ctx, BatchState& s, int32_t first, int32_t count, in
   A.ready = static_cast<int32_t*>(s.ready.ptr);
   A.error = ctx->d_error;
   A.wait_limit = 1ll << 24;  // ~1 s of 64 ns naps
+  A.perm = static_cast<const int32_t*>(s.perm.ptr);
+  A.chunk_box = static_cast<const int4*>(s.chunk_box.ptr);
+  A.chunk_begin = static_cast<const int64_t*>(s.d_chunk_begin.ptr);
   return A;
+}
+
+// Spatial chunks of instances [first, first + count) (their coordinates must be on the device).
+cudaError_t LaunchSpatial(const BatchState& s, int32_t first, int32_t count, cudaStream_t stream) {
+  if (count <= 0 || s.spatial_keys == 0) return cudaSuccess;
+  const int smem = s.spatial_keys * 8;
+  if (smem > 48 * 1024) {
+    const cudaError_t status = cudaFuncSetAttribute(batch_spatial, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (status != cudaSuccess) return status;
+  }
+  batch_spatial<<<count, kSpatialThreads, smem, stream>>>(
+      static_cast<const int2*>(s.xy.ptr), static_cast<const int64_t*>(s.d_node_begin.ptr),
+      static_cast<const int64_t*>(s.d_chunk_begin.ptr), first, static_cast<int32_t*>(s.perm.ptr),
+      static_cast<int4*>(s.chunk_box.ptr));
+  return cudaGetLastError();
 }
 
 cudaError_t QueryBatchOccupancy(BatchState& s) {
@@ -450,6 +485,7 @@ int cee_batch_prepare(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opt
   cudaEventRecord(ctx->ev[0], st);
   cudaMemcpyAsync(s.d_node_begin.ptr, b->node_begin, (b->instances + 1) * 8, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(s.d_edge_begin.ptr, b->edge_begin, (b->instances + 1) * 8, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s.d_chunk_begin.ptr, s.chunk_begin.data(), (b->instances + 1) * 8, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(s.xy.ptr, xy.data(), xy.size() * 8, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(s.uv.ptr, uv.data(), uv.size() * 8, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(s.w32.ptr, w32.data(), w32.size() * 4, cudaMemcpyHostToDevice, st);
@@ -465,7 +501,8 @@ int cee_batch_prepare(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opt
         static_cast<const int32_t*>(s.ids.ptr), static_cast<const int32_t*>(s.nbr.ptr), static_cast<const int2*>(s.xy.ptr),
         0, g.adjacency, static_cast<const int32_t*>(s.w32.ptr), g.m, g.n, static_cast<int4*>(s.slot4.ptr), ctx->d_error);
   }
-  cudaError_t status = cudaStreamSynchronize(st);  // host staging vectors die at return
+  cudaError_t status = LaunchSpatial(s, 0, b->instances, st);
+  if (status == cudaSuccess) status = cudaStreamSynchronize(st);  // host staging vectors die at return
   if (status != cudaSuccess) return CudaFail(ctx, status, "batch upload");
   cudaEventRecord(ctx->ev[1], st);
   status = QueryBatchOccupancy(s);
@@ -481,7 +518,7 @@ int cee_batch_prepare(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opt
     stats->targets = static_cast<int64_t>(s.instances) * s.opt.targets;
     stats->flag_words = s.flag_words;
     stats->resident_bytes = BatchResident(ctx);
-    stats->h2d_bytes = static_cast<int64_t>((b->instances + 1) * 16 + xy.size() * 8 + uv.size() * 12 + g.m +
+    stats->h2d_bytes = static_cast<int64_t>((b->instances + 1) * 24 + xy.size() * 8 + uv.size() * 12 + g.m +
                                             (g.n + 1) * 4 + g.adjacency * 8);
   }
   return CEE_OK;
@@ -652,9 +689,10 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
   cudaMemsetAsync(ctx->d_error, 0, sizeof(int32_t), cs);
   cudaMemcpyAsync(s.d_node_begin.ptr, b->node_begin, (b->instances + 1) * 8, cudaMemcpyHostToDevice, cs);
   cudaMemcpyAsync(s.d_edge_begin.ptr, b->edge_begin, (b->instances + 1) * 8, cudaMemcpyHostToDevice, cs);
+  cudaMemcpyAsync(s.d_chunk_begin.ptr, s.chunk_begin.data(), (b->instances + 1) * 8, cudaMemcpyHostToDevice, cs);
   const size_t T = static_cast<size_t>(s.opt.targets), NB = static_cast<size_t>(s.opt.max_neighborhood);
   const size_t FW = static_cast<size_t>(s.flag_words);
-  int64_t h2d_bytes = (b->instances + 1) * 16, d2h_bytes = 0;
+  int64_t h2d_bytes = (b->instances + 1) * 24, d2h_bytes = 0;
   // 1. every chunk's upload on the copy stream, so the copies start before the host checks
   std::vector<int32_t> bounds(static_cast<size_t>(chunks) + 1, 0);
   for (int c = 0; c <= chunks; ++c) {
@@ -711,6 +749,8 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
           static_cast<const int32_t*>(s.ids.ptr), static_cast<const int32_t*>(s.nbr.ptr), static_cast<const int2*>(s.xy.ptr),
           s0, s1, static_cast<const int32_t*>(s.w32.ptr), g.m, g.n, static_cast<int4*>(s.slot4.ptr), ctx->d_error);
     }
+    status = LaunchSpatial(s, i0, i1 - i0, cs);
+    if (status != cudaSuccess) return CudaFail(ctx, status, "batch spatial chunks");
     rc = LaunchRange(ctx, s, i0, i1 - i0, c, cs);
     if (rc != CEE_OK) return rc;
     cudaEventRecord(s.done[c], cs);

@@ -17,6 +17,13 @@
 //                     neighbours, AppendHtHamiltonRepliesUnchecked :230-269), product per pair,
 //                     the max_cd smallest (product, c, d).
 //
+// Spatial chunks: at upload, every instance of at most kSpatialMaxNodes nodes gets its nodes in
+// Morton order of their coordinates (perm) cut into chunks of 32 with their bounding boxes. A c,d
+// item then visits chunks in increasing order of the smallest doubled-midpoint distance their box
+// allows and stops once that bound exceeds the current 25th-best score: every skipped node scores
+// above it, so the neighbourhood (the NB smallest (score, node) pairs) is exactly the full scan's,
+// from a few chunks instead of the whole instance. Larger instances keep the full scan.
+//
 // The c,d items of an instance wait (bounded, with an error on timeout) for that instance's
 // target-selection item; those items come first in the queue and take a few microseconds, so
 // the wait is normally never observed. All CTAs of the grid are resident (the grid is sized
@@ -36,6 +43,9 @@ constexpr int kBatchFlagWords = (kBatchMaxPairs + 31) / 32;                     
 constexpr int32_t kBatchWaitError = 8;
 constexpr int32_t kBatchRangeError = 128;  // finalisation: instance > 65536 nodes or a product too large
 constexpr int kBatchMaxCd = 32;
+constexpr int kSpatialChunk = 32;        // nodes per spatial chunk (one warp pass)
+constexpr int kSpatialMaxNodes = 8192;   // larger instances keep the full neighbourhood scan
+constexpr int kSpatialMaxChunks = kSpatialMaxNodes / kSpatialChunk;
 
 struct BatchArgs {
   JvGraph g;                          // the union snapshot (global node and edge ids)
@@ -64,11 +74,100 @@ struct BatchArgs {
   int32_t* __restrict__ ready;        // [I] set when the instance's targets are written, zero at launch
   int32_t* __restrict__ error;
   long long wait_limit;               // spin iterations before an item gives up
+  const int32_t* __restrict__ perm;        // [n] instance nodes in Morton order (global ids)
+  const int4* __restrict__ chunk_box;      // per chunk {min x, max x, min y, max y}
+  const int64_t* __restrict__ chunk_begin; // [I + 1]; an instance without chunks has none
 };
 
 struct BatchWarpScratch {
   JvWarpScratch jv;
+  unsigned long long chunk_bound[kSpatialMaxChunks];  // c,d items: per-chunk score bounds
 };
+
+// Spatial chunks of instances [first, first + gridDim.x): one block per instance (kSpatialThreads
+// threads, dynamic shared memory for the padded key count), skipping instances without chunks.
+constexpr int kSpatialThreads = 512;
+static __global__ void __launch_bounds__(kSpatialThreads) batch_spatial(const int2* __restrict__ xy,
+                                                                         const int64_t* __restrict__ node_begin,
+                                                                         const int64_t* __restrict__ chunk_begin,
+                                                                         int32_t first, int32_t* __restrict__ perm,
+                                                                         int4* __restrict__ chunk_box) {
+  extern __shared__ unsigned long long keys[];
+  __shared__ int bounds[4];
+  const int32_t inst = first + static_cast<int32_t>(blockIdx.x);
+  const int64_t c0 = chunk_begin[inst], c1 = chunk_begin[inst + 1];
+  if (c1 == c0) return;
+  const int64_t n0 = node_begin[inst];
+  const int n = static_cast<int>(node_begin[inst + 1] - n0);
+  int N = 1;
+  while (N < n) N <<= 1;
+  if (threadIdx.x == 0) {
+    bounds[0] = bounds[2] = INT32_MAX;
+    bounds[1] = bounds[3] = INT32_MIN;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    const int2 p = xy[n0 + j];
+    atomicMin(&bounds[0], p.x);
+    atomicMax(&bounds[1], p.x);
+    atomicMin(&bounds[2], p.y);
+    atomicMax(&bounds[3], p.y);
+  }
+  __syncthreads();
+  const int64_t sx = max(1, bounds[1] - bounds[0]), sy = max(1, bounds[3] - bounds[2]);
+  for (int j = threadIdx.x; j < N; j += blockDim.x) {
+    unsigned long long key = ~0ull;
+    if (j < n) {  // 16-bit coordinates in the instance's box, bit-interleaved
+      const int2 p = xy[n0 + j];
+      const uint32_t qx = static_cast<uint32_t>((static_cast<int64_t>(p.x - bounds[0]) * 65535) / sx);
+      const uint32_t qy = static_cast<uint32_t>((static_cast<int64_t>(p.y - bounds[2]) * 65535) / sy);
+      uint32_t code = 0;
+#pragma unroll
+      for (int b = 0; b < 16; ++b) code |= (((qx >> b) & 1u) << (2 * b)) | (((qy >> b) & 1u) << (2 * b + 1));
+      key = (static_cast<unsigned long long>(code) << 32) | static_cast<uint32_t>(j);
+    }
+    keys[j] = key;
+  }
+  __syncthreads();
+  for (int k = 2; k <= N; k <<= 1) {  // bitonic sort of the N keys, ascending
+    for (int h = k >> 1; h > 0; h >>= 1) {
+      for (int j = threadIdx.x; j < N; j += blockDim.x) {
+        const int o = j ^ h;
+        if (o > j) {
+          const unsigned long long a = keys[j], b = keys[o];
+          if (((j & k) == 0) == (a > b)) {
+            keys[j] = b;
+            keys[o] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    perm[n0 + j] = static_cast<int32_t>(n0 + static_cast<int64_t>(keys[j] & 0xffffffffu));
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (int64_t c = c0 + (threadIdx.x >> 5); c < c1; c += blockDim.x >> 5) {  // one warp per chunk
+    const int j = static_cast<int>(c - c0) * kSpatialChunk + lane;
+    int2 p = make_int2(INT32_MAX, INT32_MAX), q = make_int2(INT32_MIN, INT32_MIN);
+    if (j < n) {
+      p = xy[n0 + static_cast<int64_t>(keys[j] & 0xffffffffu)];
+      q = p;
+    }
+    const int4 box = make_int4(__reduce_min_sync(kFullMask, p.x), __reduce_max_sync(kFullMask, q.x),
+                               __reduce_min_sync(kFullMask, p.y), __reduce_max_sync(kFullMask, q.y));
+    if (lane == 0) chunk_box[c] = box;
+  }
+}
+
+// Smallest (2x - mx)^2 + (2y - my)^2 over the chunk's box.
+__device__ __forceinline__ unsigned long long chunk_bound(int4 box, int64_t mx, int64_t my) {
+  const int64_t dx = max(max(2 * static_cast<int64_t>(box.x) - mx, mx - 2 * static_cast<int64_t>(box.y)), int64_t{0});
+  const int64_t dy = max(max(2 * static_cast<int64_t>(box.z) - my, my - 2 * static_cast<int64_t>(box.w)), int64_t{0});
+  return static_cast<unsigned long long>(dx * dx) + static_cast<unsigned long long>(dy * dy);
+}
 
 // ---- warp top lists ------------------------------------------------------------------
 
@@ -241,7 +340,7 @@ __device__ int32_t ht_reply_count(const JvGraph& g, int32_t u, int32_t v, int2 p
 
 template <int kSpan>
 __device__ void batch_cd_target(const BatchArgs& A, int32_t inst, int32_t t, const uint8_t* pair_i,
-                                 const uint8_t* pair_j, int lane) {
+                                 const uint8_t* pair_j, unsigned long long* bound, int lane) {
   const JvGraph& g = A.g;
   const int64_t slot = static_cast<int64_t>(inst) * A.targets + t;
   int32_t* nbhd_out = A.nbhd + slot * A.nb;
@@ -273,7 +372,55 @@ __device__ void batch_cd_target(const BatchArgs& A, int32_t inst, int32_t t, con
   // neighbourhood: the NB smallest (doubled-midpoint squared distance, node)
   uint64_t ls = kEmptyKey;
   int32_t ln = INT32_MAX;
-  for (int64_t base = n0; base < n1; base += 32) {
+  const int64_t c0 = A.chunk_begin[inst], chunks = A.chunk_begin[inst + 1] - c0;
+  if (chunks > 0) {  // spatial chunks, best bound first, until the bound exceeds the NB-th best score
+    for (int64_t c = lane; c < chunks; c += 32) bound[c] = chunk_bound(__ldg(A.chunk_box + c0 + c), mx, my);
+    __syncwarp();
+    while (true) {
+      unsigned long long best = ~0ull;
+      int bc = -1;
+      for (int c = lane; c < chunks; c += 32) {
+        if (bound[c] < best) {
+          best = bound[c];
+          bc = c;
+        }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long ob = __shfl_xor_sync(kFullMask, best, off);
+        const int oc = __shfl_xor_sync(kFullMask, bc, off);
+        if (ob < best || (ob == best && static_cast<unsigned>(oc) < static_cast<unsigned>(bc))) {
+          best = ob;
+          bc = oc;
+        }
+      }
+      const uint64_t ts = __shfl_sync(kFullMask, ls, NB - 1);
+      if (bc < 0 || best > ts) break;  // every chunk left scores above the NB-th best (ties included)
+      __syncwarp();
+      if (lane == 0) bound[bc] = ~0ull;  // visited (real bounds stay below 2^63)
+      __syncwarp();
+      const int j = bc * kSpatialChunk + lane;
+      uint64_t s = kEmptyKey;
+      int32_t node = INT32_MAX;
+      if (n0 + j < n1) {
+        const int32_t x = __ldg(A.perm + n0 + j);
+        if (x != u && x != v) {
+          const int32_t deg = __ldg(g.row_offsets + x + 1) - __ldg(g.row_offsets + x);
+          if (A.max_degree == 0 || deg <= A.max_degree) {
+            const int2 p = __ldg(g.xy + x);
+            const int64_t dx = 2 * static_cast<int64_t>(p.x) - mx, dy = 2 * static_cast<int64_t>(p.y) - my;
+            s = static_cast<uint64_t>(dx * dx) + static_cast<uint64_t>(dy * dy);
+            node = x;
+          }
+        }
+      }
+      const int32_t tn = __shfl_sync(kFullMask, ln, NB - 1);
+      if (!__any_sync(kFullMask, pair_less(s, node, ts, tn))) continue;
+      warp_sort_pairs(s, node, lane);
+      warp_merge_pairs(ls, ln, s, node, lane);
+    }
+  }
+  for (int64_t base = chunks > 0 ? n1 : n0; base < n1; base += 32) {
     const int64_t x = base + lane;
     uint64_t s = kEmptyKey;
     int32_t node = INT32_MAX;
@@ -386,7 +533,7 @@ static __global__ void __launch_bounds__(kBatchWarps * 32, 5) batch_screen_kerne
     } else {
       const int64_t s = q - n_select - n_jv;
       batch_cd_target<kSpan>(A, A.first_instance + static_cast<int32_t>(s / A.targets),
-                             static_cast<int32_t>(s % A.targets), pair_i, pair_j, lane);
+                             static_cast<int32_t>(s % A.targets), pair_i, pair_j, scratch[warp].chunk_bound, lane);
     }
     __syncwarp();
   }

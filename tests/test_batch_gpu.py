@@ -105,6 +105,40 @@ def test_degenerate_instances(ctx, port):
         check_against_oracle(port, batch, res, opt)
 
 
+def grid_knn(side, k, seed, copies=1):
+    """Points of a side x side integer grid (each repeated `copies` times at the same place), shuffled:
+    many equal doubled-midpoint distances, so the neighbourhood order hinges on the node-id ties."""
+    rng = np.random.default_rng(seed)
+    xs = np.repeat(np.tile(np.arange(side) * 7, side), copies)
+    ys = np.repeat(np.repeat(np.arange(side) * 7, side), copies)
+    order = rng.permutation(xs.shape[0])
+    xs, ys = xs[order], ys[order]
+    n = xs.shape[0]
+    d2 = (xs[:, None] - xs[None, :]) ** 2 + (ys[:, None] - ys[None, :]) ** 2
+    np.fill_diagonal(d2, np.iinfo(np.int64).max)
+    edges = set()
+    for i in range(n):
+        for j in np.lexsort((np.arange(n), d2[i]))[:k]:
+            edges.add((min(i, int(j)), max(i, int(j))))
+    return GraphSnapshot.from_edges(xs, ys, sorted(edges), 0)
+
+
+def test_spatial_chunks_ties_caps_and_large(ctx, port):
+    """The chunked neighbourhood search (instances up to 8,192 nodes) against the oracle's full scan:
+    grids with equal distances and co-located nodes (ties by node id), a degree cap that leaves few
+    eligible nodes, and an instance above the chunked size (full scan)."""
+    from helpers import knn_graph
+    graphs = [grid_knn(24, 8, seed=1), grid_knn(12, 6, seed=2, copies=3), knn_graph(600, 10, seed=3),
+              synth.uniform_knn(9000, 200_000, 6, 0, 4)]
+    batch = TinyBatch(graphs)
+    for opt in (BatchOptions(), BatchOptions(16, 25, 9, 0), BatchOptions(8, 32, 0, 1)):
+        ctx.batch_prepare(batch, opt)
+        ctx.batch_launch()
+        check_against_oracle(port, batch, ctx.batch_fetch(), opt)
+        res, _ = ctx.batch_screen(batch, opt)
+        check_against_oracle(port, batch, res, opt)
+
+
 def test_unsorted_instance_rejected(ctx):
     g = synth.batch_instance(0)
     swapped = GraphSnapshot(g.n, 0, g.x, g.y, g.edge_u[::-1].copy(), g.edge_v[::-1].copy(), g.edge_w[::-1].copy(),
