@@ -48,7 +48,9 @@ struct BatchState {
   // the union snapshot in the kernels' layout
   DevBuf d_node_begin, d_edge_begin, xy, uv, w32, active, ro, nbr, ids, slot4;
   // raw uploads of the end-to-end call (converted on the device)
-  DevBuf raw_x, raw_y, raw_u, raw_v, raw_w;
+  DevBuf raw_x, raw_y, raw_u, raw_v;
+  int32_t* w32_host = nullptr;  // pinned staging of the end-to-end call's int32 weights
+  size_t w32_host_count = 0;
   // outputs and work-queue state
   DevBuf witness, target_ids, target_count, nbhd, flags, counter, ready;
   DevBuf perm, chunk_box, d_chunk_begin;  // spatial chunks of the instances
@@ -69,7 +71,7 @@ struct BatchState {
   void Release() {
     ReleaseGraph();
     for (DevBuf* b : {&d_node_begin, &d_edge_begin, &xy, &uv, &w32, &active, &ro, &nbr, &ids, &slot4, &raw_x, &raw_y,
-                      &raw_u, &raw_v, &raw_w, &witness, &target_ids, &target_count, &nbhd, &flags, &counter, &ready,
+                      &raw_u, &raw_v, &witness, &target_ids, &target_count, &nbhd, &flags, &counter, &ready,
                       &cand_c, &cand_d, &cand_product, &cand_count, &perm, &chunk_box, &d_chunk_begin}) {
       b->Release();
     }
@@ -78,6 +80,9 @@ struct BatchState {
       if (done[i] != nullptr) cudaEventDestroy(done[i]);
       up[i] = done[i] = nullptr;
     }
+    if (w32_host != nullptr) cudaFreeHost(w32_host);
+    w32_host = nullptr;
+    w32_host_count = 0;
     if (h2d != nullptr) cudaStreamDestroy(h2d);
     if (d2h != nullptr) cudaStreamDestroy(d2h);
     h2d = d2h = nullptr;
@@ -98,7 +103,7 @@ uint64_t BatchResident(const cee_ctx* ctx) {
   if (s == nullptr) return 0;
   uint64_t bytes = 0;
   for (const DevBuf* b : {&s->d_node_begin, &s->d_edge_begin, &s->xy, &s->uv, &s->w32, &s->active, &s->ro, &s->nbr,
-                          &s->ids, &s->slot4, &s->raw_x, &s->raw_y, &s->raw_u, &s->raw_v, &s->raw_w, &s->witness,
+                          &s->ids, &s->slot4, &s->raw_x, &s->raw_y, &s->raw_u, &s->raw_v, &s->witness,
                           &s->target_ids, &s->target_count, &s->nbhd, &s->flags, &s->counter, &s->ready, &s->perm,
                           &s->chunk_box, &s->d_chunk_begin}) {
     bytes += b->capacity;
@@ -404,8 +409,8 @@ __global__ void batch_gather(const int32_t* __restrict__ ids, const int32_t* __r
 // replaced by harmless ones (node 0, weight 0) so that no later access leaves its array.
 __global__ void batch_pack(const int64_t* __restrict__ x, const int64_t* __restrict__ y, int64_t n0, int64_t n1,
                            int64_t min_x, int64_t min_y, int2* __restrict__ xy, const int32_t* __restrict__ u,
-                           const int32_t* __restrict__ v, const int64_t* __restrict__ w, int64_t e0, int64_t e1,
-                           int64_t n, int2* __restrict__ uv, int32_t* __restrict__ w32, int32_t* __restrict__ error) {
+                           const int32_t* __restrict__ v, int64_t e0, int64_t e1, int64_t n, int2* __restrict__ uv,
+                           int32_t* __restrict__ error) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   const int64_t first = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   for (int64_t i = n0 + first; i < n1; i += stride) {
@@ -419,7 +424,6 @@ __global__ void batch_pack(const int64_t* __restrict__ x, const int64_t* __restr
   }
   for (int64_t e = e0 + first; e < e1; e += stride) {
     int32_t a = u[e], b = v[e];
-    const int64_t wt = w[e];
     if (static_cast<uint64_t>(static_cast<uint32_t>(a)) >= static_cast<uint64_t>(n) ||
         static_cast<uint64_t>(static_cast<uint32_t>(b)) >= static_cast<uint64_t>(n) || a >= b) {
       atomicOr(error, 32);
@@ -430,12 +434,6 @@ __global__ void batch_pack(const int64_t* __restrict__ x, const int64_t* __restr
       if (pa > a || (pa == a && pb >= b)) atomicOr(error, 32);
     }
     uv[e] = make_int2(a, b);
-    if (wt < 0 || wt > INT32_MAX) {
-      atomicOr(error, 64);
-      w32[e] = 0;
-    } else {
-      w32[e] = static_cast<int32_t>(wt);
-    }
   }
 }
 
@@ -668,10 +666,22 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
   SetShape(s, b, options);
   rc = ReserveAll(ctx, s);
   for (const auto& [buf, bytes] : {std::pair<DevBuf*, size_t>{&s.raw_x, g.n * 8ull}, {&s.raw_y, g.n * 8ull},
-                                   {&s.raw_u, g.m * 4ull}, {&s.raw_v, g.m * 4ull}, {&s.raw_w, g.m * 8ull}}) {
+                                   {&s.raw_u, g.m * 4ull}, {&s.raw_v, g.m * 4ull}}) {
     if (rc == CEE_OK) rc = Reserve(ctx, *buf, bytes);
   }
   if (rc != CEE_OK) return rc;
+  if (s.w32_host_count < static_cast<size_t>(g.m)) {  // pinned int32 weight staging, grown geometrically
+    if (s.w32_host != nullptr) cudaFreeHost(s.w32_host);
+    s.w32_host = nullptr;
+    s.w32_host_count = 0;
+    const size_t count = std::max<size_t>(static_cast<size_t>(g.m), 1);
+    if (cudaHostAlloc(reinterpret_cast<void**>(&s.w32_host), count * sizeof(int32_t), cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      s.w32_host = nullptr;
+      return Fail(ctx, CEE_ERR_NOMEM, "pinned weight staging");
+    }
+    s.w32_host_count = count;
+  }
   cudaError_t status = cudaSuccess;
   if (s.h2d == nullptr) status = cudaStreamCreateWithFlags(&s.h2d, cudaStreamNonBlocking);
   if (status == cudaSuccess && s.d2h == nullptr) status = cudaStreamCreateWithFlags(&s.d2h, cudaStreamNonBlocking);
@@ -693,7 +703,6 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
   const size_t T = static_cast<size_t>(s.opt.targets), NB = static_cast<size_t>(s.opt.max_neighborhood);
   const size_t FW = static_cast<size_t>(s.flag_words);
   int64_t h2d_bytes = (b->instances + 1) * 24, d2h_bytes = 0;
-  // 1. every chunk's upload on the copy stream, so the copies start before the host checks
   std::vector<int32_t> bounds(static_cast<size_t>(chunks) + 1, 0);
   for (int c = 0; c <= chunks; ++c) {
     bounds[static_cast<size_t>(c)] = static_cast<int32_t>(static_cast<int64_t>(b->instances) * c / chunks);
@@ -703,47 +712,59 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
       return Fail(ctx, CEE_ERR_INVALID, "row_offsets not non-decreasing");
     }
   }
+  // Per chunk: the weights are narrowed to int32 on host threads (range-checked) into pinned staging,
+  // the chunk's arrays go up on the copy stream, and its screen is queued behind them. The O(n) host
+  // checks run once, after the first chunk's copies are queued and before any kernel reads them.
+  int64_t min_x = 0, min_y = 0;
   for (int c = 0; c < chunks; ++c) {
     const int32_t i0 = bounds[c], i1 = bounds[c + 1];
     if (i1 == i0) continue;
     const int64_t n0 = b->node_begin[i0], n1 = b->node_begin[i1], e0 = b->edge_begin[i0], e1 = b->edge_begin[i1];
     const int64_t s0 = g.row_offsets[n0], s1 = g.row_offsets[n1];
+    std::vector<uint8_t> bad_weight(16, 0);
+    ParallelRanges(e1 - e0, [&](int64_t a0, int64_t a1, int t) {
+      for (int64_t e = e0 + a0; e < e0 + a1; ++e) {
+        const int64_t w = g.edge_w[e];
+        if (w < 0 || w > INT32_MAX) bad_weight[t] = 1;
+        s.w32_host[e] = static_cast<int32_t>(w);
+      }
+    });
+    if (std::any_of(bad_weight.begin(), bad_weight.end(), [](uint8_t v) { return v != 0; })) {
+      cudaStreamSynchronize(s.h2d);  // the caller's buffers stay borrowed until the queued copies end
+      cudaStreamSynchronize(cs);
+      return Fail(ctx, CEE_ERR_RANGE, "edge weight outside [0, 2^31)");
+    }
     cudaMemcpyAsync(static_cast<int64_t*>(s.raw_x.ptr) + n0, g.x + n0, (n1 - n0) * 8, cudaMemcpyHostToDevice, s.h2d);
     cudaMemcpyAsync(static_cast<int64_t*>(s.raw_y.ptr) + n0, g.y + n0, (n1 - n0) * 8, cudaMemcpyHostToDevice, s.h2d);
     cudaMemcpyAsync(static_cast<int32_t*>(s.ro.ptr) + n0, g.row_offsets + n0, (n1 - n0 + 1) * 4, cudaMemcpyHostToDevice, s.h2d);
     cudaMemcpyAsync(static_cast<int32_t*>(s.raw_u.ptr) + e0, g.edge_u + e0, (e1 - e0) * 4, cudaMemcpyHostToDevice, s.h2d);
     cudaMemcpyAsync(static_cast<int32_t*>(s.raw_v.ptr) + e0, g.edge_v + e0, (e1 - e0) * 4, cudaMemcpyHostToDevice, s.h2d);
-    cudaMemcpyAsync(static_cast<int64_t*>(s.raw_w.ptr) + e0, g.edge_w + e0, (e1 - e0) * 8, cudaMemcpyHostToDevice, s.h2d);
+    cudaMemcpyAsync(static_cast<int32_t*>(s.w32.ptr) + e0, s.w32_host + e0, (e1 - e0) * 4, cudaMemcpyHostToDevice, s.h2d);
     cudaMemcpyAsync(static_cast<uint8_t*>(s.active.ptr) + e0, g.active + e0, e1 - e0, cudaMemcpyHostToDevice, s.h2d);
     if (s1 > s0) {
       cudaMemcpyAsync(static_cast<int32_t*>(s.nbr.ptr) + s0, g.neighbors + s0, (s1 - s0) * 4, cudaMemcpyHostToDevice, s.h2d);
       cudaMemcpyAsync(static_cast<int32_t*>(s.ids.ptr) + s0, g.csr_edge_ids + s0, (s1 - s0) * 4, cudaMemcpyHostToDevice, s.h2d);
     }
-    h2d_bytes += (n1 - n0) * 20 + 4 + (e1 - e0) * 17 + (s1 - s0) * 8;
+    h2d_bytes += (n1 - n0) * 20 + 4 + (e1 - e0) * 13 + (s1 - s0) * 8;
     cudaEventRecord(s.up[c], s.h2d);
-  }
-  // 2. while they run: row offsets and the bounding box on host threads (nothing reads the
-  //    uploads on the device before these pass)
-  int64_t box[4];
-  rc = ScanNodes(ctx, g, box);
-  if (rc != CEE_OK) {
-    cudaStreamSynchronize(s.h2d);  // the caller's buffers stay borrowed until the copies end
-    return rc;
-  }
-  const int64_t min_x = box[0], min_y = box[2];
-  s.span = span_class(box[1] - box[0], box[3] - box[2]);
-  // 3. per chunk: convert and screen (compute stream), download (second copy stream)
-  for (int c = 0; c < chunks; ++c) {
-    const int32_t i0 = bounds[c], i1 = bounds[c + 1];
-    if (i1 == i0) continue;
-    const int64_t n0 = b->node_begin[i0], n1 = b->node_begin[i1], e0 = b->edge_begin[i0], e1 = b->edge_begin[i1];
-    const int64_t s0 = g.row_offsets[n0], s1 = g.row_offsets[n1];
+    if (c == 0) {  // row offsets and the bounding box on host threads, while the first copies run
+      int64_t box[4];
+      rc = ScanNodes(ctx, g, box);
+      if (rc != CEE_OK) {
+        cudaStreamSynchronize(s.h2d);
+        cudaStreamSynchronize(cs);
+        return rc;
+      }
+      min_x = box[0];
+      min_y = box[2];
+      s.span = span_class(box[1] - box[0], box[3] - box[2]);
+    }
+    // convert and screen (compute stream), download (second copy stream)
     cudaStreamWaitEvent(cs, s.up[c], 0);
     batch_pack<<<GridFor(std::max(n1 - n0, e1 - e0), 256, ctx->sm_count * 8), 256, 0, cs>>>(
         static_cast<const int64_t*>(s.raw_x.ptr), static_cast<const int64_t*>(s.raw_y.ptr), n0, n1, min_x, min_y,
         static_cast<int2*>(s.xy.ptr), static_cast<const int32_t*>(s.raw_u.ptr), static_cast<const int32_t*>(s.raw_v.ptr),
-        static_cast<const int64_t*>(s.raw_w.ptr), e0, e1, g.n, static_cast<int2*>(s.uv.ptr),
-        static_cast<int32_t*>(s.w32.ptr), ctx->d_error);
+        e0, e1, g.n, static_cast<int2*>(s.uv.ptr), ctx->d_error);
     if (s1 > s0) {
       batch_gather<<<GridFor(s1 - s0, 256, ctx->sm_count * 8), 256, 0, cs>>>(
           static_cast<const int32_t*>(s.ids.ptr), static_cast<const int32_t*>(s.nbr.ptr), static_cast<const int2*>(s.xy.ptr),

@@ -139,6 +139,25 @@ def test_spatial_chunks_ties_caps_and_large(ctx, port):
         check_against_oracle(port, batch, res, opt)
 
 
+def test_e2e_weight_range(ctx):
+    """The end-to-end call narrows weights to int32 on the host: weights outside [0, 2^31) fail with
+    CEE_ERR_RANGE, as in the resident prepare."""
+    from cudaedgeelimination_b200._native import CEE_ERR_RANGE, NativeError
+    batch = TinyBatch([synth.batch_instance(0), synth.batch_instance(1)])
+    for bad in (-1, 1 << 31):
+        g = batch.graph.copy()
+        g.edge_w = g.edge_w.copy()
+        g.edge_w[g.m - 3] = bad
+        with pytest.raises(NativeError) as err:
+            ctx.batch_screen(batch, BatchOptions(), graph=g)
+        assert err.value.code == CEE_ERR_RANGE
+        with pytest.raises(NativeError) as err:
+            ctx.batch_prepare(batch, BatchOptions(), graph=g)
+        assert err.value.code == CEE_ERR_RANGE
+    res, _ = ctx.batch_screen(batch, BatchOptions())  # the context stays usable
+    assert res.witness.shape == (batch.graph.m,)
+
+
 def test_unsorted_instance_rejected(ctx):
     g = synth.batch_instance(0)
     swapped = GraphSnapshot(g.n, 0, g.x, g.y, g.edge_u[::-1].copy(), g.edge_v[::-1].copy(), g.edge_w[::-1].copy(),
