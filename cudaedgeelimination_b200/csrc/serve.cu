@@ -386,8 +386,10 @@ int cee_serve_add_snapshot(cee_ctx* ctx, const cee_graph_view* g, int32_t* snaps
   const size_t adj = g->m > 0 ? static_cast<size_t>(g->adjacency) : 0;
   auto up = [](size_t b) { return (b + 15) & ~size_t{15}; };
   const size_t o_xy = 0, o_uv = up(o_xy + 8 * n), o_w = up(o_uv + 8 * m), o_act = up(o_w + 4 * m);
-  const size_t o_ro = up(o_act + m), o_nbr = up(o_ro + 4 * (n + 1)), o_slot = up(o_nbr + 4 * adj);
-  const size_t bytes = up(o_slot + 4 * adj);
+  // CSR slots twice: neighbours alone (binary searches of a row) and 16-byte records {neighbour,
+  // slot weight, neighbour x, neighbour y} (one load per slot in the JV screen)
+  const size_t o_ro = up(o_act + m), o_nbr = up(o_ro + 4 * (n + 1)), o_slot4 = up(o_nbr + 4 * adj);
+  const size_t bytes = up(o_slot4 + 16 * adj);
   size_t offset = 0;
   if (!s.arena.Allocate(bytes, &offset)) return CEE_BUSY;  // over the HBM budget now
   rc = EnsurePinned(ctx, s, bytes);
@@ -420,8 +422,11 @@ int cee_serve_add_snapshot(cee_ctx* ctx, const cee_graph_view* g, int32_t* snaps
   }
   if (adj > 0) {
     std::memcpy(st + o_nbr, g->neighbors, 4 * adj);
-    int32_t* slot = reinterpret_cast<int32_t*>(st + o_slot);
-    for (size_t i = 0; i < adj; ++i) slot[i] = w32[g->csr_edge_ids[i]];
+    int4* slot4 = reinterpret_cast<int4*>(st + o_slot4);
+    for (size_t i = 0; i < adj; ++i) {
+      const int32_t c = g->neighbors[i];
+      slot4[i] = make_int4(c, w32[g->csr_edge_ids[i]], xy[static_cast<size_t>(c)].x, xy[static_cast<size_t>(c)].y);
+    }
   }
   uint8_t* base = static_cast<uint8_t*>(s.arena_buf.ptr) + offset;
   rc = QuiesceServer(ctx, s);
@@ -465,7 +470,8 @@ int cee_serve_add_snapshot(cee_ctx* ctx, const cee_graph_view* g, int32_t* snaps
   snap.g.active = base + o_act;
   snap.g.row_offsets = reinterpret_cast<const int32_t*>(base + o_ro);
   snap.g.nbr = reinterpret_cast<const int32_t*>(base + o_nbr);
-  snap.g.slot_w = reinterpret_cast<const int32_t*>(base + o_slot);
+  snap.g.slot_w = nullptr;
+  snap.g.slot4 = reinterpret_cast<const int4*>(base + o_slot4);
   *snapshot = id;
   return CEE_OK;
 }

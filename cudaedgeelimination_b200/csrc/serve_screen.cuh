@@ -256,9 +256,9 @@ static __global__ void __launch_bounds__(kServeWarps * 32, 4)
       const int64_t e1 = min(e0 + kServeJvTile, job.g.m);
       for (int64_t e = e0; e < e1; ++e) {
         const int32_t wv =
-            job.span == kSpanSmall    ? jv_screen_edge_warp<kSpanSmall>(job.g, e, jv_scratch[warp], lane, error)
-            : job.span == kSpanNarrow ? jv_screen_edge_warp<kSpanNarrow>(job.g, e, jv_scratch[warp], lane, error)
-                                      : jv_screen_edge_warp<kSpanWide>(job.g, e, jv_scratch[warp], lane, error);
+            job.span == kSpanSmall    ? jv_screen_edge_warp<kSpanSmall, true>(job.g, e, jv_scratch[warp], lane, error)
+            : job.span == kSpanNarrow ? jv_screen_edge_warp<kSpanNarrow, true>(job.g, e, jv_scratch[warp], lane, error)
+                                      : jv_screen_edge_warp<kSpanWide, true>(job.g, e, jv_scratch[warp], lane, error);
         if (lane == 0) job.witness[e] = wv;
         __syncwarp();
       }
