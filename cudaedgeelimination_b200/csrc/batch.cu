@@ -57,8 +57,8 @@ struct BatchState {
   DevBuf cand_c, cand_d, cand_product, cand_count;  // finalised c,d candidates (max_cd_candidates > 0)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  cudaStream_t h2d = nullptr, d2h = nullptr;
-  cudaEvent_t up[kMaxChunks] = {}, done[kMaxChunks] = {};
+  cudaStream_t h2d = nullptr, d2h = nullptr, prep = nullptr;
+  cudaEvent_t up[kMaxChunks] = {}, done[kMaxChunks] = {}, prepped[kMaxChunks] = {};
   int occupancy[kSpanClasses] = {1, 1, 1};  // resident screen blocks per SM, per span class
   bool prepared = false;
 
@@ -78,12 +78,15 @@ struct BatchState {
     for (int i = 0; i < kMaxChunks; ++i) {
       if (up[i] != nullptr) cudaEventDestroy(up[i]);
       if (done[i] != nullptr) cudaEventDestroy(done[i]);
-      up[i] = done[i] = nullptr;
+      if (prepped[i] != nullptr) cudaEventDestroy(prepped[i]);
+      up[i] = done[i] = prepped[i] = nullptr;
     }
     if (w32_host != nullptr) cudaFreeHost(w32_host);
     w32_host = nullptr;
     w32_host_count = 0;
     if (h2d != nullptr) cudaStreamDestroy(h2d);
+    if (prep != nullptr) cudaStreamDestroy(prep);
+    prep = nullptr;
     if (d2h != nullptr) cudaStreamDestroy(d2h);
     h2d = d2h = nullptr;
     prepared = false;
@@ -685,21 +688,27 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
   cudaError_t status = cudaSuccess;
   if (s.h2d == nullptr) status = cudaStreamCreateWithFlags(&s.h2d, cudaStreamNonBlocking);
   if (status == cudaSuccess && s.d2h == nullptr) status = cudaStreamCreateWithFlags(&s.d2h, cudaStreamNonBlocking);
+  if (status == cudaSuccess && s.prep == nullptr) status = cudaStreamCreateWithFlags(&s.prep, cudaStreamNonBlocking);
   for (int i = 0; i < kMaxChunks && status == cudaSuccess; ++i) {
     if (s.up[i] == nullptr) status = cudaEventCreateWithFlags(&s.up[i], cudaEventDisableTiming);
     if (status == cudaSuccess && s.done[i] == nullptr) status = cudaEventCreateWithFlags(&s.done[i], cudaEventDisableTiming);
+    if (status == cudaSuccess && s.prepped[i] == nullptr) {
+      status = cudaEventCreateWithFlags(&s.prepped[i], cudaEventDisableTiming);
+    }
   }
   if (status != cudaSuccess) return CudaFail(ctx, status, "batch streams");
   status = QueryBatchOccupancy(s);
   if (status != cudaSuccess) return CudaFail(ctx, status, "batch occupancy");
   const int chunks = std::max(1, std::min<int>(s.tune.chunks, b->instances));
   cudaStream_t cs = ctx->stream;
-  cudaEventRecord(ctx->ev[0], cs);
-  cudaStreamWaitEvent(s.h2d, ctx->ev[0], 0);
+  // ev[0] follows the error-word reset and the offset copies, so that the copy stream, and through it the
+  // preparation stream, starts behind them (and behind earlier work on the context's stream)
   cudaMemsetAsync(ctx->d_error, 0, sizeof(int32_t), cs);
   cudaMemcpyAsync(s.d_node_begin.ptr, b->node_begin, (b->instances + 1) * 8, cudaMemcpyHostToDevice, cs);
   cudaMemcpyAsync(s.d_edge_begin.ptr, b->edge_begin, (b->instances + 1) * 8, cudaMemcpyHostToDevice, cs);
   cudaMemcpyAsync(s.d_chunk_begin.ptr, s.chunk_begin.data(), (b->instances + 1) * 8, cudaMemcpyHostToDevice, cs);
+  cudaEventRecord(ctx->ev[0], cs);
+  cudaStreamWaitEvent(s.h2d, ctx->ev[0], 0);
   const size_t T = static_cast<size_t>(s.opt.targets), NB = static_cast<size_t>(s.opt.max_neighborhood);
   const size_t FW = static_cast<size_t>(s.flag_words);
   int64_t h2d_bytes = (b->instances + 1) * 24, d2h_bytes = 0;
@@ -731,6 +740,7 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
     });
     if (std::any_of(bad_weight.begin(), bad_weight.end(), [](uint8_t v) { return v != 0; })) {
       cudaStreamSynchronize(s.h2d);  // the caller's buffers stay borrowed until the queued copies end
+      cudaStreamSynchronize(s.prep);
       cudaStreamSynchronize(cs);
       return Fail(ctx, CEE_ERR_RANGE, "edge weight outside [0, 2^31)");
     }
@@ -759,19 +769,22 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
       min_y = box[2];
       s.span = span_class(box[1] - box[0], box[3] - box[2]);
     }
-    // convert and screen (compute stream), download (second copy stream)
-    cudaStreamWaitEvent(cs, s.up[c], 0);
-    batch_pack<<<GridFor(std::max(n1 - n0, e1 - e0), 256, ctx->sm_count * 8), 256, 0, cs>>>(
+    // convert (preparation stream: its blocks take the SMs that the previous chunk's screen frees as
+    // it drains), screen (compute stream), download (second copy stream)
+    cudaStreamWaitEvent(s.prep, s.up[c], 0);
+    batch_pack<<<GridFor(std::max(n1 - n0, e1 - e0), 256, ctx->sm_count * 8), 256, 0, s.prep>>>(
         static_cast<const int64_t*>(s.raw_x.ptr), static_cast<const int64_t*>(s.raw_y.ptr), n0, n1, min_x, min_y,
         static_cast<int2*>(s.xy.ptr), static_cast<const int32_t*>(s.raw_u.ptr), static_cast<const int32_t*>(s.raw_v.ptr),
         e0, e1, g.n, static_cast<int2*>(s.uv.ptr), ctx->d_error);
     if (s1 > s0) {
-      batch_gather<<<GridFor(s1 - s0, 256, ctx->sm_count * 8), 256, 0, cs>>>(
+      batch_gather<<<GridFor(s1 - s0, 256, ctx->sm_count * 8), 256, 0, s.prep>>>(
           static_cast<const int32_t*>(s.ids.ptr), static_cast<const int32_t*>(s.nbr.ptr), static_cast<const int2*>(s.xy.ptr),
           s0, s1, static_cast<const int32_t*>(s.w32.ptr), g.m, g.n, static_cast<int4*>(s.slot4.ptr), ctx->d_error);
     }
-    status = LaunchSpatial(s, i0, i1 - i0, cs);
+    status = LaunchSpatial(s, i0, i1 - i0, s.prep);
     if (status != cudaSuccess) return CudaFail(ctx, status, "batch spatial chunks");
+    cudaEventRecord(s.prepped[c], s.prep);
+    cudaStreamWaitEvent(cs, s.prepped[c], 0);
     rc = LaunchRange(ctx, s, i0, i1 - i0, c, cs);
     if (rc != CEE_OK) return rc;
     cudaEventRecord(s.done[c], cs);
