@@ -267,14 +267,21 @@ __device__ void batch_select_targets(const BatchArgs& A, int32_t inst, int lane)
   }
 }
 
+// Neighbour pairs (a, b), a < b, in b-major order (b(b-1)/2 + a): the first d(d-1)/2 entries are the
+// pairs of a row of d neighbours, for every d <= kReplyTableDegree.
+constexpr int kReplyTableDegree = 64;
+constexpr int kReplyTablePairs = kReplyTableDegree * (kReplyTableDegree - 1) / 2;
+
 // Number of Hamilton replies at `center` for target (u, v) (AppendHtHamiltonRepliesUnchecked,
 // src/cpu/hamilton_tutte.cpp:230-269): pairs first < second of the center's CSR neighbours whose
 // edges to the center both survive 2-opt against the target, whose node pair is not the target,
 // and with C(u,v) + C(c,first) + C(c,second) <= C(first,second) + C(u,c) + C(v,c). Whole warp; rows
 // of up to 32 neighbours keep them one per lane, longer rows re-read both neighbours per pair.
+// Pairs come from `reply_pairs` (the table above) for rows of up to kReplyTableDegree neighbours.
 template <int kSpan>
 __device__ int32_t ht_reply_count(const JvGraph& g, int32_t u, int32_t v, int2 pu, int2 pv, uint32_t cuv,
-                                  int32_t center, int2 pc, uint32_t cuc, uint32_t cvc, int lane) {
+                                  int32_t center, int2 pc, uint32_t cuc, uint32_t cvc, const uint16_t* reply_pairs,
+                                  int lane) {
   const int32_t r0 = __ldg(g.row_offsets + center), deg = __ldg(g.row_offsets + center + 1) - r0;
   if (deg < 2) return 0;
   const uint64_t center_target = static_cast<uint64_t>(cuc) + cvc;
@@ -302,7 +309,11 @@ __device__ int32_t ht_reply_count(const JvGraph& g, int32_t u, int32_t v, int2 p
   for (int64_t base = 0; base < pairs; base += 32) {
     const int64_t p = base + lane;
     int a = 0, b = 1;
-    if (p < pairs) {  // invert p = a (2 deg - a - 1) / 2 + (b - a - 1)
+    if (p < pairs && deg <= kReplyTableDegree) {  // the count is a sum: any pair order will do
+      const uint16_t ab = reply_pairs[p];
+      a = ab & 0xff;
+      b = ab >> 8;
+    } else if (p < pairs) {  // invert p = a (2 deg - a - 1) / 2 + (b - a - 1)
       const float twod = 2.0f * deg - 1.0f;
       a = static_cast<int>((twod - sqrtf(twod * twod - 8.0f * static_cast<float>(p))) * 0.5f);
       a = max(0, min(a, deg - 2));
@@ -548,7 +559,7 @@ static __global__ void __launch_bounds__(kBatchWarps * 32, 8) batch_screen_kerne
 // registers.
 template <int kSpan>
 __device__ void batch_finalize_target(const BatchArgs& A, int32_t inst, int32_t t, const uint8_t* pair_i,
-                                      const uint8_t* pair_j, int lane) {
+                                      const uint8_t* pair_j, const uint16_t* reply_pairs, int lane) {
   const JvGraph& g = A.g;
   const int64_t slot = static_cast<int64_t>(inst) * A.targets + t;
   const int32_t count = A.target_count[inst];
@@ -585,7 +596,7 @@ __device__ void batch_finalize_target(const BatchArgs& A, int32_t inst, int32_t 
       const int32_t x = __shfl_sync(kFullMask, ln, k);
       const int2 pxk = make_int2(__shfl_sync(kFullMask, px.x, k), __shfl_sync(kFullMask, px.y, k));
       const uint32_t cuk = __shfl_sync(kFullMask, cu, k), cvk = __shfl_sync(kFullMask, cv, k);
-      const int32_t r = ht_reply_count<kSpan>(g, u, v, pu, pv, cuv, x, pxk, cuk, cvk, lane);
+      const int32_t r = ht_reply_count<kSpan>(g, u, v, pu, pv, cuv, x, pxk, cuk, cvk, reply_pairs, lane);
       if (lane == k) my_replies = r;
     }
   }
@@ -636,6 +647,7 @@ __device__ void batch_finalize_target(const BatchArgs& A, int32_t inst, int32_t 
 template <int kSpan>
 static __global__ void __launch_bounds__(kBatchWarps * 32) batch_finalize_kernel(BatchArgs A) {
   __shared__ uint8_t pair_i[kBatchMaxPairs], pair_j[kBatchMaxPairs];
+  __shared__ uint16_t reply_pairs[kReplyTablePairs];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int p = threadIdx.x; p < A.nb * (A.nb - 1) / 2; p += blockDim.x) {
     int i = 0, rest = p;
@@ -646,12 +658,15 @@ static __global__ void __launch_bounds__(kBatchWarps * 32) batch_finalize_kernel
     pair_i[p] = static_cast<uint8_t>(i);
     pair_j[p] = static_cast<uint8_t>(i + 1 + rest);
   }
+  for (int b = 1 + static_cast<int>(threadIdx.x); b < kReplyTableDegree; b += blockDim.x) {
+    for (int a = 0; a < b; ++a) reply_pairs[b * (b - 1) / 2 + a] = static_cast<uint16_t>(a | (b << 8));
+  }
   __syncthreads();
   const int64_t slots = static_cast<int64_t>(A.instances) * A.targets;
   const int64_t warps = static_cast<int64_t>(gridDim.x) * kBatchWarps;
   for (int64_t q = static_cast<int64_t>(blockIdx.x) * kBatchWarps + warp; q < slots; q += warps) {
     batch_finalize_target<kSpan>(A, A.first_instance + static_cast<int32_t>(q / A.targets),
-                                 static_cast<int32_t>(q % A.targets), pair_i, pair_j, lane);
+                                 static_cast<int32_t>(q % A.targets), pair_i, pair_j, reply_pairs, lane);
     __syncwarp();
   }
 }

@@ -219,3 +219,33 @@ def test_finalised_candidates_match_reference(ctx, ref, small_batch):
             k = int(count[i, t])
             got = np.stack([c[i, t, :k] - n0, d[i, t, :k] - n0, product[i, t, :k]], 1)
             np.testing.assert_array_equal(got, want)
+
+
+def hub_graph(n, k, hub_degrees, seed):
+    """A k-nearest-neighbour graph whose hubs, the nodes nearest node 0, are joined to their nearest
+    hub_degrees[h] nodes: the first targets (node 0's edges) get neighbourhood nodes with rows
+    longer than a warp and than the pair table."""
+    from helpers import knn_graph
+    g = knn_graph(n, k, seed=seed)
+    edges = set(zip(g.edge_u.tolist(), g.edge_v.tolist()))
+    d2 = (g.x[:, None] - g.x[None, :]) ** 2 + (g.y[:, None] - g.y[None, :]) ** 2
+    hubs = np.lexsort((np.arange(n), d2[0]))[1:len(hub_degrees) + 1]
+    for h, deg in zip(hubs, hub_degrees):
+        for j in np.lexsort((np.arange(n), d2[h]))[1:deg + 1]:
+            edges.add((min(int(h), int(j)), max(int(h), int(j))))
+    return GraphSnapshot.from_edges(g.x, g.y, sorted(edges), 0)
+
+
+def test_finalised_candidates_long_rows(ctx, port):
+    # reply counts at centers of degree 20 to 140: one neighbour per lane up to 32, the shared pair
+    # table up to 64, the closed-form pair index beyond
+    graphs = [hub_graph(400, 6, [33, 64, 65, 140], seed=4), hub_graph(300, 8, [31, 32, 63, 100], seed=5)]
+    batch = TinyBatch(graphs)
+    for opt in (BatchOptions(targets=64, max_candidate_degree=0, max_cd_candidates=8),
+                BatchOptions(targets=32, max_neighborhood=32, max_candidate_degree=0, cd_mode=1, max_cd_candidates=32)):
+        ctx.batch_prepare(batch, opt)
+        ctx.batch_launch()
+        check_against_oracle(port, batch, ctx.batch_fetch(), opt)
+        cand = ctx.batch_fetch_candidates()
+        check_candidates(port, batch, opt, cand, range(batch.count))
+        assert (cand[3] > 0).any()
