@@ -331,7 +331,7 @@ BatchArgs MakeArgs(cee_ctx* ctx, BatchState& s, int32_t first, int32_t count, in
 // Spatial chunks of instances [first, first + count) (their coordinates must be on the device).
 cudaError_t LaunchSpatial(const BatchState& s, int32_t first, int32_t count, cudaStream_t stream) {
   if (count <= 0 || s.spatial_keys == 0) return cudaSuccess;
-  const int smem = s.spatial_keys * 8;
+  const int smem = s.spatial_keys * 4;
   if (smem > 48 * 1024) {
     const cudaError_t status = cudaFuncSetAttribute(batch_spatial, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (status != cudaSuccess) return status;

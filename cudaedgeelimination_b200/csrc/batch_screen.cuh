@@ -46,6 +46,7 @@ constexpr int kBatchMaxCd = 32;
 constexpr int kSpatialChunk = 32;        // nodes per spatial chunk (one warp pass)
 constexpr int kSpatialMaxNodes = 8192;   // larger instances keep the full neighbourhood scan
 constexpr int kSpatialMaxChunks = kSpatialMaxNodes / kSpatialChunk;
+static_assert(kSpatialMaxNodes <= (1 << 13), "spatial sort keys hold a 13-bit node index");
 
 struct BatchArgs {
   JvGraph g;                          // the union snapshot (global node and edge ids)
@@ -92,7 +93,7 @@ static __global__ void __launch_bounds__(kSpatialThreads) batch_spatial(const in
                                                                          const int64_t* __restrict__ chunk_begin,
                                                                          int32_t first, int32_t* __restrict__ perm,
                                                                          int4* __restrict__ chunk_box) {
-  extern __shared__ unsigned long long keys[];
+  extern __shared__ uint32_t keys[];  // Morton code << 13 | node (n <= kSpatialMaxNodes = 2^13)
   __shared__ int bounds[4];
   const int32_t inst = first + static_cast<int32_t>(blockIdx.x);
   const int64_t c0 = chunk_begin[inst], c1 = chunk_begin[inst + 1];
@@ -106,46 +107,72 @@ static __global__ void __launch_bounds__(kSpatialThreads) batch_spatial(const in
     bounds[1] = bounds[3] = INT32_MIN;
   }
   __syncthreads();
-  for (int j = threadIdx.x; j < n; j += blockDim.x) {
-    const int2 p = xy[n0 + j];
-    atomicMin(&bounds[0], p.x);
-    atomicMax(&bounds[1], p.x);
-    atomicMin(&bounds[2], p.y);
-    atomicMax(&bounds[3], p.y);
+  {  // the instance's box: per-thread, per-warp, then one shared atomic per warp
+    int lx = INT32_MAX, hx = INT32_MIN, ly = INT32_MAX, hy = INT32_MIN;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+      const int2 p = xy[n0 + j];
+      lx = min(lx, p.x);
+      hx = max(hx, p.x);
+      ly = min(ly, p.y);
+      hy = max(hy, p.y);
+    }
+    lx = __reduce_min_sync(kFullMask, lx);
+    hx = __reduce_max_sync(kFullMask, hx);
+    ly = __reduce_min_sync(kFullMask, ly);
+    hy = __reduce_max_sync(kFullMask, hy);
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(&bounds[0], lx);
+      atomicMax(&bounds[1], hx);
+      atomicMin(&bounds[2], ly);
+      atomicMax(&bounds[3], hy);
+    }
   }
   __syncthreads();
-  const int64_t sx = max(1, bounds[1] - bounds[0]), sy = max(1, bounds[3] - bounds[2]);
+  // 9-bit coordinates in the instance's box, bit-interleaved (any order of the nodes gives the same
+  // results; a compact one prunes more, and a 512 x 512 grid is finer than 32-node chunks need)
+  const float scale_x = 511.0f / static_cast<float>(max(1, bounds[1] - bounds[0]));
+  const float scale_y = 511.0f / static_cast<float>(max(1, bounds[3] - bounds[2]));
+  auto spread = [](uint32_t v) {  // bit b of v (b < 9) to bit 2b
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    return (v | (v << 1)) & 0x55555555u;
+  };
   for (int j = threadIdx.x; j < N; j += blockDim.x) {
-    unsigned long long key = ~0ull;
-    if (j < n) {  // 16-bit coordinates in the instance's box, bit-interleaved
+    uint32_t key = 0xffffffffu;  // padding sorts last: real keys are below 2^31
+    if (j < n) {
       const int2 p = xy[n0 + j];
-      const uint32_t qx = static_cast<uint32_t>((static_cast<int64_t>(p.x - bounds[0]) * 65535) / sx);
-      const uint32_t qy = static_cast<uint32_t>((static_cast<int64_t>(p.y - bounds[2]) * 65535) / sy);
-      uint32_t code = 0;
-#pragma unroll
-      for (int b = 0; b < 16; ++b) code |= (((qx >> b) & 1u) << (2 * b)) | (((qy >> b) & 1u) << (2 * b + 1));
-      key = (static_cast<unsigned long long>(code) << 32) | static_cast<uint32_t>(j);
+      const uint32_t qx = min(511u, static_cast<uint32_t>(static_cast<float>(p.x - bounds[0]) * scale_x));
+      const uint32_t qy = min(511u, static_cast<uint32_t>(static_cast<float>(p.y - bounds[2]) * scale_y));
+      key = ((spread(qx) | (spread(qy) << 1)) << 13) | static_cast<uint32_t>(j);
     }
     keys[j] = key;
   }
   __syncthreads();
-  for (int k = 2; k <= N; k <<= 1) {  // bitonic sort of the N keys, ascending
+  // bitonic sort of the N keys, ascending. Thread t takes pair (j, j + h), j = 2t - (t mod h); for
+  // h <= 32 the pairs of a warp's threads stay inside its own 64-key segments, so a stage whose
+  // neighbours are also that small needs only a warp barrier
+  for (int k = 2; k <= N; k <<= 1) {
     for (int h = k >> 1; h > 0; h >>= 1) {
-      for (int j = threadIdx.x; j < N; j += blockDim.x) {
-        const int o = j ^ h;
-        if (o > j) {
-          const unsigned long long a = keys[j], b = keys[o];
-          if (((j & k) == 0) == (a > b)) {
-            keys[j] = b;
-            keys[o] = a;
-          }
+      for (int t = threadIdx.x; t < (N >> 1); t += blockDim.x) {
+        const int j = 2 * t - (t & (h - 1)), o = j + h;
+        const uint32_t a = keys[j], b = keys[o];
+        if (((j & k) == 0) == (a > b)) {
+          keys[j] = b;
+          keys[o] = a;
         }
       }
-      __syncthreads();
+      const int next_h = h > 1 ? h >> 1 : k;
+      if (h > 32 || next_h > 32) {
+        __syncthreads();
+      } else {
+        __syncwarp();
+      }
     }
   }
+  __syncthreads();
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
-    perm[n0 + j] = static_cast<int32_t>(n0 + static_cast<int64_t>(keys[j] & 0xffffffffu));
+    perm[n0 + j] = static_cast<int32_t>(n0 + static_cast<int64_t>(keys[j] & 0x1fffu));
   }
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -153,7 +180,7 @@ static __global__ void __launch_bounds__(kSpatialThreads) batch_spatial(const in
     const int j = static_cast<int>(c - c0) * kSpatialChunk + lane;
     int2 p = make_int2(INT32_MAX, INT32_MAX), q = make_int2(INT32_MIN, INT32_MIN);
     if (j < n) {
-      p = xy[n0 + static_cast<int64_t>(keys[j] & 0xffffffffu)];
+      p = xy[n0 + static_cast<int64_t>(keys[j] & 0x1fffu)];
       q = p;
     }
     const int4 box = make_int4(__reduce_min_sync(kFullMask, p.x), __reduce_max_sync(kFullMask, q.x),
