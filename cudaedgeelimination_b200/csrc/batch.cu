@@ -721,15 +721,26 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
       return Fail(ctx, CEE_ERR_INVALID, "row_offsets not non-decreasing");
     }
   }
-  // Per chunk: the weights are narrowed to int32 on host threads (range-checked) into pinned staging,
-  // the chunk's arrays go up on the copy stream, and its screen is queued behind them. The O(n) host
-  // checks run once, after the first chunk's copies are queued and before any kernel reads them.
+  // Per chunk: the chunk's arrays go up on the copy stream while its weights are narrowed to int32 on
+  // host threads (range-checked) into pinned staging, which follows them; its screen is queued behind
+  // them. The O(n) host checks run once, after the first chunk's copies are queued and before any
+  // kernel reads them.
   int64_t min_x = 0, min_y = 0;
   for (int c = 0; c < chunks; ++c) {
     const int32_t i0 = bounds[c], i1 = bounds[c + 1];
     if (i1 == i0) continue;
     const int64_t n0 = b->node_begin[i0], n1 = b->node_begin[i1], e0 = b->edge_begin[i0], e1 = b->edge_begin[i1];
     const int64_t s0 = g.row_offsets[n0], s1 = g.row_offsets[n1];
+    cudaMemcpyAsync(static_cast<int64_t*>(s.raw_x.ptr) + n0, g.x + n0, (n1 - n0) * 8, cudaMemcpyHostToDevice, s.h2d);
+    cudaMemcpyAsync(static_cast<int64_t*>(s.raw_y.ptr) + n0, g.y + n0, (n1 - n0) * 8, cudaMemcpyHostToDevice, s.h2d);
+    cudaMemcpyAsync(static_cast<int32_t*>(s.ro.ptr) + n0, g.row_offsets + n0, (n1 - n0 + 1) * 4, cudaMemcpyHostToDevice, s.h2d);
+    cudaMemcpyAsync(static_cast<int32_t*>(s.raw_u.ptr) + e0, g.edge_u + e0, (e1 - e0) * 4, cudaMemcpyHostToDevice, s.h2d);
+    cudaMemcpyAsync(static_cast<int32_t*>(s.raw_v.ptr) + e0, g.edge_v + e0, (e1 - e0) * 4, cudaMemcpyHostToDevice, s.h2d);
+    cudaMemcpyAsync(static_cast<uint8_t*>(s.active.ptr) + e0, g.active + e0, e1 - e0, cudaMemcpyHostToDevice, s.h2d);
+    if (s1 > s0) {
+      cudaMemcpyAsync(static_cast<int32_t*>(s.nbr.ptr) + s0, g.neighbors + s0, (s1 - s0) * 4, cudaMemcpyHostToDevice, s.h2d);
+      cudaMemcpyAsync(static_cast<int32_t*>(s.ids.ptr) + s0, g.csr_edge_ids + s0, (s1 - s0) * 4, cudaMemcpyHostToDevice, s.h2d);
+    }
     std::vector<uint8_t> bad_weight(16, 0);
     ParallelRanges(e1 - e0, [&](int64_t a0, int64_t a1, int t) {
       for (int64_t e = e0 + a0; e < e0 + a1; ++e) {
@@ -744,17 +755,7 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
       cudaStreamSynchronize(cs);
       return Fail(ctx, CEE_ERR_RANGE, "edge weight outside [0, 2^31)");
     }
-    cudaMemcpyAsync(static_cast<int64_t*>(s.raw_x.ptr) + n0, g.x + n0, (n1 - n0) * 8, cudaMemcpyHostToDevice, s.h2d);
-    cudaMemcpyAsync(static_cast<int64_t*>(s.raw_y.ptr) + n0, g.y + n0, (n1 - n0) * 8, cudaMemcpyHostToDevice, s.h2d);
-    cudaMemcpyAsync(static_cast<int32_t*>(s.ro.ptr) + n0, g.row_offsets + n0, (n1 - n0 + 1) * 4, cudaMemcpyHostToDevice, s.h2d);
-    cudaMemcpyAsync(static_cast<int32_t*>(s.raw_u.ptr) + e0, g.edge_u + e0, (e1 - e0) * 4, cudaMemcpyHostToDevice, s.h2d);
-    cudaMemcpyAsync(static_cast<int32_t*>(s.raw_v.ptr) + e0, g.edge_v + e0, (e1 - e0) * 4, cudaMemcpyHostToDevice, s.h2d);
     cudaMemcpyAsync(static_cast<int32_t*>(s.w32.ptr) + e0, s.w32_host + e0, (e1 - e0) * 4, cudaMemcpyHostToDevice, s.h2d);
-    cudaMemcpyAsync(static_cast<uint8_t*>(s.active.ptr) + e0, g.active + e0, e1 - e0, cudaMemcpyHostToDevice, s.h2d);
-    if (s1 > s0) {
-      cudaMemcpyAsync(static_cast<int32_t*>(s.nbr.ptr) + s0, g.neighbors + s0, (s1 - s0) * 4, cudaMemcpyHostToDevice, s.h2d);
-      cudaMemcpyAsync(static_cast<int32_t*>(s.ids.ptr) + s0, g.csr_edge_ids + s0, (s1 - s0) * 4, cudaMemcpyHostToDevice, s.h2d);
-    }
     h2d_bytes += (n1 - n0) * 20 + 4 + (e1 - e0) * 13 + (s1 - s0) * 8;
     cudaEventRecord(s.up[c], s.h2d);
     if (c == 0) {  // row offsets and the bounding box on host threads, while the first copies run
