@@ -701,6 +701,14 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
   if (status != cudaSuccess) return CudaFail(ctx, status, "batch occupancy");
   const int chunks = std::max(1, std::min<int>(s.tune.chunks, b->instances));
   cudaStream_t cs = ctx->stream;
+  // every early return after the first queued copy: the caller's buffers stay borrowed until all queued
+  // copies (uploads, and downloads of finished chunks) have ended
+  auto drain = [&] {
+    cudaStreamSynchronize(s.h2d);
+    cudaStreamSynchronize(s.prep);
+    cudaStreamSynchronize(cs);
+    cudaStreamSynchronize(s.d2h);
+  };
   // ev[0] follows the error-word reset and the offset copies, so that the copy stream, and through it the
   // preparation stream, starts behind them (and behind earlier work on the context's stream)
   cudaMemsetAsync(ctx->d_error, 0, sizeof(int32_t), cs);
@@ -718,6 +726,7 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
     // the chunks' CSR slices are copied before the full row-offset check: their end points first
     const int32_t slot = g.row_offsets[b->node_begin[bounds[static_cast<size_t>(c)]]];
     if (slot < 0 || slot > g.adjacency || (c > 0 && slot < g.row_offsets[b->node_begin[bounds[c - 1]]])) {
+      drain();
       return Fail(ctx, CEE_ERR_INVALID, "row_offsets not non-decreasing");
     }
   }
@@ -750,9 +759,7 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
       }
     });
     if (std::any_of(bad_weight.begin(), bad_weight.end(), [](uint8_t v) { return v != 0; })) {
-      cudaStreamSynchronize(s.h2d);  // the caller's buffers stay borrowed until the queued copies end
-      cudaStreamSynchronize(s.prep);
-      cudaStreamSynchronize(cs);
+      drain();
       return Fail(ctx, CEE_ERR_RANGE, "edge weight outside [0, 2^31)");
     }
     cudaMemcpyAsync(static_cast<int32_t*>(s.w32.ptr) + e0, s.w32_host + e0, (e1 - e0) * 4, cudaMemcpyHostToDevice, s.h2d);
@@ -762,8 +769,7 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
       int64_t box[4];
       rc = ScanNodes(ctx, g, box);
       if (rc != CEE_OK) {
-        cudaStreamSynchronize(s.h2d);
-        cudaStreamSynchronize(cs);
+        drain();
         return rc;
       }
       min_x = box[0];
@@ -783,11 +789,17 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
           s0, s1, static_cast<const int32_t*>(s.w32.ptr), g.m, g.n, static_cast<int4*>(s.slot4.ptr), ctx->d_error);
     }
     status = LaunchSpatial(s, i0, i1 - i0, s.prep);
-    if (status != cudaSuccess) return CudaFail(ctx, status, "batch spatial chunks");
+    if (status != cudaSuccess) {
+      drain();
+      return CudaFail(ctx, status, "batch spatial chunks");
+    }
     cudaEventRecord(s.prepped[c], s.prep);
     cudaStreamWaitEvent(cs, s.prepped[c], 0);
     rc = LaunchRange(ctx, s, i0, i1 - i0, c, cs);
-    if (rc != CEE_OK) return rc;
+    if (rc != CEE_OK) {
+      drain();
+      return rc;
+    }
     cudaEventRecord(s.done[c], cs);
     // download the chunk's results (second copy stream)
     cudaStreamWaitEvent(s.d2h, s.done[c], 0);
