@@ -359,6 +359,11 @@ int CheckDeviceError(cee_ctx* ctx, const char* what) {
   return CEE_OK;
 }
 
+int Drained(cee_ctx* ctx, int rc) {
+  cudaStreamSynchronize(ctx->stream);
+  return rc;
+}
+
 int JvFetch(cee_ctx* ctx, int32_t* witness_out) {
   JvState& s = ctx->jv;
   if (!s.prepared) return Fail(ctx, CEE_ERR_STATE, "cee_jv_fetch before cee_jv_prepare");
@@ -694,6 +699,28 @@ int CanonicalTable(cee_ctx* ctx, uint32_t k, const KoptTable** out) {
   return CEE_OK;
 }
 
+// cee_kopt_prepare_multi without the final wait: its copies stay queued for the calls that launch next.
+int KoptPrepareMulti(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x, const int64_t* y, int32_t segments,
+                     const uint32_t* ks, const cee_kopt_task* const* tasks, const int64_t* rows,
+                     cee_kopt_stats* stats) {
+  int rc = Activate(ctx);
+  if (rc != CEE_OK) return rc;
+  if (stats != nullptr) *stats = cee_kopt_stats{};
+  if (segments < 1 || segments > kKoptMaxSegments || ks == nullptr || tasks == nullptr || rows == nullptr) {
+    return Fail(ctx, CEE_ERR_INVALID, "bad k-opt segment description");
+  }
+  bool snapshot_hit = false;
+  rc = KoptCoords(ctx, n, dist_type, x, y, &snapshot_hit);
+  if (rc != CEE_OK) return rc;
+  const KoptTable* tables[kKoptMaxSegments];
+  for (int32_t i = 0; i < segments; ++i) {
+    if (ks[i] < 3 || ks[i] > 5) return Fail(ctx, CEE_ERR_INVALID, "k must lie in [3,5]");
+    rc = CanonicalTable(ctx, ks[i], &tables[i]);
+    if (rc != CEE_OK) return rc;
+  }
+  return KoptPrepareSegments(ctx, segments, ks, tables, tasks, rows, stats, snapshot_hit, true);
+}
+
 // ---------------------------------------------------------------- c,d -------------------
 
 bool HostHasActiveEdge(const cee_graph_view* g, int32_t u, int32_t v) {
@@ -868,7 +895,11 @@ int cee_jv_prepare(cee_ctx* ctx, const cee_graph_view* graph, cee_jv_stats* stat
   int rc = Activate(ctx);
   if (rc != CEE_OK) return rc;
   if (stats != nullptr) *stats = cee_jv_stats{};
-  return JvPrepare(ctx, graph, stats);
+  rc = JvPrepare(ctx, graph, stats);
+  const cudaError_t status = cudaStreamSynchronize(ctx->stream);  // the graph's arrays are released on return
+  if (rc != CEE_OK) return rc;
+  if (status != cudaSuccess) return CudaFail(ctx, status, "JV upload");
+  return CEE_OK;
 }
 
 int cee_jv_launch(cee_ctx* ctx) {
@@ -888,10 +919,10 @@ int cee_jv_screen(cee_ctx* ctx, const cee_graph_view* graph, int32_t* witness_ou
   if (rc != CEE_OK) return rc;
   cee_jv_stats local{};
   rc = JvPrepare(ctx, graph, &local);
-  if (rc != CEE_OK) return rc;
+  if (rc != CEE_OK) return Drained(ctx, rc);
   cudaEventRecord(ctx->ev[2], ctx->stream);
   rc = JvLaunch(ctx);
-  if (rc != CEE_OK) return rc;
+  if (rc != CEE_OK) return Drained(ctx, rc);
   cudaEventRecord(ctx->ev[3], ctx->stream);
   rc = JvFetch(ctx, witness_out);
   cudaEventRecord(ctx->ev[4], ctx->stream);
@@ -938,10 +969,10 @@ int cee_kopt_costs(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x,
   const cee_kopt_task* task_list[1] = {tasks};
   cee_kopt_stats local{};
   rc = KoptPrepareSegments(ctx, 1, &k, tables, task_list, &rows, &local, snapshot_hit, template_hit);
-  if (rc != CEE_OK) return rc;
+  if (rc != CEE_OK) return Drained(ctx, rc);
   cudaEventRecord(ctx->ev[2], ctx->stream);
   rc = KoptLaunchPrepared(ctx);
-  if (rc != CEE_OK) return rc;
+  if (rc != CEE_OK) return Drained(ctx, rc);
   cudaEventRecord(ctx->ev[3], ctx->stream);
   int64_t* outs[1] = {costs_out};
   rc = KoptFetch(ctx, outs);
@@ -959,22 +990,12 @@ int cee_kopt_costs(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x,
 int cee_kopt_prepare_multi(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x, const int64_t* y,
                            int32_t segments, const uint32_t* ks, const cee_kopt_task* const* tasks,
                            const int64_t* rows, cee_kopt_stats* stats) {
-  int rc = Activate(ctx);
+  const int rc = KoptPrepareMulti(ctx, n, dist_type, x, y, segments, ks, tasks, rows, stats);
+  if (ctx == nullptr) return rc;
+  const cudaError_t status = cudaStreamSynchronize(ctx->stream);  // the task arrays are released on return
   if (rc != CEE_OK) return rc;
-  if (stats != nullptr) *stats = cee_kopt_stats{};
-  if (segments < 1 || segments > kKoptMaxSegments || ks == nullptr || tasks == nullptr || rows == nullptr) {
-    return Fail(ctx, CEE_ERR_INVALID, "bad k-opt segment description");
-  }
-  bool snapshot_hit = false;
-  rc = KoptCoords(ctx, n, dist_type, x, y, &snapshot_hit);
-  if (rc != CEE_OK) return rc;
-  const KoptTable* tables[kKoptMaxSegments];
-  for (int32_t i = 0; i < segments; ++i) {
-    if (ks[i] < 3 || ks[i] > 5) return Fail(ctx, CEE_ERR_INVALID, "k must lie in [3,5]");
-    rc = CanonicalTable(ctx, ks[i], &tables[i]);
-    if (rc != CEE_OK) return rc;
-  }
-  return KoptPrepareSegments(ctx, segments, ks, tables, tasks, rows, stats, snapshot_hit, true);
+  if (status != cudaSuccess) return CudaFail(ctx, status, "k-opt upload");
+  return CEE_OK;
 }
 
 int cee_kopt_launch(cee_ctx* ctx) {
@@ -996,8 +1017,8 @@ int cee_kopt_improving_multi(cee_ctx* ctx, int32_t n, int32_t dist_type, const i
                              int64_t* const* costs_out, cee_kopt_stats* stats) {
   cee_kopt_stats local{};
   if (masks_out == nullptr || first_out == nullptr) return Fail(ctx, CEE_ERR_INVALID, "null improving-set outputs");
-  int rc = cee_kopt_prepare_multi(ctx, n, dist_type, x, y, segments, ks, tasks, rows, &local);
-  if (rc != CEE_OK) return rc;
+  int rc = KoptPrepareMulti(ctx, n, dist_type, x, y, segments, ks, tasks, rows, &local);
+  if (rc != CEE_OK) return ctx != nullptr ? Drained(ctx, rc) : rc;
   KoptState& s = ctx->kopt;
   int64_t words = 0, total_rows = 0;
   for (int32_t i = 0; i < segments; ++i) {
@@ -1006,7 +1027,7 @@ int cee_kopt_improving_multi(cee_ctx* ctx, int32_t n, int32_t dist_type, const i
   }
   cudaError_t status = s.masks.Reserve(static_cast<size_t>(words) * 4 + 16, nullptr);
   if (status == cudaSuccess) status = s.firsts.Reserve(static_cast<size_t>(total_rows) * 4 + 16, nullptr);
-  if (status != cudaSuccess) return CudaFail(ctx, status, "k-opt improving-set allocation");
+  if (status != cudaSuccess) return Drained(ctx, CudaFail(ctx, status, "k-opt improving-set allocation"));
   int64_t word_at = 0, row_at = 0;
   for (int32_t i = 0; i < segments; ++i) {
     KoptSegment& seg = s.launch.seg[i];
@@ -1019,13 +1040,15 @@ int cee_kopt_improving_multi(cee_ctx* ctx, int32_t n, int32_t dist_type, const i
   }
   cudaEventRecord(ctx->ev[2], ctx->stream);
   rc = KoptLaunchPrepared(ctx);
-  if (rc != CEE_OK) return rc;
+  if (rc != CEE_OK) return Drained(ctx, rc);
   cudaEventRecord(ctx->ev[3], ctx->stream);
   int64_t d2h = 0;
   for (int32_t i = 0; i < segments; ++i) {
     const KoptSegment& seg = s.launch.seg[i];
     if (rows[i] == 0) continue;
-    if (masks_out[i] == nullptr || first_out[i] == nullptr) return Fail(ctx, CEE_ERR_INVALID, "null improving-set output");
+    if (masks_out[i] == nullptr || first_out[i] == nullptr) {
+      return Drained(ctx, Fail(ctx, CEE_ERR_INVALID, "null improving-set output"));
+    }
     const size_t mb = static_cast<size_t>(rows[i]) * seg.mask_words * 4;
     cudaMemcpyAsync(masks_out[i], seg.improving, mb, cudaMemcpyDeviceToHost, ctx->stream);
     cudaMemcpyAsync(first_out[i], seg.first, static_cast<size_t>(rows[i]) * 4, cudaMemcpyDeviceToHost, ctx->stream);
@@ -1054,11 +1077,11 @@ int cee_kopt_costs_multi(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64
                          int32_t segments, const uint32_t* ks, const cee_kopt_task* const* tasks,
                          const int64_t* rows, int64_t* const* costs_out, cee_kopt_stats* stats) {
   cee_kopt_stats local{};
-  int rc = cee_kopt_prepare_multi(ctx, n, dist_type, x, y, segments, ks, tasks, rows, &local);
-  if (rc != CEE_OK) return rc;
+  int rc = KoptPrepareMulti(ctx, n, dist_type, x, y, segments, ks, tasks, rows, &local);
+  if (rc != CEE_OK) return ctx != nullptr ? Drained(ctx, rc) : rc;
   cudaEventRecord(ctx->ev[2], ctx->stream);
   rc = KoptLaunchPrepared(ctx);
-  if (rc != CEE_OK) return rc;
+  if (rc != CEE_OK) return Drained(ctx, rc);
   cudaEventRecord(ctx->ev[3], ctx->stream);
   rc = cee_kopt_fetch(ctx, costs_out);
   cudaEventRecord(ctx->ev[4], ctx->stream);
@@ -1123,7 +1146,7 @@ int cee_cd_screen(cee_ctx* ctx, const cee_graph_view* graph, int32_t u, int32_t 
         s.dist_type, mode, static_cast<uint8_t*>(s.flags.ptr), ctx->d_error);
   });
   status = cudaGetLastError();
-  if (status != cudaSuccess) return CudaFail(ctx, status, "cd_screen_kernel launch");
+  if (status != cudaSuccess) return Drained(ctx, CudaFail(ctx, status, "cd_screen_kernel launch"));
   cudaMemcpyAsync(flags_out, s.flags.ptr, static_cast<size_t>(count), cudaMemcpyDeviceToHost, st);
   cudaMemcpyAsync(ctx->h_error, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
   status = cudaStreamSynchronize(st);

@@ -162,6 +162,9 @@ int PackCoordinates(cee_ctx* ctx, int32_t n, const int64_t* x, const int64_t* y,
 int GridFor(int64_t work, int per_block, int max_blocks);
 float EventMs(cudaEvent_t a, cudaEvent_t b);
 int CheckDeviceError(cee_ctx* ctx, const char* what);
+// Returns rc after the context stream has finished: for error returns once copies from or to caller
+// buffers are queued, so that none of them runs after the call returns.
+int Drained(cee_ctx* ctx, int rc);
 void ReleaseBatch(cee_ctx* ctx);
 uint64_t BatchResident(const cee_ctx* ctx);
 void ReleaseServe(cee_ctx* ctx, int32_t* error_word = nullptr);

@@ -390,7 +390,7 @@ extern "C" int cee_jv_eliminate(cee_ctx* ctx, const cee_graph_view* g, uint32_t 
   WithSpan(span, [&](auto S) {
     status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, epoch_screen<S.value>, kJvWarpsPerBlock * 32, 0);
   });
-  if (status != cudaSuccess) return CudaFail(ctx, status, "epoch occupancy");
+  if (status != cudaSuccess) return Drained(ctx, CudaFail(ctx, status, "epoch occupancy"));
   const int screen_blocks = GridFor(m, kJvWarpsPerBlock, ctx->sm_count * std::max(1, occ));
   int32_t* counters = static_cast<int32_t*>(s.counters.ptr);  // [0] committed, [1] undecided
   int cur = 0;
@@ -426,7 +426,7 @@ extern "C" int cee_jv_eliminate(cee_ctx* ctx, const cee_graph_view* g, uint32_t 
                                                           static_cast<int32_t*>(s.flag.ptr));
     int32_t* total = nullptr;
     status = Scan(s, static_cast<const int32_t*>(s.flag.ptr), static_cast<int32_t*>(s.pos.ptr), m, st, &total);
-    if (status != cudaSuccess) return CudaFail(ctx, status, "epoch scan");
+    if (status != cudaSuccess) return Drained(ctx, CudaFail(ctx, status, "epoch scan"));
     epoch_fill<<<GridFor(m, 256, grid), 256, 0, st>>>(
         static_cast<const int32_t*>(s.order.ptr), static_cast<const int32_t*>(s.flag.ptr),
         static_cast<const int32_t*>(s.pos.ptr), m, static_cast<int32_t*>(s.cand.ptr),
@@ -485,14 +485,14 @@ extern "C" int cee_jv_eliminate(cee_ctx* ctx, const cee_graph_view* g, uint32_t 
                                                         static_cast<const uint8_t*>(s.active.ptr), len);
     cudaMemsetAsync(len + n, 0, sizeof(int32_t), st);
     status = Scan(s, len, static_cast<int32_t*>(s.ro[nxt].ptr), static_cast<int64_t>(n) + 1, st, &total);
-    if (status != cudaSuccess) return CudaFail(ctx, status, "epoch CSR scan");
+    if (status != cudaSuccess) return Drained(ctx, CudaFail(ctx, status, "epoch CSR scan"));
     csr_fill<<<GridFor(n, 256, grid), 256, 0, st>>>(
         static_cast<const int32_t*>(s.ro[cur].ptr), n, static_cast<const int32_t*>(s.ro[nxt].ptr),
         static_cast<const int32_t*>(s.ids[cur].ptr), static_cast<const int32_t*>(s.nbr[cur].ptr),
         static_cast<const int4*>(s.slot4[cur].ptr), static_cast<const uint8_t*>(s.active.ptr),
         static_cast<int32_t*>(s.ids[nxt].ptr), static_cast<int32_t*>(s.nbr[nxt].ptr), static_cast<int4*>(s.slot4[nxt].ptr));
     status = cudaGetLastError();
-    if (status != cudaSuccess) return CudaFail(ctx, status, "epoch CSR compaction");
+    if (status != cudaSuccess) return Drained(ctx, CudaFail(ctx, status, "epoch CSR compaction"));
     cur = nxt;
   }
   if (m > 0) {

@@ -12,7 +12,8 @@
  *     raised before a context exists).
  *   - A cee_ctx belongs to one host thread and one device, owns a CUDA stream and all device
  *     buffers it allocates; calls on one ctx are serialised on its stream. Caller buffers are
- *     borrowed for the duration of the call only.
+ *     borrowed for the duration of the call only (error returns included), except a serving
+ *     job's buffers, which stay borrowed until cee_serve_poll returns the job.
  *   - Host-buffer entry points copy inputs to the device, run, copy results back and
  *     synchronise before returning. Pinned host buffers are copied directly; pageable ones
  *     go through the CUDA driver's staging.
@@ -158,8 +159,9 @@ typedef struct {
 int cee_jv_screen(cee_ctx* ctx, const cee_graph_view* graph, int32_t* witness_out,
                   cee_jv_stats* stats);
 /* The three phases of cee_jv_screen, for callers that keep the snapshot resident and time
- * the kernel alone: prepare uploads, launch enqueues the screen on the context stream
- * (no synchronisation), fetch copies the witnesses back and checks the device error word. */
+ * the kernel alone: prepare uploads (and waits for the copies), launch enqueues the screen on
+ * the context stream (no synchronisation), fetch copies the witnesses back and checks the
+ * device error word. */
 int cee_jv_prepare(cee_ctx* ctx, const cee_graph_view* graph, cee_jv_stats* stats);
 int cee_jv_launch(cee_ctx* ctx);
 int cee_jv_fetch(cee_ctx* ctx, int32_t* witness_out);
@@ -338,7 +340,7 @@ int cee_kopt_improving_multi(cee_ctx* ctx, int32_t n, int32_t dist_type, const i
                              const cee_kopt_task* const* tasks, const int64_t* rows,
                              uint32_t* const* masks_out, int32_t* const* first_out,
                              int64_t* const* costs_out, cee_kopt_stats* stats);
-/* Phases of cee_kopt_costs_multi (prepare = upload, launch = enqueue, fetch = copy back). */
+/* Phases of cee_kopt_costs_multi (prepare = upload and wait for it, launch = enqueue, fetch = copy back). */
 int cee_kopt_prepare_multi(cee_ctx* ctx, int32_t n, int32_t dist_type, const int64_t* x,
                            const int64_t* y, int32_t segments, const uint32_t* ks,
                            const cee_kopt_task* const* tasks, const int64_t* rows,
@@ -465,8 +467,10 @@ int cee_serve_release_snapshot(cee_ctx* ctx, int32_t snapshot);
 int cee_serve_submit_jv(cee_ctx* ctx, int32_t snapshot, int32_t* witness_out, uint64_t tag,
                         int32_t* job);
 /* k-opt leaf costs of 1..3 segments (k = ks[s], rows[s] rows at tasks[s], output costs_out[s],
- * rows x template_count(k) cells) on the snapshot's coordinates. Task rows are copied at
- * submission. CEE_BUSY: no slot or arena room now. */
+ * rows x template_count(k) cells) on the snapshot's coordinates. The task rows go up by a copy
+ * queued at submission: pageable rows are staged before the call returns, pinned ones are read
+ * while the job runs, so keep them unchanged until cee_serve_poll returns the job.
+ * CEE_BUSY: no slot or arena room now. */
 int cee_serve_submit_kopt(cee_ctx* ctx, int32_t snapshot, int32_t segments, const uint32_t* ks,
                           const cee_kopt_task* const* tasks, const int64_t* rows,
                           int64_t* const* costs_out, uint64_t tag, int32_t* job);
