@@ -86,6 +86,8 @@ class Port:
         L.ceo_cd_finalize.restype = ctypes.c_int64
         L.ceo_cd_finalize.argtypes = [G, ctypes.c_int32, ctypes.c_int32, i32p, i32p, u8p, ctypes.c_int64,
                                       ctypes.c_uint32, i32p, i32p, u64p]
+        L.ceo_batch_expect.argtypes = [G, i64p, i64p, ctypes.c_int64, ctypes.c_int64] + [ctypes.c_uint32] * 3 + \
+            [ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32] + [vp] * 9
         self.L = L
 
     def graph(self, g) -> CeoGraph:
@@ -227,6 +229,68 @@ class Port:
         out[:, 2] = np.minimum(op[:count], np.uint64(np.iinfo(np.int64).max)).astype(np.int64)
         return out
 
+    def batch_expect(self, batch, opt, threads: int | None = None):
+        """The batched step of every instance of `batch` (node_begin, edge_begin, graph = the
+        disjoint union), as the reference's CPU code computes it, in the batched screen's output
+        layout: a dict of witness [m], target_ids [I, T], target_count [I], nbhd [I, T, NB],
+        flags [I, T, words] and, when opt.max_cd_candidates > 0, cand_c / cand_d / cand_product
+        [I, T, K] and cand_count [I, T]. Instance ranges run on `threads` host threads."""
+        import concurrent.futures
+        import os
+        g = batch.graph
+        node_begin = np.ascontiguousarray(batch.node_begin, np.int64)
+        edge_begin = np.ascontiguousarray(batch.edge_begin, np.int64)
+        I, T, NB, K = int(node_begin.shape[0] - 1), opt.targets, opt.max_neighborhood, opt.max_cd_candidates
+        W = opt.flag_words
+        out = {"witness": np.empty(g.edge_u.shape[0], np.int32), "target_ids": np.empty((I, T), np.int32),
+               "target_count": np.empty(I, np.int32), "nbhd": np.empty((I, T, NB), np.int32),
+               "flags": np.empty((I, T, W), np.uint32)}
+        if K > 0:
+            out.update(cand_c=np.empty((I, T, K), np.int32), cand_d=np.empty((I, T, K), np.int32),
+                       cand_product=np.empty((I, T, K), np.int64), cand_count=np.empty((I, T), np.int32))
+        view = self.graph(g)
+
+        def ptr(name):
+            return ctypes.c_void_p(out[name].ctypes.data) if name in out else None
+
+        def run(first, last):
+            rc = self.L.ceo_batch_expect(view, _p(node_begin, ctypes.c_int64), _p(edge_begin, ctypes.c_int64), first,
+                                         last, T, NB, opt.max_candidate_degree, opt.cd_mode, W, K, ptr("witness"),
+                                         ptr("target_ids"), ptr("target_count"), ptr("nbhd"), ptr("flags"),
+                                         ptr("cand_c"), ptr("cand_d"), ptr("cand_product"), ptr("cand_count"))
+            if rc != 0:
+                raise MemoryError("ceo_batch_expect ran out of memory")
+
+        threads = threads or os.cpu_count() or 1
+        step = max(1, min(64, -(-I // (4 * threads))))
+        with concurrent.futures.ThreadPoolExecutor(max_workers=threads) as pool:
+            list(pool.map(lambda f: run(f, min(I, f + step)), range(0, I, step)))
+        return out
+
+    def kopt_costs_parallel(self, g, k: int, tasks: np.ndarray, threads: int | None = None,
+                            mates: np.ndarray | None = None) -> np.ndarray:
+        """kopt_costs over row blocks on `threads` host threads (the same matrix)."""
+        import concurrent.futures
+        import os
+        if mates is None:
+            mates, _ = self.kopt_templates(k)
+        mates = np.ascontiguousarray(mates, np.uint8)
+        tasks = np.ascontiguousarray(tasks)
+        rows = tasks.shape[0]
+        costs = np.empty((rows, mates.shape[0]), np.int64)
+        threads = threads or os.cpu_count() or 1
+        step = max(1, -(-rows // (4 * threads)))
+
+        def run(first):
+            last = min(rows, first + step)
+            self.L.ceo_kopt_costs(g.dist_type, _p(g.x, ctypes.c_int64), _p(g.y, ctypes.c_int64), k,
+                                  tasks.ctypes.data + first * tasks.itemsize, last - first, _p(mates, ctypes.c_uint8),
+                                  mates.shape[0], _p(costs[first:last], ctypes.c_int64))
+
+        with concurrent.futures.ThreadPoolExecutor(max_workers=threads) as pool:
+            list(pool.map(run, range(0, rows, step)))
+        return costs
+
     def ht_reply_count(self, g, u: int, v: int, center: int) -> int:
         return int(self.L.ceo_ht_reply_count(self.graph(g), min(u, v), max(u, v), center))
 
@@ -274,6 +338,10 @@ class Reference:
                                    u8p, ctypes.c_int64]
         L.ref_cd_screen_cpu.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, i32p, i32p, u8p, ctypes.c_int64,
                                         ctypes.c_int, u8p]
+        L.ref_set_omp_threads.argtypes = [ctypes.c_int]
+        L.ref_graph_new_many.argtypes = [ctypes.c_int32, ctypes.c_int] + [vp] * 9
+        L.ref_batch_step.argtypes = [vp, ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                     ctypes.c_int, ctypes.c_int32, i64p, i64p]
         self.L = L
 
     def error(self) -> str:
@@ -300,6 +368,45 @@ class Reference:
         h = ctypes.c_uint64(0)
         count = self._check(self.L.ref_kopt_table(k, _p(mates, ctypes.c_uint8), ctypes.byref(h)))
         return mates[:count].copy(), int(h.value)
+
+    def set_omp_threads(self, threads: int) -> None:
+        """OpenMP threads of this host thread's next parallel regions (EvaluateKOptTemplateCosts(kCpu)
+        caps them at 8 itself)."""
+        self.L.ref_set_omp_threads(int(threads))
+
+    def batch_graphs(self, batch) -> "RefBatch":
+        """GraphSnapshots of every instance of a disjoint union (node_begin, edge_begin, graph)."""
+        return RefBatch(self, batch)
+
+
+class RefBatch:
+    """The reference's GraphSnapshots of every instance of a batch, built once."""
+
+    def __init__(self, ref: Reference, batch):
+        g = batch.graph
+        arrays = [np.ascontiguousarray(batch.node_begin, np.int64), np.ascontiguousarray(batch.edge_begin, np.int64),
+                  g.x, g.y, g.edge_u, g.edge_v, g.edge_w, g.active]
+        self.ref = ref
+        self.count = int(batch.node_begin.shape[0] - 1)
+        self.handles = (vp * self.count)()
+        ref._check(ref.L.ref_graph_new_many(self.count, g.dist_type, *(a.ctypes.data for a in arrays), self.handles))
+
+    def step(self, instances, threads: int, targets: int = 64, nb: int = 25, max_deg: int = 50, mode: int = 0):
+        """One ref_batch_step over the given instance indices: FindJvCandidatesCpu, then
+        SelectHtTargetEdgeIds and BuildCdScreenTasks + ScreenCdTasksCpu for the first `targets`
+        targets, per instance, on `threads` host threads. Returns (edges, c,d tasks) screened."""
+        chosen = (vp * len(instances))(*[self.handles[i] for i in instances])
+        edges, tasks = ctypes.c_int64(0), ctypes.c_int64(0)
+        self.ref._check(self.ref.L.ref_batch_step(chosen, len(instances), targets, nb, max_deg, mode, threads,
+                                                  ctypes.byref(edges), ctypes.byref(tasks)))
+        return int(edges.value), int(tasks.value)
+
+    def __del__(self):
+        if getattr(self, "handles", None) is not None:
+            for h in self.handles:
+                if h:
+                    self.ref.L.ref_graph_free(h)
+            self.handles = None
 
 
 class RefGraph:

@@ -695,8 +695,9 @@ int64_t ceo_cd_finalize(const ceo_graph* g, int32_t u, int32_t v, const int32_t*
 
 /* ---- SelectHtTargetEdgeIds: src/cpu/ht_scan.cpp:316-345 ---- */
 
-static const ceo_graph* g_target_graph;
-static int32_t g_target_order;
+/* Per thread, so that several host threads may check instances at once. */
+static _Thread_local const ceo_graph* g_target_graph;
+static _Thread_local int32_t g_target_order;
 
 static int cmp_target(const void* lhs, const void* rhs) {
   const int32_t a = *(const int32_t*)lhs, b = *(const int32_t*)rhs;
@@ -718,4 +719,143 @@ int64_t ceo_ht_targets(const ceo_graph* g, int32_t order, int32_t* out) {
   g_target_order = order;
   qsort(out, (size_t)count, sizeof(int32_t), cmp_target);
   return count;
+}
+
+/* ---- The batched step of one instance range, in the batched screen's output layout ----
+ *
+ * For instances [first, last) of a disjoint union (instance i owns nodes
+ * [node_begin[i], node_begin[i+1]) and edges [edge_begin[i], edge_begin[i+1])), writes what the
+ * reference's CPU code computes for the step, with global node and edge ids:
+ *   witness[e]                  FindJvCandidatesCpu (src/cpu/jv_elimination.cpp:209-224)
+ *   target_ids[i][t], count[i]  SelectHtTargetEdgeIds (src/cpu/ht_scan.cpp:316-345), first `targets`
+ *   nbhd[i][t][NB]              the ranked neighbourhood of BuildCdScreenTasks
+ *                               (src/cpu/hamilton_tutte.cpp:168-216), -1 padded
+ *   flags[i][t][words]          ScreenCdTasksCpu (:218-228) of its pairs i < j, bit p = task p
+ *   cand_*[i][t][max_cd], cand_count[i][t]  FinalizeCdCandidates (:283-327), when max_cd > 0
+ * Returns 0, or -1 when memory runs out. */
+int ceo_batch_expect(const ceo_graph* g, const int64_t* node_begin, const int64_t* edge_begin, int64_t first,
+                     int64_t last, uint32_t targets, uint32_t max_neighborhood, uint32_t max_candidate_degree,
+                     int32_t mode, uint32_t flag_words, uint32_t max_cd, int32_t* witness, int32_t* target_ids,
+                     int32_t* target_count, int32_t* nbhd, uint32_t* flags, int32_t* cand_c, int32_t* cand_d,
+                     int64_t* cand_product, int32_t* cand_count) {
+  int64_t max_nodes = 1, max_edges = 1;
+  for (int64_t i = first; i < last; ++i) {
+    if (node_begin[i + 1] - node_begin[i] > max_nodes) max_nodes = node_begin[i + 1] - node_begin[i];
+    if (edge_begin[i + 1] - edge_begin[i] > max_edges) max_edges = edge_begin[i + 1] - edge_begin[i];
+  }
+  const int64_t pair_cap = (int64_t)max_neighborhood * (max_neighborhood > 0 ? max_neighborhood - 1 : 0) / 2 + 1;
+  int32_t* order = malloc(sizeof(int32_t) * (size_t)max_edges);
+  ranked_node* ranked = malloc(sizeof(ranked_node) * (size_t)max_nodes);
+  int32_t* tc = malloc(sizeof(int32_t) * (size_t)pair_cap);
+  int32_t* td = malloc(sizeof(int32_t) * (size_t)pair_cap);
+  uint8_t* ta = malloc((size_t)pair_cap);
+  uint8_t* tf = malloc((size_t)pair_cap);
+  int32_t* oc = malloc(sizeof(int32_t) * (size_t)pair_cap);
+  int32_t* od = malloc(sizeof(int32_t) * (size_t)pair_cap);
+  uint64_t* op = malloc(sizeof(uint64_t) * (size_t)pair_cap);
+  int rc = 0;
+  if (!order || !ranked || !tc || !td || !ta || !tf || !oc || !od || !op) {
+    rc = -1;
+    goto done;
+  }
+  for (int64_t i = first; i < last; ++i) {
+    const int64_t n0 = node_begin[i], n1 = node_begin[i + 1], e0 = edge_begin[i], e1 = edge_begin[i + 1];
+    ceo_jv_screen_range(g, e0, e1, witness, NULL);
+    /* targets: the instance's eligible edges in SelectHtTargetEdgeIds order */
+    int64_t count = 0;
+    for (int64_t e = e0; e < e1; ++e) {
+      if (g->active[e] && degree(g, g->edge_u[e]) > 2 && degree(g, g->edge_v[e]) > 2) order[count++] = (int32_t)e;
+    }
+    g_target_graph = g;
+    g_target_order = 1;
+    qsort(order, (size_t)count, sizeof(int32_t), cmp_target);
+    if (count > (int64_t)targets) count = targets;
+    target_count[i] = (int32_t)count;
+    for (uint32_t t = 0; t < targets; ++t) {
+      const size_t slot = (size_t)i * targets + t;
+      int32_t* hood = nbhd + slot * max_neighborhood;
+      uint32_t* words = flags + slot * flag_words;
+      for (uint32_t k = 0; k < max_neighborhood; ++k) hood[k] = -1;
+      for (uint32_t k = 0; k < flag_words; ++k) words[k] = 0;
+      if (max_cd > 0) {
+        cand_count[slot] = 0;
+        for (uint32_t k = 0; k < max_cd; ++k) {
+          cand_c[slot * max_cd + k] = -1;
+          cand_d[slot * max_cd + k] = -1;
+          cand_product[slot * max_cd + k] = -1;
+        }
+      }
+      if ((int64_t)t >= count) {
+        target_ids[slot] = -1;
+        continue;
+      }
+      const int32_t e = order[t];
+      target_ids[slot] = e;
+      const int32_t u = g->edge_u[e], v = g->edge_v[e];
+      /* the ranked neighbourhood, as ceo_cd_tasks ranks it, over this instance's nodes */
+      /* the first max_neighborhood by (score, node): a sorted list with insertion, which keeps
+       * exactly the prefix that sorting every eligible node would give */
+      int64_t size = 0;
+      for (int64_t node = n0; node < n1; ++node) {
+        if (node == u || node == v ||
+            (max_candidate_degree != 0 && (uint32_t)degree(g, (int32_t)node) > max_candidate_degree)) {
+          continue;
+        }
+        const __int128 dx = (__int128)2 * g->x[node] - g->x[u] - g->x[v];
+        const __int128 dy = (__int128)2 * g->y[node] - g->y[u] - g->y[v];
+        const ranked_node entry = {dx * dx + dy * dy, (int32_t)node};
+        int64_t pos = size;
+        if (size == (int64_t)max_neighborhood) {
+          if (max_neighborhood == 0 || cmp_ranked(&entry, &ranked[size - 1]) >= 0) continue;
+          pos = size - 1;
+        } else {
+          ++size;
+        }
+        while (pos > 0 && cmp_ranked(&entry, &ranked[pos - 1]) < 0) {
+          ranked[pos] = ranked[pos - 1];
+          --pos;
+        }
+        ranked[pos] = entry;
+      }
+      int64_t tasks = 0;
+      for (int64_t a = 0; a < size; ++a) {
+        hood[a] = ranked[a].node;
+        for (int64_t b = a + 1; b < size; ++b) {
+          const int32_t p = ranked[a].node, q = ranked[b].node;
+          tc[tasks] = p < q ? p : q;
+          td[tasks] = p < q ? q : p;
+          ta[tasks] = (uint8_t)has_active_edge(g, tc[tasks], td[tasks]);
+          ++tasks;
+        }
+      }
+      ceo_cd_screen(g, u, v, tc, td, ta, tasks, mode, tf);
+      for (int64_t p = 0; p < tasks; ++p) {
+        if (tf[p]) words[p >> 5] |= 1u << (p & 31);
+      }
+      if (max_cd > 0) {
+        const int64_t kept = ceo_cd_finalize(g, u, v, tc, td, tf, tasks, max_cd, oc, od, op);
+        if (kept < 0) {
+          rc = -1;
+          goto done;
+        }
+        cand_count[slot] = (int32_t)kept;
+        for (int64_t k = 0; k < kept; ++k) {
+          cand_c[slot * max_cd + k] = oc[k];
+          cand_d[slot * max_cd + k] = od[k];
+          cand_product[slot * max_cd + k] = op[k] > (uint64_t)INT64_MAX ? INT64_MAX : (int64_t)op[k];
+        }
+      }
+    }
+  }
+done:
+  free(order);
+  free(ranked);
+  free(tc);
+  free(td);
+  free(ta);
+  free(tf);
+  free(oc);
+  free(od);
+  free(op);
+  return rc;
 }

@@ -102,6 +102,14 @@ int64_t ceo_cd_finalize(const ceo_graph* g, int32_t u, int32_t v, const int32_t*
                         uint64_t* out_product);
 /* HT scan target order (weight descending when order == 1, else canonical). */
 int64_t ceo_ht_targets(const ceo_graph* g, int32_t order, int32_t* out);
+/* The batched step (JV witnesses, HT targets, c,d neighbourhoods and flag words, optional
+ * finalised candidates) of instances [first, last) of a disjoint union, in the batched
+ * screen's output layout with global ids. */
+int ceo_batch_expect(const ceo_graph* g, const int64_t* node_begin, const int64_t* edge_begin, int64_t first,
+                     int64_t last, uint32_t targets, uint32_t max_neighborhood, uint32_t max_candidate_degree,
+                     int32_t mode, uint32_t flag_words, uint32_t max_cd, int32_t* witness, int32_t* target_ids,
+                     int32_t* target_count, int32_t* nbhd, uint32_t* flags, int32_t* cand_c, int32_t* cand_d,
+                     int64_t* cand_product, int32_t* cand_count);
 
 #ifdef __cplusplus
 }

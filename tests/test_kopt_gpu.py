@@ -191,22 +191,25 @@ def expected_improving(costs, deleted):
 
 
 @pytest.mark.parametrize("with_costs", [False, True], ids=["masks-only", "with-costs"])
-def test_improving_sets(kc, with_costs):
+def test_improving_sets(kc, port, with_costs):
     """Fused leaf consume: improving-template masks and first improving template per row equal the
-    ones derived from the full cost matrix (walk rows and rows with shifted deleted costs)."""
+    ones the reference's consumer would try -- templates whose oracle cost is strictly below the
+    row's deleted cost (src/cpu/kopt_search.cpp:694-715) -- on walk rows whose deleted costs are
+    shifted both ways (kept >= 0, as ValidateKOptCostTask requires, :784-807)."""
     g, rows = synth.kopt_instance(rows=6000, n=3000)
     lists = []
     rng = np.random.default_rng(3)
     for k in (3, 4, 5):
         t = rows[k].copy()
-        t["deleted_cost"] += rng.integers(-2000, 2000, t.shape[0])  # a spread of improving and not
+        shifted = t["deleted_cost"] + rng.integers(-2000, 2000, t.shape[0])  # a spread of improving and not
+        t["deleted_cost"] = np.maximum(shifted, 0)
         lists.append(t)
-    full, _ = kc.kopt_costs_multi(g, [3, 4, 5], lists)
+    oracle_costs = [port.kopt_costs(g, k, t) for k, t in zip((3, 4, 5), lists)]
     masks, firsts, costs, stats = kc.kopt_improving_multi(g, [3, 4, 5], lists, with_costs=with_costs)
     for seg in range(3):
-        want_m, want_f = expected_improving(full[seg], lists[seg]["deleted_cost"])
+        want_m, want_f = expected_improving(oracle_costs[seg], lists[seg]["deleted_cost"])
         np.testing.assert_array_equal(masks[seg], want_m)
         np.testing.assert_array_equal(firsts[seg], want_f)
         if with_costs:
-            np.testing.assert_array_equal(costs[seg], full[seg])
+            np.testing.assert_array_equal(costs[seg], oracle_costs[seg])
     assert any((f >= 0).any() for f in firsts) and any((f < 0).any() for f in firsts)
