@@ -22,7 +22,20 @@ CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 INCLUDE = ROOT / "include"
 ORACLE = ROOT / "oracle"
-REFERENCE = pathlib.Path(os.environ.get("CEE_REFERENCE_DIR", "/root/reference"))
+
+
+def reference_dir() -> pathlib.Path | None:
+    """The reference source tree: $CEE_REFERENCE_DIR, else the oracle recipe's default location
+    (`make -C oracle ref-dir`); None when neither holds the reference sources."""
+    env = os.environ.get("CEE_REFERENCE_DIR")
+    if env:
+        path = pathlib.Path(env)
+    else:
+        proc = subprocess.run(["make", "-s", "-C", str(ORACLE), "ref-dir"], capture_output=True, text=True)
+        if proc.returncode != 0 or not proc.stdout.strip():
+            return None
+        path = pathlib.Path(proc.stdout.strip())
+    return path if (path / "src" / "cpu" / "jv_elimination.cpp").exists() else None
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
@@ -89,13 +102,19 @@ def build_synth(force: bool = False) -> pathlib.Path:
 
 def build_oracle(force: bool = False) -> None:
     """The plain-C oracle; plus, when the reference tree is present, the reference library
-    compiled from its own sources and the reference with this project's shim dropped in."""
-    make = ["make", "-C", str(ORACLE), f"REF={REFERENCE}"]
+    compiled from its own sources, the reference with this project's shim dropped in, and the
+    reference's own unit tests built against each of the two."""
+    reference = reference_dir()
+    make = ["make", "-C", str(ORACLE)] + ([f"REF={reference}"] if reference is not None else [])
     if force:
         _run(make + ["clean"])
     _run(make + ["port"])
-    if (REFERENCE / "src" / "cpu" / "jv_elimination.cpp").exists():
+    if reference is not None:
         _run(make + ["-j8", "ref", "dropin"])
+        _run(make + ["-j8", "unit"])
+    else:
+        print("reference sources not found (set CEE_REFERENCE_DIR): the reference library is not rebuilt",
+              file=sys.stderr)
 
 
 def build_all(force: bool = False) -> None:

@@ -20,6 +20,8 @@
 #include <string>
 #include <vector>
 
+#include <omp.h>
+
 namespace {
 
 thread_local std::string g_error;
@@ -286,6 +288,36 @@ int ref_kopt_costs(void* handle, uint32_t k, const void* tasks, int64_t rows, in
 }
 
 void ref_kopt_clear_cuda_cache() { cudaee::detail::ClearKOptCostCudaCache(); }
+
+// The OpenMP thread count of the calling thread's next parallel regions (omp_set_num_threads):
+// EvaluateKOptTemplateCosts(kCpu) uses min(kKOptCpuMaxThreads = 8, this, the processor count)
+// threads (src/cpu/kopt_search.cpp:37-40, 1069-1089).
+void ref_set_omp_threads(int threads) { omp_set_num_threads(threads > 0 ? threads : 1); }
+
+// Snapshots of every instance of a disjoint union (instance i owns nodes [node_begin[i],
+// node_begin[i+1]) and edges [edge_begin[i], edge_begin[i+1]), global ids), each built through
+// ref_graph_new with local ids, for callers that build every snapshot before a timed region.
+int ref_graph_new_many(int32_t count, int dist_type, const int64_t* node_begin, const int64_t* edge_begin,
+                       const int64_t* x, const int64_t* y, const int32_t* eu, const int32_t* ev,
+                       const int64_t* w, const uint8_t* active, void** out) {
+  std::vector<int32_t> local_u, local_v;
+  for (int32_t i = 0; i < count; ++i) {
+    const int64_t n0 = node_begin[i], e0 = edge_begin[i], m = edge_begin[i + 1] - e0;
+    local_u.resize(static_cast<std::size_t>(m));
+    local_v.resize(static_cast<std::size_t>(m));
+    for (int64_t e = 0; e < m; ++e) {
+      local_u[e] = static_cast<int32_t>(eu[e0 + e] - n0);
+      local_v[e] = static_cast<int32_t>(ev[e0 + e] - n0);
+    }
+    const int rc = ref_graph_new(static_cast<int32_t>(node_begin[i + 1] - n0), dist_type, x + n0, y + n0, m,
+                                 local_u.data(), local_v.data(), w + e0, active + e0, &out[i]);
+    if (rc != 0) {
+      for (int32_t j = 0; j < i; ++j) delete AsGraph(out[j]);
+      return rc;
+    }
+  }
+  return 0;
+}
 
 // EvaluateHtCdCandidates (src/cpu/hamilton_tutte.cpp:662-704). backend: 1 = kCpu, 2 = kCuda.
 // out[3*i..] = (c, d, reply_product clipped to int64).

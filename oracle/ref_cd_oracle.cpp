@@ -6,7 +6,11 @@
 // symbol of that file is still provided exactly once.
 #include "src/cpu/hamilton_tutte.cpp"
 
+#include "cuda_edge_elimination/elimination.hpp"
+
+#include <atomic>
 #include <cstring>
+#include <thread>
 
 extern "C" {
 
@@ -46,6 +50,55 @@ int ref_cd_screen_cpu(void* handle, int32_t u, int32_t v, const int32_t* c, cons
   } catch (...) {
     return -1;
   }
+}
+
+// The reference's CPU code for one step of the batching workload, over prebuilt snapshots (the
+// timed CPU baseline; nothing is built or marshalled inside it): per snapshot FindJvCandidatesCpu
+// (src/cpu/jv_elimination.cpp:209-224), SelectHtTargetEdgeIds in weight order
+// (src/cpu/ht_scan.cpp:316-345) and, for its first `targets` targets, BuildCdScreenTasks +
+// ScreenCdTasksCpu (:168-228). Snapshots are taken by `threads` host threads from a shared
+// counter. Writes the active edges screened and the c,d tasks screened; returns 0, or -1 when
+// the reference threw.
+int ref_batch_step(void* const* handles, int32_t count, uint32_t targets, uint32_t max_neighborhood,
+                   uint32_t max_candidate_degree, int mode, int32_t threads, int64_t* edges_out,
+                   int64_t* cd_tasks_out) {
+  std::atomic<int32_t> next{0};
+  std::atomic<int64_t> edges{0}, tasks_screened{0};
+  std::atomic<bool> failed{false};
+  cudaee::HtShallowOptions options;
+  options.max_neighborhood = max_neighborhood;
+  options.max_candidate_degree = max_candidate_degree;
+  const auto work = [&] {
+    try {
+      int64_t local_edges = 0, local_tasks = 0;
+      for (int32_t i = next++; i < count && !failed; i = next++) {
+        const auto* graph = static_cast<const cudaee::GraphSnapshot*>(handles[i]);
+        const auto candidates = cudaee::FindJvCandidatesCpu(*graph);
+        (void)candidates;
+        for (const auto& edge : graph->edges) local_edges += edge.active ? 1 : 0;
+        const auto ids = cudaee::SelectHtTargetEdgeIds(*graph, cudaee::HtTargetOrder::kWeightDescending);
+        const std::size_t used = std::min<std::size_t>(ids.size(), targets);
+        for (std::size_t t = 0; t < used; ++t) {
+          const cudaee::Edge& e = graph->edges[static_cast<std::size_t>(ids[t])];
+          const cudaee::NodeEdge target{e.u, e.v};
+          const auto tasks = cudaee::BuildCdScreenTasks(*graph, target, options);
+          const auto flags = cudaee::ScreenCdTasksCpu(*graph, target, tasks, static_cast<cudaee::HtCdMode>(mode));
+          local_tasks += static_cast<int64_t>(flags.size());
+        }
+      }
+      edges += local_edges;
+      tasks_screened += local_tasks;
+    } catch (...) {
+      failed = true;
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int32_t t = 1; t < threads; ++t) pool.emplace_back(work);
+  work();
+  for (auto& th : pool) th.join();
+  *edges_out = edges;
+  *cd_tasks_out = tasks_screened;
+  return failed ? -1 : 0;
 }
 
 } // extern "C"

@@ -26,7 +26,20 @@ sys.path.insert(0, str(ROOT))
 import oracle  # noqa: E402
 from cudaedgeelimination_b200 import GraphSnapshot, synth  # noqa: E402
 
-REFERENCE = pathlib.Path(os.environ.get("CEE_REFERENCE_DIR", "/root/reference"))
+def _reference_dir() -> pathlib.Path:
+    """$CEE_REFERENCE_DIR, else the directory the oracle recipe compiles the reference from."""
+    env = os.environ.get("CEE_REFERENCE_DIR")
+    if env:
+        return pathlib.Path(env)
+    import subprocess
+    out = subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "ref-dir"], capture_output=True, text=True)
+    path = pathlib.Path(out.stdout.strip()) if out.returncode == 0 and out.stdout.strip() else None
+    if path is None or not (path / "tests" / "data").exists():
+        raise SystemExit("make_golden.py reads the reference's test data: set CEE_REFERENCE_DIR to its source tree")
+    return path
+
+
+REFERENCE = _reference_dir()
 
 
 def snapshot_arrays(g) -> dict:
