@@ -62,6 +62,7 @@ def parse():
     p.add_argument("--part", default="all", choices=["all", "batch", "kopt", "serve", "epochs"],
                    help="profiling aid: run only the batched screen, the k-opt part or the serving loop")
     p.add_argument("--cpu-budget-s", type=float, default=12.0)
+    p.add_argument("--cpu-leg", default=None, help=argparse.SUPPRESS)
     return p.parse_args()
 
 
@@ -159,54 +160,82 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- CPU reference -----------
 
-def reference_step_rate(batch, budget_s: float, threads: int, targets: int = 64, nb: int = 25, max_deg: int = 50):
-    """The reference's CPU code for one instance of the step -- FindJvCandidatesCpu, then
-    SelectHtTargetEdgeIds and BuildCdScreenTasks + ScreenCdTasksCpu for the first `targets`
-    targets -- over instances in order until the budget is spent, `threads` instances at a time.
-    Returns (edges screened/s, kind, sample description)."""
-    import oracle
-    kind = "reference" if oracle.reference_available() else "port"
-    if kind == "reference":
-        ref = oracle.Reference()
+def host_cpu():
+    """The host's CPU model, sockets and cores (lscpu), and the threads this process may use."""
+    info = {"threads_available": os.cpu_count() or 1}
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for line in out.splitlines():
+            key, _, value = line.partition(":")
+            key, value = key.strip(), value.strip()
+            if key == "Model name":
+                info["model"] = value
+            elif key == "Socket(s)":
+                info["sockets"] = int(value)
+            elif key == "Core(s) per socket":
+                info["cores_per_socket"] = int(value)
+            elif key == "Thread(s) per core":
+                info["threads_per_core"] = int(value)
+    except (OSError, ValueError, subprocess.SubprocessError):
+        pass
+    return info
 
-        def screen(g):
-            rg = ref.graph(g)
-            rg.jv_cpu()
-            for t in rg.ht_targets(1)[:targets]:
-                u, v = int(g.edge_u[t]), int(g.edge_v[t])
-                c, d, a = rg.cd_tasks(u, v, nb, max_deg)
-                rg.cd_screen(u, v, c, d, a, 0)
-    else:
-        port = oracle.Port()
 
-        def screen(g):
-            port.jv_screen(g)
-            for t in port.ht_targets(g)[:targets]:
-                u, v = int(g.edge_u[t]), int(g.edge_v[t])
-                c, d, a = port.cd_tasks(g, u, v, nb, max_deg)
-                port.cd_screen(g, u, v, c, d, a, 0)
-    edges = 0
-    done = 0
-    lock = threading.Lock()
-    stop = time.perf_counter() + budget_s
-    start = time.perf_counter()
+class ReferenceStep:
+    """The reference's own CPU code for the batched step (oracle/_ref, compiled from the reference
+    sources): per instance FindJvCandidatesCpu, then SelectHtTargetEdgeIds and BuildCdScreenTasks +
+    ScreenCdTasksCpu for the first 64 targets (neighbourhood 25, degree cap 50,
+    active-incompatible), instances on `threads` host threads inside one C++ call. Every
+    instance's GraphSnapshot is built before any timing. Without the compiled reference it falls
+    back to the C restatement (oracle/_build) over the same instances."""
 
-    def work(i):
-        nonlocal edges, done
-        if time.perf_counter() > stop:
-            return
-        g = batch.instance(i)
-        screen(g)
-        with lock:
-            edges += int(g.active.sum())
-            done += 1
+    def __init__(self, batch, threads: int):
+        import oracle
+        self.batch, self.threads = batch, threads
+        self.kind = "reference" if oracle.reference_available() else "port"
+        if self.kind == "reference":
+            self.graphs = oracle.Reference().batch_graphs(batch)
+        else:
+            self.port = oracle.Port()
 
-    with concurrent.futures.ThreadPoolExecutor(max_workers=threads) as pool:
-        list(pool.map(work, range(batch.count)))
-    elapsed = time.perf_counter() - start
-    sample = (f"{done} of {batch.count} instances ({edges} edges, JV screen + {targets} c,d root screens each), "
-              f"{threads} threads, {elapsed:.1f} s")
-    return edges / elapsed, kind, sample
+    def run(self, instances):
+        """Screens the given instances; returns (active edges screened, seconds)."""
+        instances = list(instances)
+        t0 = time.perf_counter()
+        if self.kind == "reference":
+            edges, _ = self.graphs.step(instances, self.threads)
+        else:
+            from cudaedgeelimination_b200.api import BatchOptions
+            sub = _SubBatch(self.batch, instances)
+            self.port.batch_expect(sub, BatchOptions(), self.threads)
+            edges = int(sub.graph.active.sum())
+        return edges, time.perf_counter() - t0
+
+
+class _SubBatch:
+    """A batch made of some instances of another (the C restatement's batch checker takes a union)."""
+
+    def __init__(self, batch, instances):
+        from cudaedgeelimination_b200 import GraphSnapshot
+        parts = [batch.instance(i) for i in instances]
+        nb = np.cumsum([0] + [g.n for g in parts]).astype(np.int64)
+        eb = np.cumsum([0] + [g.m for g in parts]).astype(np.int64)
+        self.node_begin, self.edge_begin = nb, eb
+        self.graph = GraphSnapshot(int(nb[-1]), parts[0].dist_type, np.concatenate([g.x for g in parts]),
+                                   np.concatenate([g.y for g in parts]),
+                                   np.concatenate([g.edge_u + nb[i] for i, g in enumerate(parts)]),
+                                   np.concatenate([g.edge_v + nb[i] for i, g in enumerate(parts)]),
+                                   np.concatenate([g.edge_w for g in parts]), np.concatenate([g.active for g in parts]))
+
+
+def workload_config(batch, world: int):
+    """The bench line's `config`, the same in both arms."""
+    g = batch.graph
+    return {"workload": f"batching mix: {batch.count} instances, n log-uniform [100,5000], uniform/clustered 50/50, "
+                        "10-NN, EUC_2D; per step the JV screen of every active edge plus the HT c,d root screen of "
+                        "64 targets per instance (neighbourhood 25, degree cap 50, active-incompatible)",
+            "instances": batch.count, "nodes": int(g.n), "edges": int(g.m),
+            "l2": "inputs (~1.1 GB) larger than L2, no flush", "parallelism": f"replicas x{world}"}
 
 
 # ---------------------------------------------------------------- our arm -----------------
@@ -226,6 +255,25 @@ def spot_check(batch, res, opt):
         u, v = int(inst.edge_u[local]), int(inst.edge_v[local])
         c, d, a = port.cd_tasks(inst, u, v, opt.max_neighborhood, opt.max_candidate_degree)
         assert (res.pair_flags(i, 0) == port.cd_screen(inst, u, v, c, d, a, opt.cd_mode)).all()
+
+
+def check_batch_full(batch, res, cand, fin_opt):
+    """Every instance of the step against the C oracle on host threads: JV witnesses, HT targets,
+    c,d neighbourhoods and flag words, and the finalised candidates of the finalised step."""
+    import oracle
+    t0 = time.perf_counter()
+    want = oracle.Port().batch_expect(batch, fin_opt)
+    for name in ("witness", "target_ids", "target_count", "nbhd", "flags"):
+        assert np.array_equal(getattr(res, name), want[name]), f"batched step differs from the oracle in {name}"
+    c, d, product, count = cand
+    assert np.array_equal(count, want["cand_count"]), "finalised candidate counts differ from the oracle"
+    keep = np.arange(c.shape[2])[None, None, :] < count[:, :, None]
+    for got, name in ((c, "cand_c"), (d, "cand_d"), (product, "cand_product")):
+        assert np.array_equal(np.where(keep, got, -1), np.where(keep, want[name], -1)), f"{name} differs"
+    return {"instances": batch.count, "edges": int(res.witness.shape[0]), "targets": int(count.size),
+            "checked": "every JV witness, HT target, c,d neighbourhood, flag word and finalised candidate; "
+                       "graph launch, plain launches and the end-to-end call give the same bytes",
+            "oracle": "oracle/cee_oracle.c on host threads", "seconds": time.perf_counter() - t0, "ok": True}
 
 
 def pinned_copy(arr: np.ndarray):
@@ -302,7 +350,8 @@ def run_ours(args, rank: int, world: int, device: int):
     f1.record(stream)
     f1.synchronize()
     fin_ms = max_over_ranks(f0.elapsed_time(f1), world) / args.steps
-    fin_counts = ctx.batch_fetch_candidates()[3]
+    fin_cand = ctx.batch_fetch_candidates()
+    fin_counts = fin_cand[3]
     ctx.batch_prepare(batch, opt)
     ctx.set_batch_tuning(tuning.jv_tile, tuning.blocks_per_sm, tuning.chunks)
 
@@ -355,14 +404,10 @@ def run_ours(args, rank: int, world: int, device: int):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded; TSPLIB/ElimTSP inputs not shipped)",
-        "config": {"workload": f"batching mix: {batch.count} instances, n log-uniform [100,5000], uniform/clustered "
-                               "50/50, 10-NN, EUC_2D; per step the JV screen of every active edge plus the HT c,d "
-                               "root screen of 64 targets per instance (neighbourhood 25, degree cap 50), one "
-                               "persistent graph-captured launch",
-                   "instances": batch.count, "nodes": n, "edges": m, "targets": targets, "cd_tasks": pairs,
-                   "tuning": {"jv_tile": tuning.jv_tile, "blocks_per_sm": tuning.blocks_per_sm,
-                              "chunks": tuning.chunks},
-                   "l2": "inputs (~1.1 GB) larger than L2, no flush", "parallelism": f"replicas x{world}"},
+        "config": workload_config(batch, world),
+        "launch": "one persistent, CUDA-graph-captured launch per step",
+        "tuning": {"jv_tile": tuning.jv_tile, "blocks_per_sm": tuning.blocks_per_sm, "chunks": tuning.chunks},
+        "targets": targets, "cd_tasks": pairs,
         "cd_tasks_per_s": pairs * world / (ms_step / 1e3),
         "with_cd_finalisation": {"ms_per_step": fin_ms, "value": edges_step * world / (fin_ms / 1e3), "unit": UNIT,
                                  "candidates": int(fin_counts.sum()),
@@ -398,22 +443,78 @@ def run_ours(args, rank: int, world: int, device: int):
         result["roofline"]["jv_distance_evals_per_edge"] = per_edge
         result["roofline"]["distance_evals_per_s"] = (per_edge * edges_step + 351 * targets) / (ms_step / 1e3)
 
+    parity = {}
     if not args.no_kopt and args.part == "all":
-        result["kopt"] = run_kopt(args, ctx, stream, device, world)
+        result["kopt"] = run_kopt(args, ctx, stream, device, world, parity if rank == 0 else None)
     if not args.no_serve and args.part == "all":
-        result["serve"] = run_serve(args, device, world)
+        result["serve"] = run_serve(args, device, world, parity if rank == 0 else None)
     if not args.no_epochs and args.part == "all" and rank == 0:
         result["jv_fixed_point"] = run_fixed_point(args, device)
 
     if rank == 0:
-        rate, kind, sample = reference_step_rate(batch, args.cpu_budget_s, os.cpu_count() or 1)
-        result["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": kind,
-                                  "sample": sample}
+        # the reference's CPU code on the same step: every instance, one pass, all host threads
+        threads = os.cpu_count() or 1
+        step = ReferenceStep(batch, threads)
+        cpu_edges, cpu_s = step.run(range(batch.count))
+        result["cpu_baseline"] = {
+            "value": cpu_edges / cpu_s, "unit": UNIT, "cores": threads, "kind": step.kind,
+            "sample": f"all {batch.count} instances ({cpu_edges} edges, JV screen + 64 c,d root screens each) in "
+                      f"{cpu_s:.1f} s, one C++ call on {threads} host threads, snapshots built before timing"}
+        result["host_cpu"] = host_cpu()
+        # full-size parity: every instance of the timed step against the C oracle
+        parity["batch"] = check_batch_full(batch, res, fin_cand, fin_opt)
+        result["parity"] = parity
     ctx.close()
     return result
 
 
-def run_kopt(args, ctx, stream, device, world):
+OMP_ENV = {"OMP_DYNAMIC": "FALSE", "OMP_PROC_BIND": "spread", "OMP_PLACES": "cores"}
+
+
+def cpu_leg(name: str, timeout_s: float = 600.0):
+    """Runs one CPU-baseline leg (`bench.py --cpu-leg name`) in a child process with the reference
+    benchmarks' OpenMP settings, which bind threads and so stay out of this (GPU-driving) process."""
+    env = dict(os.environ, **OMP_ENV)
+    proc = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--cpu-leg", name], capture_output=True, text=True,
+                          env=env, timeout=timeout_s)
+    if proc.returncode != 0:
+        raise RuntimeError(f"CPU baseline leg {name} failed:\n{proc.stdout}\n{proc.stderr}")
+    return json.loads(proc.stdout.strip().splitlines()[-1])
+
+
+def cpu_leg_kopt():
+    """EvaluateKOptTemplateCosts(kCpu) -- the reference's OpenMP cost-matrix path
+    (src/cpu/kopt_search.cpp:1069-1089, at most kKOptCpuMaxThreads = 8 threads) -- on the 200,000-row
+    matrix, k = 3, 4, 5 one call each, at 1 and at 8 threads: the median of 3 repetitions after one
+    warm-up, as benchmarks/kopt_cost_benchmark.cpp:53-64 times it."""
+    import oracle
+    from cudaedgeelimination_b200 import synth
+    ref = oracle.Reference()
+    g, tasks = synth.kopt_instance()
+    rg = ref.graph(g)
+    cells = sum(t.shape[0] * {3: 4, 4: 25, 5: 208}[k] for k, t in tasks.items())
+    out = {}
+    for threads in (1, 8):
+        ref.set_omp_threads(threads)
+        used = 0
+        for k, t in tasks.items():
+            used = max(used, int(rg.kopt_costs(k, t, 1)[1][0]))
+        samples = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            for k, t in tasks.items():
+                rg.kopt_costs(k, t, 1)
+            samples.append(time.perf_counter() - t0)
+        sec = float(np.median(samples))
+        out[f"threads_{threads}"] = {"value": cells / sec, "unit": "cells/s", "ms": sec * 1e3, "threads_used": used}
+    return {"value": out["threads_8"]["value"], "unit": "cells/s", "cores": out["threads_8"]["threads_used"],
+            "kind": "reference", "one_thread": out["threads_1"],
+            "sample": f"the whole 200,000-row matrix ({cells} cells), k = 3/4/5 one call each, median of 3 after a "
+                      "warm-up; EvaluateKOptTemplateCosts(kCpu), OMP_DYNAMIC=FALSE OMP_PROC_BIND=spread OMP_PLACES=cores",
+            "host_cpu": host_cpu()}
+
+
+def run_kopt(args, ctx, stream, device, world, parity=None):
     import torch
     from cudaedgeelimination_b200 import synth
     from cudaedgeelimination_b200.api import KOPT_TEMPLATE_COUNTS
@@ -461,6 +562,27 @@ def run_kopt(args, ctx, stream, device, world):
     peak, peak_kind = load_peaks()
     alg_bytes = rows * 48 + cells * 8 + 8 * g.n
     achieved = alg_bytes / (ms / 1e3) / 1e9
+    large = run_kopt_large(args, ctx, stream, device, world, g, parity)
+    extra = {}
+    if parity is not None:
+        import oracle
+        port = oracle.Port()
+        t0 = time.perf_counter()
+        for k, t, got, m, f in zip(ks, lists, outs, masks, firsts):
+            want = port.kopt_costs_parallel(g, k, t)
+            assert np.array_equal(got, want), f"k-opt matrix differs from the oracle (k={k})"
+            better = want < t["deleted_cost"][:, None]
+            words = np.zeros_like(m)
+            for j in range(want.shape[1]):
+                words[:, j // 32] |= better[:, j].astype(np.uint32) << np.uint32(j % 32)
+            assert np.array_equal(m, words), f"improving masks differ from the oracle (k={k})"
+            assert np.array_equal(f, np.where(better.any(axis=1), better.argmax(axis=1), -1)), "first improving"
+        parity["kopt"] = {"rows": rows, "cells": cells, "checked": "every cell of the resident and end-to-end "
+                          "matrices, every improving-template mask and first improving template",
+                          "oracle": "oracle/cee_oracle.c on host threads", "seconds": time.perf_counter() - t0,
+                          "ok": True}
+        extra["cpu_baseline"] = cpu_leg("kopt")
+        extra["vs_cpu_8_threads"] = (cells / (ms / 1e3)) / extra["cpu_baseline"]["value"]
     return {"metric": "k-opt cost cells/s", "value": cells * world / (ms / 1e3), "unit": "cells/s",
             "ms_per_step": ms, "rows": rows, "cells": cells,
             "config": "15,000-node CEIL_2D instance in [0,1e6)^2, 200,000 rows k=3/4/5 in thirds, one launch; "
@@ -477,7 +599,53 @@ def run_kopt(args, ctx, stream, device, world):
                          "traffic": load_traffic().get("kopt_cost_kernel"), "traffic_unit": "DRAM bytes per launch (ncu)",
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "issue": issue_roofline("kopt_cost_kernel", ms, clock_summary.get("sm_mhz"), device)},
-            "clocks": clock_summary}
+            "clocks": clock_summary, "larger_than_l2": large, **extra}
+
+
+def run_kopt_large(args, ctx, stream, device, world, g, parity):
+    """The same kernel on 1,000,000 rows (k = 3/4/5 in thirds, 632 MB of output, five times L2), so
+    that the cells it writes must reach DRAM within the timed launch."""
+    import torch
+    from cudaedgeelimination_b200 import synth
+    from cudaedgeelimination_b200.api import KOPT_TEMPLATE_COUNTS
+    big_g, tasks = synth.kopt_instance(rows=1_000_000)
+    ks = [3, 4, 5]
+    lists = [tasks[k] for k in ks]
+    rows = sum(t.shape[0] for t in lists)
+    cells = sum(t.shape[0] * KOPT_TEMPLATE_COUNTS[k] for k, t in zip(ks, lists))
+    ctx.kopt_prepare_multi(big_g, ks, lists)
+    for _ in range(args.warmup):
+        ctx.kopt_launch()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(device)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.kopt_launch()
+    e1.record(stream)
+    e1.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+    peak, peak_kind = load_peaks()
+    alg_bytes = rows * 48 + cells * 8 + 8 * big_g.n
+    out = {"rows": rows, "cells": cells, "ms_per_launch": ms, "value": cells * world / (ms / 1e3), "unit": "cells/s",
+           "roofline": {"kernel": "kopt_cost_kernel", "bound": "hbm", "achieved": alg_bytes / (ms / 1e3) / 1e9,
+                        "peak": peak, "unit": "GB/s", "frac": alg_bytes / (ms / 1e3) / 1e9 / peak,
+                        "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": alg_bytes,
+                        "traffic": load_traffic().get("kopt_cost_kernel_1m"),
+                        "traffic_unit": "DRAM bytes per launch (ncu)"},
+           "config": "1,000,000 rows of the same 15,000-node CEIL_2D instance's walks, back-to-back launches (the "
+                     "632 MB output is five times L2, so every launch writes DRAM)"}
+    if parity is not None:
+        import oracle
+        port = oracle.Port()
+        outs = [np.empty((t.shape[0], KOPT_TEMPLATE_COUNTS[k]), np.int64) for k, t in zip(ks, lists)]
+        ctx.kopt_fetch(outs)
+        t0 = time.perf_counter()
+        for k, t, got in zip(ks, lists, outs):
+            assert np.array_equal(got, port.kopt_costs_parallel(big_g, k, t)), f"1M-row matrix differs (k={k})"
+        parity["kopt_1m_rows"] = {"rows": rows, "cells": cells, "checked": "every cell",
+                                  "seconds": time.perf_counter() - t0, "ok": True}
+    return out
 
 
 def _pinned_pool(count: int, nbytes: int):
@@ -563,7 +731,37 @@ def plain_drive(ctx, wl, arrivals, buffer, keep_every: int):
     return latency, service, time.perf_counter() - t0, kept
 
 
-def run_serve(args, device, world):
+def cpu_leg_serve(jobs: int, budget_s: float = 12.0):
+    """The serving stream's jobs in arrival order, one at a time, on the reference's own CPU code:
+    FindJvCandidatesCpu for a JV epoch job, EvaluateKOptTemplateCosts(kCpu) per k for a k-opt job
+    (OpenMP as the reference sets it: up to 8 threads). Every snapshot is built before timing; jobs
+    run until the budget is spent."""
+    import oracle
+    from cudaedgeelimination_b200 import synth
+    ref = oracle.Reference()
+    wl = synth.ServeWorkload(jobs=jobs)
+    jv_graphs = [ref.graph(g) for g in wl.jv]
+    kopt_graphs = [ref.graph(g) for g, _ in wl.kopt]
+    done = {"jv": 0, "kopt": 0}
+    t0 = time.perf_counter()
+    for job in wl.jobs:
+        if time.perf_counter() - t0 > budget_s:
+            break
+        if job[0] == "jv":
+            jv_graphs[job[1]].jv_cpu()
+        else:
+            for k, t in zip((3, 4, 5), wl.kopt_tasks(job)):
+                kopt_graphs[job[1]].kopt_costs(k, t, 1)
+        done[job[0]] += 1
+    sec = time.perf_counter() - t0
+    count = done["jv"] + done["kopt"]
+    return {"value": count / sec, "unit": "jobs/s", "cores": min(8, os.cpu_count() or 1), "kind": "reference",
+            "sample": f"the first {count} of {len(wl.jobs)} jobs in arrival order ({done['jv']} JV epochs, "
+                      f"{done['kopt']} k-opt batches) run one at a time in {sec:.1f} s; FindJvCandidatesCpu (1 thread) "
+                      "and EvaluateKOptTemplateCosts(kCpu) (OpenMP, at most 8 threads); snapshots built before timing"}
+
+
+def run_serve(args, device, world, parity=None):
     """The serving stream (Poisson arrivals at 0.8 x the loop's measured capacity) through the
     serving loop, and the same jobs run plain-sequentially through the regular entry points."""
     from cudaedgeelimination_b200 import Context, synth
@@ -612,6 +810,25 @@ def run_serve(args, device, world):
             assert all((a == b).all() for a, b in zip(got, want)), f"serve/plain mismatch on job {idx}"
         else:
             assert (got == want).all(), f"serve/plain mismatch on job {idx}"
+    extra = {}
+    if parity is not None:  # the same sample against the C oracle
+        import oracle
+        port = oracle.Port()
+        t0 = time.perf_counter()
+        for idx, got in kept.items():
+            job = wl.jobs[idx]
+            if job[0] == "jv":
+                assert np.array_equal(got, port.jv_screen(wl.jv[job[1]])), f"served JV job {idx} differs from the oracle"
+            else:
+                g = wl.kopt[job[1]][0]
+                for k, t, a in zip((3, 4, 5), wl.kopt_tasks(job), got):
+                    assert np.array_equal(a, port.kopt_costs_parallel(g, k, t)), f"served k-opt job {idx} differs"
+        parity["serve"] = {"jobs": len(kept), "of": len(wl.jobs), "checked": "every output of every sampled job "
+                           "(each 100th of the Poisson run) against the C oracle and the regular entry points",
+                           "seconds": time.perf_counter() - t0, "ok": True}
+        extra["cpu_baseline"] = cpu_leg(f"serve:{len(wl.jobs)}")
+    kinds = np.array([j[0] == "jv" for j in wl.jobs])
+    per_kind = {"jv": _latency_summary(lat[kinds]), "kopt": _latency_summary(lat[~kinds])}
     del owners, pinned_pools
     jv_jobs = sum(1 for j in wl.jobs if j[0] == "jv")
     return {
@@ -624,13 +841,16 @@ def run_serve(args, device, world):
                   "service_p99_ms": float(np.percentile(service, 99) * 1e3),
                   "api": "cee_jv_screen / cee_kopt_costs_multi, one job at a time"},
         "capacity_speedup": capacity / plain_capacity,
+        "per_kind": per_kind,
         "d2h_bytes": int(sum(wl.output_bytes(j) for j in wl.jobs)),
+        "d2h_gb_per_s_at_capacity": sum(wl.output_bytes(j) for j in wl.jobs) / cap_s / 1e9,
         "config": f"{len(wl.jobs)} jobs, Poisson arrivals at 0.8 x measured serving capacity; 70% JV epochs on "
                   f"{len(wl.jv)} resident instances of the batching mix (n log-uniform [200,20000]), 30% k-opt "
                   f"batches of 1k-50k rows (k = 3/4/5 in thirds) on {len(wl.kopt)} resident CEIL_2D instances; "
                   f"{slots} slots, k-opt rows and results in pinned host buffers; latency = arrival to results "
                   "on the host",
         "checked_jobs": len(plain_kept),
+        **extra,
     }
 
 
@@ -687,28 +907,35 @@ def max_over_ranks(value: float, world: int) -> float:
     return float(t.item())
 
 
-def run_reference(args, rank: int):
+def run_reference(args, rank: int, world: int):
+    """The reference arm: the reference's own CPU code for the batched step (ReferenceStep) on every
+    host thread. A step is a stratified eighth of the batch -- instances s mod 8, s + 8, ... for
+    step s -- so eight consecutive steps cover every instance once; value = edges / seconds over
+    the timed steps. Under torchrun only rank 0 runs it."""
     if rank != 0:
         return None
     from cudaedgeelimination_b200 import synth
     batch = synth.BatchUnion(args.instances)
     threads = os.cpu_count() or 1
-    # each step: the reference's CPU JV screen over a bounded sample of the batch
-    budget = max(2.0, min(20.0, 120.0 / max(1, args.steps + args.warmup)))
-    for _ in range(args.warmup):
-        reference_step_rate(batch, budget / 4, threads)
-    rates = []
-    sample = ""
-    kind = "reference"
-    for _ in range(args.steps):
-        rate, kind, sample = reference_step_rate(batch, budget, threads)
-        rates.append(rate)
-    value = float(np.median(rates))
+    step = ReferenceStep(batch, threads)
+    stride = 8
+    for s in range(args.warmup):
+        step.run(range(s % stride, batch.count, stride))
+    edges = seconds = 0.0
+    for s in range(args.steps):
+        e, sec = step.run(range(s % stride, batch.count, stride))
+        edges += e
+        seconds += sec
+    value = edges / seconds
+    sample = (f"each step every {stride}th instance ({batch.count // stride} of {batch.count}; offsets rotate so "
+              f"{stride} steps cover the batch), {int(edges)} edges over {args.steps} steps in {seconds:.1f} s, "
+              f"one C++ call per step on {threads} host threads, snapshots built before timing")
     return {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)",
-            "config": {"workload": f"batching mix: {batch.count} instances (bounded sample per step)"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": seconds / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic (seeded; TSPLIB/ElimTSP inputs not shipped)", "config": workload_config(batch, world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": step.kind, "sample": sample},
+            "host_cpu": host_cpu(),
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -717,8 +944,13 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.cpu_leg is not None:  # a CPU-baseline child process (see cpu_leg)
+        name, _, arg = args.cpu_leg.partition(":")
+        out = cpu_leg_kopt() if name == "kopt" else cpu_leg_serve(int(arg or 10_000), args.cpu_budget_s)
+        print(json.dumps(out), flush=True)
+        return
     if args.impl == "reference":
-        out = run_reference(args, rank)
+        out = run_reference(args, rank, world)
         if out is not None:
             print(json.dumps(out), flush=True)
         return
