@@ -270,19 +270,21 @@ class ServeMixin:
         self._serve_jobs[job.value] = outs
         return job.value
 
-    def serve_poll(self, capacity: int = 256):
-        """Completed jobs as (job, tag, outputs) tuples."""
+    def serve_poll(self, capacity: int = 256, with_status: bool = False):
+        """Completed jobs as (job, tag, outputs) tuples; a job that failed raises NativeError, unless
+        with_status, which returns (job, tag, outputs, status) tuples instead."""
         events = getattr(self, "_serve_events", None)
         if events is None or len(events) < capacity:
             events = self._serve_events = (_native.ServeEvent * capacity)()
         count = ctypes.c_int32(0)
         _native.check(self.handle, _native.lib().cee_serve_poll(self.handle, events, capacity, ctypes.byref(count)))
-        done = []
-        for i in range(count.value):
-            ev = events[i]
-            _native.check(self.handle, ev.status)
-            done.append((ev.job, ev.tag, self._serve_jobs.pop(ev.job)))
-        return done
+        done = [(events[i].job, events[i].tag, self._serve_jobs.pop(events[i].job), events[i].status)
+                for i in range(count.value)]
+        if with_status:
+            return done
+        for _, _, _, status in done:
+            _native.check(self.handle, status)
+        return [d[:3] for d in done]
 
     def serve_pending(self) -> tuple[int, int]:
         jobs = ctypes.c_int32(0)

@@ -45,8 +45,9 @@ __device__ __forceinline__ float sqrt_estimate(float x) {
 // candidate answer r (nearest for EUC_2D, up for CEIL_2D), then checked and corrected with the
 // exact residual t = s - r^2. dx and dy are exact in FP32; the FP32 sum of squares carries a
 // relative error of at most 2u + u^2 (u = 2^-24), which the root halves; sqrt.approx.f32 adds
-// at most 2^-23.25 (its largest relative error over every float in [1, 2^46), measured
-// exhaustively on the B200). So |f - sqrt(s)| <= sqrt(s) * 2^-22.58 <
+// at most 2^-23.25 (its largest relative error over every float in [1, 2^44), the range the
+// FP32 sums of squares of this class fall in, measured exhaustively on the B200 by
+// cee_sqrt_estimate_error). So |f - sqrt(s)| <= sqrt(s) * 2^-22.58 <
 // 2^21.5 * 2^-22.58 < 0.48, the candidate is within one of the answer, and t lies well inside
 // int32, so it is exact when computed modulo 2^32 from wrapped 32-bit products. The answer is r
 // iff -r < t <= r (EUC_2D: (r - 1/2)^2 < s < (r + 1/2)^2) or -(2r - 1) < t <= 0 (CEIL_2D:

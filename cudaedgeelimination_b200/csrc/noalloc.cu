@@ -50,6 +50,7 @@ enum : int32_t {
   kBadRowOffsets = 4,
   kBadNeighbor = 8,
   kBadEdgeId = 16,
+  kBadRowOrder = 32,  // a CSR row not strictly ascending by neighbour
 };
 
 // Validates the caller's device snapshot and builds the slot weights in the scratch array;
@@ -80,6 +81,19 @@ __global__ void noalloc_prepare(cee_device_graph g, int32_t* __restrict__ slot_w
     const bool bad = here < 0 || here > g.adjacency || (i == 0 && here != 0) || (i == g.n && here != g.adjacency) ||
                      (i < g.n && g.row_offsets[i + 1] < here);
     if (bad) atomicOr(status, kBadRowOffsets);
+    // rows must ascend by neighbour (the warp screen finds N(a) members by search or lane match);
+    // only rows whose bounds are in range are read
+    if (i < g.n) {
+      const int32_t next = g.row_offsets[i + 1];
+      if (here >= 0 && here <= next && next <= g.adjacency) {
+        for (int32_t s = here + 1; s < next; ++s) {
+          if (g.neighbors[s - 1] >= g.neighbors[s]) {
+            atomicOr(status, kBadRowOrder);
+            break;
+          }
+        }
+      }
+    }
   }
   for (int64_t e = first; e < g.m; e += stride) {
     const int32_t u = g.edge_uv[2 * e], v = g.edge_uv[2 * e + 1];

@@ -184,15 +184,16 @@ int FreeSlot(const ServeState& s) {
   return -1;
 }
 
-// Publishes `desc` in `slot` with ordered copies: state = 0, descriptor, ticket and done =
-// generation << 32, state = generation. The pinned sources of a slot are rewritten only after
-// its previous job finished, i.e. after the copies that read them ran.
+// Publishes `desc` in `slot` with ordered copies: state = 0, the slot's error word = 0, descriptor,
+// ticket and done = generation << 32, state = generation. The pinned sources of a slot are
+// rewritten only after its previous job finished, i.e. after the copies that read them ran.
 int Publish(cee_ctx* ctx, ServeState& s, int slot, const ServeJob& desc) {
   ServeControl* ctl = static_cast<ServeControl*>(s.control.ptr);
   s.desc_host[slot] = desc;
   s.words_host[2 + slot] = desc.generation;
   s.tickets_host[slot] = static_cast<uint64_t>(desc.generation) << 32;
   cudaMemcpyAsync(&ctl->state[slot], &s.words_host[0], sizeof(uint32_t), cudaMemcpyHostToDevice, s.copy);
+  cudaMemcpyAsync(&ctl->slot_error[slot], &s.words_host[0], sizeof(int32_t), cudaMemcpyHostToDevice, s.copy);
   cudaMemcpyAsync(&ctl->jobs[slot], &s.desc_host[slot], sizeof(ServeJob), cudaMemcpyHostToDevice, s.copy);
   cudaMemcpyAsync(&ctl->ticket[slot], &s.tickets_host[slot], sizeof(uint64_t), cudaMemcpyHostToDevice, s.copy);
   cudaMemcpyAsync(&ctl->done[slot], &s.tickets_host[slot], sizeof(uint64_t), cudaMemcpyHostToDevice, s.copy);
@@ -714,7 +715,7 @@ int cee_serve_stop(cee_ctx* ctx) {
   int32_t error_word = 0;
   ReleaseServe(ctx, &error_word);
   if (error_word != 0) {
-    return Fail(ctx, CEE_ERR_INVALID, "serving loop: device bounds check rejected an out-of-range index (code " +
+    return Fail(ctx, CEE_ERR_INVALID, "serving loop: a claimed work item's job never became visible (code " +
                                           std::to_string(error_word) + ")");
   }
   return CEE_OK;

@@ -11,7 +11,7 @@
 // check and its atomicAdd): the warp then reads that generation's descriptor and runs the item,
 // so no item is ever lost; indices past a job's item count are simply dropped. The warp that
 // finishes a job's last item (done counter) makes the job's outputs visible and writes the
-// loop's error word, then the generation, into the slot's words of a host-mapped array; the host
+// job's error word, then the generation, into the slot's words of a host-mapped array; the host
 // then copies the results back. Jobs that arrive while others run share the warps item by item
 // (continuous batching). Every wait is bounded: a warp that finds no work for `idle_limit`
 // scans, or sees the stop word, leaves after its current item; the host relaunches the kernel
@@ -61,8 +61,11 @@ struct ServeControl {
   unsigned long long ticket[kServeMaxSlots];  // generation << 32 | next item
   unsigned long long done[kServeMaxSlots];    // generation << 32 | items finished
   uint32_t state[kServeMaxSlots];
+  // per job slot: the device bounds checks of the job now in the slot (1); reset when a job is
+  // published there, so one job's bad index is reported for that job alone
+  int32_t slot_error[kServeMaxSlots];
   uint32_t stop;
-  int32_t error;  // sticky word: bounds checks (1), a descriptor that never appeared (8)
+  int32_t error;  // loop-wide, sticky: a descriptor that never appeared (8)
 };
 
 // Bounded wait (about a second) for the descriptor of a generation whose item a claim returned.
@@ -174,7 +177,6 @@ __device__ __forceinline__ void serve_kopt_item(const ServeJob& job, const Serve
 static __global__ void __launch_bounds__(kServeWarps * 32, 4)
     serve_kernel(ServeControl* ctl, uint32_t* finished, const uint8_t* templates, int32_t slots,
                  long long idle_limit) {
-  int32_t* error = &ctl->error;
   __shared__ JvWarpScratch jv_scratch[kServeWarps];
   __shared__ __align__(16) unsigned char kopt_scratch[kServeWarps][kServeKoptScratch];
   __shared__ ServeJob job_copy[kServeWarps];
@@ -234,7 +236,7 @@ static __global__ void __launch_bounds__(kServeWarps * 32, 4)
       }
       if (!found) {
         if (lane == 0 && volatile_load(&ctl->state[slot]) == 0) {  // the publication never completed
-          atomicOr(error, 8);
+          atomicOr(&ctl->error, 8);
           __threadfence_system();
           reinterpret_cast<volatile uint32_t*>(finished)[kServeLostWord] = 1u;
         }
@@ -250,6 +252,7 @@ static __global__ void __launch_bounds__(kServeWarps * 32, 4)
     }
     held = slot;
     idle = 0;
+    int32_t* error = &ctl->slot_error[slot];
     const long long local = index;
     if (job.type == kServeJv) {
       const int64_t e0 = local * kServeJvTile;
@@ -282,11 +285,12 @@ static __global__ void __launch_bounds__(kServeWarps * 32, 4)
     __syncwarp();
     if (lane == 0) {
       const unsigned long long d = atomicAdd(&ctl->done[slot], 1ull);
-      // the job's last item: finished[kServeMaxSlots + slot] = error word, then finished[slot] = generation
+      // the job's last item: finished[kServeMaxSlots + slot] = the job's error word, then
+      // finished[slot] = generation
       if (static_cast<uint32_t>(d >> 32) == job.generation && static_cast<uint32_t>(d) + 1 == job.items) {
         __threadfence_system();
         reinterpret_cast<volatile uint32_t*>(finished)[kServeMaxSlots + slot] =
-            volatile_load(reinterpret_cast<uint32_t*>(error));
+            volatile_load(reinterpret_cast<uint32_t*>(&ctl->slot_error[slot]));
         __threadfence_system();
         reinterpret_cast<volatile uint32_t*>(finished)[slot] = job.generation;
       }

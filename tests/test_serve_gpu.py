@@ -259,3 +259,48 @@ def test_malformed_requests(snapshots):
         c.serve_stop()
     finally:
         c.close()
+
+
+def test_job_errors_stay_with_their_job(ctx, snapshots):
+    """Device bounds checks are reported per job. A k-opt job whose pinned rows the caller rewrites
+    with an out-of-range node after the submit-time check (the device copies them late) may fail
+    with CEE_ERR_INVALID -- but only that job: a job run beside it and the jobs after it return
+    CEE_OK with the regular entry point's results, and the loop stops cleanly."""
+    import torch
+    from cudaedgeelimination_b200._native import CEE_OK
+    g, kt = snapshots["kopt"], snapshots["_ktasks"]
+    good = kt[4][:500]
+    want = ctx.kopt_costs_multi(g, [4], [good])[0][0]
+    rows = np.tile(kt[5], 20)[:50_000]
+    owner = torch.from_numpy(rows.view(np.uint8).reshape(-1).copy()).pin_memory()
+    c = Context(0)
+    saw_error = False
+    try:
+        c.serve_start(ServeConfig(hbm_budget_bytes=256 << 20, slots=4, idle_ms=20))
+        sid = c.serve_add_snapshot(g)
+        for attempt in range(12):
+            pinned = owner.numpy().view(KOPT_TASK_DTYPE)
+            pinned[:] = rows
+            c.serve_submit_kopt(sid, [5], [pinned], tag=1)
+            pinned["port_nodes"][-2000:, 0] = g.n + 7  # after the check, before or after the copy
+            c.serve_submit_kopt(sid, [4], [good], tag=2)
+            status, out = {}, {}
+            t0 = time.time()
+            while len(status) < 2:
+                for _, tag, res, st in c.serve_poll(with_status=True):
+                    status[tag], out[tag] = st, res
+                assert time.time() - t0 < 60, "serving loop stalled"
+            assert status[2] == CEE_OK
+            np.testing.assert_array_equal(out[2][0], want)
+            assert status[1] in (CEE_OK, CEE_ERR_INVALID)
+            c.serve_submit_kopt(sid, [4], [good], tag=3)  # the job after a failed one
+            after = drain(c, 1)
+            np.testing.assert_array_equal(after[3][0], want)
+            if status[1] == CEE_ERR_INVALID:
+                saw_error = True
+                break
+        c.serve_stop()
+    finally:
+        c.close()
+    if not saw_error:
+        pytest.skip("the rewritten rows were always copied before the rewrite; isolation checked on clean jobs only")

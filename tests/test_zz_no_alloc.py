@@ -60,6 +60,40 @@ def test_noalloc_matches_regular_entry_point_twice(ctx):
     assert (got_first >= 0).any() and (got_second >= 0).any()
 
 
+def test_noalloc_rejects_unsorted_row():
+    """A device snapshot whose CSR row is not ascending by neighbour fails validation
+    (CEE_ERR_INVALID) instead of screening with the wrong N(a) membership."""
+    import torch
+    torch.cuda.set_device(0)
+    g = synth.jv_small()
+    bad = g.copy()
+    bad.neighbors = g.neighbors.copy()
+    bad.csr_edge_ids = g.csr_edge_ids.copy()
+    row = int(np.flatnonzero(np.diff(g.row_offsets) >= 3)[0])
+    lo = int(g.row_offsets[row])
+    for arr in (bad.neighbors, bad.csr_edge_ids):
+        arr[lo], arr[lo + 1] = arr[lo + 1], arr[lo]
+    view, keep = device_snapshot(bad)
+    out = torch.full((g.m,), -7, dtype=torch.int32, device="cuda:0")
+    stream = torch.cuda.current_stream(0).cuda_stream
+    status = _native.lib().cee_jv_screen_noalloc(ctypes.byref(view), ctypes.c_void_p(out.data_ptr()),
+                                                 ctypes.c_void_p(stream))
+    assert status == _native.CEE_ERR_INVALID
+    assert b"failed validation" in _native.lib().cee_last_error(None)
+    # the next call with a valid snapshot still matches the regular entry point
+    np.testing.assert_array_equal(screen_noalloc(g), regular_screen(g))
+
+
+def regular_screen(g):
+    """The regular entry point's witnesses (cee_jv_screen) on a fresh context."""
+    from cudaedgeelimination_b200 import Context
+    c = Context(0)
+    try:
+        return c.jv_screen(g)[0]
+    finally:
+        c.close()
+
+
 def test_noalloc_rejects_oversize_adjacency():
     view = _native.DeviceGraph()
     view.n, view.dist_type, view.m, view.adjacency = 10, 0, 5, (1 << 22) + 2
