@@ -1,0 +1,38 @@
+// Test infrastructure (oracle). Runs the reference's own Hamilton-Tutte unit tests
+// (tests/unit/test_hamilton_tutte.cpp, compiled from the reference tree at build time, not copied)
+// against the reference with this project's CUDA seam, built with CUDAEE_HAS_CUDA as the
+// reference's CUDA build is.
+//
+// This project replaces three CUDA units of the reference (JV candidates, k-opt costs, c,d screen);
+// the HT prover's own CUDA units (wavefront propagation, path append, Hamilton and end replies)
+// stay the reference's stubs, outside its scope. One test, TestRecursivePointProof, takes the
+// c,d backend answering as the sign of a full CUDA build and then drives every HT CUDA unit
+// (test_hamilton_tutte.cpp:1303-1330), so this driver leaves it out; its CPU checks run in the
+// reference's CPU-only build of the same file. Every other test runs, including the c,d CPU/CUDA
+// parity test (TestCdCandidatesCpuCuda) on this project's kernels.
+#define main cee_reference_ht_unit_main
+#include "tests/unit/test_hamilton_tutte.cpp"
+#undef main
+
+int main() {
+  try {
+    TestHamiltonRepliesAgainstReferenceFormula();
+    TestHamiltonReplyBatch();
+    TestEndReplyBatch();
+    TestCdCandidatesCpuCuda();
+    TestDfsWavefrontRandomDifferential();
+    TestVacuousAndProofAndTamperRejection();
+    TestNonemptyAndProof();
+    TestRecursiveEndProof();
+    TestPathAppendBatch();
+#ifdef CUDAEE_HAS_CUDA
+    TestCudaWavefrontTruthTable();
+#endif
+    std::cout << "Hamilton-Tutte tests passed (TestRecursivePointProof not run: it needs the HT prover's "
+                 "own CUDA units)\n";
+    return 0;
+  } catch (const std::exception& error) {
+    std::cerr << error.what() << '\n';
+    return 1;
+  }
+}

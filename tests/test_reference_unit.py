@@ -10,7 +10,9 @@ the reference, compiled from its sources by `make -C oracle unit`):
     invariance over CUDA cost batches (:608-897), and c,d candidates (test_hamilton_tutte.cpp:404-442).
 
 test_kopt runs through oracle/ref_kopt_unit.cpp, which leaves out the one test that needs the
-un-vendored ElimTSP swap oracle."""
+un-vendored ElimTSP swap oracle; the drop-in test_hamilton_tutte runs through oracle/ref_ht_unit.cpp,
+which leaves out TestRecursivePointProof, whose CUDA part drives the HT prover's own CUDA units
+(wavefront, path append, replies) -- reference stubs here, outside this project's scope."""
 import pathlib
 import subprocess
 
