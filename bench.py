@@ -63,6 +63,9 @@ def parse():
                    help="profiling aid: run only the batched screen, the k-opt part or the serving loop")
     p.add_argument("--cpu-budget-s", type=float, default=12.0)
     p.add_argument("--cpu-leg", default=None, help=argparse.SUPPRESS)
+    p.add_argument("--record-traffic", nargs=6, default=None,
+                   metavar=("CSV", "KEY", "KERNEL", "PROFILE", "CAPTURE", "SCALE"),
+                   help="record one ncu capture's per-launch figures in profiles/ncu_traffic.json and exit")
     return p.parse_args()
 
 
@@ -74,19 +77,79 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+# The product sources each profiled kernel is compiled from: a capture in profiles/ncu_traffic.json
+# records their digest, and a figure whose sources changed since is reported as not current.
+KERNEL_SOURCES = {
+    "batch_screen_kernel": ["batch_screen.cuh", "jv_screen.cuh", "device_common.cuh", "batch.cu"],
+    "kopt_rows_kernel": ["kopt_rows.cuh", "kopt_cost.cuh", "device_common.cuh"],
+}
+
+
+def source_digest(kernel: str) -> str:
+    import hashlib
+    h = hashlib.sha256()
+    for name in KERNEL_SOURCES[kernel]:
+        h.update(name.encode())
+        h.update((ROOT / "cudaedgeelimination_b200" / "csrc" / name).read_bytes())
+    return h.hexdigest()
+
+
 def load_traffic():
     path = ROOT / "profiles" / "ncu_traffic.json"
     if path.exists():
-        return json.loads(path.read_text())
+        return json.loads(path.read_text()).get("captures", {})
     return {}
 
 
-def issue_roofline(kernel: str, ms_per_launch: float, sm_mhz, device):
-    """The instruction-issue ceiling of an ALU-bound kernel: its warp instructions per launch (one ncu
-    capture, profiles/ncu_traffic.json) over the live launch time, against SMs x 4 schedulers x the
+def traffic_fields(key: str) -> dict:
+    """The ncu figures of capture `key` (DRAM bytes per launch and their provenance), marked
+    current only while the kernel's sources still have the digest recorded with the capture."""
+    rec = load_traffic().get(key)
+    if rec is None:
+        return {"traffic": None, "traffic_unit": "DRAM bytes per launch (ncu)"}
+    return {"traffic": rec["dram_bytes"], "traffic_unit": "DRAM bytes per launch (ncu)",
+            "traffic_source": rec["profile"], "traffic_capture": rec["capture"],
+            "traffic_current": rec["source_sha256"] == source_digest(rec["kernel"])}
+
+
+def record_traffic(csv_path: str, key: str, kernel: str, profile: str, capture: str, scale: float) -> None:
+    """Adds capture `key` to profiles/ncu_traffic.json from an ncu CSV of one launch of `kernel`
+    (`ncu ... --csv --page raw`, or `--metrics ... --csv`): dram__bytes_read.sum +
+    dram__bytes_write.sum and smsp__inst_executed.sum, times `scale` (1 for a full-size launch),
+    with the digest of the kernel's sources."""
+    import csv
+    rows = list(csv.reader(open(csv_path)))
+    values = {}
+    if "Metric Name" in rows[0]:  # --metrics --csv: one row per metric
+        i_name, i_val = rows[0].index("Metric Name"), rows[0].index("Metric Value")
+        for r in rows[1:]:
+            values[r[i_name]] = float(r[i_val].replace(",", ""))
+    else:  # --page raw --csv: header, units, one row per launch
+        hdr = rows[0]
+        for name in ("dram__bytes_read.sum", "dram__bytes_write.sum", "smsp__inst_executed.sum"):
+            if name in hdr:
+                raw = float(rows[2][hdr.index(name)].replace(",", ""))
+                unit = rows[1][hdr.index(name)]
+                values[name] = raw * {"Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}.get(unit, 1.0)
+    path = ROOT / "profiles" / "ncu_traffic.json"
+    data = json.loads(path.read_text()) if path.exists() else {}
+    data.setdefault("note", "Per-launch ncu figures behind bench.py's roofline objects (bench.py --record-traffic).")
+    entry = {"kernel": kernel, "dram_bytes": int(round((values["dram__bytes_read.sum"] +
+                                                        values["dram__bytes_write.sum"]) * scale)),
+             "profile": profile, "capture": capture, "scale": scale, "source_sha256": source_digest(kernel)}
+    if "smsp__inst_executed.sum" in values:
+        entry["warp_instructions"] = int(round(values["smsp__inst_executed.sum"] * scale))
+    data.setdefault("captures", {})[key] = entry
+    path.write_text(json.dumps(data, indent=1) + "\n")
+
+
+def issue_roofline(key: str, ms_per_launch: float, sm_mhz, device):
+    """The instruction-issue ceiling of an ALU-bound kernel: its warp instructions per launch (capture
+    `key` of profiles/ncu_traffic.json) over the live launch time, against SMs x 4 schedulers x the
     SM clock sampled during the timed region (one warp instruction per scheduler per cycle)."""
     import torch
-    count = load_traffic().get("warp_instructions", {}).get(kernel)
+    rec = load_traffic().get(key)
+    count = None if rec is None else rec.get("warp_instructions")
     if count is None or not sm_mhz:
         return None
     sms = torch.cuda.get_device_properties(device).multi_processor_count
@@ -94,7 +157,8 @@ def issue_roofline(kernel: str, ms_per_launch: float, sm_mhz, device):
     achieved = count / (ms_per_launch / 1e3)
     return {"unit": "warp instructions/s", "warp_instructions_per_launch": count, "achieved": achieved,
             "peak": peak, "frac": achieved / peak,
-            "peak_source": f"{sms} SMs x 4 schedulers x {float(sm_mhz):.0f} MHz sampled"}
+            "peak_source": f"{sms} SMs x 4 schedulers x {float(sm_mhz):.0f} MHz sampled",
+            "current": rec["source_sha256"] == source_digest(rec["kernel"])}
 
 
 class ClockSampler:
@@ -420,7 +484,7 @@ def run_ours(args, rank: int, world: int, device: int):
                 "api": "cee_batch_screen (pinned host buffers, chunked copy/compute overlap)"},
         "roofline": {"kernel": "batch_screen_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
-                     "traffic": load_traffic().get("batch_screen_kernel"), "traffic_unit": "DRAM bytes per launch (ncu)",
+                     **traffic_fields("batch_screen_kernel"),
                      "algorithmic_bytes_per_launch": alg_bytes,
                      "issue": issue_roofline("batch_screen_kernel", ms_step, clock_summary.get("sm_mhz"), device),
                      "note": "the screen is instruction-issue bound (integer and FP32 exact-distance work, warp "
@@ -594,11 +658,13 @@ def run_kopt(args, ctx, stream, device, world, parity=None):
                              "kernel_ms": lstats.kernel_ms, "d2h_bytes_per_step": int(lstats.d2h_bytes),
                              "rows_with_improving_template": improving_rows,
                              "api": "cee_kopt_improving_multi (host rows in, improving-template masks out)"},
-            "roofline": {"kernel": "kopt_cost_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
+            "roofline": {"kernel": "kopt_rows_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
-                         "traffic": load_traffic().get("kopt_cost_kernel"), "traffic_unit": "DRAM bytes per launch (ncu)",
+                         **traffic_fields("kopt_rows_kernel_200k"),
                          "algorithmic_bytes_per_launch": alg_bytes,
-                         "issue": issue_roofline("kopt_cost_kernel", ms, clock_summary.get("sm_mhz"), device)},
+                         "issue": issue_roofline("kopt_rows_kernel_200k", ms, clock_summary.get("sm_mhz"), device),
+                         "note": "the 126 MB output about fills L2, so part of it is still in L2 when the launch "
+                                 "ends; larger_than_l2 is the DRAM-bound figure"},
             "clocks": clock_summary, "larger_than_l2": large, **extra}
 
 
@@ -628,11 +694,10 @@ def run_kopt_large(args, ctx, stream, device, world, g, parity):
     peak, peak_kind = load_peaks()
     alg_bytes = rows * 48 + cells * 8 + 8 * big_g.n
     out = {"rows": rows, "cells": cells, "ms_per_launch": ms, "value": cells * world / (ms / 1e3), "unit": "cells/s",
-           "roofline": {"kernel": "kopt_cost_kernel", "bound": "hbm", "achieved": alg_bytes / (ms / 1e3) / 1e9,
+           "roofline": {"kernel": "kopt_rows_kernel", "bound": "hbm", "achieved": alg_bytes / (ms / 1e3) / 1e9,
                         "peak": peak, "unit": "GB/s", "frac": alg_bytes / (ms / 1e3) / 1e9 / peak,
                         "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": alg_bytes,
-                        "traffic": load_traffic().get("kopt_cost_kernel_1m"),
-                        "traffic_unit": "DRAM bytes per launch (ncu)"},
+                        **traffic_fields("kopt_rows_kernel_1m")},
            "config": "1,000,000 rows of the same 15,000-node CEIL_2D instance's walks, back-to-back launches (the "
                      "632 MB output is five times L2, so every launch writes DRAM)"}
     if parity is not None:
@@ -944,6 +1009,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.record_traffic is not None:
+        csv_path, key, kernel, profile, capture, scale = args.record_traffic
+        record_traffic(csv_path, key, kernel, profile, capture, float(scale))
+        return
     if args.cpu_leg is not None:  # a CPU-baseline child process (see cpu_leg)
         name, _, arg = args.cpu_leg.partition(":")
         out = cpu_leg_kopt() if name == "kopt" else cpu_leg_serve(int(arg or 10_000), args.cpu_budget_s)

@@ -28,6 +28,7 @@ OPT_JV_WAVES = 2
 OPT_KOPT_ROWS_K3 = 3
 OPT_KOPT_ROWS_K4 = 4
 OPT_KOPT_ROWS_K5 = 5
+OPT_KOPT_KERNEL = 6
 
 
 class GraphView(ctypes.Structure):

@@ -6,6 +6,7 @@
 #include "cd_screen.cuh"
 #include "jv_screen.cuh"
 #include "kopt_cost.cuh"
+#include "kopt_rows.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -518,6 +519,24 @@ std::vector<uint32_t> GapPatternMasks(uint32_t k, const std::vector<uint8_t>& pa
   return masks;
 }
 
+// Whether `mates` is the proper table of k byte for byte (the one kopt_rows.cuh compiles in).
+template <int K>
+bool SameAsCanon(const uint8_t* mates, int32_t count) {
+  const KoptCanonTable<K>& tab = KoptCanon<K>::value;
+  if (count != tab.count) return false;
+  for (int t = 0; t < count; ++t) {
+    for (int p = 0; p < 14; ++p) {
+      const uint8_t want = p < 2 * K ? tab.mate[t][p] : 0xff;
+      if (mates[14 * t + p] != want && p < 2 * K) return false;
+    }
+  }
+  return true;
+}
+
+bool IsCanonicalTable(uint32_t k, const uint8_t* mates, int32_t count) {
+  return k == 3 ? SameAsCanon<3>(mates, count) : (k == 4 ? SameAsCanon<4>(mates, count) : SameAsCanon<5>(mates, count));
+}
+
 int EnsureTable(cee_ctx* ctx, KoptTable* table, uint32_t k, const uint8_t* mates, int32_t count,
                 uint64_t hash, bool* hit) {
   const size_t bytes = static_cast<size_t>(count) * 14;
@@ -539,7 +558,19 @@ int EnsureTable(cee_ctx* ctx, KoptTable* table, uint32_t k, const uint8_t* mates
   if (status == cudaSuccess) {
     status = cudaMemcpy(table->patterns.ptr, masks.data(), masks.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
   }
+  // the same bits by pattern: word [g][w] holds bit (t mod 32) for templates t of word w
+  const int words = (count + 31) / 32;
+  std::vector<uint32_t> by_pattern(static_cast<size_t>(32) * words, 0);
+  for (int g = 0; g < 32; ++g) {
+    for (int t = 0; t < count; ++t) by_pattern[g * words + t / 32] |= ((masks[t] >> g) & 1u) << (t % 32);
+  }
+  if (status == cudaSuccess) status = table->validity.Reserve(by_pattern.size() * sizeof(uint32_t) + 16, nullptr);
+  if (status == cudaSuccess) {
+    status = cudaMemcpy(table->validity.ptr, by_pattern.data(), by_pattern.size() * sizeof(uint32_t),
+                        cudaMemcpyHostToDevice);
+  }
   if (status != cudaSuccess) return CudaFail(ctx, status, "k-opt template pattern upload");
+  table->canonical = IsCanonicalTable(k, mates, count);
   table->k = k;
   table->hash = hash;
   table->T = count;
@@ -592,7 +623,7 @@ int KoptPrepareSegments(cee_ctx* ctx, int32_t segments, const uint32_t* ks, cons
     if (rows[i] > 0 && tasks[i] == nullptr) return Fail(ctx, CEE_ERR_INVALID, "null k-opt tasks");
     cost_offset[i] = total_cells;
     total_rows += rows[i];
-    total_cells += (rows[i] * tables[i]->T + 1) & ~int64_t{1};  // keep each segment 16-byte aligned
+    total_cells += (rows[i] * tables[i]->T + 15) & ~int64_t{15};  // each segment starts on a 128-byte line
   }
   bool grew = false;
   cudaError_t status = s.tasks.Reserve(static_cast<size_t>(total_rows) * sizeof(cee_kopt_task) + 16, &grew);
@@ -619,6 +650,8 @@ int KoptPrepareSegments(cee_ctx* ctx, int32_t segments, const uint32_t* ks, cons
     seg.rows = rows[i];
     seg.pairs = static_cast<const uint8_t*>(tables[i]->pairs.ptr);
     seg.patterns = static_cast<const uint32_t*>(tables[i]->patterns.ptr);
+    seg.validity = static_cast<const uint32_t*>(tables[i]->validity.ptr);
+    seg.canonical = tables[i]->canonical ? 1 : 0;
     seg.k = static_cast<int32_t>(ks[i]);
     seg.templates = tables[i]->T;
     seg.write_costs = 1;
@@ -645,10 +678,94 @@ int KoptPrepareSegments(cee_ctx* ctx, int32_t segments, const uint32_t* ks, cons
   return CEE_OK;
 }
 
+// cuTensorMapEncodeTiled, from the driver through the runtime (the library links only cudart).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn TensorMapEncoder() {
+  static const EncodeTiledFn fn = [] {
+    void* entry = nullptr;
+    cudaDriverEntryPointQueryResult found = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &entry, 12000, cudaEnableDefault, &found) !=
+            cudaSuccess ||
+        found != cudaDriverEntryPointSuccess) {
+      return static_cast<EncodeTiledFn>(nullptr);
+    }
+    return reinterpret_cast<EncodeTiledFn>(entry);
+  }();
+  return fn;
+}
+
+// The tensor map of a k = 5 segment's cost matrix: [rows][208] int64, boxes of 16 cells x 32 rows,
+// 128-byte swizzle (the layout kopt_rows_warp stages).
+bool EncodeKopt5Map(CUtensorMap* map, int64_t* costs, int64_t rows) {
+  const EncodeTiledFn encode = TensorMapEncoder();
+  if (encode == nullptr) return false;
+  const cuuint64_t dims[2] = {208, static_cast<cuuint64_t>(rows)};
+  const cuuint64_t strides[1] = {208 * sizeof(int64_t)};
+  const cuuint32_t box[2] = {kKopt5Box, 32};
+  const cuuint32_t step[2] = {1, 1};
+  return encode(map, CU_TENSOR_MAP_DATA_TYPE_INT64, 2, costs, dims, strides, box, step, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The one-thread-per-row kernel (kopt_rows.cuh) when every segment uses the proper templates and
+// the coordinates are not of the wide span class: 256 rows per block, 32 per warp. Returns false
+// when it does not apply; *status carries a launch error.
+bool KoptRowsLaunch(cee_ctx* ctx, cudaError_t* status) {
+  KoptState& s = ctx->kopt;
+  if (ctx->kopt_kernel == 0 || s.span == kSpanWide) return false;
+  bool masks = false;
+  for (int32_t i = 0; i < s.segments; ++i) {
+    if (s.launch.seg[i].canonical == 0 || s.launch.seg[i].rows >= (int64_t{1} << 31)) return false;
+    masks = masks || s.launch.seg[i].mask_words > 0;
+  }
+  // blocks of the heavier rows first (k = 5, then 4, then 3), so that the light tiles fill the tail;
+  // the kernel maps a block to its segment by tile_begin, so the segments are listed in that order
+  KoptRowsParams P{};  // about 2 KB; the launch copies it
+  KoptLaunch& L = P.L;
+  L = s.launch;
+  std::stable_sort(L.seg, L.seg + L.segments, [](const KoptSegment& a, const KoptSegment& b) { return a.k > b.k; });
+  int32_t tile = 0;
+  for (int32_t i = 0; i < L.segments; ++i) {
+    KoptSegment& seg = L.seg[i];
+    seg.tile_begin = tile;
+    tile += static_cast<int32_t>((seg.rows + kKoptRowThreads - 1) / kKoptRowThreads);
+    if (seg.k == 5 && seg.write_costs != 0 && seg.rows > 0 && !EncodeKopt5Map(&P.box5[i], seg.costs, seg.rows)) {
+      *status = cudaErrorInvalidValue;
+      return true;
+    }
+  }
+  if (tile == 0) return true;
+  WithSpan(s.span, [&](auto S) {
+    if constexpr (S.value != kSpanWide) {
+      auto launch = [&](auto kernel) {
+        *status = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kKoptRowsSmem);
+        if (*status == cudaSuccess) kernel<<<tile, kKoptRowThreads, kKoptRowsSmem, ctx->stream>>>(P, ctx->d_error);
+      };
+      if (masks) {
+        launch(kopt_rows_kernel<S.value, true>);
+      } else {
+        launch(kopt_rows_kernel<S.value, false>);
+      }
+    }
+  });
+  return true;
+}
+
 int KoptLaunchPrepared(cee_ctx* ctx) {
   KoptState& s = ctx->kopt;
   if (!s.prepared) return Fail(ctx, CEE_ERR_STATE, "cee_kopt_launch before prepare");
   if (s.tiles == 0) return CEE_OK;
+  {
+    cudaError_t status = cudaSuccess;
+    if (KoptRowsLaunch(ctx, &status)) {
+      if (status == cudaSuccess) status = cudaGetLastError();
+      if (status != cudaSuccess) return CudaFail(ctx, status, "kopt_rows_kernel launch (tensor map or launch)");
+      return CEE_OK;
+    }
+  }
   int smem = 0;
   for (int32_t i = 0; i < s.segments; ++i) {
     smem = std::max(smem, kopt_tile_smem(s.launch.seg[i].k, s.launch.seg[i].rows_per_tile, s.launch.seg[i].mask_words));
@@ -884,6 +1001,10 @@ int cee_ctx_set_option(cee_ctx* ctx, int32_t option, int64_t value) {
       ctx->kopt_rows_per_tile[k - 3] = static_cast<int>(value);
       return CEE_OK;
     }
+    case CEE_OPT_KOPT_KERNEL:
+      if (value != 0 && value != 1) return Fail(ctx, CEE_ERR_INVALID, "k-opt kernel must be 0 (tiled) or 1 (rows)");
+      ctx->kopt_kernel = static_cast<int>(value);
+      return CEE_OK;
     default:
       return Fail(ctx, CEE_ERR_INVALID, "unknown option");
   }

@@ -55,9 +55,13 @@ struct KoptTable {
   std::vector<uint8_t> mates;
   DevBuf pairs;     // T x k pair indices
   DevBuf patterns;  // T: gap patterns on which the template is invalid (kopt_cost.cuh)
+  DevBuf validity;  // 32 x ceil(T/32): the same bits by pattern (kopt_rows.cuh)
+  bool canonical = false;  // the proper templates of k, byte for byte
   void Release() {
     pairs.Release();
     patterns.Release();
+    validity.Release();
+    canonical = false;
     k = 0;
     T = 0;
     mates.clear();
@@ -125,6 +129,7 @@ struct cee_ctx {
   int occ_jv_thread[cee::kSpanClasses] = {1, 1, 1};  // resident blocks per SM, per span class
   int occ_jv_warp[cee::kSpanClasses] = {1, 1, 1};
   int kopt_rows_per_tile[3] = {0, 0, 0};  // 0 = default tile for k = 3, 4, 5
+  int kopt_kernel = 1;                    // 1 = the one-thread-per-row kernel where it applies, 0 = tiled
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[6] = {};
   int32_t* d_error = nullptr;  // device bounds-check word

@@ -72,7 +72,7 @@ constexpr uint8_t kKoptReaddsDeleted = 0xff;
 constexpr uint8_t kKoptGeneralRow = 0xff;  // fastpat of a row that is not a gap-pattern row
 
 // pair index of ports p < q among 2k ports (row-major upper triangle)
-__host__ __device__ __forceinline__ int kopt_pair_index(int p, int q, int ports) {
+__host__ __device__ constexpr int kopt_pair_index(int p, int q, int ports) {
   return p * ports - (p * (p + 1)) / 2 + (q - p - 1);
 }
 
@@ -82,6 +82,8 @@ struct KoptSegment {
   int64_t rows;
   const uint8_t* __restrict__ pairs;  // T x k pair indices (device)
   const uint32_t* __restrict__ patterns;  // T: bit g = the template is invalid on rows of gap pattern g
+  const uint32_t* __restrict__ validity;  // 32 x ceil(T/32): bit t % 32 of word [g][t / 32] = patterns[t] bit g
+  int32_t canonical;                      // 1: the table is the proper one (kopt_rows.cuh may serve it)
   uint32_t* __restrict__ improving;   // rows x mask_words: bit t = template t improves the row
   int32_t* __restrict__ first;        // rows: first improving template, or -1
   int32_t k;

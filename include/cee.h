@@ -81,7 +81,9 @@ enum cee_option {
   CEE_OPT_JV_WAVES = 2,     /* grid of the thread-per-edge screen, in waves of resident blocks */
   CEE_OPT_KOPT_ROWS_K3 = 3, /* rows per k-opt tile for k = 3 / 4 / 5 (0 = default, even) */
   CEE_OPT_KOPT_ROWS_K4 = 4,
-  CEE_OPT_KOPT_ROWS_K5 = 5
+  CEE_OPT_KOPT_ROWS_K5 = 5,
+  CEE_OPT_KOPT_KERNEL = 6   /* k-opt matrix kernel: 1 = one thread per row with the proper templates
+                               compiled in, where it applies (default); 0 = the tiled kernel always */
 };
 /* Sets a launch-shape option of this context; results never depend on it. */
 int cee_ctx_set_option(cee_ctx* ctx, int32_t option, int64_t value);

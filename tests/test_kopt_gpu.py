@@ -9,13 +9,18 @@ from cudaedgeelimination_b200._native import NativeError
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(params=[0, 2], ids=["default-tiles", "small-tiles"])
+@pytest.fixture(params=[(1, 0), (0, 0), (0, 2)], ids=["rows-kernel", "tiled-default", "tiled-small"])
 def kc(ctx, request):
-    """The context with the default k-opt tiles, then with small tiles (many partial tiles)."""
+    """The context with each k-opt kernel: the one-thread-per-row kernel with the proper templates
+    compiled in (the default wherever it applies), then the tiled kernel with its default tiles and
+    with small tiles (many partial tiles)."""
+    kernel, tile = request.param
+    ctx.set_option(_native.OPT_KOPT_KERNEL, kernel)
     for opt, rows in zip((_native.OPT_KOPT_ROWS_K3, _native.OPT_KOPT_ROWS_K4, _native.OPT_KOPT_ROWS_K5),
-                         (request.param * 4, request.param * 3, request.param)):
+                         (tile * 4, tile * 3, tile)):
         ctx.set_option(opt, rows)
     yield ctx
+    ctx.set_option(_native.OPT_KOPT_KERNEL, 1)
     for opt in (_native.OPT_KOPT_ROWS_K3, _native.OPT_KOPT_ROWS_K4, _native.OPT_KOPT_ROWS_K5):
         ctx.set_option(opt, 0)
 
