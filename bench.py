@@ -20,7 +20,10 @@ instance. metric = JV edges screened per second over the whole job (c,d tasks/s 
              instance): cells/s resident and end to end, with its own roofline
   cpu_baseline  the reference's own CPU code for the same step (oracle/_ref, compiled from the
              reference sources): FindJvCandidatesCpu plus BuildCdScreenTasks + ScreenCdTasksCpu
-             for the same targets, on a bounded sample of the instances, threads over instances
+             for the same targets, every instance, threads over instances
+  reference_gpu  the reference's own CUDA units built for sm_100a (oracle/_ref/libcudaee_refcuda.so)
+             against this project's kernels behind the same reference API (the drop-in): JV,
+             k-opt and c,d seam calls, and RunJvElimination(kCuda) end to end
 
 --impl reference times the reference's CPU implementation of the same step on the host cores.
 Multi-GPU: one process per GPU, independent replicas (the screen shards by instance with no
@@ -59,7 +62,8 @@ def parse():
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--serve-jobs", type=int, default=10_000)
     p.add_argument("--no-epochs", action="store_true")
-    p.add_argument("--part", default="all", choices=["all", "batch", "kopt", "serve", "epochs"],
+    p.add_argument("--no-refgpu", action="store_true")
+    p.add_argument("--part", default="all", choices=["all", "batch", "kopt", "serve", "epochs", "refgpu"],
                    help="profiling aid: run only the batched screen, the k-opt part or the serving loop")
     p.add_argument("--cpu-budget-s", type=float, default=12.0)
     p.add_argument("--cpu-leg", default=None, help=argparse.SUPPRESS)
@@ -359,9 +363,13 @@ def run_ours(args, rank: int, world: int, device: int):
         ctx.close()
         return out
     if args.part == "serve":
-        return run_serve(args, device, world)
+        from cudaedgeelimination_b200 import synth as _synth
+        wl = _synth.ServeWorkload(jobs=args.serve_jobs)
+        return {"serve": run_serve(args, device, world, wl=wl), "serve_leaf": run_serve(args, device, world, leaf=True, wl=wl)}
     if args.part == "epochs":
         return run_fixed_point(args, device)
+    if args.part == "refgpu":
+        return run_reference_gpu(args, device)
     from cudaedgeelimination_b200.api import BatchOptions
     batch = synth.BatchUnion(args.instances)
     g = batch.graph
@@ -372,7 +380,12 @@ def run_ours(args, rank: int, world: int, device: int):
 
     # ---- resident timing of the batched launch ----
     ctx.batch_prepare(batch, opt)
-    tuning = ctx.batch_autotune(reps=2)
+    from cudaedgeelimination_b200 import TuningCache
+    cache = TuningCache()
+    cached = cache.get(cache.key(ctx.sm_count, "batch",
+                                 largest_instance=int(np.diff(batch.node_begin).max()), instances=batch.count,
+                                 edges=int(g.m))) is not None
+    tuning = ctx.batch_autotune(reps=2, cache=cache)
     for _ in range(args.warmup):
         ctx.batch_launch()
     res = ctx.batch_fetch()
@@ -470,7 +483,8 @@ def run_ours(args, rank: int, world: int, device: int):
         "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded; TSPLIB/ElimTSP inputs not shipped)",
         "config": workload_config(batch, world),
         "launch": "one persistent, CUDA-graph-captured launch per step",
-        "tuning": {"jv_tile": tuning.jv_tile, "blocks_per_sm": tuning.blocks_per_sm, "chunks": tuning.chunks},
+        "tuning": {"jv_tile": tuning.jv_tile, "blocks_per_sm": tuning.blocks_per_sm, "chunks": tuning.chunks,
+                   "source": "tuning cache" if cached else "cee_batch_autotune (stored in the tuning cache)"},
         "targets": targets, "cd_tasks": pairs,
         "cd_tasks_per_s": pairs * world / (ms_step / 1e3),
         "with_cd_finalisation": {"ms_per_step": fin_ms, "value": edges_step * world / (fin_ms / 1e3), "unit": UNIT,
@@ -511,9 +525,14 @@ def run_ours(args, rank: int, world: int, device: int):
     if not args.no_kopt and args.part == "all":
         result["kopt"] = run_kopt(args, ctx, stream, device, world, parity if rank == 0 else None)
     if not args.no_serve and args.part == "all":
-        result["serve"] = run_serve(args, device, world, parity if rank == 0 else None)
+        from cudaedgeelimination_b200 import synth as _synth
+        wl = _synth.ServeWorkload(jobs=args.serve_jobs)
+        result["serve"] = run_serve(args, device, world, parity if rank == 0 else None, wl=wl)
+        result["serve_leaf"] = run_serve(args, device, world, parity if rank == 0 else None, leaf=True, wl=wl)
     if not args.no_epochs and args.part == "all" and rank == 0:
         result["jv_fixed_point"] = run_fixed_point(args, device)
+    if not args.no_refgpu and args.part == "all" and rank == 0:
+        result["reference_gpu"] = run_reference_gpu(args, device)
 
     if rank == 0:
         # the reference's CPU code on the same step: every instance, one pass, all host threads
@@ -589,6 +608,9 @@ def run_kopt(args, ctx, stream, device, world, parity=None):
     rows = sum(t.shape[0] for t in lists)
     cells = sum(t.shape[0] * KOPT_TEMPLATE_COUNTS[k] for k, t in zip(ks, lists))
     ctx.kopt_prepare_multi(g, ks, lists)
+    from cudaedgeelimination_b200 import TuningCache
+    ktune = ctx.kopt_autotune(reps=3, cache=TuningCache())
+    kname = "kopt_rows_kernel" if ktune.kernel == 1 else "kopt_cost_kernel"
     for _ in range(args.warmup):
         ctx.kopt_launch()
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)
@@ -626,7 +648,7 @@ def run_kopt(args, ctx, stream, device, world, parity=None):
     peak, peak_kind = load_peaks()
     alg_bytes = rows * 48 + cells * 8 + 8 * g.n
     achieved = alg_bytes / (ms / 1e3) / 1e9
-    large = run_kopt_large(args, ctx, stream, device, world, g, parity)
+    large = run_kopt_large(args, ctx, stream, device, world, g, parity, kname)
     extra = {}
     if parity is not None:
         import oracle
@@ -649,6 +671,8 @@ def run_kopt(args, ctx, stream, device, world, parity=None):
         extra["vs_cpu_8_threads"] = (cells / (ms / 1e3)) / extra["cpu_baseline"]["value"]
     return {"metric": "k-opt cost cells/s", "value": cells * world / (ms / 1e3), "unit": "cells/s",
             "ms_per_step": ms, "rows": rows, "cells": cells,
+            "tuning": {"kernel": "rows" if ktune.kernel == 1 else "tiled", "rows_per_tile": list(ktune.rows_per_tile),
+                       "api": "cee_kopt_autotune through the tuning cache"},
             "config": "15,000-node CEIL_2D instance in [0,1e6)^2, 200,000 rows k=3/4/5 in thirds, one launch; "
                       "L2 flushed (256 MB write) between timed launches",
             "e2e": {"value": cells * world / e2e_s, "unit": "cells/s", "ms_per_step": e2e_s * 1e3,
@@ -658,17 +682,17 @@ def run_kopt(args, ctx, stream, device, world, parity=None):
                              "kernel_ms": lstats.kernel_ms, "d2h_bytes_per_step": int(lstats.d2h_bytes),
                              "rows_with_improving_template": improving_rows,
                              "api": "cee_kopt_improving_multi (host rows in, improving-template masks out)"},
-            "roofline": {"kernel": "kopt_rows_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
+            "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
-                         **traffic_fields("kopt_rows_kernel_200k"),
+                         **traffic_fields(f"{kname}_200k"),
                          "algorithmic_bytes_per_launch": alg_bytes,
-                         "issue": issue_roofline("kopt_rows_kernel_200k", ms, clock_summary.get("sm_mhz"), device),
+                         "issue": issue_roofline(f"{kname}_200k", ms, clock_summary.get("sm_mhz"), device),
                          "note": "the 126 MB output about fills L2, so part of it is still in L2 when the launch "
                                  "ends; larger_than_l2 is the DRAM-bound figure"},
             "clocks": clock_summary, "larger_than_l2": large, **extra}
 
 
-def run_kopt_large(args, ctx, stream, device, world, g, parity):
+def run_kopt_large(args, ctx, stream, device, world, g, parity, kname):
     """The same kernel on 1,000,000 rows (k = 3/4/5 in thirds, 632 MB of output, five times L2), so
     that the cells it writes must reach DRAM within the timed launch."""
     import torch
@@ -694,10 +718,10 @@ def run_kopt_large(args, ctx, stream, device, world, g, parity):
     peak, peak_kind = load_peaks()
     alg_bytes = rows * 48 + cells * 8 + 8 * big_g.n
     out = {"rows": rows, "cells": cells, "ms_per_launch": ms, "value": cells * world / (ms / 1e3), "unit": "cells/s",
-           "roofline": {"kernel": "kopt_rows_kernel", "bound": "hbm", "achieved": alg_bytes / (ms / 1e3) / 1e9,
+           "roofline": {"kernel": kname, "bound": "hbm", "achieved": alg_bytes / (ms / 1e3) / 1e9,
                         "peak": peak, "unit": "GB/s", "frac": alg_bytes / (ms / 1e3) / 1e9 / peak,
                         "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": alg_bytes,
-                        **traffic_fields("kopt_rows_kernel_1m")},
+                        **traffic_fields(f"{kname}_1m")},
            "config": "1,000,000 rows of the same 15,000-node CEIL_2D instance's walks, back-to-back launches (the "
                      "632 MB output is five times L2, so every launch writes DRAM)"}
     if parity is not None:
@@ -720,15 +744,37 @@ def _pinned_pool(count: int, nbytes: int):
     return owners, [t.numpy() for t in owners]
 
 
-def _job_outputs(wl, job, buf):
-    """Output arrays of `job` carved from one pinned buffer."""
+def _job_outputs(wl, job, buf, leaf: bool = False):
+    """Output arrays of `job` carved from one pinned buffer: a witness array, the k-opt cost
+    matrices, or with `leaf` the improving-template masks and first improving templates."""
     if job[0] == "jv":
         return buf[:4 * wl.jv[job[1]].m].view(np.int32)
     outs, at = [], 0
+    if leaf:
+        masks, firsts = [], []
+        for (c, _), t in zip(job[2], (4, 25, 208)):
+            w = (t + 31) // 32
+            masks.append(buf[at:at + 4 * c * w].view(np.uint32).reshape(c, w))
+            at += 4 * c * w
+            firsts.append(buf[at:at + 4 * c].view(np.int32))
+            at += 4 * c
+        return masks, firsts
     for (c, _), t in zip(job[2], (4, 25, 208)):
         outs.append(buf[at:at + 8 * c * t].view(np.int64).reshape(c, t))
         at += 8 * c * t
     return outs
+
+
+def _job_output_bytes(wl, job, leaf: bool = False) -> int:
+    if job[0] == "jv" or not leaf:
+        return wl.output_bytes(job)
+    return sum(4 * c * ((t + 31) // 32 + 1) for (c, _), t in zip(job[2], (4, 25, 208)))
+
+
+def _copy_result(res):
+    if isinstance(res, tuple):
+        return tuple([a.copy() for a in part] for part in res)
+    return np.array(res, copy=True) if not isinstance(res, list) else [r.copy() for r in res]
 
 
 def _latency_summary(lat_s):
@@ -737,7 +783,7 @@ def _latency_summary(lat_s):
             "mean_ms": float(ms.mean()), "max_ms": float(ms.max())}
 
 
-def serve_drive(ctx, wl, sids, ksids, arrivals, buffers, keep_every: int):
+def serve_drive(ctx, wl, sids, ksids, arrivals, buffers, keep_every: int, leaf: bool = False):
     """Feeds the jobs into the serving loop at their arrival times (admitting while it accepts
     them), polls completions, and returns (completion - arrival latencies, wall seconds, kept
     sample outputs)."""
@@ -752,9 +798,11 @@ def serve_drive(ctx, wl, sids, ksids, arrivals, buffers, keep_every: int):
         now = time.perf_counter() - t0
         while nxt < n and arrivals[nxt] <= now and free:
             job = wl.jobs[nxt]
-            out = _job_outputs(wl, job, buffers[free[-1]])
+            out = _job_outputs(wl, job, buffers[free[-1]], leaf)
             if job[0] == "jv":
                 jid = ctx.serve_submit_jv(sids[job[1]], wl.jv[job[1]].m, nxt, out=out)
+            elif leaf:
+                jid = ctx.serve_submit_kopt_improving(ksids[job[1]], [3, 4, 5], wl.kopt_tasks(job), nxt, outs=out)
             else:
                 jid = ctx.serve_submit_kopt(ksids[job[1]], [3, 4, 5], wl.kopt_tasks(job), nxt, outs=out)
             if jid is None:  # no slot or arena room: poll first
@@ -765,15 +813,16 @@ def serve_drive(ctx, wl, sids, ksids, arrivals, buffers, keep_every: int):
             idx, b = inflight.pop(jid)
             latency[idx] = time.perf_counter() - t0 - arrivals[idx]
             if idx % keep_every == 0:
-                kept[idx] = np.array(res, copy=True) if not isinstance(res, list) else [r.copy() for r in res]
+                kept[idx] = _copy_result(res)
             free.append(b)
             done += 1
     return latency, time.perf_counter() - t0, kept
 
 
-def plain_drive(ctx, wl, arrivals, buffer, keep_every: int):
+def plain_drive(ctx, wl, arrivals, buffer, keep_every: int, leaf: bool = False):
     """The same jobs one at a time through the regular entry points (cee_jv_screen,
-    cee_kopt_costs_multi), each started at max(arrival, previous completion)."""
+    cee_kopt_costs_multi, or with `leaf` cee_kopt_improving_multi), each started at
+    max(arrival, previous completion)."""
     n = len(wl.jobs)
     latency = np.zeros(n)
     service = np.zeros(n)
@@ -783,16 +832,20 @@ def plain_drive(ctx, wl, arrivals, buffer, keep_every: int):
         while time.perf_counter() - t0 < arrivals[idx]:
             pass
         s0 = time.perf_counter()
-        out = _job_outputs(wl, job, buffer)
         if job[0] == "jv":
+            out = _job_outputs(wl, job, buffer)
             ctx.jv_screen(wl.jv[job[1]], out=out)
+        elif leaf:
+            masks, firsts, _, _ = ctx.kopt_improving_multi(wl.kopt[job[1]][0], [3, 4, 5], wl.kopt_tasks(job))
+            out = (masks, firsts)
         else:
+            out = _job_outputs(wl, job, buffer)
             ctx.kopt_costs_multi(wl.kopt[job[1]][0], [3, 4, 5], wl.kopt_tasks(job), outs=out)
         end = time.perf_counter()
         service[idx] = end - s0
         latency[idx] = end - t0 - arrivals[idx]
         if idx % keep_every == 0:
-            kept[idx] = np.array(out, copy=True) if not isinstance(out, list) else [r.copy() for r in out]
+            kept[idx] = _copy_result(out)
     return latency, service, time.perf_counter() - t0, kept
 
 
@@ -826,13 +879,32 @@ def cpu_leg_serve(jobs: int, budget_s: float = 12.0):
                       "and EvaluateKOptTemplateCosts(kCpu) (OpenMP, at most 8 threads); snapshots built before timing"}
 
 
-def run_serve(args, device, world, parity=None):
+def pcie_d2h_gbs(device) -> float:
+    """Pinned device-to-host bandwidth of this box: 8 copies of 512 MB."""
+    import torch
+    dev = torch.empty(512 << 20, dtype=torch.uint8, device=device)
+    host = torch.empty(512 << 20, dtype=torch.uint8).pin_memory()
+    host.copy_(dev, non_blocking=True)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for _ in range(8):
+        host.copy_(dev, non_blocking=True)
+    torch.cuda.synchronize(device)
+    return 8 * (512 << 20) / (time.perf_counter() - t0) / 1e9
+
+
+def run_serve(args, device, world, parity=None, leaf: bool = False, wl=None):
     """The serving stream (Poisson arrivals at 0.8 x the loop's measured capacity) through the
-    serving loop, and the same jobs run plain-sequentially through the regular entry points."""
+    serving loop, and the same jobs run plain-sequentially through the regular entry points. With
+    `leaf` the k-opt jobs return improving-template sets (the fused leaf consume) instead of cost
+    matrices, in both arms."""
     from cudaedgeelimination_b200 import Context, synth
     from cudaedgeelimination_b200.api import ServeConfig
 
-    wl = synth.ServeWorkload(jobs=args.serve_jobs)
+    base = synth.ServeWorkload(jobs=args.serve_jobs) if wl is None else wl
+    wl = synth.ServeWorkload.__new__(synth.ServeWorkload)  # a copy whose row pools this run pins
+    wl.__dict__.update(base.__dict__)
+    wl.kopt = list(base.kopt)
     pinned_pools = []  # k-opt row pools in page-locked memory, as a serving caller would keep them
     for i, (g, pools) in enumerate(wl.kopt):
         pinned = {}
@@ -842,7 +914,7 @@ def run_serve(args, device, world, parity=None):
             pinned[k] = view
         wl.kopt[i] = (g, pinned)
     slots = 32
-    max_bytes = max(wl.output_bytes(j) for j in wl.jobs)
+    max_bytes = max(_job_output_bytes(wl, j, leaf) for j in wl.jobs)
     owners, buffers = _pinned_pool(slots + 1, max_bytes)
     ctx = Context(device)
     ctx.serve_start(ServeConfig(hbm_budget_bytes=8 << 30, slots=slots, idle_ms=20))
@@ -854,24 +926,29 @@ def run_serve(args, device, world, parity=None):
     warm = synth.ServeWorkload.__new__(synth.ServeWorkload)
     warm.__dict__.update(wl.__dict__)
     warm.jobs = wl.jobs[:min(200, len(wl.jobs))]
-    serve_drive(ctx, warm, sids, ksids, np.zeros(len(warm.jobs)), buffers[:slots], keep_every)
-    _, cap_s, _ = serve_drive(ctx, wl, sids, ksids, np.zeros(len(wl.jobs)), buffers[:slots], keep_every)
+    serve_drive(ctx, warm, sids, ksids, np.zeros(len(warm.jobs)), buffers[:slots], keep_every, leaf)
+    _, cap_s, _ = serve_drive(ctx, wl, sids, ksids, np.zeros(len(wl.jobs)), buffers[:slots], keep_every, leaf)
     capacity = len(wl.jobs) / cap_s
     lam = 0.8 * capacity
     arrivals = np.cumsum(wl.gaps) / lam
-    lat, wall, kept = serve_drive(ctx, wl, sids, ksids, arrivals, buffers[:slots], keep_every)
+    lat, wall, kept = serve_drive(ctx, wl, sids, ksids, arrivals, buffers[:slots], keep_every, leaf)
     ctx.serve_stop()
     ctx.close()
 
     plain_ctx = Context(device)
-    _, service, plain_closed_s, _ = plain_drive(plain_ctx, warm, np.zeros(len(warm.jobs)), buffers[slots], keep_every)
-    _, service, plain_closed_s, _ = plain_drive(plain_ctx, wl, np.zeros(len(wl.jobs)), buffers[slots], keep_every)
+    _, service, plain_closed_s, _ = plain_drive(plain_ctx, warm, np.zeros(len(warm.jobs)), buffers[slots], keep_every,
+                                                leaf)
+    _, service, plain_closed_s, _ = plain_drive(plain_ctx, wl, np.zeros(len(wl.jobs)), buffers[slots], keep_every,
+                                                leaf)
     plain_capacity = len(wl.jobs) / plain_closed_s
-    plain_lat, _, plain_wall, plain_kept = plain_drive(plain_ctx, wl, arrivals, buffers[slots], keep_every)
+    plain_lat, _, plain_wall, plain_kept = plain_drive(plain_ctx, wl, arrivals, buffers[slots], keep_every, leaf)
     plain_ctx.close()
     for idx, want in plain_kept.items():  # served results equal the regular entry points' results
         got = kept[idx]
-        if isinstance(want, list):
+        if isinstance(want, tuple):
+            assert all((a == b).all() for g_, w_ in zip(got, want) for a, b in zip(g_, w_)), \
+                f"serve/plain mismatch on job {idx}"
+        elif isinstance(want, list):
             assert all((a == b).all() for a, b in zip(got, want)), f"serve/plain mismatch on job {idx}"
         else:
             assert (got == want).all(), f"serve/plain mismatch on job {idx}"
@@ -886,14 +963,28 @@ def run_serve(args, device, world, parity=None):
                 assert np.array_equal(got, port.jv_screen(wl.jv[job[1]])), f"served JV job {idx} differs from the oracle"
             else:
                 g = wl.kopt[job[1]][0]
-                for k, t, a in zip((3, 4, 5), wl.kopt_tasks(job), got):
-                    assert np.array_equal(a, port.kopt_costs_parallel(g, k, t)), f"served k-opt job {idx} differs"
-        parity["serve"] = {"jobs": len(kept), "of": len(wl.jobs), "checked": "every output of every sampled job "
-                           "(each 100th of the Poisson run) against the C oracle and the regular entry points",
-                           "seconds": time.perf_counter() - t0, "ok": True}
-        extra["cpu_baseline"] = cpu_leg(f"serve:{len(wl.jobs)}")
+                for j, (k, t) in enumerate(zip((3, 4, 5), wl.kopt_tasks(job))):
+                    want = port.kopt_costs_parallel(g, k, t)
+                    if not leaf:
+                        assert np.array_equal(got[j], want), f"served k-opt job {idx} differs"
+                        continue
+                    better = want < t["deleted_cost"][:, None]
+                    words = np.zeros_like(got[0][j])
+                    for c in range(want.shape[1]):
+                        words[:, c // 32] |= better[:, c].astype(np.uint32) << np.uint32(c % 32)
+                    first = np.where(better.any(axis=1), better.argmax(axis=1), -1)
+                    assert np.array_equal(got[0][j], words) and np.array_equal(got[1][j], first), \
+                        f"served improving sets of job {idx} differ"
+        parity["serve_leaf" if leaf else "serve"] = {
+            "jobs": len(kept), "of": len(wl.jobs), "checked": "every output of every sampled job "
+            "(each 100th of the Poisson run) against the C oracle and the regular entry points",
+            "seconds": time.perf_counter() - t0, "ok": True}
+        if not leaf:
+            extra["cpu_baseline"] = cpu_leg(f"serve:{len(wl.jobs)}")
     kinds = np.array([j[0] == "jv" for j in wl.jobs])
     per_kind = {"jv": _latency_summary(lat[kinds]), "kopt": _latency_summary(lat[~kinds])}
+    d2h_bytes = sum(_job_output_bytes(wl, j, leaf) for j in wl.jobs)
+    ceiling = pcie_d2h_gbs(device)
     del owners, pinned_pools
     jv_jobs = sum(1 for j in wl.jobs if j[0] == "jv")
     return {
@@ -904,14 +995,21 @@ def run_serve(args, device, world, parity=None):
         "plain": {"capacity_jobs_per_s": plain_capacity, "jobs_per_s": len(wl.jobs) / plain_wall,
                   **_latency_summary(plain_lat), "service_p50_ms": float(np.percentile(service, 50) * 1e3),
                   "service_p99_ms": float(np.percentile(service, 99) * 1e3),
-                  "api": "cee_jv_screen / cee_kopt_costs_multi, one job at a time"},
+                  "api": "cee_jv_screen / " + ("cee_kopt_improving_multi" if leaf else "cee_kopt_costs_multi") +
+                         ", one job at a time"},
         "capacity_speedup": capacity / plain_capacity,
         "per_kind": per_kind,
-        "d2h_bytes": int(sum(wl.output_bytes(j) for j in wl.jobs)),
-        "d2h_gb_per_s_at_capacity": sum(wl.output_bytes(j) for j in wl.jobs) / cap_s / 1e9,
+        "d2h_bytes": int(d2h_bytes),
+        "d2h_gb_per_s_at_capacity": d2h_bytes / cap_s / 1e9,
+        "pcie_d2h_gb_per_s": ceiling,
+        "copy_engine_busy_frac": d2h_bytes / 1e9 / ceiling / cap_s,
+        "copy_engine_note": "time the results need at the measured pinned D2H bandwidth (512 MB copies) over the "
+                            "capacity run's wall time: near 1 means the loop is bound by PCIe, not by the SMs",
         "config": f"{len(wl.jobs)} jobs, Poisson arrivals at 0.8 x measured serving capacity; 70% JV epochs on "
                   f"{len(wl.jv)} resident instances of the batching mix (n log-uniform [200,20000]), 30% k-opt "
-                  f"batches of 1k-50k rows (k = 3/4/5 in thirds) on {len(wl.kopt)} resident CEIL_2D instances; "
+                  f"batches of 1k-50k rows (k = 3/4/5 in thirds) on {len(wl.kopt)} resident CEIL_2D instances, "
+                  + ("returning improving-template sets (the fused leaf consume)" if leaf else
+                     "returning full cost matrices") + f"; "
                   f"{slots} slots, k-opt rows and results in pinned host buffers; latency = arrival to results "
                   "on the host",
         "checked_jobs": len(plain_kept),
@@ -949,6 +1047,84 @@ def run_fixed_point(args, device):
             row["speedup_vs_reference"] = rwall / wall
         out.append(row)
     ctx.close()
+    return out
+
+
+def run_reference_gpu(args, device):
+    """The reference's own GPU path on this B200 -- its CUDA units (src/cuda/jv_cuda.cu, kopt_cost.cu,
+    ht_cd.cu) compiled for sm_100a by oracle/Makefile into oracle/_ref/libcudaee_refcuda.so -- against
+    this project's kernels behind the same reference API (oracle/_ref/libcudaee_dropin.so). Each CUDA
+    seam call is timed on the host around the call (its uploads, launch and download included: what
+    the reference's callers wait for), and RunJvElimination(kCuda) is timed end to end."""
+    import oracle
+    from cudaedgeelimination_b200 import synth
+    if not (oracle.reference_available(variant="refcuda") and oracle.reference_available(dropin=True)):
+        return {"unavailable": "oracle/_ref/libcudaee_refcuda.so or libcudaee_dropin.so is not built"}
+    arms = {"reference": oracle.Reference(variant="refcuda"), "ours": oracle.Reference(dropin=True)}
+    out = {"api": "the reference's CUDA seam (FindJvCandidatesCuda, detail::EvaluateKOptTemplateCostsCuda, "
+                  "detail::ScreenHtCdCandidatesCuda) and RunJvElimination(kCuda); reference = its own CUDA units "
+                  "built for sm_100a, ours = the drop-in shim over libcee.so",
+           "timing": "host clock around each call, warm calls (caches filled by a first call, reported apart)"}
+    reps = 7
+    jv = []
+    cases = [("3,000-node clustered (8-NN + quadrant neighbours), EUC_2D", synth.jv_clustered()),
+             ("50,000-node uniform in [0,10^7)^2, 10-NN, EUC_2D", synth.uniform_knn(50_000, 10_000_000, 10, 0, 7))]
+    for name, g in cases:
+        row = {"workload": name, "nodes": g.n, "edges": g.m}
+        witnesses = {}
+        for arm, ref in arms.items():
+            ms, w = ref.graph(g).seam_jv_timed(reps)
+            warm = float(np.median(ms[1:]))
+            row[arm] = {"first_call_ms": float(ms[0]), "ms_per_call": warm, "edges_per_s": g.m / (warm / 1e3)}
+            witnesses[arm] = w
+        row["same_witnesses"] = bool(np.array_equal(witnesses["reference"], witnesses["ours"]))
+        row["speedup"] = row["reference"]["ms_per_call"] / row["ours"]["ms_per_call"]
+        jv.append(row)
+    out["jv_seam"] = jv
+    g = cases[0][1]
+    loop = {"workload": cases[0][0]}
+    records = {}
+    for arm, ref in arms.items():
+        rg = ref.graph(g)
+        t0 = time.perf_counter()
+        stats, rec, _, _ = rg.run_jv(2)
+        loop[arm] = {"ms": (time.perf_counter() - t0) * 1e3, "epochs": int(stats.shape[0])}
+        records[arm] = rec
+    loop["same_records"] = bool(np.array_equal(records["reference"], records["ours"]))
+    loop["speedup"] = loop["reference"]["ms"] / loop["ours"]["ms"]
+    loop["api"] = "RunJvElimination(kCuda) to a fixed point: seam screen, CPU verify, commit, hash per epoch"
+    out["jv_elimination_loop"] = loop
+    kg, tasks = synth.kopt_instance()
+    kopt = {"workload": "200,000 rows k = 3/4/5 in thirds, 15,000-node CEIL_2D", "cells": 0}
+    mats = {}
+    for arm, ref in arms.items():
+        rg = ref.graph(kg)
+        total = first = 0.0
+        mats[arm] = []
+        for k in (3, 4, 5):
+            ms, costs = rg.seam_kopt_timed(k, tasks[k], 4)
+            total += float(np.median(ms[1:]))
+            first += float(ms[0])
+            mats[arm].append(costs)
+        kopt[arm] = {"ms_per_matrix": total, "first_call_ms": first}
+    kopt["cells"] = int(sum(m.size for m in mats["ours"]))
+    for arm in arms:
+        kopt[arm]["cells_per_s"] = kopt["cells"] / (kopt[arm]["ms_per_matrix"] / 1e3)
+    kopt["same_cells"] = all(np.array_equal(a, b) for a, b in zip(mats["reference"], mats["ours"]))
+    kopt["speedup"] = kopt["reference"]["ms_per_matrix"] / kopt["ours"]["ms_per_matrix"]
+    out["kopt_seam"] = kopt
+    batch = synth.BatchUnion(256)
+    cd = {"workload": "the first 256 instances of the batching mix, their first 64 targets each "
+                      "(neighbourhood 25, degree cap 50, active-incompatible); task lists built before timing"}
+    flags = {}
+    for arm, ref in arms.items():
+        rb = ref.batch_graphs(batch)
+        sec, count, set_ = rb.seam_cd_timed(list(range(batch.count)))
+        cd[arm] = {"seconds": sec, "cd_tasks": count, "cd_tasks_per_s": count / sec}
+        flags[arm] = (count, set_)
+    cd["same_flags_checksum"] = flags["reference"] == flags["ours"]
+    cd["speedup"] = cd["reference"]["seconds"] / cd["ours"]["seconds"]
+    out["cd_seam"] = cd
     return out
 
 

@@ -83,6 +83,10 @@ class BatchTuning(ctypes.Structure):
     _fields_ = [("jv_tile", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32), ("chunks", ctypes.c_int32)]
 
 
+class KoptTuning(ctypes.Structure):
+    _fields_ = [("kernel", ctypes.c_int32), ("rows_per_tile", ctypes.c_int32 * 3), ("ms", ctypes.c_float)]
+
+
 class BatchStats(ctypes.Structure):
     _fields_ = [("nodes", ctypes.c_int64), ("edges", ctypes.c_int64), ("adjacency", ctypes.c_int64),
                 ("targets", ctypes.c_int64), ("pairs", ctypes.c_int64), ("flag_words", ctypes.c_int64),
@@ -132,6 +136,10 @@ def lib() -> ctypes.CDLL:
             "cee_last_error": (ctypes.c_char_p, [vp]),
             "cee_ctx_device": (ctypes.c_int, [vp]),
             "cee_ctx_stream": (vp, [vp]),
+            "cee_ctx_sm_count": (ctypes.c_int, [vp]),
+            "cee_kopt_set_tuning": (ctypes.c_int, [vp, ctypes.POINTER(KoptTuning)]),
+            "cee_kopt_get_tuning": (ctypes.c_int, [vp, ctypes.POINTER(KoptTuning)]),
+            "cee_kopt_autotune": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.POINTER(KoptTuning)]),
             "cee_ctx_synchronize": (ctypes.c_int, [vp]),
             "cee_ctx_resident_bytes": (ctypes.c_uint64, [vp]),
             "cee_ctx_clear": (ctypes.c_int, [vp, ctypes.c_uint]),
@@ -190,6 +198,10 @@ def lib() -> ctypes.CDLL:
             "cee_serve_submit_kopt": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint32),
                                                      ctypes.POINTER(vp), c_i64p, ctypes.POINTER(vp), ctypes.c_uint64,
                                                      c_i32p]),
+            "cee_serve_submit_kopt_improving": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32,
+                                                               ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(vp),
+                                                               c_i64p, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                                               ctypes.POINTER(vp), ctypes.c_uint64, c_i32p]),
             "cee_serve_poll": (ctypes.c_int, [vp, ctypes.POINTER(ServeEvent), ctypes.c_int32, c_i32p]),
             "cee_serve_pending": (ctypes.c_int, [vp, c_i32p, c_u64p]),
             "cee_serve_stop": (ctypes.c_int, [vp]),

@@ -14,6 +14,10 @@ per-device caches (src/cuda/jv_cuda.cu:138-139). Errors raise NativeError (a Run
 from __future__ import annotations
 
 import ctypes
+import json
+import math
+import os
+import pathlib
 import threading
 from dataclasses import dataclass
 
@@ -194,9 +198,23 @@ class BatchMixin:
         t = _native.BatchTuning(jv_tile, blocks_per_sm, chunks)
         _native.check(self.handle, _native.lib().cee_batch_set_tuning(self.handle, ctypes.byref(t)))
 
-    def batch_autotune(self, reps: int = 3) -> _native.BatchTuning:
+    def batch_autotune(self, reps: int = 3, cache: "TuningCache | None" = None) -> _native.BatchTuning:
+        """cee_batch_autotune on the prepared batch. With a cache, a shape stored for this device's SM
+        count and the batch's size bucket is applied instead of timing, and a timed one is stored."""
+        key = None
+        if cache is not None and getattr(self, "_batch", None) is not None:
+            batch, graph, _ = self._batch
+            sizes = np.diff(np.asarray(batch.node_begin, np.int64))
+            key = cache.key(self.sm_count, "batch", largest_instance=int(sizes.max(initial=0)),
+                            instances=int(sizes.shape[0]), edges=int(graph.m))
+            hit = cache.get(key)
+            if hit is not None:
+                self.set_batch_tuning(hit["jv_tile"], hit["blocks_per_sm"], hit["chunks"])
+                return _native.BatchTuning(hit["jv_tile"], hit["blocks_per_sm"], hit["chunks"])
         t = _native.BatchTuning()
         _native.check(self.handle, _native.lib().cee_batch_autotune(self.handle, reps, ctypes.byref(t)))
+        if key is not None:
+            cache.put(key, {"jv_tile": t.jv_tile, "blocks_per_sm": t.blocks_per_sm, "chunks": t.chunks})
         return t
 
 
@@ -270,6 +288,33 @@ class ServeMixin:
         self._serve_jobs[job.value] = outs
         return job.value
 
+    def serve_submit_kopt_improving(self, sid: int, ks, task_lists, tag: int = 0, outs=None) -> int | None:
+        """The same k-opt job returning kopt_improving_multi's outputs instead of the cost matrices:
+        serve_poll gives (masks, firsts), one array of each per segment. `outs` = (masks, firsts) to
+        write into (caller buffers, e.g. page-locked)."""
+        tasks = [np.ascontiguousarray(t, dtype=KOPT_TASK_DTYPE) for t in task_lists]
+        n = len(ks)
+        if outs is None:
+            masks = [np.empty((t.shape[0], (KOPT_TEMPLATE_COUNTS.get(k, 0) + 31) // 32), np.uint32)
+                     for k, t in zip(ks, tasks)]
+            firsts = [np.empty(t.shape[0], np.int32) for t in tasks]
+        else:
+            masks, firsts = outs
+        karr = (ctypes.c_uint32 * n)(*ks)
+        tptr = (ctypes.c_void_p * n)(*[t.ctypes.data for t in tasks])
+        rows = np.array([t.shape[0] for t in tasks], np.int64)
+        mptr = (ctypes.c_void_p * n)(*[m.ctypes.data for m in masks])
+        fptr = (ctypes.c_void_p * n)(*[f.ctypes.data for f in firsts])
+        job = ctypes.c_int32(-1)
+        rc = _native.lib().cee_serve_submit_kopt_improving(self.handle, sid, n, karr, tptr,
+                                                           rows.ctypes.data_as(_native.c_i64p), mptr, fptr, None,
+                                                           tag, ctypes.byref(job))
+        if rc == _native.CEE_BUSY:
+            return None
+        _native.check(self.handle, rc)
+        self._serve_jobs[job.value] = (masks, firsts)
+        return job.value
+
     def serve_poll(self, capacity: int = 256, with_status: bool = False):
         """Completed jobs as (job, tag, outputs) tuples; a job that failed raises NativeError, unless
         with_status, which returns (job, tag, outputs, status) tuples instead."""
@@ -297,6 +342,43 @@ class ServeMixin:
         _native.check(self.handle, _native.lib().cee_serve_stop(self.handle))
 
 
+class TuningCache:
+    """Launch shapes chosen by the autotuners, kept in a JSON file across runs and keyed by the
+    device's SM count and a size bucket of the workload (each size rounded to a power of two), so
+    that a later run on a similar workload applies the stored shape without timing. The file is
+    $CEE_TUNING_CACHE, else ~/.cache/cudaedgeelimination_b200/tuning.json, unless a path is given."""
+
+    VERSION = 1
+
+    def __init__(self, path: str | os.PathLike | None = None):
+        default = pathlib.Path.home() / ".cache" / "cudaedgeelimination_b200" / "tuning.json"
+        self.path = pathlib.Path(path or os.environ.get("CEE_TUNING_CACHE") or default)
+        self._entries = {}
+        try:
+            data = json.loads(self.path.read_text())
+            if data.get("version") == self.VERSION:
+                self._entries = dict(data.get("entries", {}))
+        except (OSError, ValueError):
+            pass
+
+    @staticmethod
+    def bucket(value: int) -> int:
+        return 0 if value <= 0 else 1 << math.ceil(math.log2(value))
+
+    def key(self, sm_count: int, kind: str, **sizes: int) -> str:
+        return f"sm{sm_count}/{kind}/" + ",".join(f"{k}={self.bucket(v)}" for k, v in sorted(sizes.items()))
+
+    def get(self, key: str):
+        return self._entries.get(key)
+
+    def put(self, key: str, value: dict) -> None:
+        self._entries[key] = value
+        self.path.parent.mkdir(parents=True, exist_ok=True)
+        tmp = self.path.with_suffix(f".{os.getpid()}.tmp")
+        tmp.write_text(json.dumps({"version": self.VERSION, "entries": self._entries}, indent=1, sort_keys=True))
+        os.replace(tmp, self.path)
+
+
 class Context(BatchMixin, ServeMixin):
     """One cee_ctx: a device, a stream and the resident caches."""
 
@@ -321,6 +403,10 @@ class Context(BatchMixin, ServeMixin):
     @property
     def stream(self) -> int:
         return _native.lib().cee_ctx_stream(self.handle) or 0
+
+    @property
+    def sm_count(self) -> int:
+        return int(_native.lib().cee_ctx_sm_count(self.handle))
 
     def synchronize(self) -> None:
         _native.check(self.handle, _native.lib().cee_ctx_synchronize(self.handle))
@@ -458,6 +544,9 @@ class Context(BatchMixin, ServeMixin):
 
     def kopt_prepare_multi(self, graph: GraphSnapshot, ks, task_lists) -> _native.KoptStats:
         tasks, karr, tptr, rows = self._multi_args(ks, task_lists)
+        self._kopt_rows = {}
+        for k, r in zip(ks, rows):
+            self._kopt_rows[int(k)] = self._kopt_rows.get(int(k), 0) + int(r)
         stats = _native.KoptStats()
         _native.check(self.handle, _native.lib().cee_kopt_prepare_multi(
             self.handle, graph.n, graph.dist_type, graph.x.ctypes.data_as(_native.c_i64p),
@@ -467,6 +556,32 @@ class Context(BatchMixin, ServeMixin):
 
     def kopt_launch(self) -> None:
         _native.check(self.handle, _native.lib().cee_kopt_launch(self.handle))
+
+    def kopt_tuning(self) -> _native.KoptTuning:
+        t = _native.KoptTuning()
+        _native.check(self.handle, _native.lib().cee_kopt_get_tuning(self.handle, ctypes.byref(t)))
+        return t
+
+    def set_kopt_tuning(self, kernel: int, rows_per_tile=(0, 0, 0)) -> None:
+        t = _native.KoptTuning(kernel, (ctypes.c_int32 * 3)(*rows_per_tile), 0.0)
+        _native.check(self.handle, _native.lib().cee_kopt_set_tuning(self.handle, ctypes.byref(t)))
+
+    def kopt_autotune(self, reps: int = 3, cache: "TuningCache | None" = None) -> _native.KoptTuning:
+        """cee_kopt_autotune on the prepared k-opt launch (see kopt_prepare_multi). With a cache, a shape
+        stored for this device's SM count and the launch's rows per k is applied instead of timing,
+        and a timed one is stored."""
+        key = None
+        if cache is not None and getattr(self, "_kopt_rows", None) is not None:
+            key = cache.key(self.sm_count, "kopt", **{f"k{k}_rows": r for k, r in self._kopt_rows.items()})
+            hit = cache.get(key)
+            if hit is not None:
+                self.set_kopt_tuning(hit["kernel"], hit["rows_per_tile"])
+                return self.kopt_tuning()
+        t = _native.KoptTuning()
+        _native.check(self.handle, _native.lib().cee_kopt_autotune(self.handle, reps, ctypes.byref(t)))
+        if key is not None:
+            cache.put(key, {"kernel": t.kernel, "rows_per_tile": list(t.rows_per_tile), "ms": t.ms})
+        return t
 
     def kopt_fetch(self, outs) -> None:
         optr = (ctypes.c_void_p * len(outs))(*[o.ctypes.data for o in outs])

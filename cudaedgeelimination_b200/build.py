@@ -40,7 +40,7 @@ def reference_dir() -> pathlib.Path | None:
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-Wall", f"-I{INCLUDE}", f"-I{CSRC}"]
-CUDA_SOURCES = ["cee_api.cu", "batch.cu", "noalloc.cu", "serve.cu", "epoch.cu", "proof.cu"]
+CUDA_SOURCES = ["cee_api.cu", "batch.cu", "noalloc.cu", "serve.cu", "epoch.cu", "proof.cu", "host_copy.cu"]
 
 
 def _host_cxx() -> str:
@@ -102,15 +102,16 @@ def build_synth(force: bool = False) -> pathlib.Path:
 
 def build_oracle(force: bool = False) -> None:
     """The plain-C oracle; plus, when the reference tree is present, the reference library
-    compiled from its own sources, the reference with this project's shim dropped in, and the
-    reference's own unit tests built against each of the two."""
+    compiled from its own sources, the reference with this project's shim dropped in, the
+    reference with its own CUDA units built for sm_100a (the GPU comparison arm), and the
+    reference's own unit tests built against the first two."""
     reference = reference_dir()
     make = ["make", "-C", str(ORACLE)] + ([f"REF={reference}"] if reference is not None else [])
     if force:
         _run(make + ["clean"])
     _run(make + ["port"])
     if reference is not None:
-        _run(make + ["-j8", "ref", "dropin"])
+        _run(make + ["-j8", "ref", "dropin", "refcuda"])
         _run(make + ["-j8", "unit"])
     else:
         print("reference sources not found (set CEE_REFERENCE_DIR): the reference library is not rebuilt",

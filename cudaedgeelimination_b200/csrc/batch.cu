@@ -45,6 +45,7 @@ struct BatchState {
   std::vector<int64_t> node_begin, edge_begin;
   std::vector<int64_t> chunk_begin;  // spatial chunks per instance (batch_screen.cuh)
   int spatial_keys = 0;               // padded key count of the largest chunked instance
+  bool local = false;                 // every instance has at most kJvLocalSpan nodes
   // the union snapshot in the kernels' layout
   DevBuf d_node_begin, d_edge_begin, xy, uv, w32, active, ro, nbr, ids, slot4;
   // raw uploads of the end-to-end call (converted on the device)
@@ -270,8 +271,10 @@ void SetShape(BatchState& s, const cee_batch_view* b, const cee_batch_options* o
   s.edge_begin.assign(b->edge_begin, b->edge_begin + b->instances + 1);
   s.chunk_begin.assign(static_cast<size_t>(b->instances) + 1, 0);
   s.spatial_keys = 0;
+  s.local = true;
   for (int32_t i = 0; i < b->instances; ++i) {
     const int64_t n = b->node_begin[i + 1] - b->node_begin[i];
+    s.local = s.local && n <= kJvLocalSpan;
     const int64_t chunks = n <= kSpatialMaxNodes ? (n + kSpatialChunk - 1) / kSpatialChunk : 0;
     s.chunk_begin[i + 1] = s.chunk_begin[i] + chunks;
     if (chunks > 0) {
@@ -348,7 +351,10 @@ cudaError_t QueryBatchOccupancy(BatchState& s) {
   for (int span = 0; span < kSpanClasses && status == cudaSuccess; ++span) {
     WithSpan(span, [&](auto S) {
       int blocks = 0;
-      status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, batch_screen_kernel<S.value>, kBatchWarps * 32, 0);
+      status = s.local ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, batch_screen_kernel<S.value, true>,
+                                                                       kBatchWarps * 32, 0)
+                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, batch_screen_kernel<S.value, false>,
+                                                                       kBatchWarps * 32, 0);
       s.occupancy[span] = std::max(1, blocks);
     });
   }
@@ -368,7 +374,13 @@ int LaunchRange(cee_ctx* ctx, BatchState& s, int32_t first, int32_t count, int c
   cudaMemsetAsync(A.counter, 0, sizeof(unsigned long long), stream);
   cudaMemsetAsync(A.ready + first, 0, static_cast<size_t>(count) * 4, stream);
   const int blocks = Grid(ctx, s, items);
-  WithSpan(s.span, [&](auto S) { batch_screen_kernel<S.value><<<blocks, kBatchWarps * 32, 0, stream>>>(A); });
+  WithSpan(s.span, [&](auto S) {
+    if (s.local) {
+      batch_screen_kernel<S.value, true><<<blocks, kBatchWarps * 32, 0, stream>>>(A);
+    } else {
+      batch_screen_kernel<S.value, false><<<blocks, kBatchWarps * 32, 0, stream>>>(A);
+    }
+  });
   if (A.max_cd > 0) {  // FinalizeCdCandidates for every target of the range
     const int fin_blocks = GridFor(static_cast<int64_t>(count) * s.opt.targets, kBatchWarps, ctx->sm_count * 8);
     WithSpan(s.span, [&](auto S) { batch_finalize_kernel<S.value><<<fin_blocks, kBatchWarps * 32, 0, stream>>>(A); });

@@ -533,9 +533,10 @@ __device__ void batch_cd_target(const BatchArgs& A, int32_t inst, int32_t t, con
   }
 }
 
-template <int kSpan>
 // Eight blocks of eight warps per SM (32 registers, a few spilled): a full SM of warps hides the screen's
 // dependent loads and shuffle latencies better than five blocks at 48 registers (19.7 vs 21.8 ms per step).
+// kLocal: every instance has at most kJvLocalSpan nodes (the JV screen's instance-relative keys).
+template <int kSpan, bool kLocal>
 static __global__ void __launch_bounds__(kBatchWarps * 32, 8) batch_screen_kernel(BatchArgs A) {
   __shared__ BatchWarpScratch scratch[kBatchWarps];
   __shared__ uint8_t pair_i[kBatchMaxPairs], pair_j[kBatchMaxPairs];
@@ -566,7 +567,7 @@ static __global__ void __launch_bounds__(kBatchWarps * 32, 8) batch_screen_kerne
       const int64_t e0 = A.jv_first + (q - n_select) * A.jv_tile;
       const int64_t e1 = min(e0 + A.jv_tile, A.jv_last);
       for (int64_t e = e0; e < e1; ++e) {
-        const int32_t w = jv_screen_edge_warp<kSpan, true>(A.g, e, scratch[warp].jv, lane, A.error);
+        const int32_t w = jv_screen_edge_warp<kSpan, true, kLocal>(A.g, e, scratch[warp].jv, lane, A.error);
         if (lane == 0) A.witness[e] = w;
         __syncwarp();
       }

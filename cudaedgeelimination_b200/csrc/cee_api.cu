@@ -287,12 +287,11 @@ int JvPrepare(cee_ctx* ctx, const cee_graph_view* g, cee_jv_stats* stats) {
     if (status != cudaSuccess) return CudaFail(ctx, status, "JV workspace allocation");
   }
   cudaMemsetAsync(ctx->d_error, 0, sizeof(int32_t), st);
-  cudaMemcpyAsync(s.active.ptr, g->active, m, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(s.ro.ptr, g->row_offsets, (static_cast<size_t>(g->n) + 1) * 4, cudaMemcpyHostToDevice, st);
-  if (adj > 0) {
-    cudaMemcpyAsync(s.nbr.ptr, g->neighbors, adj * 4, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(s.ids.ptr, g->csr_edge_ids, adj * 4, cudaMemcpyHostToDevice, st);
-  }
+  status = CopyFromHost(ctx, s.active.ptr, g->active, m);
+  if (status == cudaSuccess) status = CopyFromHost(ctx, s.ro.ptr, g->row_offsets, (static_cast<size_t>(g->n) + 1) * 4);
+  if (status == cudaSuccess) status = CopyFromHost(ctx, s.nbr.ptr, g->neighbors, adj * 4);
+  if (status == cudaSuccess) status = CopyFromHost(ctx, s.ids.ptr, g->csr_edge_ids, adj * 4);
+  if (status != cudaSuccess) return CudaFail(ctx, status, "JV snapshot upload");
   h2d += static_cast<int64_t>(m + (static_cast<size_t>(g->n) + 1) * 4 + adj * 8);
   cudaEventRecord(ctx->ev[1], st);
   if (adj > 0) {
@@ -369,12 +368,8 @@ int JvFetch(cee_ctx* ctx, int32_t* witness_out) {
   JvState& s = ctx->jv;
   if (!s.prepared) return Fail(ctx, CEE_ERR_STATE, "cee_jv_fetch before cee_jv_prepare");
   if (s.m > 0 && witness_out == nullptr) return Fail(ctx, CEE_ERR_INVALID, "null witness output");
-  if (s.m > 0) {
-    cudaMemcpyAsync(witness_out, s.witness.ptr, static_cast<size_t>(s.m) * 4, cudaMemcpyDeviceToHost,
-                    ctx->stream);
-  }
   cudaMemcpyAsync(ctx->h_error, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
-  const cudaError_t status = cudaStreamSynchronize(ctx->stream);
+  const cudaError_t status = CopyToHost(ctx, witness_out, s.witness.ptr, static_cast<size_t>(s.m) * 4);
   if (status != cudaSuccess) return CudaFail(ctx, status, "JV screen");
   return CheckDeviceError(ctx, "JV screen");
 }
@@ -609,6 +604,20 @@ int KoptTemplatesFor(int k) { return k == 3 ? 4 : (k == 4 ? 25 : 208); }
 
 int DefaultRowsPerTile(uint32_t k) { return k == 3 ? 96 : (k == 4 ? 56 : 32); }  // ~22 KB tiles: nine blocks per SM
 
+// The tiled kernel's tiles of the prepared segments, from the context's rows-per-tile options.
+void KoptRetile(cee_ctx* ctx) {
+  KoptState& s = ctx->kopt;
+  int32_t tile = 0;
+  for (int32_t i = 0; i < s.launch.segments; ++i) {
+    KoptSegment& seg = s.launch.seg[i];
+    const int option = ctx->kopt_rows_per_tile[seg.k - 3];
+    seg.rows_per_tile = option > 0 ? option : DefaultRowsPerTile(static_cast<uint32_t>(seg.k));
+    seg.tile_begin = tile;
+    tile += static_cast<int32_t>((seg.rows + seg.rows_per_tile - 1) / seg.rows_per_tile);
+  }
+  s.tiles = tile;
+}
+
 // Uploads the rows of every segment and records the launch description.
 int KoptPrepareSegments(cee_ctx* ctx, int32_t segments, const uint32_t* ks, const KoptTable* const* tables,
                         const cee_kopt_task* const* tasks, const int64_t* rows, cee_kopt_stats* stats,
@@ -633,7 +642,6 @@ int KoptPrepareSegments(cee_ctx* ctx, int32_t segments, const uint32_t* ks, cons
   cudaEventRecord(ctx->ev[0], st);
   cudaMemsetAsync(ctx->d_error, 0, sizeof(int32_t), st);
   int64_t row_offset = 0;
-  int32_t tile = 0;
   KoptLaunch& L = s.launch;
   L = KoptLaunch{};
   L.segments = segments;
@@ -643,7 +651,8 @@ int KoptPrepareSegments(cee_ctx* ctx, int32_t segments, const uint32_t* ks, cons
   for (int32_t i = 0; i < segments; ++i) {
     const size_t bytes = static_cast<size_t>(rows[i]) * sizeof(cee_kopt_task);
     cee_kopt_task* dst = static_cast<cee_kopt_task*>(s.tasks.ptr) + row_offset;
-    if (bytes > 0) cudaMemcpyAsync(dst, tasks[i], bytes, cudaMemcpyHostToDevice, st);
+    status = CopyFromHost(ctx, dst, tasks[i], bytes);
+    if (status != cudaSuccess) return CudaFail(ctx, status, "k-opt task upload");
     KoptSegment& seg = L.seg[i];
     seg.tasks = reinterpret_cast<const int32_t*>(dst);
     seg.costs = static_cast<int64_t*>(s.costs.ptr) + cost_offset[i];
@@ -655,16 +664,12 @@ int KoptPrepareSegments(cee_ctx* ctx, int32_t segments, const uint32_t* ks, cons
     seg.k = static_cast<int32_t>(ks[i]);
     seg.templates = tables[i]->T;
     seg.write_costs = 1;
-    seg.rows_per_tile = ctx->kopt_rows_per_tile[ks[i] - 3] > 0 ? ctx->kopt_rows_per_tile[ks[i] - 3]
-                                                                : DefaultRowsPerTile(ks[i]);
-    seg.tile_begin = tile;
-    tile += static_cast<int32_t>((rows[i] + seg.rows_per_tile - 1) / seg.rows_per_tile);
     row_offset += rows[i];
     s.seg_rows[i] = rows[i];
     s.seg_T[i] = tables[i]->T;
   }
-  s.tiles = tile;
   s.segments = segments;
+  KoptRetile(ctx);
   cudaEventRecord(ctx->ev[1], st);
   s.prepared = true;
   s.last_h2d_bytes = total_rows * static_cast<int64_t>(sizeof(cee_kopt_task));
@@ -697,7 +702,7 @@ EncodeTiledFn TensorMapEncoder() {
 }
 
 // The tensor map of a k = 5 segment's cost matrix: [rows][208] int64, boxes of 16 cells x 32 rows,
-// 128-byte swizzle (the layout kopt_rows_warp stages).
+// 128-byte swizzle (the layout kopt_proper_rows_warp stages).
 bool EncodeKopt5Map(CUtensorMap* map, int64_t* costs, int64_t rows) {
   const EncodeTiledFn encode = TensorMapEncoder();
   if (encode == nullptr) return false;
@@ -789,13 +794,16 @@ int KoptFetch(cee_ctx* ctx, int64_t* const* costs_out) {
   int64_t bytes = 0;
   for (int32_t i = 0; i < s.segments; ++i) {
     const size_t n = static_cast<size_t>(s.seg_rows[i]) * static_cast<size_t>(s.seg_T[i]) * 8;
-    if (n == 0) continue;
-    if (costs_out[i] == nullptr) return Fail(ctx, CEE_ERR_INVALID, "null k-opt cost output");
-    cudaMemcpyAsync(costs_out[i], s.launch.seg[i].costs, n, cudaMemcpyDeviceToHost, ctx->stream);
-    bytes += static_cast<int64_t>(n);
+    if (n > 0 && costs_out[i] == nullptr) return Fail(ctx, CEE_ERR_INVALID, "null k-opt cost output");
   }
   cudaMemcpyAsync(ctx->h_error, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
-  const cudaError_t status = cudaStreamSynchronize(ctx->stream);
+  cudaError_t status = cudaSuccess;
+  for (int32_t i = 0; i < s.segments && status == cudaSuccess; ++i) {
+    const size_t n = static_cast<size_t>(s.seg_rows[i]) * static_cast<size_t>(s.seg_T[i]) * 8;
+    status = CopyToHost(ctx, costs_out[i], s.launch.seg[i].costs, n);
+    bytes += static_cast<int64_t>(n);
+  }
+  if (status == cudaSuccess) status = cudaStreamSynchronize(ctx->stream);
   if (status != cudaSuccess) return CudaFail(ctx, status, "k-opt cost matrix");
   s.last_d2h_bytes = bytes;
   return CheckDeviceError(ctx, "k-opt cost matrix");
@@ -934,6 +942,7 @@ void cee_destroy(cee_ctx* ctx) {
   ctx->jv.Release();
   ctx->kopt.Release();
   ctx->cd.Release();
+  ctx->stage.Release();
   if (ctx->d_error != nullptr) cudaFree(ctx->d_error);
   if (ctx->h_error != nullptr) cudaFreeHost(ctx->h_error);
   for (auto& ev : ctx->ev) {
@@ -951,6 +960,8 @@ const char* cee_last_error(const cee_ctx* ctx) {
 int cee_ctx_device(const cee_ctx* ctx) { return ctx != nullptr ? ctx->device : -1; }
 
 void* cee_ctx_stream(cee_ctx* ctx) { return ctx != nullptr ? static_cast<void*>(ctx->stream) : nullptr; }
+
+int cee_ctx_sm_count(const cee_ctx* ctx) { return ctx != nullptr ? ctx->sm_count : 0; }
 
 int cee_ctx_synchronize(cee_ctx* ctx) {
   int rc = Activate(ctx);
@@ -999,6 +1010,7 @@ int cee_ctx_set_option(cee_ctx* ctx, int32_t option, int64_t value) {
         return Fail(ctx, CEE_ERR_INVALID, "k-opt rows per tile must be even and fit the shared-memory tile");
       }
       ctx->kopt_rows_per_tile[k - 3] = static_cast<int>(value);
+      if (ctx->kopt.prepared) KoptRetile(ctx);
       return CEE_OK;
     }
     case CEE_OPT_KOPT_KERNEL:
@@ -1123,6 +1135,59 @@ int cee_kopt_launch(cee_ctx* ctx) {
   int rc = Activate(ctx);
   if (rc != CEE_OK) return rc;
   return KoptLaunchPrepared(ctx);
+}
+
+int cee_kopt_set_tuning(cee_ctx* ctx, const cee_kopt_tuning* tuning) {
+  if (ctx == nullptr || tuning == nullptr) return Fail(ctx, CEE_ERR_INVALID, "null k-opt tuning");
+  int rc = cee_ctx_set_option(ctx, CEE_OPT_KOPT_KERNEL, tuning->kernel);
+  for (int k = 0; k < 3 && rc == CEE_OK; ++k) {
+    rc = cee_ctx_set_option(ctx, CEE_OPT_KOPT_ROWS_K3 + k, tuning->rows_per_tile[k]);
+  }
+  return rc;
+}
+
+int cee_kopt_get_tuning(const cee_ctx* ctx, cee_kopt_tuning* tuning) {
+  if (ctx == nullptr || tuning == nullptr) return Fail(nullptr, CEE_ERR_INVALID, "null k-opt tuning");
+  tuning->kernel = ctx->kopt_kernel;
+  for (int k = 0; k < 3; ++k) tuning->rows_per_tile[k] = ctx->kopt_rows_per_tile[k];
+  tuning->ms = 0.0f;
+  return CEE_OK;
+}
+
+int cee_kopt_autotune(cee_ctx* ctx, int32_t reps, cee_kopt_tuning* chosen) {
+  int rc = Activate(ctx);
+  if (rc != CEE_OK) return rc;
+  if (!ctx->kopt.prepared) return Fail(ctx, CEE_ERR_STATE, "cee_kopt_autotune before prepare");
+  reps = std::max(1, reps);
+  std::vector<cee_kopt_tuning> candidates;
+  candidates.push_back({1, {0, 0, 0}, 0.0f});
+  for (const int scale : {1, 2, 4}) {  // half, default and double tiles (even row counts)
+    cee_kopt_tuning t{0, {0, 0, 0}, 0.0f};
+    for (int k = 3; k <= 5; ++k) t.rows_per_tile[k - 3] = std::max(2, DefaultRowsPerTile(k) * scale / 2) & ~1;
+    candidates.push_back(t);
+  }
+  cee_kopt_tuning best{};
+  float best_ms = 1e30f;
+  for (cee_kopt_tuning& t : candidates) {
+    rc = cee_kopt_set_tuning(ctx, &t);
+    if (rc == CEE_OK) rc = KoptLaunchPrepared(ctx);  // warm-up
+    if (rc != CEE_OK) return rc;
+    cudaEventRecord(ctx->ev[4], ctx->stream);
+    for (int r = 0; r < reps && rc == CEE_OK; ++r) rc = KoptLaunchPrepared(ctx);
+    if (rc != CEE_OK) return rc;
+    cudaEventRecord(ctx->ev[5], ctx->stream);
+    const cudaError_t status = cudaEventSynchronize(ctx->ev[5]);
+    if (status != cudaSuccess) return CudaFail(ctx, status, "k-opt autotune");
+    t.ms = EventMs(ctx->ev[4], ctx->ev[5]) / reps;
+    if (t.ms < best_ms) {
+      best_ms = t.ms;
+      best = t;
+    }
+  }
+  rc = cee_kopt_set_tuning(ctx, &best);
+  if (rc != CEE_OK) return rc;
+  if (chosen != nullptr) *chosen = best;
+  return CEE_OK;
 }
 
 int cee_kopt_fetch(cee_ctx* ctx, int64_t* const* costs_out) {

@@ -121,6 +121,22 @@ struct EpochState;
 
 }  // namespace cee
 
+namespace cee {
+// Pinned staging buffers of a context for copies to and from pageable caller memory (host_copy.cu).
+constexpr int kStageBuffers = 3;
+struct HostStage {
+  uint8_t* buf[kStageBuffers] = {};
+  cudaEvent_t ev[kStageBuffers] = {};  // the last copy that used each buffer
+  bool ready = false;
+  void Release();
+};
+// Device -> caller memory on the context's stream; returns after the data is in `dst`.
+cudaError_t CopyToHost(cee_ctx* ctx, void* dst, const void* src, size_t bytes);
+// Caller memory -> device on the context's stream; returns once `src` may be reused (the copy to
+// the device may still be queued on the stream).
+cudaError_t CopyFromHost(cee_ctx* ctx, void* dst, const void* src, size_t bytes);
+}  // namespace cee
+
 struct cee_ctx {
   int device = -1;
   int sm_count = 148;
@@ -141,6 +157,7 @@ struct cee_ctx {
   cee::BatchState* batch = nullptr;
   cee::ServeState* serve = nullptr;
   cee::EpochState* epoch = nullptr;
+  cee::HostStage stage;
 };
 
 namespace cee {

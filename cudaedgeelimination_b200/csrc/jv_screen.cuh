@@ -31,6 +31,9 @@
 namespace cee {
 
 constexpr int kJvMaxCandidates = 10;  // src/cpu/jv_elimination.cpp:28
+// Components (instances) of at most kJvLocalSpan nodes with consecutive ids let the warp screen
+// key candidates by node id relative to the edge's endpoint (the kLocal screens).
+constexpr int kJvLocalSpan = 8192;
 constexpr int kJvWarpsPerBlock = 8;
 constexpr int kJvThreadBlock = 128;
 
@@ -159,8 +162,10 @@ struct JvWarpScratch {
 };
 
 // Screens edge e with the calling (full) warp; returns the witness or -1 on every lane. With
-// kSlot4 a CSR slot's neighbour, weight and neighbour coordinates come from one 16-byte load.
-template <int kSpan, bool kSlot4 = false>
+// kSlot4 a CSR slot's neighbour, weight and neighbour coordinates come from one 16-byte load; with
+// kLocal the caller guarantees that every neighbour of a or b has an id within kJvLocalSpan - 1 of a
+// (the snapshot, or each instance of a batch union, has at most kJvLocalSpan nodes).
+template <int kSpan, bool kSlot4 = false, bool kLocal = false>
 __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t e, JvWarpScratch& s,
                                                        int lane, int32_t* __restrict__ error) {
   if (__ldg(g.active + e) == 0) return -1;
@@ -172,6 +177,10 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
   if (da <= 2 || db <= 2) return -1;
   const int2 pa = __ldg(g.xy + a), pb = __ldg(g.xy + b);
   const int64_t cab = __ldg(g.edge_w + e);
+  // neighbours must lie in [lo, lo + range): the snapshot's ids, or with kLocal also within
+  // kJvLocalSpan - 1 of a (the one test bounds both the gathers and the instance-relative keys)
+  const int32_t lo = kLocal ? max(a - (kJvLocalSpan - 1), 0) : 0;
+  const uint32_t range = static_cast<uint32_t>(kLocal ? min(g.n, a + kJvLocalSpan) - lo : g.n);
 
   uint64_t top = kEmptyKey;
   const int total = da + db;
@@ -193,16 +202,32 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
         c = __ldg(g.nbr + slot);
       }
       ok = c != a && c != b;
-      if (ok && static_cast<uint32_t>(c) >= static_cast<uint32_t>(g.n)) {
+      if (ok && static_cast<uint32_t>(c - lo) >= range) {
         atomicOr(error, 1);
         ok = false;
       }
     }
+#ifndef CEE_JV_MATCH
+#define CEE_JV_MATCH 1
+#endif
     if (total <= 32) {
+#if CEE_JV_MATCH
       // one round: N(a) sits on lanes [0, da), so a node of N(b) already scored through N(a)
       // is found by matching lane values (other lanes hold distinct negative placeholders)
       const unsigned same = __match_any_sync(kFullMask, ok ? c : -1 - lane);
       if (ok && second) ok = (same & ((1u << da) - 1u)) == 0;
+#else
+      // one round: N(a) sits on lanes [0, da) in ascending order, so each lane of N(b) finds its
+      // node there by a binary search over those lanes (five shuffles)
+      int pos = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const int32_t probe = __shfl_sync(kFullMask, c, (pos + step - 1) & 31);
+        if (pos + step <= da && probe < c) pos += step;
+      }
+      const int32_t at = __shfl_sync(kFullMask, c, pos & 31);
+      if (ok && second && pos < da && at == c) ok = false;
+#endif
     } else if (ok && second) {
       ok = !row_contains(g.nbr, ra0, ra1, c);
     }
@@ -215,7 +240,21 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
       score = static_cast<uint64_t>(static_cast<uint32_t>(sw)) + exact_distance<kSpan>(pc, second ? pa : pb, g.dist_type);
       key = (score << 32) | static_cast<uint32_t>(c);
     }
-    if (total <= 32) {
+    if (kLocal && total <= 32) {
+      // kLocal: every node of the edge's component has an id within kJvLocalSpan - 1 of a, so
+      // (score, c - a + kJvLocalSpan) in 32 bits keeps the order of the 64-bit keys whenever every
+      // score fits 18 bits -- one vote instead of the three warp reductions below (a neighbour
+      // outside that range, a CSR row that leaves its instance, failed the bounds test above)
+      if (__all_sync(kFullMask, !ok || score < (1u << 18) - 1u)) {
+        uint32_t k32 = ok ? (static_cast<uint32_t>(score) << 14) | static_cast<uint32_t>(c - a + kJvLocalSpan)
+                          : 0xffffffffu;
+        k32 = warp_sort_asc32(k32, lane);
+        top = k32 == 0xffffffffu ? kEmptyKey
+                                 : (static_cast<uint64_t>(k32 >> 14) << 32) |
+                                       static_cast<uint32_t>(static_cast<int32_t>(k32 & 0x3fffu) - kJvLocalSpan + a);
+        break;
+      }
+    } else if (total <= 32) {
       // compact keys: (score, node - min node) in 32 bits sort in half the shuffles; used when
       // every score and the node spread fit (the order is the same as the 64-bit keys')
       const uint32_t cmin = __reduce_min_sync(kFullMask, ok ? static_cast<uint32_t>(c) : 0xffffffffu);
@@ -292,7 +331,16 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
       const int32_t row = s.row[hi];
       if (hj < s.end[hi] - row) hit = compatible_pair(hi, row + hj);
     }
+#ifndef CEE_JV_HEADVOTE
+#define CEE_JV_HEADVOTE 0
+#endif
+#if CEE_JV_HEADVOTE
+    // candidate i's head pairs sit on lanes 3i .. 3i + 2: lane i folds its three bits of the ballot
+    const uint32_t hits = __ballot_sync(kFullMask, hit);
+    compatible = __ballot_sync(kFullMask, lane < nc && ((hits >> ((kHead * lane) & 31)) & 7u) != 0);
+#else
     compatible = __reduce_or_sync(kFullMask, hit ? 1u << hi : 0u);
+#endif
   }
   const uint32_t all = (1u << nc) - 1u;
   uint32_t open = all & ~compatible;

@@ -321,7 +321,7 @@ __device__ void kopt_general_rows(const KoptLaunch& L, const KoptSegment& S, int
 
 // The warp's rows row0 .. row0 + rows - 1 (rows <= 32) of segment S, row row0 + lane on this lane.
 template <int K, int kSpan, bool kMasks>
-__device__ __forceinline__ void kopt_rows_warp(const KoptLaunch& L, const KoptSegment& S, const CUtensorMap* box5,
+__device__ __forceinline__ void kopt_proper_rows_warp(const KoptLaunch& L, const KoptSegment& S, const CUtensorMap* box5,
                                                int64_t row0, int rows, unsigned char* stage, int32_t* error) {
   using Tab = KoptCanonTable<K>;
   constexpr int P = Tab::P, NP = Tab::NP, T = Tab::T, W = Tab::W;
@@ -495,13 +495,13 @@ static __global__ void __launch_bounds__(kKoptRowThreads, 6)
   unsigned char* stage = kopt_rows_stage(smem, S.k, warp);
   switch (S.k) {
     case 3:
-      kopt_rows_warp<3, kSpan, kMasks>(L, S, &P.box5[si], row0, rows, stage, error);
+      kopt_proper_rows_warp<3, kSpan, kMasks>(L, S, &P.box5[si], row0, rows, stage, error);
       break;
     case 4:
-      kopt_rows_warp<4, kSpan, kMasks>(L, S, &P.box5[si], row0, rows, stage, error);
+      kopt_proper_rows_warp<4, kSpan, kMasks>(L, S, &P.box5[si], row0, rows, stage, error);
       break;
     default:
-      kopt_rows_warp<5, kSpan, kMasks>(L, S, &P.box5[si], row0, rows, stage, error);
+      kopt_proper_rows_warp<5, kSpan, kMasks>(L, S, &P.box5[si], row0, rows, stage, error);
       break;
   }
 }

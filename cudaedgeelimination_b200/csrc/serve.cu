@@ -6,6 +6,8 @@
 
 #include "serve_screen.cuh"
 
+#include <cuda.h>  // CUstream / CUdeviceptr and the stream wait flags (the types only)
+
 #include <algorithm>
 #include <cstring>
 #include <map>
@@ -96,7 +98,24 @@ struct ServeJobHost {
   std::vector<std::pair<size_t, size_t>> regions;  // arena (offset, bytes) to free
   std::vector<Download> downloads;
   cudaEvent_t downloaded = nullptr;
+  bool armed = false;  // the downloads are queued behind a device wait on the job's finished word
 };
+
+// cuStreamWaitValue32, from the driver through the runtime (the library links only cudart).
+using WaitValue32Fn = CUresult (*)(CUstream, CUdeviceptr, cuuint32_t, unsigned int);
+WaitValue32Fn StreamWaitValue32() {
+  static const WaitValue32Fn fn = [] {
+    void* entry = nullptr;
+    cudaDriverEntryPointQueryResult found = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuStreamWaitValue32", &entry, 12000, cudaEnableDefault, &found) !=
+            cudaSuccess ||
+        found != cudaDriverEntryPointSuccess) {
+      return static_cast<WaitValue32Fn>(nullptr);
+    }
+    return reinterpret_cast<WaitValue32Fn>(entry);
+  }();
+  return fn;
+}
 
 }  // namespace
 
@@ -113,6 +132,9 @@ struct ServeState {
   uint8_t* pinned_stage = nullptr;    // snapshot packing
   size_t pinned_stage_bytes = 0;
   cudaStream_t server = nullptr, copy = nullptr, d2h = nullptr;
+  // per slot: the downloads of the slot's job, queued at submission behind a wait for the job's
+  // finished word, so the copy engine starts them the moment the kernel finishes the job
+  cudaStream_t slot_d2h[kServeMaxSlots] = {};
   cudaEvent_t kernel_done = nullptr;
   bool launched = false;
   int grid = 1;
@@ -235,6 +257,40 @@ void ReleaseJob(ServeState& s, ServeJobHost& job) {
   --s.pending;
 }
 
+// Queues the job's downloads on its slot's stream behind a device wait for finished[slot] ==
+// generation (written by the kernel when the job's last item ends), then its download event. Jobs
+// of one slot are armed in submission order, so each waits behind the previous one's copies.
+int ArmDownloads(cee_ctx* ctx, ServeState& s, ServeJobHost& job) {
+  const WaitValue32Fn wait = StreamWaitValue32();
+  if (wait == nullptr) return ServeFail(ctx, CEE_ERR_CUDA, "cuStreamWaitValue32 is not available");
+  cudaStream_t st = s.slot_d2h[job.slot];
+  if (wait(reinterpret_cast<CUstream>(st), reinterpret_cast<CUdeviceptr>(s.finished_dev + job.slot), job.generation,
+           CU_STREAM_WAIT_VALUE_EQ) != CUDA_SUCCESS) {
+    return ServeFail(ctx, CEE_ERR_CUDA, "stream wait on a job's finished word");
+  }
+  const uint8_t* arena = static_cast<const uint8_t*>(s.arena_buf.ptr);
+  for (const Download& d : job.downloads) {
+    cudaMemcpyAsync(d.host, arena + d.device_offset, d.bytes, cudaMemcpyDeviceToHost, st);
+  }
+  cudaError_t status = cudaSuccess;
+  if (job.downloaded == nullptr) status = cudaEventCreateWithFlags(&job.downloaded, cudaEventDisableTiming);
+  if (status == cudaSuccess) status = cudaEventRecord(job.downloaded, st);
+  if (status == cudaSuccess) status = cudaGetLastError();
+  if (status != cudaSuccess) return CudaFail(ctx, status, "serve download queue");
+  job.armed = true;
+  return CEE_OK;
+}
+
+// A job whose finished word the kernel will not write (the loop broke, or it is being torn down):
+// the host writes it, so the waiting downloads run now, and waits for them, so that nothing is
+// written into the job's buffers after it is reported or dropped.
+void DisarmDownloads(ServeState& s, ServeJobHost& job) {
+  if (!job.armed) return;
+  reinterpret_cast<volatile uint32_t*>(s.finished_host)[job.slot] = job.generation;
+  if (job.downloaded != nullptr) cudaEventSynchronize(job.downloaded);
+  job.armed = false;
+}
+
 }  // namespace
 
 void ReleaseServe(cee_ctx* ctx, int32_t* error_word) {
@@ -247,6 +303,12 @@ void ReleaseServe(cee_ctx* ctx, int32_t* error_word) {
   }
   if (s->server != nullptr) cudaStreamSynchronize(s->server);
   if (s->copy != nullptr) cudaStreamSynchronize(s->copy);
+  for (ServeJobHost& job : s->jobs) {
+    if (job.live && job.phase == 0) DisarmDownloads(*s, job);
+  }
+  for (cudaStream_t st : s->slot_d2h) {
+    if (st != nullptr) cudaStreamSynchronize(st);
+  }
   if (s->d2h != nullptr) cudaStreamSynchronize(s->d2h);
   if (error_word != nullptr && s->control.ptr != nullptr) {
     cudaMemcpy(error_word, &static_cast<ServeControl*>(s->control.ptr)->error, sizeof(int32_t), cudaMemcpyDeviceToHost);
@@ -263,6 +325,9 @@ void ReleaseServe(cee_ctx* ctx, int32_t* error_word) {
   if (s->tickets_host != nullptr) cudaFreeHost(s->tickets_host);
   if (s->pinned_stage != nullptr) cudaFreeHost(s->pinned_stage);
   for (cudaStream_t st : {s->server, s->copy, s->d2h}) {
+    if (st != nullptr) cudaStreamDestroy(st);
+  }
+  for (cudaStream_t st : s->slot_d2h) {
     if (st != nullptr) cudaStreamDestroy(st);
   }
   if (s->kernel_done != nullptr) cudaEventDestroy(s->kernel_done);
@@ -316,6 +381,10 @@ int cee_serve_start(cee_ctx* ctx, const cee_serve_config* config) {
   for (cudaStream_t* st : {&s.server, &s.copy, &s.d2h}) {
     if (status == cudaSuccess) status = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
   }
+  for (int i = 0; i < config->slots && status == cudaSuccess; ++i) {
+    status = cudaStreamCreateWithFlags(&s.slot_d2h[i], cudaStreamNonBlocking);
+  }
+  if (status == cudaSuccess && StreamWaitValue32() == nullptr) status = cudaErrorNotSupported;
   if (status == cudaSuccess) status = cudaEventCreateWithFlags(&s.kernel_done, cudaEventDisableTiming);
   int per_sm = 0;
   if (status == cudaSuccess) {
@@ -543,38 +612,51 @@ int cee_serve_submit_jv(cee_ctx* ctx, int32_t snapshot, int32_t* witness_out, ui
   ++snap.refs;
   ++s.pending;
   *job_out = id;
+  rc = ArmDownloads(ctx, s, job);
+  if (rc != CEE_OK) {
+    ReleaseJob(s, job);
+    return rc;
+  }
   return Publish(ctx, s, slot, desc);
 }
 
-int cee_serve_submit_kopt(cee_ctx* ctx, int32_t snapshot, int32_t segments, const uint32_t* ks,
-                          const cee_kopt_task* const* tasks, const int64_t* rows, int64_t* const* costs_out,
-                          uint64_t tag, int32_t* job_out) {
+}  // extern "C"
+
+namespace cee {
+namespace {
+
+// A k-opt job of 1..3 segments: the cost matrices (costs_out, or null for none), and with
+// masks_out / first_out the improving-template sets (cee_kopt_improving_multi's outputs).
+int SubmitKopt(cee_ctx* ctx, int32_t snapshot, int32_t segments, const uint32_t* ks, const cee_kopt_task* const* tasks,
+               const int64_t* rows, int64_t* const* costs_out, uint32_t* const* masks_out, int32_t* const* first_out,
+               uint64_t tag, int32_t* job_out) {
   int rc = Activate(ctx);
   if (rc != CEE_OK) return rc;
   ServeState* sp = Serving(ctx);
   if (sp == nullptr) return ServeFail(ctx, CEE_ERR_STATE, "not started");
   ServeState& s = *sp;
   if (s.broken) return ServeFail(ctx, CEE_ERR_TIMEOUT, "loop lost a work item; restart it");
+  const bool sets = masks_out != nullptr;
   if (snapshot < 0 || snapshot >= static_cast<int>(s.snapshots.size()) || !s.snapshots[snapshot].live ||
-      segments < 1 || segments > 3 || ks == nullptr || tasks == nullptr || rows == nullptr || costs_out == nullptr ||
-      job_out == nullptr) {
+      segments < 1 || segments > 3 || ks == nullptr || tasks == nullptr || rows == nullptr ||
+      (costs_out == nullptr && !sets) || (sets && first_out == nullptr) || job_out == nullptr) {
     return ServeFail(ctx, CEE_ERR_INVALID, "bad k-opt job");
   }
   ServeSnapshotHost& snap = s.snapshots[snapshot];
+  auto words = [](uint32_t k) { return (TemplateCount(static_cast<int>(k)) + 31) / 32; };
+  auto rounded = [](size_t bytes) { return (bytes + 255) & ~size_t{255}; };
   size_t in_bytes = 0, out_bytes = 0;
   int64_t items = 0;
   for (int i = 0; i < segments; ++i) {
-    if (ks[i] < 3 || ks[i] > 5 || rows[i] < 0 || (rows[i] > 0 && (tasks[i] == nullptr || costs_out[i] == nullptr))) {
+    if (ks[i] < 3 || ks[i] > 5 || rows[i] < 0 ||
+        (rows[i] > 0 && (tasks[i] == nullptr || (costs_out != nullptr && costs_out[i] == nullptr) ||
+                         (sets && (masks_out[i] == nullptr || first_out[i] == nullptr))))) {
       return ServeFail(ctx, CEE_ERR_INVALID, "bad k-opt segment");
     }
-    for (int64_t r = 0; r < rows[i]; ++r) {
-      for (uint32_t p = 0; p < 2 * ks[i]; ++p) {
-        const int32_t node = tasks[i][r].port_nodes[p];
-        if (node < 0 || node >= snap.n) return ServeFail(ctx, CEE_ERR_INVALID, "k-opt port node out of range");
-      }
-    }
-    in_bytes += (static_cast<size_t>(rows[i]) * sizeof(cee_kopt_task) + 255) & ~size_t{255};
-    out_bytes += (static_cast<size_t>(rows[i]) * TemplateCount(ks[i]) * 8 + 255) & ~size_t{255};
+    const size_t r = static_cast<size_t>(rows[i]);
+    in_bytes += rounded(r * sizeof(cee_kopt_task));
+    if (costs_out != nullptr) out_bytes += rounded(r * TemplateCount(ks[i]) * 8);
+    if (sets) out_bytes += rounded(r * words(ks[i]) * 4) + rounded(r * 4);
     items += (rows[i] + kServeKoptRowsPerItem - 1) / kServeKoptRowsPerItem;
   }
   const int id = NewJob(s);
@@ -610,20 +692,30 @@ int cee_serve_submit_kopt(cee_ctx* ctx, int32_t snapshot, int32_t segments, cons
   int64_t item_at = 0;
   for (int i = 0; i < segments; ++i) {
     ServeSegment& seg = desc.seg[i];
+    const size_t r = static_cast<size_t>(rows[i]);
     seg.tasks = reinterpret_cast<const int32_t*>(arena + in_at);
-    seg.costs = reinterpret_cast<int64_t*>(arena + out_at);
     seg.rows = rows[i];
     seg.k = static_cast<int32_t>(ks[i]);
     seg.T = TemplateCount(seg.k);
     seg.item_begin = item_at;
     if (rows[i] > 0) {
-      cudaMemcpyAsync(arena + in_at, tasks[i], static_cast<size_t>(rows[i]) * sizeof(cee_kopt_task),
-                      cudaMemcpyHostToDevice, s.copy);
-      job.downloads.push_back({costs_out[i], out_at, static_cast<size_t>(rows[i]) * seg.T * 8});
+      cudaMemcpyAsync(arena + in_at, tasks[i], r * sizeof(cee_kopt_task), cudaMemcpyHostToDevice, s.copy);
+    }
+    in_at += rounded(r * sizeof(cee_kopt_task));
+    if (costs_out != nullptr) {
+      seg.costs = reinterpret_cast<int64_t*>(arena + out_at);
+      if (rows[i] > 0) job.downloads.push_back({costs_out[i], out_at, r * seg.T * 8});
+      out_at += rounded(r * seg.T * 8);
+    }
+    if (sets) {
+      seg.improving = reinterpret_cast<uint32_t*>(arena + out_at);
+      if (rows[i] > 0) job.downloads.push_back({masks_out[i], out_at, r * words(ks[i]) * 4});
+      out_at += rounded(r * words(ks[i]) * 4);
+      seg.first = reinterpret_cast<int32_t*>(arena + out_at);
+      if (rows[i] > 0) job.downloads.push_back({first_out[i], out_at, r * 4});
+      out_at += rounded(r * 4);
     }
     item_at += (rows[i] + kServeKoptRowsPerItem - 1) / kServeKoptRowsPerItem;
-    in_at += (static_cast<size_t>(rows[i]) * sizeof(cee_kopt_task) + 255) & ~size_t{255};
-    out_at += (static_cast<size_t>(rows[i]) * seg.T * 8 + 255) & ~size_t{255};
   }
   desc.items = static_cast<uint32_t>(items);
   s.slot_busy[slot] = true;
@@ -637,7 +729,32 @@ int cee_serve_submit_kopt(cee_ctx* ctx, int32_t snapshot, int32_t segments, cons
   ++snap.refs;
   ++s.pending;
   *job_out = id;
+  rc = ArmDownloads(ctx, s, job);
+  if (rc != CEE_OK) {
+    ReleaseJob(s, job);
+    return rc;
+  }
   return Publish(ctx, s, slot, desc);
+}
+
+}  // namespace
+}  // namespace cee
+
+extern "C" {
+
+int cee_serve_submit_kopt(cee_ctx* ctx, int32_t snapshot, int32_t segments, const uint32_t* ks,
+                          const cee_kopt_task* const* tasks, const int64_t* rows, int64_t* const* costs_out,
+                          uint64_t tag, int32_t* job_out) {
+  if (costs_out == nullptr) return ServeFail(ctx, CEE_ERR_INVALID, "bad k-opt job");
+  return SubmitKopt(ctx, snapshot, segments, ks, tasks, rows, costs_out, nullptr, nullptr, tag, job_out);
+}
+
+int cee_serve_submit_kopt_improving(cee_ctx* ctx, int32_t snapshot, int32_t segments, const uint32_t* ks,
+                                    const cee_kopt_task* const* tasks, const int64_t* rows,
+                                    uint32_t* const* masks_out, int32_t* const* first_out, int64_t* const* costs_out,
+                                    uint64_t tag, int32_t* job_out) {
+  if (masks_out == nullptr || first_out == nullptr) return ServeFail(ctx, CEE_ERR_INVALID, "null improving-set outputs");
+  return SubmitKopt(ctx, snapshot, segments, ks, tasks, rows, costs_out, masks_out, first_out, tag, job_out);
 }
 
 int cee_serve_poll(cee_ctx* ctx, cee_serve_event* events, int32_t capacity, int32_t* count) {
@@ -676,6 +793,7 @@ int cee_serve_poll(cee_ctx* ctx, cee_serve_event* events, int32_t capacity, int3
     if (!job.live || job.phase == 2) continue;
     if (job.phase == 0 && s.broken &&
         *reinterpret_cast<volatile uint32_t*>(s.finished_host + job.slot) != job.generation) {
+      DisarmDownloads(s, job);
       job.status = Fail(ctx, CEE_ERR_TIMEOUT, "serving loop lost a work item; restart it with cee_serve_start");
       if (!report(id, job)) break;
       continue;
@@ -688,12 +806,7 @@ int cee_serve_poll(cee_ctx* ctx, cee_serve_event* events, int32_t capacity, int3
       if (reinterpret_cast<volatile uint32_t*>(s.finished_host)[kServeMaxSlots + job.slot] != 0) {
         job.status = Fail(ctx, CEE_ERR_INVALID, "serving loop: device bounds check rejected an out-of-range index");
       }
-      uint8_t* arena = static_cast<uint8_t*>(s.arena_buf.ptr);
-      for (const Download& d : job.downloads) {
-        cudaMemcpyAsync(d.host, arena + d.device_offset, d.bytes, cudaMemcpyDeviceToHost, s.d2h);
-      }
-      if (job.downloaded == nullptr) cudaEventCreateWithFlags(&job.downloaded, cudaEventDisableTiming);
-      cudaEventRecord(job.downloaded, s.d2h);
+      job.armed = false;  // its downloads were queued at submission and are running now
       job.phase = 1;
     }
     const cudaError_t q = cudaEventQuery(job.downloaded);

@@ -38,10 +38,12 @@ constexpr int kServeKoptRowsPerItem = 64; // k-opt rows per item, processed in c
 
 struct ServeSegment {
   const int32_t* tasks;  // 48-byte rows
-  int64_t* costs;        // rows x T
+  int64_t* costs;        // rows x T, or null (improving sets only)
   int64_t rows;
   int64_t item_begin;    // first item (relative to the job) of this segment
   int32_t k, T, pad0, pad1;
+  uint32_t* improving;   // rows x ceil(T / 32): bit t = template t improves the row, or null
+  int32_t* first;        // rows: the first improving template, or -1
 };
 
 struct ServeJob {
@@ -116,13 +118,39 @@ __device__ void kopt_rows_warp(const ServeSegment& S, int64_t row_begin, int64_t
       kopt_pair_entry<K, kSpan>(sm, r, i - r * NP, xy, dist_type);
     }
     __syncwarp();
-    long long* out = reinterpret_cast<long long*>(S.costs + row0 * T);
-    for (int j = lane; j < rows * T; j += 32) {
-      const int r = j / T, t = j - (j / T) * T;
-      int pid[K];
+    if (S.costs != nullptr) {
+      long long* out = reinterpret_cast<long long*>(S.costs + row0 * T);
+      for (int j = lane; j < rows * T; j += 32) {
+        const int r = j / T, t = j - (j / T) * T;
+        int pid[K];
 #pragma unroll
-      for (int i = 0; i < K; ++i) pid[i] = tpairs[t * K + i];
-      __stcs(out + j, static_cast<long long>(kopt_cell<K, kSpan>(sm, r, pid)));
+        for (int i = 0; i < K; ++i) pid[i] = tpairs[t * K + i];
+        __stcs(out + j, static_cast<long long>(kopt_cell<K, kSpan>(sm, r, pid)));
+      }
+    }
+    if (S.improving != nullptr) {
+      // the fused leaf consume: templates whose cost is below the row's deleted cost, the ones the
+      // reference's consumer tries (src/cpu/kopt_search.cpp:694-715), 32 per ballot
+      constexpr int W = (T + 31) / 32;
+      for (int r = 0; r < rows; ++r) {
+        const int64_t row = row0 + r;
+        const long long deleted = __ldcg(reinterpret_cast<const long long*>(S.tasks + row * 12 + 10));
+        int first = -1;
+        for (int t0 = 0; t0 < T; t0 += 32) {
+          const int t = t0 + lane;
+          long long v = INT64_MAX;
+          if (t < T) {
+            int pid[K];
+#pragma unroll
+            for (int i = 0; i < K; ++i) pid[i] = tpairs[t * K + i];
+            v = static_cast<long long>(kopt_cell<K, kSpan>(sm, r, pid));
+          }
+          const unsigned word = __ballot_sync(kFullMask, t < T && v < deleted);
+          if (lane == 0) S.improving[row * W + t0 / 32] = word;
+          if (first < 0 && word != 0) first = t0 + __ffs(word) - 1;
+        }
+        if (lane == 0) S.first[row] = first;
+      }
     }
   }
   __syncwarp();

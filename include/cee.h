@@ -72,6 +72,8 @@ const char* cee_last_error(const cee_ctx* ctx);
 int cee_ctx_device(const cee_ctx* ctx);
 /* The cudaStream_t every launch of this context goes to. */
 void* cee_ctx_stream(cee_ctx* ctx);
+/* Streaming multiprocessors of the context's device (keys of autotuning caches). */
+int cee_ctx_sm_count(const cee_ctx* ctx);
 int cee_ctx_synchronize(cee_ctx* ctx);
 /* Device bytes currently held by the context's caches and workspaces. */
 uint64_t cee_ctx_resident_bytes(const cee_ctx* ctx);
@@ -349,6 +351,20 @@ int cee_kopt_prepare_multi(cee_ctx* ctx, int32_t n, int32_t dist_type, const int
                            cee_kopt_stats* stats);
 int cee_kopt_launch(cee_ctx* ctx);
 int cee_kopt_fetch(cee_ctx* ctx, int64_t* const* costs_out);
+/* No counterpart in the reference: the launch shape of the k-opt matrix kernels of this context
+ * (the same choices as CEE_OPT_KOPT_KERNEL and CEE_OPT_KOPT_ROWS_K3..K5; results never depend on
+ * it). */
+typedef struct {
+  int32_t kernel;           /* 1 = one thread per row with the proper templates (where it applies), 0 = tiled */
+  int32_t rows_per_tile[3]; /* tiled kernel: rows per tile for k = 3, 4, 5 (0 = default) */
+  float ms;                 /* cee_kopt_autotune: the chosen shape's launch time */
+} cee_kopt_tuning;
+int cee_kopt_set_tuning(cee_ctx* ctx, const cee_kopt_tuning* tuning);
+int cee_kopt_get_tuning(const cee_ctx* ctx, cee_kopt_tuning* tuning);
+/* Times every candidate shape (the row kernel; the tiled kernel with half, default and double
+ * tiles) on the prepared k-opt launch, `reps` launches each (CUDA events), keeps the fastest and
+ * writes it to *chosen. */
+int cee_kopt_autotune(cee_ctx* ctx, int32_t reps, cee_kopt_tuning* chosen);
 
 /* ---- HT c,d root screen --------------------------------------------------------------- */
 
@@ -471,17 +487,30 @@ int cee_serve_submit_jv(cee_ctx* ctx, int32_t snapshot, int32_t* witness_out, ui
 /* k-opt leaf costs of 1..3 segments (k = ks[s], rows[s] rows at tasks[s], output costs_out[s],
  * rows x template_count(k) cells) on the snapshot's coordinates. The task rows go up by a copy
  * queued at submission: pageable rows are staged before the call returns, pinned ones are read
- * while the job runs, so keep them unchanged until cee_serve_poll returns the job.
+ * while the job runs, so keep them unchanged until cee_serve_poll returns the job. The rows are
+ * not read on the host: a port node outside [0, n) is found by the device's bounds checks, and
+ * the job then completes with status CEE_ERR_INVALID (other jobs are unaffected).
  * CEE_BUSY: no slot or arena room now. */
 int cee_serve_submit_kopt(cee_ctx* ctx, int32_t snapshot, int32_t segments, const uint32_t* ks,
                           const cee_kopt_task* const* tasks, const int64_t* rows,
                           int64_t* const* costs_out, uint64_t tag, int32_t* job);
+/* The same job producing cee_kopt_improving_multi's outputs: per segment the improving-template
+ * masks (rows x ceil(template_count / 32) words, bit t = template t's cost is below the row's
+ * deleted cost) and the first improving template per row (-1: none); costs_out may be null (no
+ * cost matrix). */
+int cee_serve_submit_kopt_improving(cee_ctx* ctx, int32_t snapshot, int32_t segments, const uint32_t* ks,
+                                    const cee_kopt_task* const* tasks, const int64_t* rows,
+                                    uint32_t* const* masks_out, int32_t* const* first_out,
+                                    int64_t* const* costs_out, uint64_t tag, int32_t* job);
 /* Returns up to `capacity` completed jobs (their host outputs are written) and relaunches the
- * kernel if it went idle while jobs wait. */
+ * kernel if it went idle while jobs wait. A job's downloads are queued at submission behind a
+ * device wait for its completion, so they run as soon as the job ends, whether or not the host
+ * is polling. */
 int cee_serve_poll(cee_ctx* ctx, cee_serve_event* events, int32_t capacity, int32_t* count);
 /* Jobs admitted and not yet returned by cee_serve_poll, and arena bytes in use. */
 int cee_serve_pending(const cee_ctx* ctx, int32_t* jobs, uint64_t* arena_used);
-/* Stops the kernel and frees the arena (outstanding jobs are dropped). */
+/* Stops the kernel and frees the arena. Outstanding jobs are dropped; a dropped job's downloads
+ * (results complete or not) may still write its output buffers until this call returns. */
 int cee_serve_stop(cee_ctx* ctx);
 
 #ifdef __cplusplus

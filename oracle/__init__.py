@@ -3,7 +3,9 @@
   Port       -- oracle/_build/libcee_oracle.so, the plain-C restatement (cee_oracle.c)
   Reference  -- oracle/_ref/libcudaee_ref.so, the reference's own CPU sources compiled by
                 oracle/Makefile (CUDA seam = the reference's stubs), or, with dropin=True,
-                oracle/_ref/libcudaee_dropin.so (CUDA seam = this project's shim over libcee.so)
+                oracle/_ref/libcudaee_dropin.so (CUDA seam = this project's shim over libcee.so),
+                or, with variant="refcuda", oracle/_ref/libcudaee_refcuda.so (CUDA seam = the
+                reference's own CUDA units built for sm_100a: the comparison arm)
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this package, and only
 as the checker or as the timed CPU baseline.
@@ -20,6 +22,8 @@ HERE = pathlib.Path(__file__).resolve().parent
 PORT_LIB = HERE / "_build" / "libcee_oracle.so"
 REF_LIB = HERE / "_ref" / "libcudaee_ref.so"
 DROPIN_LIB = HERE / "_ref" / "libcudaee_dropin.so"
+REFCUDA_LIB = HERE / "_ref" / "libcudaee_refcuda.so"
+LIBS = {"ref": REF_LIB, "dropin": DROPIN_LIB, "refcuda": REFCUDA_LIB}
 
 i32p = ctypes.POINTER(ctypes.c_int32)
 i64p = ctypes.POINTER(ctypes.c_int64)
@@ -295,15 +299,15 @@ class Port:
         return int(self.L.ceo_ht_reply_count(self.graph(g), min(u, v), max(u, v), center))
 
 
-def reference_available(dropin: bool = False) -> bool:
-    return (DROPIN_LIB if dropin else REF_LIB).exists()
+def reference_available(dropin: bool = False, variant: str | None = None) -> bool:
+    return LIBS[variant or ("dropin" if dropin else "ref")].exists()
 
 
 class Reference:
     """The reference library itself (compiled from its sources by oracle/Makefile)."""
 
-    def __init__(self, dropin: bool = False):
-        path = DROPIN_LIB if dropin else REF_LIB
+    def __init__(self, dropin: bool = False, variant: str | None = None):
+        path = LIBS[variant or ("dropin" if dropin else "ref")]
         if not path.exists():
             raise FileNotFoundError(f"{path} is not built (oracle/Makefile needs the reference sources)")
         L = ctypes.CDLL(str(path))
@@ -342,6 +346,11 @@ class Reference:
         L.ref_graph_new_many.argtypes = [ctypes.c_int32, ctypes.c_int] + [vp] * 9
         L.ref_batch_step.argtypes = [vp, ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                      ctypes.c_int, ctypes.c_int32, i64p, i64p]
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.ref_seam_jv_timed.argtypes = [vp, ctypes.c_int32, dp, i32p]
+        L.ref_seam_kopt_timed.argtypes = [vp, ctypes.c_uint32, vp, ctypes.c_int64, ctypes.c_int32, dp, i64p]
+        L.ref_seam_cd_timed.argtypes = [vp, ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                        ctypes.c_int, dp, i64p, i64p]
         self.L = L
 
     def error(self) -> str:
@@ -400,6 +409,14 @@ class RefBatch:
         self.ref._check(self.ref.L.ref_batch_step(chosen, len(instances), targets, nb, max_deg, mode, threads,
                                                   ctypes.byref(edges), ctypes.byref(tasks)))
         return int(edges.value), int(tasks.value)
+
+    def seam_cd_timed(self, instances, targets: int = 64, nb: int = 25, max_deg: int = 50, mode: int = 0):
+        """ref_seam_cd_timed over the given instances: (seconds, c,d tasks screened, flags set)."""
+        chosen = (vp * len(instances))(*[self.handles[i] for i in instances])
+        sec, tasks, flags = ctypes.c_double(0), ctypes.c_int64(0), ctypes.c_int64(0)
+        self.ref._check(self.ref.L.ref_seam_cd_timed(chosen, len(instances), targets, nb, max_deg, mode,
+                                                     ctypes.byref(sec), ctypes.byref(tasks), ctypes.byref(flags)))
+        return float(sec.value), int(tasks.value), int(flags.value)
 
     def __del__(self):
         if getattr(self, "handles", None) is not None:
@@ -480,6 +497,23 @@ class RefGraph:
 
     def jv_verify(self, edge_id: int, witness: int) -> bool:
         return bool(self.ref.L.ref_jv_verify(self.handle, edge_id, witness))
+
+    def seam_jv_timed(self, reps: int):
+        """ref_seam_jv_timed: (ms of each of `reps` FindJvCandidatesCuda calls, last witnesses)."""
+        ms = np.zeros(reps, np.float64)
+        w = np.empty(self.m, np.int32)
+        self.ref._check(self.ref.L.ref_seam_jv_timed(self.handle, reps, _p(ms, ctypes.c_double), _p(w, ctypes.c_int32)))
+        return ms, w
+
+    def seam_kopt_timed(self, k: int, tasks: np.ndarray, reps: int):
+        """ref_seam_kopt_timed: (ms of each of `reps` EvaluateKOptTemplateCostsCuda calls, last matrix)."""
+        tasks = np.ascontiguousarray(tasks)
+        T = {3: 4, 4: 25, 5: 208}[k]
+        ms = np.zeros(reps, np.float64)
+        costs = np.empty((tasks.shape[0], T), np.int64)
+        self.ref._check(self.ref.L.ref_seam_kopt_timed(self.handle, k, tasks.ctypes.data, tasks.shape[0], reps,
+                                                       _p(ms, ctypes.c_double), _p(costs, ctypes.c_int64)))
+        return ms, costs
 
     def run_jv(self, backend: int, max_rounds: int = 100):
         """RunJvElimination in place; backend 1 = CPU, 2 = CUDA. Returns (epoch stats [e,3],

@@ -1,7 +1,8 @@
 // Test infrastructure (oracle). A flat extern "C" view of the reference library's own CPU
 // entry points, so that pytest can drive the reference through ctypes. Linked into
-// oracle/_ref/libcudaee_ref.so (reference CUDA seam = the reference's stubs) and into
-// oracle/_ref/libcudaee_dropin.so (reference CUDA seam = this project's shim).
+// oracle/_ref/libcudaee_ref.so (reference CUDA seam = the reference's stubs), into
+// oracle/_ref/libcudaee_dropin.so (reference CUDA seam = this project's shim) and into
+// oracle/_ref/libcudaee_refcuda.so (reference CUDA seam = the reference's own CUDA units).
 //
 // Every function returns 0 on success and a negative value when the reference threw; the
 // message is then available from ref_last_error().
@@ -12,6 +13,7 @@
 #include "cuda_edge_elimination/local_search.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -288,6 +290,52 @@ int ref_kopt_costs(void* handle, uint32_t k, const void* tasks, int64_t rows, in
 }
 
 void ref_kopt_clear_cuda_cache() { cudaee::detail::ClearKOptCostCudaCache(); }
+
+// The CUDA seam calls themselves, timed on the host (steady clock around each call; each call
+// returns its results to host memory, so it includes its uploads, launch and download). With
+// libcudaee_refcuda.so they run the reference's own kernels, with libcudaee_dropin.so this
+// project's: the same reference API either way. ms[i] = duration of call i; the first call (its
+// caches cold) is reported too.
+
+// FindJvCandidatesCuda (include/cuda_edge_elimination/elimination.hpp:333-338), `reps` calls on
+// one snapshot; the last call's witnesses per edge.
+int ref_seam_jv_timed(void* handle, int32_t reps, double* ms, int32_t* witness_per_edge) {
+  return Guard([&] {
+    const cudaee::GraphSnapshot* graph = AsGraph(handle);
+    std::vector<cudaee::Candidate> candidates;
+    for (int32_t i = 0; i < reps; ++i) {
+      int device = -1;
+      const auto t0 = std::chrono::steady_clock::now();
+      candidates = cudaee::FindJvCandidatesCuda(*graph, &device, nullptr);
+      ms[i] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    std::fill(witness_per_edge, witness_per_edge + graph->edges.size(), -1);
+    for (const auto& c : candidates) witness_per_edge[c.edge_id] = c.witness;
+    return static_cast<int>(candidates.size());
+  });
+}
+
+// detail::EvaluateKOptTemplateCostsCuda (local_search.hpp:235-242) with the proper templates of
+// k, `reps` calls (no CPU certification: that belongs to the dispatcher around the seam); the
+// last call's cost matrix.
+int ref_seam_kopt_timed(void* handle, uint32_t k, const void* tasks, int64_t rows, int32_t reps, double* ms,
+                        int64_t* costs) {
+  return Guard([&] {
+    std::vector<cudaee::KOptCostTask> list(static_cast<std::size_t>(rows));
+    std::memcpy(list.data(), tasks, sizeof(cudaee::KOptCostTask) * list.size());
+    const cudaee::KOptReconnectTable table = cudaee::BuildKOptReconnectTable(k);
+    std::vector<std::int64_t> out;
+    for (int32_t i = 0; i < reps; ++i) {
+      int device = -1;
+      cudaee::KOptCudaCacheUsage cache;
+      const auto t0 = std::chrono::steady_clock::now();
+      out = cudaee::detail::EvaluateKOptTemplateCostsCuda(*AsGraph(handle), table, list, &device, &cache);
+      ms[i] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    std::copy(out.begin(), out.end(), costs);
+    return static_cast<int>(table.templates.size());
+  });
+}
 
 // The OpenMP thread count of the calling thread's next parallel regions (omp_set_num_threads):
 // EvaluateKOptTemplateCosts(kCpu) uses min(kKOptCpuMaxThreads = 8, this, the processor count)

@@ -9,6 +9,7 @@
 #include "cuda_edge_elimination/elimination.hpp"
 
 #include <atomic>
+#include <chrono>
 #include <cstring>
 #include <thread>
 
@@ -99,6 +100,52 @@ int ref_batch_step(void* const* handles, int32_t count, uint32_t targets, uint32
   *edges_out = edges;
   *cd_tasks_out = tasks_screened;
   return failed ? -1 : 0;
+}
+
+// detail::ScreenHtCdCandidatesCuda (include/cuda_edge_elimination/hamilton_tutte.hpp:527-531)
+// over prebuilt snapshots: for each snapshot its first `targets` SelectHtTargetEdgeIds targets,
+// their BuildCdScreenTasks lists built before the clock starts, then every (snapshot, target)
+// screened through the seam, timed on the host (steady clock around all the calls). Writes the
+// seconds, the tasks screened and the flags set (a checksum for comparing two seams).
+int ref_seam_cd_timed(void* const* handles, int32_t count, uint32_t targets, uint32_t max_neighborhood,
+                      uint32_t max_candidate_degree, int mode, double* seconds, int64_t* tasks_out,
+                      int64_t* flags_set) {
+  try {
+    cudaee::HtShallowOptions options;
+    options.max_neighborhood = max_neighborhood;
+    options.max_candidate_degree = max_candidate_degree;
+    struct Item {
+      const cudaee::GraphSnapshot* graph;
+      cudaee::NodeEdge target;
+      std::vector<cudaee::HtCdScreenTask> tasks;
+    };
+    std::vector<Item> items;
+    for (int32_t i = 0; i < count; ++i) {
+      const auto* graph = static_cast<const cudaee::GraphSnapshot*>(handles[i]);
+      const auto ids = cudaee::SelectHtTargetEdgeIds(*graph, cudaee::HtTargetOrder::kWeightDescending);
+      const std::size_t used = std::min<std::size_t>(ids.size(), targets);
+      for (std::size_t t = 0; t < used; ++t) {
+        const cudaee::Edge& e = graph->edges[static_cast<std::size_t>(ids[t])];
+        const cudaee::NodeEdge target{e.u, e.v};
+        items.push_back({graph, target, cudaee::BuildCdScreenTasks(*graph, target, options)});
+      }
+    }
+    int64_t screened = 0, set = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (const Item& item : items) {
+      int device = -1;
+      const auto flags = cudaee::detail::ScreenHtCdCandidatesCuda(*item.graph, item.target, item.tasks,
+                                                                  static_cast<cudaee::HtCdMode>(mode), &device);
+      screened += static_cast<int64_t>(flags.size());
+      for (const std::uint8_t f : flags) set += f;
+    }
+    *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *tasks_out = screened;
+    *flags_set = set;
+    return 0;
+  } catch (...) {
+    return -1;
+  }
 }
 
 } // extern "C"

@@ -170,6 +170,31 @@ def test_unsorted_instance_rejected(ctx):
         ctx.batch_screen(batch, BatchOptions())
 
 
+def test_csr_row_leaving_its_instance(ctx):
+    """Every instance here has at most 8,192 nodes, so the screen keys candidates by node id relative
+    to the edge's endpoint; a CSR row that names a node of another instance more than 8,191 ids away
+    fails the neighbour bounds test (CEE_ERR_INVALID), resident and end to end, and the context stays
+    usable."""
+    from cudaedgeelimination_b200._native import CEE_ERR_INVALID, NativeError
+    batch = TinyBatch([synth.batch_instance(0, n_lo=300, n_hi=300), synth.batch_instance(1, n_lo=8000, n_hi=8000),
+                       synth.batch_instance(2, n_lo=300, n_hi=300)])
+    g = batch.graph.copy()
+    g.neighbors = g.neighbors.copy()
+    far = int(batch.node_begin[3]) - 1  # the last node of the third instance
+    for x in range(0, 300, 37):  # the last slot of a few rows of the first instance (rows stay ascending)
+        g.neighbors[g.row_offsets[x + 1] - 1] = far
+    with pytest.raises(NativeError) as err:
+        ctx.batch_prepare(batch, BatchOptions(), graph=g)
+        ctx.batch_launch()
+        ctx.batch_fetch()
+    assert err.value.code == CEE_ERR_INVALID
+    with pytest.raises(NativeError) as err:
+        ctx.batch_screen(batch, BatchOptions(), graph=g)
+    assert err.value.code == CEE_ERR_INVALID
+    res, _ = ctx.batch_screen(batch, BatchOptions())
+    assert res.witness.shape == (batch.graph.m,)
+
+
 def check_candidates(port, batch, opt, cand, instances):
     """Finalised c,d candidates equal FinalizeCdCandidates over the oracle's tasks and flags."""
     c, d, product, count = cand

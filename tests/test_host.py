@@ -68,3 +68,20 @@ def test_batch_union_matches_instances(port):
         w_inst = port.jv_screen(inst)
         seg = w_union[int(b.edge_begin[i]):int(b.edge_begin[i + 1])]
         np.testing.assert_array_equal(seg, np.where(w_inst >= 0, w_inst + int(b.node_begin[i]), -1))
+
+
+def test_tuning_cache_roundtrip(tmp_path):
+    """Autotuned shapes persist in a JSON file keyed by SM count and power-of-two size buckets."""
+    from cudaedgeelimination_b200 import TuningCache
+    path = tmp_path / "tuning.json"
+    cache = TuningCache(path)
+    key = cache.key(148, "batch", largest_instance=5000, instances=4096, edges=30_775_204)
+    assert key == "sm148/batch/edges=33554432,instances=4096,largest_instance=8192"
+    assert cache.key(148, "batch", largest_instance=4100, instances=4000, edges=17_000_000) == key
+    assert cache.key(132, "batch", largest_instance=5000, instances=4096, edges=30_775_204) != key
+    assert cache.get(key) is None
+    cache.put(key, {"jv_tile": 64, "blocks_per_sm": 8, "chunks": 8})
+    again = TuningCache(path)
+    assert again.get(key) == {"jv_tile": 64, "blocks_per_sm": 8, "chunks": 8}
+    path.write_text('{"version": 0, "entries": {"x": 1}}')  # another format: ignored, not an error
+    assert TuningCache(path).get("x") is None

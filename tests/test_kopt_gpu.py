@@ -218,3 +218,33 @@ def test_improving_sets(kc, port, with_costs):
         if with_costs:
             np.testing.assert_array_equal(costs[seg], oracle_costs[seg])
     assert any((f >= 0).any() for f in firsts) and any((f < 0).any() for f in firsts)
+
+
+def test_autotune_keeps_cells_and_caches_the_shape(ctx, port, tmp_path):
+    """cee_kopt_autotune times the row kernel and three tiled shapes on the prepared launch and keeps
+    the fastest; the cells are the oracle's under the chosen shape, and a second context applies the
+    shape stored in the tuning cache instead of timing."""
+    from cudaedgeelimination_b200 import Context, TuningCache
+    g, tasks = synth.kopt_instance(rows=6000, n=3000)
+    ks = [3, 4, 5]
+    lists = [tasks[k] for k in ks]
+    cache = TuningCache(tmp_path / "tuning.json")
+    try:
+        ctx.kopt_prepare_multi(g, ks, lists)
+        chosen = ctx.kopt_autotune(reps=2, cache=cache)
+        assert chosen.kernel in (0, 1) and chosen.ms > 0
+        ctx.kopt_launch()
+        outs = [np.empty((t.shape[0], {3: 4, 4: 25, 5: 208}[k]), np.int64) for k, t in zip(ks, lists)]
+        ctx.kopt_fetch(outs)
+        for k, t, got in zip(ks, lists, outs):
+            np.testing.assert_array_equal(got, port.kopt_costs(g, k, t))
+        stored = TuningCache(tmp_path / "tuning.json")
+        other = Context(0)
+        try:
+            other.kopt_prepare_multi(g, ks, lists)
+            again = other.kopt_autotune(reps=2, cache=stored)
+            assert again.kernel == chosen.kernel and list(again.rows_per_tile) == list(chosen.rows_per_tile)
+        finally:
+            other.close()
+    finally:
+        ctx.set_kopt_tuning(1, (0, 0, 0))

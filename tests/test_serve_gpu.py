@@ -78,6 +78,12 @@ def job_list(snaps):
             tag += 1
     jobs.append((tag, "ceil", "kopt", ([4, 3], [random_tasks(snaps["ceil"], 4, 50, 61, True),
                                               random_tasks(snaps["ceil"], 3, 1, 62)])))
+    tag += 1
+    # improving-template sets (the fused leaf consume), on walk rows and on random repeated ports
+    jobs.append((tag, "kopt", "improving", ([3, 4, 5], [kt[3][:1000], kt[4][:999], kt[5][:1001]])))
+    tag += 1
+    jobs.append((tag, "wide", "improving", ([5, 4], [random_tasks(snaps["wide"], 5, 130, 71, True),
+                                                   random_tasks(snaps["wide"], 4, 77, 72)])))
     return jobs
 
 
@@ -86,6 +92,8 @@ def run_jobs(c, snaps, ids, jobs):
     for tag, name, kind, payload in jobs:
         if kind == "jv":
             _, seen = submit(c, c.serve_submit_jv, ids[name], snaps[name].m, tag)
+        elif kind == "improving":
+            _, seen = submit(c, c.serve_submit_kopt_improving, ids[name], payload[0], payload[1], tag)
         else:
             _, seen = submit(c, c.serve_submit_kopt, ids[name], payload[0], payload[1], tag)
         results.update(seen)
@@ -98,6 +106,9 @@ def expected(ctx, snaps, job):
     g = snaps[name]
     if kind == "jv":
         return ctx.jv_screen(g)[0]
+    if kind == "improving":
+        masks, firsts, _, _ = ctx.kopt_improving_multi(g, payload[0], payload[1])
+        return masks, firsts
     outs, _ = ctx.kopt_costs_multi(g, payload[0], payload[1])
     return outs
 
@@ -105,6 +116,11 @@ def expected(ctx, snaps, job):
 def assert_same(kind, got, want):
     if kind == "jv":
         np.testing.assert_array_equal(got, want)
+    elif kind == "improving":
+        for got_list, want_list in zip(got, want):
+            assert len(got_list) == len(want_list)
+            for a, b in zip(got_list, want_list):
+                np.testing.assert_array_equal(a, b)
     else:
         assert len(got) == len(want)
         for a, b in zip(got, want):
@@ -145,9 +161,18 @@ def test_oracle_small(port, snapshots):
         sid = c.serve_add_snapshot(g)
         c.serve_submit_jv(sid, g.m, tag=1)
         c.serve_submit_kopt(sid, [4], [k_tasks], tag=2)
-        res = drain(c, 2)
+        c.serve_submit_kopt_improving(sid, [4], [k_tasks], tag=3)
+        res = drain(c, 3)
         np.testing.assert_array_equal(res[1], port.jv_screen(g))
-        np.testing.assert_array_equal(res[2][0], port.kopt_costs(g, 4, k_tasks))
+        costs = port.kopt_costs(g, 4, k_tasks)
+        np.testing.assert_array_equal(res[2][0], costs)
+        better = costs < k_tasks["deleted_cost"][:, None]  # the reference's consumer's test
+        masks, firsts = res[3]
+        want = np.zeros_like(masks[0])
+        for t in range(costs.shape[1]):
+            want[:, t // 32] |= better[:, t].astype(np.uint32) << np.uint32(t % 32)
+        np.testing.assert_array_equal(masks[0], want)
+        np.testing.assert_array_equal(firsts[0], np.where(better.any(axis=1), better.argmax(axis=1), -1))
         c.serve_stop()
     finally:
         c.close()
@@ -214,6 +239,53 @@ def test_admission_and_release(snapshots):
         c.close()
 
 
+def test_downloads_start_without_polling(ctx, snapshots):
+    """A job's downloads are queued at submission behind a device wait for its completion: jobs left
+    alone finish and land in their host buffers with no poll in between, so the first poll after a
+    pause returns every one of them, with the regular entry points' results."""
+    c = Context(0)
+    try:
+        c.serve_start(ServeConfig(hbm_budget_bytes=64 << 20, slots=8, idle_ms=2000))
+        jobs = job_list(snapshots)[:8]
+        ids = {name: c.serve_add_snapshot(snapshots[name]) for name in {j[1] for j in jobs}}
+        for tag, name, kind, payload in jobs:
+            if kind == "jv":
+                assert c.serve_submit_jv(ids[name], snapshots[name].m, tag) is not None
+            else:
+                assert c.serve_submit_kopt(ids[name], payload[0], payload[1], tag) is not None
+        time.sleep(2.0)
+        first = {tag: res for _, tag, res in c.serve_poll()}
+        assert sorted(first) == sorted(j[0] for j in jobs)
+        for job in jobs:
+            assert_same(job[2], first[job[0]], expected(ctx, snapshots, job))
+        c.serve_stop()
+    finally:
+        c.close()
+
+
+def test_stop_with_jobs_in_flight(snapshots):
+    """cee_serve_stop with jobs still on the GPU returns (their queued downloads are released), and
+    the context serves again after a new cee_serve_start."""
+    big = synth.uniform_knn(20_000, 1_000_000, 10, 0, 78)
+    c = Context(0)
+    try:
+        for _ in range(2):
+            c.serve_start(ServeConfig(hbm_budget_bytes=256 << 20, slots=16, idle_ms=50))
+            sid = c.serve_add_snapshot(big)
+            for t in range(16):
+                assert c.serve_submit_jv(sid, big.m, tag=t) is not None
+            t0 = time.monotonic()
+            c.serve_stop()
+            assert time.monotonic() - t0 < 30
+        c.serve_start(ServeConfig(hbm_budget_bytes=64 << 20, slots=4, idle_ms=50))
+        sid = c.serve_add_snapshot(snapshots["small"])
+        c.serve_submit_jv(sid, snapshots["small"].m, tag=7)
+        np.testing.assert_array_equal(drain(c, 1)[7], c.jv_screen(snapshots["small"])[0])
+        c.serve_stop()
+    finally:
+        c.close()
+
+
 def test_empty_jobs(snapshots):
     g = snapshots["small"].copy()
     g.active[:] = 0
@@ -250,11 +322,18 @@ def test_malformed_requests(snapshots):
             with pytest.raises(NativeError) as e:
                 bad()
             assert e.value.code == CEE_ERR_INVALID
+        # a port node out of range is found by the device bounds checks (the submission reads no
+        # row on the host): that job completes with CEE_ERR_INVALID, the next one with CEE_OK
         bad_ports = random_tasks(g, 3, 4, 1)
-        bad_ports["port_nodes"][2, 1] = g.n + 3  # out of range: rejected at submission
-        with pytest.raises(NativeError) as e:
-            c.serve_submit_kopt(sid, [3], [bad_ports], tag=1)
-        assert e.value.code == CEE_ERR_INVALID
+        bad_ports["port_nodes"][2, 1] = g.n + 3
+        bad_id = c.serve_submit_kopt(sid, [3], [bad_ports], tag=1)
+        good_id = c.serve_submit_kopt(sid, [3], [random_tasks(g, 3, 4, 2)], tag=2)
+        status = {}
+        t0 = time.monotonic()
+        while len(status) < 2 and time.monotonic() - t0 < 30:
+            for job, tag, _, st in c.serve_poll(with_status=True):
+                status[job] = st
+        assert status == {bad_id: CEE_ERR_INVALID, good_id: 0}
         assert c.serve_pending()[0] == 0
         c.serve_stop()
     finally:
