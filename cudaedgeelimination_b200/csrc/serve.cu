@@ -6,11 +6,14 @@
 
 #include "serve_screen.cuh"
 
-#include <cuda.h>  // CUstream / CUdeviceptr and the stream wait flags (the types only)
-
 #include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
 #include <cstring>
 #include <map>
+#include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -97,25 +100,21 @@ struct ServeJobHost {
   int status = CEE_OK;
   std::vector<std::pair<size_t, size_t>> regions;  // arena (offset, bytes) to free
   std::vector<Download> downloads;
-  cudaEvent_t downloaded = nullptr;
-  bool armed = false;  // the downloads are queued behind a device wait on the job's finished word
 };
 
-// cuStreamWaitValue32, from the driver through the runtime (the library links only cudart).
-using WaitValue32Fn = CUresult (*)(CUstream, CUdeviceptr, cuuint32_t, unsigned int);
-WaitValue32Fn StreamWaitValue32() {
-  static const WaitValue32Fn fn = [] {
-    void* entry = nullptr;
-    cudaDriverEntryPointQueryResult found = cudaDriverEntryPointSymbolNotFound;
-    if (cudaGetDriverEntryPointByVersion("cuStreamWaitValue32", &entry, 12000, cudaEnableDefault, &found) !=
-            cudaSuccess ||
-        found != cudaDriverEntryPointSuccess) {
-      return static_cast<WaitValue32Fn>(nullptr);
-    }
-    return reinterpret_cast<WaitValue32Fn>(entry);
-  }();
-  return fn;
-}
+// The downloads of a slot's current job, shared by the API thread (which fills the ticket at
+// submission, before publishing the job) and the downloader thread (which issues the copies the
+// moment it sees the job's finished word). Whichever thread first moves state from kArmed to
+// kIssuing issues them; the job is reported once `event` has completed.
+constexpr int kTicketIdle = 0, kTicketArmed = 1, kTicketIssuing = 2, kTicketIssued = 3;
+constexpr int kMaxDownloads = 9;  // three segments x (costs, masks, first)
+struct SlotTicket {
+  std::atomic<int> state{kTicketIdle};
+  uint32_t generation = 0;
+  int count = 0;
+  Download downloads[kMaxDownloads];
+  cudaEvent_t event = nullptr;  // recorded on the download stream after the copies
+};
 
 }  // namespace
 
@@ -132,9 +131,14 @@ struct ServeState {
   uint8_t* pinned_stage = nullptr;    // snapshot packing
   size_t pinned_stage_bytes = 0;
   cudaStream_t server = nullptr, copy = nullptr, d2h = nullptr;
-  // per slot: the downloads of the slot's job, queued at submission behind a wait for the job's
-  // finished word, so the copy engine starts them the moment the kernel finishes the job
-  cudaStream_t slot_d2h[kServeMaxSlots] = {};
+  SlotTicket tickets[kServeMaxSlots];
+  // the downloader thread: issues a job's copies as soon as its finished word lands, whether or not
+  // the caller is polling (it sleeps while no job is armed)
+  std::thread downloader;
+  std::atomic<bool> downloader_stop{false};
+  std::atomic<int> armed{0};
+  std::mutex wake_mutex;
+  std::condition_variable wake;
   cudaEvent_t kernel_done = nullptr;
   bool launched = false;
   int grid = 1;
@@ -225,12 +229,8 @@ int Publish(cee_ctx* ctx, ServeState& s, int slot, const ServeJob& desc) {
   return LaunchServer(ctx, s);
 }
 
-// Clears a job record, keeping its download event for reuse.
-void ResetJob(ServeJobHost& job) {
-  cudaEvent_t ev = job.downloaded;
-  job = ServeJobHost{};
-  job.downloaded = ev;
-}
+// Clears a job record.
+void ResetJob(ServeJobHost& job) { job = ServeJobHost{}; }
 
 int NewJob(ServeState& s) {
   for (int i = 0; i < static_cast<int>(s.jobs.size()); ++i) {
@@ -244,7 +244,10 @@ void ReleaseJob(ServeState& s, ServeJobHost& job) {
   for (const auto& [offset, bytes] : job.regions) s.arena.Free(offset, bytes);
   job.regions.clear();
   job.downloads.clear();
-  if (job.slot >= 0) s.slot_busy[job.slot] = false;
+  if (job.slot >= 0) {
+    s.tickets[job.slot].state.store(kTicketIdle, std::memory_order_release);
+    s.slot_busy[job.slot] = false;
+  }
   if (job.snapshot >= 0) {
     ServeSnapshotHost& snap = s.snapshots[job.snapshot];
     --snap.refs;
@@ -257,38 +260,81 @@ void ReleaseJob(ServeState& s, ServeJobHost& job) {
   --s.pending;
 }
 
-// Queues the job's downloads on its slot's stream behind a device wait for finished[slot] ==
-// generation (written by the kernel when the job's last item ends), then its download event. Jobs
-// of one slot are armed in submission order, so each waits behind the previous one's copies.
+// Fills the slot's ticket with the job's downloads and arms it (before the job is published, so the
+// finished word of this generation cannot land before the ticket is armed).
 int ArmDownloads(cee_ctx* ctx, ServeState& s, ServeJobHost& job) {
-  const WaitValue32Fn wait = StreamWaitValue32();
-  if (wait == nullptr) return ServeFail(ctx, CEE_ERR_CUDA, "cuStreamWaitValue32 is not available");
-  cudaStream_t st = s.slot_d2h[job.slot];
-  if (wait(reinterpret_cast<CUstream>(st), reinterpret_cast<CUdeviceptr>(s.finished_dev + job.slot), job.generation,
-           CU_STREAM_WAIT_VALUE_EQ) != CUDA_SUCCESS) {
-    return ServeFail(ctx, CEE_ERR_CUDA, "stream wait on a job's finished word");
+  SlotTicket& t = s.tickets[job.slot];
+  if (static_cast<int>(job.downloads.size()) > kMaxDownloads) return ServeFail(ctx, CEE_ERR_INVALID, "too many outputs");
+  if (t.event == nullptr) {
+    const cudaError_t status = cudaEventCreateWithFlags(&t.event, cudaEventDisableTiming);
+    if (status != cudaSuccess) return CudaFail(ctx, status, "serve download event");
   }
-  const uint8_t* arena = static_cast<const uint8_t*>(s.arena_buf.ptr);
-  for (const Download& d : job.downloads) {
-    cudaMemcpyAsync(d.host, arena + d.device_offset, d.bytes, cudaMemcpyDeviceToHost, st);
+  t.generation = job.generation;
+  t.count = static_cast<int>(job.downloads.size());
+  for (int i = 0; i < t.count; ++i) t.downloads[i] = job.downloads[static_cast<size_t>(i)];
+  t.state.store(kTicketArmed, std::memory_order_release);
+  {
+    std::lock_guard<std::mutex> lock(s.wake_mutex);
+    s.armed.fetch_add(1);
   }
-  cudaError_t status = cudaSuccess;
-  if (job.downloaded == nullptr) status = cudaEventCreateWithFlags(&job.downloaded, cudaEventDisableTiming);
-  if (status == cudaSuccess) status = cudaEventRecord(job.downloaded, st);
-  if (status == cudaSuccess) status = cudaGetLastError();
-  if (status != cudaSuccess) return CudaFail(ctx, status, "serve download queue");
-  job.armed = true;
+  s.wake.notify_one();
   return CEE_OK;
 }
 
-// A job whose finished word the kernel will not write (the loop broke, or it is being torn down):
-// the host writes it, so the waiting downloads run now, and waits for them, so that nothing is
-// written into the job's buffers after it is reported or dropped.
-void DisarmDownloads(ServeState& s, ServeJobHost& job) {
-  if (!job.armed) return;
-  reinterpret_cast<volatile uint32_t*>(s.finished_host)[job.slot] = job.generation;
-  if (job.downloaded != nullptr) cudaEventSynchronize(job.downloaded);
-  job.armed = false;
+// Issues the slot's downloads if its ticket is armed and no other thread got there first.
+void IssueDownloads(ServeState& s, int slot) {
+  SlotTicket& t = s.tickets[slot];
+  int expected = kTicketArmed;
+  if (!t.state.compare_exchange_strong(expected, kTicketIssuing, std::memory_order_acq_rel)) return;
+  const uint8_t* arena = static_cast<const uint8_t*>(s.arena_buf.ptr);
+  for (int i = 0; i < t.count; ++i) {
+    cudaMemcpyAsync(t.downloads[i].host, arena + t.downloads[i].device_offset, t.downloads[i].bytes,
+                    cudaMemcpyDeviceToHost, s.d2h);
+  }
+  cudaEventRecord(t.event, s.d2h);
+  s.armed.fetch_sub(1);
+  t.state.store(kTicketIssued, std::memory_order_release);
+}
+
+bool Finished(const ServeState& s, int slot, uint32_t generation) {
+  return reinterpret_cast<const volatile uint32_t*>(s.finished_host)[slot] == generation;
+}
+
+void DownloaderLoop(ServeState* s, int device) {
+  cudaSetDevice(device);
+  while (!s->downloader_stop.load()) {
+    if (s->armed.load() == 0) {
+      std::unique_lock<std::mutex> lock(s->wake_mutex);
+      s->wake.wait_for(lock, std::chrono::milliseconds(50),
+                       [s] { return s->downloader_stop.load() || s->armed.load() > 0; });
+      continue;
+    }
+    for (int slot = 0; slot < s->cfg.slots; ++slot) {
+      SlotTicket& t = s->tickets[slot];
+      if (t.state.load(std::memory_order_acquire) == kTicketArmed && Finished(*s, slot, t.generation)) {
+        IssueDownloads(*s, slot);
+      }
+    }
+    std::this_thread::yield();
+  }
+}
+
+// The ticket of a job that will not finish (the loop broke): nothing is issued for it any more.
+void DropTicket(ServeState& s, int slot) {
+  SlotTicket& t = s.tickets[slot];
+  int expected = kTicketArmed;
+  if (t.state.compare_exchange_strong(expected, kTicketIdle, std::memory_order_acq_rel)) s.armed.fetch_sub(1);
+  while (t.state.load(std::memory_order_acquire) == kTicketIssuing) std::this_thread::yield();
+}
+
+void StopDownloader(ServeState& s) {
+  if (!s.downloader.joinable()) return;
+  {
+    std::lock_guard<std::mutex> lock(s.wake_mutex);
+    s.downloader_stop.store(true);
+  }
+  s.wake.notify_one();
+  s.downloader.join();
 }
 
 }  // namespace
@@ -301,20 +347,15 @@ void ReleaseServe(cee_ctx* ctx, int32_t* error_word) {
     const uint32_t one = 1;
     cudaMemcpy(&static_cast<ServeControl*>(s->control.ptr)->stop, &one, sizeof(one), cudaMemcpyHostToDevice);
   }
+  StopDownloader(*s);
   if (s->server != nullptr) cudaStreamSynchronize(s->server);
   if (s->copy != nullptr) cudaStreamSynchronize(s->copy);
-  for (ServeJobHost& job : s->jobs) {
-    if (job.live && job.phase == 0) DisarmDownloads(*s, job);
-  }
-  for (cudaStream_t st : s->slot_d2h) {
-    if (st != nullptr) cudaStreamSynchronize(st);
-  }
   if (s->d2h != nullptr) cudaStreamSynchronize(s->d2h);
   if (error_word != nullptr && s->control.ptr != nullptr) {
     cudaMemcpy(error_word, &static_cast<ServeControl*>(s->control.ptr)->error, sizeof(int32_t), cudaMemcpyDeviceToHost);
   }
-  for (ServeJobHost& job : s->jobs) {
-    if (job.downloaded != nullptr) cudaEventDestroy(job.downloaded);
+  for (SlotTicket& t : s->tickets) {
+    if (t.event != nullptr) cudaEventDestroy(t.event);
   }
   s->arena_buf.Release();
   s->control.Release();
@@ -325,9 +366,6 @@ void ReleaseServe(cee_ctx* ctx, int32_t* error_word) {
   if (s->tickets_host != nullptr) cudaFreeHost(s->tickets_host);
   if (s->pinned_stage != nullptr) cudaFreeHost(s->pinned_stage);
   for (cudaStream_t st : {s->server, s->copy, s->d2h}) {
-    if (st != nullptr) cudaStreamDestroy(st);
-  }
-  for (cudaStream_t st : s->slot_d2h) {
     if (st != nullptr) cudaStreamDestroy(st);
   }
   if (s->kernel_done != nullptr) cudaEventDestroy(s->kernel_done);
@@ -381,10 +419,6 @@ int cee_serve_start(cee_ctx* ctx, const cee_serve_config* config) {
   for (cudaStream_t* st : {&s.server, &s.copy, &s.d2h}) {
     if (status == cudaSuccess) status = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
   }
-  for (int i = 0; i < config->slots && status == cudaSuccess; ++i) {
-    status = cudaStreamCreateWithFlags(&s.slot_d2h[i], cudaStreamNonBlocking);
-  }
-  if (status == cudaSuccess && StreamWaitValue32() == nullptr) status = cudaErrorNotSupported;
   if (status == cudaSuccess) status = cudaEventCreateWithFlags(&s.kernel_done, cudaEventDisableTiming);
   int per_sm = 0;
   if (status == cudaSuccess) {
@@ -421,6 +455,7 @@ int cee_serve_start(cee_ctx* ctx, const cee_serve_config* config) {
     ReleaseServe(ctx);
     return code;
   }
+  s.downloader = std::thread(DownloaderLoop, &s, ctx->device);
   return CEE_OK;
 }
 
@@ -793,7 +828,7 @@ int cee_serve_poll(cee_ctx* ctx, cee_serve_event* events, int32_t capacity, int3
     if (!job.live || job.phase == 2) continue;
     if (job.phase == 0 && s.broken &&
         *reinterpret_cast<volatile uint32_t*>(s.finished_host + job.slot) != job.generation) {
-      DisarmDownloads(s, job);
+      DropTicket(s, job.slot);
       job.status = Fail(ctx, CEE_ERR_TIMEOUT, "serving loop lost a work item; restart it with cee_serve_start");
       if (!report(id, job)) break;
       continue;
@@ -806,10 +841,15 @@ int cee_serve_poll(cee_ctx* ctx, cee_serve_event* events, int32_t capacity, int3
       if (reinterpret_cast<volatile uint32_t*>(s.finished_host)[kServeMaxSlots + job.slot] != 0) {
         job.status = Fail(ctx, CEE_ERR_INVALID, "serving loop: device bounds check rejected an out-of-range index");
       }
-      job.armed = false;  // its downloads were queued at submission and are running now
+      IssueDownloads(s, job.slot);  // unless the downloader thread already has
+      int state = kTicketIssuing;
+      while ((state = s.tickets[job.slot].state.load(std::memory_order_acquire)) == kTicketIssuing) {
+        std::this_thread::yield();
+      }
+      if (state != kTicketIssued) return ServeFail(ctx, CEE_ERR_STATE, "a finished job's downloads were not queued");
       job.phase = 1;
     }
-    const cudaError_t q = cudaEventQuery(job.downloaded);
+    const cudaError_t q = cudaEventQuery(s.tickets[job.slot].event);
     if (q == cudaErrorNotReady) continue;
     if (q != cudaSuccess) return CudaFail(ctx, q, "serve download");
     if (!report(id, job)) break;

@@ -503,9 +503,8 @@ int cee_serve_submit_kopt_improving(cee_ctx* ctx, int32_t snapshot, int32_t segm
                                     uint32_t* const* masks_out, int32_t* const* first_out,
                                     int64_t* const* costs_out, uint64_t tag, int32_t* job);
 /* Returns up to `capacity` completed jobs (their host outputs are written) and relaunches the
- * kernel if it went idle while jobs wait. A job's downloads are queued at submission behind a
- * device wait for its completion, so they run as soon as the job ends, whether or not the host
- * is polling. */
+ * kernel if it went idle while jobs wait. A job's downloads are issued by the loop's own host
+ * thread as soon as the job ends, whether or not the caller is polling. */
 int cee_serve_poll(cee_ctx* ctx, cee_serve_event* events, int32_t capacity, int32_t* count);
 /* Jobs admitted and not yet returned by cee_serve_poll, and arena bytes in use. */
 int cee_serve_pending(const cee_ctx* ctx, int32_t* jobs, uint64_t* arena_used);
