@@ -240,8 +240,11 @@ class ServeMixin:
 
     def serve_start(self, config: ServeConfig | None = None) -> None:
         config = ServeConfig() if config is None else config
+        # a running loop is released first (its in-flight downloads land before that returns): only
+        # then may the buffers of its jobs go
+        rc = _native.lib().cee_serve_start(self.handle, ctypes.byref(config.native()))
         self._serve_jobs = {}
-        _native.check(self.handle, _native.lib().cee_serve_start(self.handle, ctypes.byref(config.native())))
+        _native.check(self.handle, rc)
 
     def serve_add_snapshot(self, graph: GraphSnapshot) -> int | None:
         sid = ctypes.c_int32(-1)
@@ -338,8 +341,11 @@ class ServeMixin:
         return jobs.value, used.value
 
     def serve_stop(self) -> None:
+        # the loop's queued downloads into dropped jobs' buffers complete inside cee_serve_stop:
+        # the buffers are released after it
+        rc = _native.lib().cee_serve_stop(self.handle)
         self._serve_jobs = {}
-        _native.check(self.handle, _native.lib().cee_serve_stop(self.handle))
+        _native.check(self.handle, rc)
 
 
 class TuningCache:

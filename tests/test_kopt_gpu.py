@@ -248,3 +248,16 @@ def test_autotune_keeps_cells_and_caches_the_shape(ctx, port, tmp_path):
             other.close()
     finally:
         ctx.set_kopt_tuning(1, (0, 0, 0))
+
+
+def test_large_pageable_copies(ctx, port):
+    """Matrices and task rows above the staging threshold, in pageable memory, go through the
+    context's pinned staging buffers (several 16 MB chunks, host threads, odd sizes): the cells still
+    equal the oracle's, for rows uploaded and cells downloaded that way."""
+    g, tasks = synth.kopt_instance(rows=360_003, n=5000)
+    k5 = np.ascontiguousarray(tasks[5][:120_001])  # 5.8 MB of rows in, 200 MB of cells out
+    k3 = np.ascontiguousarray(tasks[3][:1001])
+    outs, _ = ctx.kopt_costs_multi(g, [5, 3], [k5, k3])
+    assert outs[0].nbytes > (64 << 20)
+    np.testing.assert_array_equal(outs[0], port.kopt_costs_parallel(g, 5, k5))
+    np.testing.assert_array_equal(outs[1], port.kopt_costs(g, 3, k3))
