@@ -207,27 +207,11 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
         ok = false;
       }
     }
-#ifndef CEE_JV_MATCH
-#define CEE_JV_MATCH 1
-#endif
     if (total <= 32) {
-#if CEE_JV_MATCH
       // one round: N(a) sits on lanes [0, da), so a node of N(b) already scored through N(a)
       // is found by matching lane values (other lanes hold distinct negative placeholders)
       const unsigned same = __match_any_sync(kFullMask, ok ? c : -1 - lane);
       if (ok && second) ok = (same & ((1u << da) - 1u)) == 0;
-#else
-      // one round: N(a) sits on lanes [0, da) in ascending order, so each lane of N(b) finds its
-      // node there by a binary search over those lanes (five shuffles)
-      int pos = 0;
-#pragma unroll
-      for (int step = 16; step > 0; step >>= 1) {
-        const int32_t probe = __shfl_sync(kFullMask, c, (pos + step - 1) & 31);
-        if (pos + step <= da && probe < c) pos += step;
-      }
-      const int32_t at = __shfl_sync(kFullMask, c, pos & 31);
-      if (ok && second && pos < da && at == c) ok = false;
-#endif
     } else if (ok && second) {
       ok = !row_contains(g.nbr, ra0, ra1, c);
     }
@@ -331,16 +315,7 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
       const int32_t row = s.row[hi];
       if (hj < s.end[hi] - row) hit = compatible_pair(hi, row + hj);
     }
-#ifndef CEE_JV_HEADVOTE
-#define CEE_JV_HEADVOTE 0
-#endif
-#if CEE_JV_HEADVOTE
-    // candidate i's head pairs sit on lanes 3i .. 3i + 2: lane i folds its three bits of the ballot
-    const uint32_t hits = __ballot_sync(kFullMask, hit);
-    compatible = __ballot_sync(kFullMask, lane < nc && ((hits >> ((kHead * lane) & 31)) & 7u) != 0);
-#else
     compatible = __reduce_or_sync(kFullMask, hit ? 1u << hi : 0u);
-#endif
   }
   const uint32_t all = (1u << nc) - 1u;
   uint32_t open = all & ~compatible;

@@ -108,6 +108,7 @@ struct ServeJobHost {
 // kIssuing issues them; the job is reported once `event` has completed.
 constexpr int kTicketIdle = 0, kTicketArmed = 1, kTicketIssuing = 2, kTicketIssued = 3;
 constexpr int kMaxDownloads = 9;  // three segments x (costs, masks, first)
+constexpr size_t kServeSmallDownload = size_t{4} << 20;
 struct SlotTicket {
   std::atomic<int> state{kTicketIdle};
   uint32_t generation = 0;
@@ -130,7 +131,9 @@ struct ServeState {
   uint64_t* tickets_host = nullptr;   // pinned: generation of slot s << 32 (ticket and done resets)
   uint8_t* pinned_stage = nullptr;    // snapshot packing
   size_t pinned_stage_bytes = 0;
-  cudaStream_t server = nullptr, copy = nullptr, d2h = nullptr;
+  // downloads: jobs whose outputs total under kServeSmallDownload on d2h_small, larger ones on d2h, so a
+  // witness array never queues behind a large k-opt matrix
+  cudaStream_t server = nullptr, copy = nullptr, d2h = nullptr, d2h_small = nullptr;
   SlotTicket tickets[kServeMaxSlots];
   // the downloader thread: issues a job's copies as soon as its finished word lands, whether or not
   // the caller is polling (it sleeps while no job is armed)
@@ -287,11 +290,14 @@ void IssueDownloads(ServeState& s, int slot) {
   int expected = kTicketArmed;
   if (!t.state.compare_exchange_strong(expected, kTicketIssuing, std::memory_order_acq_rel)) return;
   const uint8_t* arena = static_cast<const uint8_t*>(s.arena_buf.ptr);
+  size_t bytes = 0;
+  for (int i = 0; i < t.count; ++i) bytes += t.downloads[i].bytes;
+  cudaStream_t st = bytes < kServeSmallDownload ? s.d2h_small : s.d2h;
   for (int i = 0; i < t.count; ++i) {
     cudaMemcpyAsync(t.downloads[i].host, arena + t.downloads[i].device_offset, t.downloads[i].bytes,
-                    cudaMemcpyDeviceToHost, s.d2h);
+                    cudaMemcpyDeviceToHost, st);
   }
-  cudaEventRecord(t.event, s.d2h);
+  cudaEventRecord(t.event, st);
   s.armed.fetch_sub(1);
   t.state.store(kTicketIssued, std::memory_order_release);
 }
@@ -351,6 +357,7 @@ void ReleaseServe(cee_ctx* ctx, int32_t* error_word) {
   if (s->server != nullptr) cudaStreamSynchronize(s->server);
   if (s->copy != nullptr) cudaStreamSynchronize(s->copy);
   if (s->d2h != nullptr) cudaStreamSynchronize(s->d2h);
+  if (s->d2h_small != nullptr) cudaStreamSynchronize(s->d2h_small);
   if (error_word != nullptr && s->control.ptr != nullptr) {
     cudaMemcpy(error_word, &static_cast<ServeControl*>(s->control.ptr)->error, sizeof(int32_t), cudaMemcpyDeviceToHost);
   }
@@ -365,7 +372,7 @@ void ReleaseServe(cee_ctx* ctx, int32_t* error_word) {
   if (s->words_host != nullptr) cudaFreeHost(s->words_host);
   if (s->tickets_host != nullptr) cudaFreeHost(s->tickets_host);
   if (s->pinned_stage != nullptr) cudaFreeHost(s->pinned_stage);
-  for (cudaStream_t st : {s->server, s->copy, s->d2h}) {
+  for (cudaStream_t st : {s->server, s->copy, s->d2h, s->d2h_small}) {
     if (st != nullptr) cudaStreamDestroy(st);
   }
   if (s->kernel_done != nullptr) cudaEventDestroy(s->kernel_done);
@@ -416,7 +423,7 @@ int cee_serve_start(cee_ctx* ctx, const cee_serve_config* config) {
     status = cudaHostAlloc(reinterpret_cast<void**>(&s.tickets_host), kServeMaxSlots * sizeof(uint64_t),
                            cudaHostAllocDefault);
   }
-  for (cudaStream_t* st : {&s.server, &s.copy, &s.d2h}) {
+  for (cudaStream_t* st : {&s.server, &s.copy, &s.d2h, &s.d2h_small}) {
     if (status == cudaSuccess) status = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
   }
   if (status == cudaSuccess) status = cudaEventCreateWithFlags(&s.kernel_done, cudaEventDisableTiming);
