@@ -406,7 +406,7 @@ int cee_serve_start(cee_ctx* ctx, const cee_serve_config* config) {
   cudaError_t status = s.arena_buf.Reserve(static_cast<size_t>(config->hbm_budget_bytes), nullptr);
   if (status == cudaSuccess) status = s.control.Reserve(sizeof(ServeControl), nullptr);
   if (status == cudaSuccess) status = cudaMemset(s.control.ptr, 0, sizeof(ServeControl));
-  if (status == cudaSuccess) status = s.templates.Reserve(kServeTemplateBytes, nullptr);
+  if (status == cudaSuccess) status = s.templates.Reserve(kServeTemplateBytes + kServeValidityWords * 4, nullptr);
   if (status == cudaSuccess) {
     status = cudaHostAlloc(reinterpret_cast<void**>(&s.finished_host), (kServeLostWord + 1) * sizeof(uint32_t),
                            cudaHostAllocMapped);
@@ -456,6 +456,21 @@ int cee_serve_start(cee_ctx* ctx, const cee_serve_config* config) {
       }
     }
   }
+  // then the validity words of the proper templates by gap pattern, from the compile-time tables
+  std::vector<uint32_t> valid(kServeValidityWords, 0);
+  auto fill = [&](const auto& tab, int k) {
+    const int words = (tab.count + 31) / 32;
+    for (int g = 0; g < 32; ++g) {
+      for (int t = 0; t < tab.count; ++t) {
+        valid[serve_validity_offset(k) + g * words + t / 32] |= ((tab.invalid_on[t] >> g) & 1u) << (t % 32);
+      }
+    }
+  };
+  fill(KoptCanon<3>::value, 3);
+  fill(KoptCanon<4>::value, 4);
+  fill(KoptCanon<5>::value, 5);
+  table.resize(kServeTemplateBytes + kServeValidityWords * 4);
+  std::memcpy(table.data() + kServeTemplateBytes, valid.data(), valid.size() * 4);
   status = cudaMemcpy(s.templates.ptr, table.data(), table.size(), cudaMemcpyHostToDevice);
   if (status != cudaSuccess) {
     const int code = CudaFail(ctx, status, "serve templates");

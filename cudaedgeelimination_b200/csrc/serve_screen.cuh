@@ -26,6 +26,7 @@
 
 #include "jv_screen.cuh"
 #include "kopt_cost.cuh"
+#include "kopt_rows.cuh"
 
 namespace cee {
 
@@ -80,7 +81,8 @@ constexpr int kServeLostWord = 2 * kServeMaxSlots;
 __host__ __device__ constexpr int serve_rows_per_chunk(int k) { return k == 3 ? 8 : (k == 4 ? 4 : 2); }
 
 // One warp's k-opt tile (kopt_cost.cuh's layout), sized for the largest chunk of any k.
-constexpr int kServeKoptScratch = 1936;
+// (also the staging buffer of kopt_serve_proper32: one box of 16 cells x 32 rows)
+constexpr int kServeKoptScratch = 4096;
 static_assert(kopt_tile_smem(3, serve_rows_per_chunk(3)) <= kServeKoptScratch, "k = 3 chunk tile");
 static_assert(kopt_tile_smem(4, serve_rows_per_chunk(4)) <= kServeKoptScratch, "k = 4 chunk tile");
 static_assert(kopt_tile_smem(5, serve_rows_per_chunk(5)) <= kServeKoptScratch, "k = 5 chunk tile");
@@ -159,6 +161,135 @@ __device__ void kopt_rows_warp(const ServeSegment& S, int64_t row_begin, int64_t
 // Canonical template pair tables for k = 3, 4, 5 packed back to back (4*3 + 25*4 + 208*5 bytes).
 constexpr int kServeTemplateBytes = 4 * 3 + 25 * 4 + 208 * 5;
 __host__ __device__ __forceinline__ int serve_template_offset(int k) { return k == 3 ? 0 : (k == 4 ? 12 : 112); }
+// After them, the proper templates' validity words by gap pattern (kopt_rows.cuh): word [g][w] of k
+// holds bit t mod 32 for template t = 32 w + ... invalid on gap-pattern rows of pattern g; 32 x 1,
+// 32 x 1 and 32 x 7 words for k = 3, 4, 5.
+constexpr int kServeValidityWords = 32 * (1 + 1 + 7);
+static_assert(kServeTemplateBytes % 16 == 0, "validity words start 16-byte aligned");
+__host__ __device__ __forceinline__ int serve_validity_offset(int k) { return k == 3 ? 0 : (k == 4 ? 32 : 64); }
+
+// 32 rows [row0, row0 + rows) of a segment, one per lane, with the proper templates compiled in
+// (kopt_rows.cuh's row routine at warp size): the k(2k-1) pair distances in registers, each cell k-1
+// adds, a validity bit and its store. k = 5 cells go out a box of 16 cells x 32 rows at a time
+// through the warp's shared buffer, as whole 128-byte lines of each row with coalesced stores;
+// k = 4 and 3 rows are stored from registers. A warp holding a row that is not a gap-pattern row
+// scores its rows with the chunked class-code routine instead.
+template <int K, int kSpan>
+__device__ void kopt_serve_proper32(const ServeJob& job, const ServeSegment& S, int64_t row0, int rows,
+                                    const uint32_t* __restrict__ valid, const uint8_t* tpairs,
+                                    unsigned char* scratch, int lane, int32_t* error) {
+  using Tab = KoptCanonTable<K>;
+  constexpr int P = Tab::P, NP = Tab::NP, T = Tab::T, W = Tab::W;
+  const bool live = lane < rows;
+  const int64_t row = row0 + lane;
+  int32_t nd[P];
+  int64_t deleted = 0;
+  {
+    int4 q[3] = {make_int4(0, 0, 0, 0), make_int4(0, 0, 0, 0), make_int4(0, 0, 0, 0)};
+    if (live) {
+      const int4* src = reinterpret_cast<const int4*>(S.tasks + row * 12);
+      q[0] = __ldcg(src);
+      q[1] = __ldcg(src + 1);
+      q[2] = __ldcg(src + 2);
+    }
+    const int32_t words[12] = {q[0].x, q[0].y, q[0].z, q[0].w, q[1].x, q[1].y, q[1].z, q[1].w,
+                               q[2].x, q[2].y, q[2].z, q[2].w};
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      nd[p] = words[p];
+      if (static_cast<uint32_t>(nd[p]) >= static_cast<uint32_t>(job.g.n)) {
+        atomicOr(error, 1);
+        nd[p] = 0;
+      }
+    }
+    deleted = static_cast<int64_t>((static_cast<uint64_t>(static_cast<uint32_t>(words[11])) << 32) |
+                                   static_cast<uint32_t>(words[10]));
+  }
+  int equal = 0;
+  uint32_t g = 0;
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+#pragma unroll
+    for (int q = p + 1; q < P; ++q) equal += nd[p] == nd[q] ? 1 : 0;
+  }
+#pragma unroll
+  for (int e = 0; e < K; ++e) g |= (nd[2 * e + 1] == nd[(2 * e + 2) % P] ? 1u : 0u) << e;
+  if (__ballot_sync(kFullMask, live && equal != __popc(g)) != 0) {
+    kopt_rows_warp<K, kSpan>(S, row0, row0 + rows, tpairs, job.g.xy, job.g.n, job.g.dist_type, scratch, lane, error);
+    return;
+  }
+  uint32_t d[NP];
+  {
+    int2 c[P];
+    static_for<0, P>([&](auto pc) { c[decltype(pc)::value] = __ldg(job.g.xy + nd[decltype(pc)::value]); });
+    static_for<0, P>([&](auto pc) {
+      constexpr int p = decltype(pc)::value;
+      static_for<p + 1, P>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        d[kopt_pair_index(p, q, P)] = exact_distance<kSpan>(c[p], c[q], job.g.dist_type);
+      });
+    });
+  }
+  const uint32_t dl = deleted <= 0 ? 0u : (deleted >= 0xffffffffll ? 0xffffffffu : static_cast<uint32_t>(deleted));
+  const uint32_t* vrow = valid + serve_validity_offset(K) + g * W;
+  const bool sets = S.improving != nullptr;
+  uint32_t valid_word = 0, improving_word = 0;
+  int first = -1;
+  auto cell = [&](auto tc) -> uint2 {
+    constexpr int t = decltype(tc)::value;
+    if constexpr (t % 32 == 0) valid_word = __ldg(vrow + t / 32);
+    uint32_t sum = d[kKoptCanonPair<K, t, 0>];
+    static_for<1, K>([&](auto ic) { sum += d[kKoptCanonPair<K, t, decltype(ic)::value>]; });
+    const bool bad = ((valid_word >> (t % 32)) & 1u) != 0;
+    improving_word |= static_cast<uint32_t>(!bad && sum < dl) << (t % 32);
+    if constexpr (t % 32 == 31 || t == T - 1) {
+      if (sets && live) S.improving[row * W + t / 32] = improving_word;
+      if (first < 0 && improving_word != 0) first = (t & ~31) + __ffs(improving_word) - 1;
+      improving_word = 0;
+    }
+    return kopt_cell_word(sum, bad);
+  };
+  if (S.costs == nullptr) {
+    static_for<0, T>([&](auto tc) { (void)cell(tc); });
+  } else if constexpr (K == 5) {
+    const int swz = lane & 7;
+    static_for<0, T / 16>([&](auto jc) {
+      constexpr int j = decltype(jc)::value;
+      __syncwarp();  // the previous box has been read out
+      static_for<0, 8>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        const uint2 a = cell(std::integral_constant<int, 16 * j + 2 * i>{});
+        const uint2 b = cell(std::integral_constant<int, 16 * j + 2 * i + 1>{});
+        *reinterpret_cast<uint4*>(scratch + lane * 128 + ((i ^ swz) << 4)) = make_uint4(a.x, a.y, b.x, b.y);
+      });
+      __syncwarp();
+#pragma unroll
+      for (int v = 0; v < 8; ++v) {  // 16-byte unit u = lane + 32 v: part u & 7 of row u >> 3
+        const int u = lane + 32 * v, r = u >> 3, part = u & 7;
+        if (r < rows) {
+          const uint4 x = *reinterpret_cast<const uint4*>(scratch + r * 128 + ((part ^ (r & 7)) << 4));
+          __stcs(reinterpret_cast<uint4*>(S.costs + (row0 + r) * T + 16 * j) + part, x);
+        }
+      }
+    });
+  } else if constexpr (K == 4) {
+    uint2* out = reinterpret_cast<uint2*>(S.costs + row * T);
+    static_for<0, T>([&](auto tc) {
+      const uint2 v = cell(tc);
+      if (live) __stcs(out + decltype(tc)::value, v);
+    });
+  } else {
+    uint2 v[T];
+    static_for<0, T>([&](auto tc) { v[decltype(tc)::value] = cell(tc); });
+    if (live) {
+      uint4* out = reinterpret_cast<uint4*>(S.costs + row * T);
+      __stcs(out, make_uint4(v[0].x, v[0].y, v[1].x, v[1].y));
+      __stcs(out + 1, make_uint4(v[2].x, v[2].y, v[3].x, v[3].y));
+    }
+  }
+  if (sets && live) S.first[row] = first;
+  __syncwarp();
+}
 
 __device__ __forceinline__ uint32_t volatile_load(const uint32_t* p) { return *reinterpret_cast<const volatile uint32_t*>(p); }
 __device__ __forceinline__ unsigned long long volatile_load(const unsigned long long* p) {
@@ -189,19 +320,29 @@ __device__ __forceinline__ unsigned long long serve_take(ServeControl* ctl, int 
   return __shfl_sync(kFullMask, t, 0);
 }
 
+// Rows [r0, r1) of a segment: the proper-template row routine 32 rows at a time (coordinates of span
+// < 2^26), else the chunked class-code routine.
 template <int K>
 __device__ __forceinline__ void serve_kopt_item(const ServeJob& job, const ServeSegment& S, int64_t r0, int64_t r1,
-                                                const uint8_t* tpairs, unsigned char* scratch, int lane,
-                                                int32_t* error) {
-  if (job.span == kSpanSmall) {
-    kopt_rows_warp<K, kSpanSmall>(S, r0, r1, tpairs, job.g.xy, job.g.n, job.g.dist_type, scratch, lane, error);
-  } else if (job.span == kSpanNarrow) {
-    kopt_rows_warp<K, kSpanNarrow>(S, r0, r1, tpairs, job.g.xy, job.g.n, job.g.dist_type, scratch, lane, error);
-  } else {
+                                                const uint8_t* tpairs, const uint32_t* valid, unsigned char* scratch,
+                                                int lane, int32_t* error) {
+  if (job.span == kSpanWide) {
     kopt_rows_warp<K, kSpanWide>(S, r0, r1, tpairs, job.g.xy, job.g.n, job.g.dist_type, scratch, lane, error);
+    return;
+  }
+  for (int64_t g0 = r0; g0 < r1; g0 += 32) {
+    const int rows = static_cast<int>(min(static_cast<int64_t>(32), r1 - g0));
+    if (job.span == kSpanSmall) {
+      kopt_serve_proper32<K, kSpanSmall>(job, S, g0, rows, valid, tpairs, scratch, lane, error);
+    } else {
+      kopt_serve_proper32<K, kSpanNarrow>(job, S, g0, rows, valid, tpairs, scratch, lane, error);
+    }
   }
 }
 
+// Four blocks per SM (64 registers): JV items want the warps; the k-opt row routine spills some of its
+// 45 pair distances at this budget, and 3 or 2 blocks (80 / 128 registers) measured no faster for
+// k-opt jobs, whose results are bound by the PCIe download, and slower for JV jobs.
 static __global__ void __launch_bounds__(kServeWarps * 32, 4)
     serve_kernel(ServeControl* ctl, uint32_t* finished, const uint8_t* templates, int32_t slots,
                  long long idle_limit) {
@@ -301,12 +442,13 @@ static __global__ void __launch_bounds__(kServeWarps * 32, 4)
       const int64_t r1 = min(r0 + kServeKoptRowsPerItem, S.rows);
       const uint8_t* tp = tpairs + serve_template_offset(S.k);
       unsigned char* ks = kopt_scratch[warp];
+      const uint32_t* valid = reinterpret_cast<const uint32_t*>(templates + kServeTemplateBytes);
       if (S.k == 3) {
-        serve_kopt_item<3>(job, S, r0, r1, tp, ks, lane, error);
+        serve_kopt_item<3>(job, S, r0, r1, tp, valid, ks, lane, error);
       } else if (S.k == 4) {
-        serve_kopt_item<4>(job, S, r0, r1, tp, ks, lane, error);
+        serve_kopt_item<4>(job, S, r0, r1, tp, valid, ks, lane, error);
       } else {
-        serve_kopt_item<5>(job, S, r0, r1, tp, ks, lane, error);
+        serve_kopt_item<5>(job, S, r0, r1, tp, valid, ks, lane, error);
       }
     }
     __threadfence();  // this warp's outputs before its done count
