@@ -534,7 +534,8 @@ __device__ void batch_cd_target(const BatchArgs& A, int32_t inst, int32_t t, con
 }
 
 // Eight blocks of eight warps per SM (32 registers, a few spilled): a full SM of warps hides the screen's
-// dependent loads and shuffle latencies better than five blocks at 48 registers (19.7 vs 21.8 ms per step).
+// dependent loads and shuffle latencies better than six blocks at 40 registers (18.22 vs 18.70 ms per step)
+// or five at 48 (19.7 vs 21.8 ms before the instance-relative keys).
 // kLocal: every instance has at most kJvLocalSpan nodes (the JV screen's instance-relative keys).
 template <int kSpan, bool kLocal>
 static __global__ void __launch_bounds__(kBatchWarps * 32, 8) batch_screen_kernel(BatchArgs A) {
