@@ -109,6 +109,10 @@ class ServeEvent(ctypes.Structure):
     _fields_ = [("job", ctypes.c_int32), ("status", ctypes.c_int32), ("tag", ctypes.c_uint64)]
 
 
+class ServeStats(ctypes.Structure):
+    _fields_ = [("jobs", ctypes.c_uint64), ("rows_bytes", ctypes.c_uint64), ("download_bytes", ctypes.c_uint64)]
+
+
 class NativeError(RuntimeError):
     """A non-zero status from libcee; `code` is the CEE_ERR_* value."""
 
@@ -204,6 +208,7 @@ def lib() -> ctypes.CDLL:
                                                                ctypes.POINTER(vp), ctypes.c_uint64, c_i32p]),
             "cee_serve_poll": (ctypes.c_int, [vp, ctypes.POINTER(ServeEvent), ctypes.c_int32, c_i32p]),
             "cee_serve_pending": (ctypes.c_int, [vp, c_i32p, c_u64p]),
+            "cee_serve_get_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServeStats)]),
             "cee_serve_stop": (ctypes.c_int, [vp]),
         }
         for name, (res, args) in sig.items():

@@ -244,6 +244,8 @@ class ServeMixin:
         # then may the buffers of its jobs go
         rc = _native.lib().cee_serve_start(self.handle, ctypes.byref(config.native()))
         self._serve_jobs = {}
+        # k-opt task arrays by job: page-locked rows are read in place while the job runs
+        self._serve_rows = {}
         _native.check(self.handle, rc)
 
     def serve_add_snapshot(self, graph: GraphSnapshot) -> int | None:
@@ -289,6 +291,7 @@ class ServeMixin:
             return None
         _native.check(self.handle, rc)
         self._serve_jobs[job.value] = outs
+        self._serve_rows[job.value] = tasks
         return job.value
 
     def serve_submit_kopt_improving(self, sid: int, ks, task_lists, tag: int = 0, outs=None) -> int | None:
@@ -316,6 +319,7 @@ class ServeMixin:
             return None
         _native.check(self.handle, rc)
         self._serve_jobs[job.value] = (masks, firsts)
+        self._serve_rows[job.value] = tasks
         return job.value
 
     def serve_poll(self, capacity: int = 256, with_status: bool = False):
@@ -328,6 +332,8 @@ class ServeMixin:
         _native.check(self.handle, _native.lib().cee_serve_poll(self.handle, events, capacity, ctypes.byref(count)))
         done = [(events[i].job, events[i].tag, self._serve_jobs.pop(events[i].job), events[i].status)
                 for i in range(count.value)]
+        for d in done:
+            self._serve_rows.pop(d[0], None)
         if with_status:
             return done
         for _, _, _, status in done:
@@ -340,11 +346,18 @@ class ServeMixin:
         _native.check(self.handle, _native.lib().cee_serve_pending(self.handle, ctypes.byref(jobs), ctypes.byref(used)))
         return jobs.value, used.value
 
+    def serve_stats(self) -> dict:
+        """Totals since serve_start: jobs posted, k-opt row bytes uploaded, result bytes downloaded."""
+        st = _native.ServeStats()
+        _native.check(self.handle, _native.lib().cee_serve_get_stats(self.handle, ctypes.byref(st)))
+        return {name: int(getattr(st, name)) for name, _ in st._fields_}
+
     def serve_stop(self) -> None:
         # the loop's queued downloads into dropped jobs' buffers complete inside cee_serve_stop:
         # the buffers are released after it
         rc = _native.lib().cee_serve_stop(self.handle)
         self._serve_jobs = {}
+        self._serve_rows = {}
         _native.check(self.handle, rc)
 
 

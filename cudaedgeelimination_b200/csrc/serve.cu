@@ -1,6 +1,6 @@
 // Host side of the serving loop (serve_screen.cuh): HBM-budget admission into a device arena,
-// device-resident snapshots kept across jobs until released, job publication into the persistent
-// kernel's slot table, completion polling and result download.
+// device-resident snapshots kept across jobs until released, job posting through a host-mapped
+// mailbox that the persistent kernel's dispatcher warp reads, completion polling and result download.
 #include "cee.h"
 #include "cee_internal.h"
 
@@ -126,11 +126,12 @@ struct ServeState {
   // mapped: [slot] generation done, [kServeMaxSlots + slot] error word, [kServeLostWord] lost item
   uint32_t* finished_host = nullptr;
   uint32_t* finished_dev = nullptr;
-  ServeJob* desc_host = nullptr;      // pinned staging, one descriptor per slot
+  ServeMailbox* mailbox_host = nullptr;  // mapped: posted jobs (serve_screen.cuh)
+  ServeMailbox* mailbox_dev = nullptr;
   uint32_t* words_host = nullptr;     // pinned: [0] = 0, [1] = 1, [2 + s] = generation of slot s
-  uint64_t* tickets_host = nullptr;   // pinned: generation of slot s << 32 (ticket and done resets)
   uint8_t* pinned_stage = nullptr;    // snapshot packing
   size_t pinned_stage_bytes = 0;
+  cee_serve_stats stats{};
   // downloads: jobs whose outputs total under kServeSmallDownload on d2h_small, larger ones on d2h, so a
   // witness array never queues behind a large k-opt matrix
   cudaStream_t server = nullptr, copy = nullptr, d2h = nullptr, d2h_small = nullptr;
@@ -196,8 +197,8 @@ int LaunchServer(cee_ctx* ctx, ServeState& s) {
   ServeControl* ctl = static_cast<ServeControl*>(s.control.ptr);
   cudaMemsetAsync(&ctl->stop, 0, sizeof(uint32_t), s.server);
   serve_kernel<<<s.grid, kServeWarps * 32, 0, s.server>>>(
-      static_cast<ServeControl*>(s.control.ptr), s.finished_dev, static_cast<const uint8_t*>(s.templates.ptr),
-      s.cfg.slots, s.idle_limit);
+      static_cast<ServeControl*>(s.control.ptr), s.mailbox_dev, s.finished_dev,
+      static_cast<const uint8_t*>(s.templates.ptr), s.cfg.slots, s.idle_limit);
   cudaError_t status = cudaGetLastError();
   if (status == cudaSuccess) status = cudaEventRecord(s.kernel_done, s.server);
   if (status != cudaSuccess) return CudaFail(ctx, status, "serve kernel launch");
@@ -213,22 +214,15 @@ int FreeSlot(const ServeState& s) {
   return -1;
 }
 
-// Publishes `desc` in `slot` with ordered copies: state = 0, the slot's error word = 0, descriptor,
-// ticket and done = generation << 32, state = generation. The pinned sources of a slot are
-// rewritten only after its previous job finished, i.e. after the copies that read them ran.
+// Posts `desc` in `slot`: the descriptor, then (release) its generation, into the mapped mailbox,
+// which the kernel's dispatcher warp installs in the slot table. A slot's mailbox entry is rewritten
+// only after its previous job was reported, so the dispatcher installed that one long before.
 int Publish(cee_ctx* ctx, ServeState& s, int slot, const ServeJob& desc) {
-  ServeControl* ctl = static_cast<ServeControl*>(s.control.ptr);
-  s.desc_host[slot] = desc;
-  s.words_host[2 + slot] = desc.generation;
-  s.tickets_host[slot] = static_cast<uint64_t>(desc.generation) << 32;
-  cudaMemcpyAsync(&ctl->state[slot], &s.words_host[0], sizeof(uint32_t), cudaMemcpyHostToDevice, s.copy);
-  cudaMemcpyAsync(&ctl->slot_error[slot], &s.words_host[0], sizeof(int32_t), cudaMemcpyHostToDevice, s.copy);
-  cudaMemcpyAsync(&ctl->jobs[slot], &s.desc_host[slot], sizeof(ServeJob), cudaMemcpyHostToDevice, s.copy);
-  cudaMemcpyAsync(&ctl->ticket[slot], &s.tickets_host[slot], sizeof(uint64_t), cudaMemcpyHostToDevice, s.copy);
-  cudaMemcpyAsync(&ctl->done[slot], &s.tickets_host[slot], sizeof(uint64_t), cudaMemcpyHostToDevice, s.copy);
-  cudaMemcpyAsync(&ctl->state[slot], &s.words_host[2 + slot], sizeof(uint32_t), cudaMemcpyHostToDevice, s.copy);
-  const cudaError_t status = cudaGetLastError();
-  if (status != cudaSuccess) return CudaFail(ctx, status, "serve publish");
+  s.mailbox_host->desc[slot] = desc;
+  std::atomic_thread_fence(std::memory_order_release);
+  reinterpret_cast<volatile uint32_t*>(s.mailbox_host->posted)[slot] = desc.generation;
+  std::atomic_thread_fence(std::memory_order_seq_cst);
+  ++s.stats.jobs;
   return LaunchServer(ctx, s);
 }
 
@@ -274,7 +268,10 @@ int ArmDownloads(cee_ctx* ctx, ServeState& s, ServeJobHost& job) {
   }
   t.generation = job.generation;
   t.count = static_cast<int>(job.downloads.size());
-  for (int i = 0; i < t.count; ++i) t.downloads[i] = job.downloads[static_cast<size_t>(i)];
+  for (int i = 0; i < t.count; ++i) {
+    t.downloads[i] = job.downloads[static_cast<size_t>(i)];
+    s.stats.download_bytes += t.downloads[i].bytes;
+  }
   t.state.store(kTicketArmed, std::memory_order_release);
   {
     std::lock_guard<std::mutex> lock(s.wake_mutex);
@@ -368,9 +365,8 @@ void ReleaseServe(cee_ctx* ctx, int32_t* error_word) {
   s->control.Release();
   s->templates.Release();
   if (s->finished_host != nullptr) cudaFreeHost(s->finished_host);
-  if (s->desc_host != nullptr) cudaFreeHost(s->desc_host);
+  if (s->mailbox_host != nullptr) cudaFreeHost(s->mailbox_host);
   if (s->words_host != nullptr) cudaFreeHost(s->words_host);
-  if (s->tickets_host != nullptr) cudaFreeHost(s->tickets_host);
   if (s->pinned_stage != nullptr) cudaFreeHost(s->pinned_stage);
   for (cudaStream_t st : {s->server, s->copy, s->d2h, s->d2h_small}) {
     if (st != nullptr) cudaStreamDestroy(st);
@@ -413,14 +409,11 @@ int cee_serve_start(cee_ctx* ctx, const cee_serve_config* config) {
   }
   if (status == cudaSuccess) status = cudaHostGetDevicePointer(reinterpret_cast<void**>(&s.finished_dev), s.finished_host, 0);
   if (status == cudaSuccess) {
-    status = cudaHostAlloc(reinterpret_cast<void**>(&s.desc_host), kServeMaxSlots * sizeof(ServeJob), cudaHostAllocDefault);
+    status = cudaHostAlloc(reinterpret_cast<void**>(&s.mailbox_host), sizeof(ServeMailbox), cudaHostAllocMapped);
   }
+  if (status == cudaSuccess) status = cudaHostGetDevicePointer(reinterpret_cast<void**>(&s.mailbox_dev), s.mailbox_host, 0);
   if (status == cudaSuccess) {
     status = cudaHostAlloc(reinterpret_cast<void**>(&s.words_host), (kServeMaxSlots + 2) * sizeof(uint32_t),
-                           cudaHostAllocDefault);
-  }
-  if (status == cudaSuccess) {
-    status = cudaHostAlloc(reinterpret_cast<void**>(&s.tickets_host), kServeMaxSlots * sizeof(uint64_t),
                            cudaHostAllocDefault);
   }
   for (cudaStream_t* st : {&s.server, &s.copy, &s.d2h, &s.d2h_small}) {
@@ -437,6 +430,7 @@ int cee_serve_start(cee_ctx* ctx, const cee_serve_config* config) {
     return code;
   }
   std::memset(s.finished_host, 0, (kServeLostWord + 1) * sizeof(uint32_t));
+  std::memset(static_cast<void*>(s.mailbox_host), 0, sizeof(ServeMailbox));
   s.words_host[0] = 0;
   s.words_host[1] = 1;
   per_sm = std::max(1, config->blocks_per_sm > 0 ? std::min(per_sm, config->blocks_per_sm) : per_sm);
@@ -750,13 +744,14 @@ int SubmitKopt(cee_ctx* ctx, int32_t snapshot, int32_t segments, const uint32_t*
   for (int i = 0; i < segments; ++i) {
     ServeSegment& seg = desc.seg[i];
     const size_t r = static_cast<size_t>(rows[i]);
-    seg.tasks = reinterpret_cast<const int32_t*>(arena + in_at);
     seg.rows = rows[i];
     seg.k = static_cast<int32_t>(ks[i]);
     seg.T = TemplateCount(seg.k);
     seg.item_begin = item_at;
+    seg.tasks = reinterpret_cast<const int32_t*>(arena + in_at);
     if (rows[i] > 0) {
       cudaMemcpyAsync(arena + in_at, tasks[i], r * sizeof(cee_kopt_task), cudaMemcpyHostToDevice, s.copy);
+      s.stats.rows_bytes += r * sizeof(cee_kopt_task);
     }
     in_at += rounded(r * sizeof(cee_kopt_task));
     if (costs_out != nullptr) {
@@ -775,6 +770,11 @@ int SubmitKopt(cee_ctx* ctx, int32_t snapshot, int32_t segments, const uint32_t*
     item_at += (rows[i] + kServeKoptRowsPerItem - 1) / kServeKoptRowsPerItem;
   }
   desc.items = static_cast<uint32_t>(items);
+  desc.rows_gate = 1;
+  // after the rows: the slot's rows-ready word = generation (the dispatcher installs the job then)
+  s.words_host[2 + slot] = desc.generation;
+  cudaMemcpyAsync(&static_cast<ServeControl*>(s.control.ptr)->rows_ready[slot], &s.words_host[2 + slot],
+                  sizeof(uint32_t), cudaMemcpyHostToDevice, s.copy);
   s.slot_busy[slot] = true;
   s.next_slot = (slot + 1) % s.cfg.slots;
   job.live = true;
@@ -893,6 +893,12 @@ int cee_serve_stop(cee_ctx* ctx) {
     return Fail(ctx, CEE_ERR_INVALID, "serving loop: a claimed work item's job never became visible (code " +
                                           std::to_string(error_word) + ")");
   }
+  return CEE_OK;
+}
+
+int cee_serve_get_stats(const cee_ctx* ctx, cee_serve_stats* stats) {
+  if (ctx == nullptr || stats == nullptr) return Fail(nullptr, CEE_ERR_INVALID, "null argument");
+  *stats = ctx->serve == nullptr ? cee_serve_stats{} : ctx->serve->stats;
   return CEE_OK;
 }
 

@@ -1,14 +1,20 @@
 // Device side of the serving loop: one persistent kernel runs every admitted job.
 //
-// The host publishes a job in a slot of a fixed table with ordered copies: state word = 0, the
-// job's descriptor, the slot's ticket and done counters = generation << 32, state word =
-// generation (a seqlock: see serve_read_job). Work is claimed with one atomicAdd on the slot's
+// The host posts a job into a host-mapped mailbox (the descriptor, then its generation) with plain
+// stores: no copy or other CUDA call per job, so a submission does not queue behind the copy
+// engines' result downloads (while those fill the link, each small host-to-device copy waits tens of
+// microseconds). One dispatcher warp (the last warp of block 0) polls the mailbox over PCIe and
+// installs each posted job into the device slot table in seqlock order: state word = 0, the job's
+// descriptor, the slot's ticket and done counters = generation << 32, state word = generation (see
+// serve_read_job). A k-opt job's rows go up by one bulk copy per segment followed by the slot's
+// rows-ready word (= generation), and the dispatcher installs the job only once that word shows its
+// generation. Every other warp is a worker. Work is claimed with one atomicAdd on the slot's
 // ticket, whose high half names the generation the item belongs to and whose low half the item
 // index, so claims never retry however many warps contend. A warp keeps claiming from the job it
 // holds while that job has items left; otherwise it scans the slots for the oldest published job
 // with items left (jobs only get younger, so this keeps oldest-first order). A claim may land on
-// a newer generation than the warp expected (the host republished the slot between the warp's
-// check and its atomicAdd): the warp then reads that generation's descriptor and runs the item,
+// a newer generation than the warp expected (the dispatcher republished the slot between the
+// warp's check and its atomicAdd): the warp then reads that generation's descriptor and runs the item,
 // so no item is ever lost; indices past a job's item count are simply dropped. The warp that
 // finishes a job's last item (done counter) makes the job's outputs visible and writes the
 // job's error word, then the generation, into the slot's words of a host-mapped array; the host
@@ -21,7 +27,8 @@
 // because the host never writes snapshot memory while a launch runs: a snapshot upload first
 // stops the kernel (stop word, wait for it to end) and the next launch starts with a clean L1.
 // Per-job inputs (k-opt rows) are written into reused arena memory while the kernel runs, so
-// they are read L2-coherently (__ldcg); the control table is read with volatile loads.
+// they are read L2-coherently (__ldcg); the control table and the mailbox are read with volatile
+// loads.
 #pragma once
 
 #include "jv_screen.cuh"
@@ -53,7 +60,7 @@ struct ServeJob {
   int32_t span;  // span class of the snapshot's coordinates (kSpanSmall / kSpanNarrow / kSpanWide)
   int32_t segments;
   uint32_t items;
-  uint32_t pad;
+  uint32_t rows_gate;  // 1: install only once the slot's rows-ready word equals the generation
   JvGraph g;  // JV jobs; k-opt jobs use g.xy / g.n / g.dist_type
   int32_t* witness;
   ServeSegment seg[3];
@@ -67,8 +74,17 @@ struct ServeControl {
   // per job slot: the device bounds checks of the job now in the slot (1); reset when a job is
   // published there, so one job's bad index is reported for that job alone
   int32_t slot_error[kServeMaxSlots];
+  uint32_t rows_ready[kServeMaxSlots];  // generation whose k-opt rows have landed in the arena
   uint32_t stop;
   int32_t error;  // loop-wide, sticky: a descriptor that never appeared (8)
+};
+
+// Host-mapped: the host writes a job's descriptor into desc[slot] and then its generation into
+// posted[slot]; a slot is posted again only after its previous job has been reported, long after
+// the dispatcher installed that one.
+struct ServeMailbox {
+  ServeJob desc[kServeMaxSlots];
+  uint32_t posted[kServeMaxSlots];
 };
 
 // Bounded wait (about a second) for the descriptor of a generation whose item a claim returned.
@@ -320,6 +336,97 @@ __device__ __forceinline__ unsigned long long serve_take(ServeControl* ctl, int 
   return __shfl_sync(kFullMask, t, 0);
 }
 
+__device__ __forceinline__ uint32_t acquire_load_sys(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Installs the job posted in `slot` with generation `gen` (all lanes): the descriptor is read from
+// the mailbox after the posted word (acquire) and checked against `gen`, then written into the
+// slot table in seqlock order. Returns false (nothing written) when the mailbox still shows an
+// older descriptor or the job's rows have not landed yet; the dispatcher tries again on its next
+// pass.
+__device__ __forceinline__ bool serve_install(ServeControl* ctl, const ServeMailbox* mb, int slot, uint32_t gen,
+                                              int lane) {
+  constexpr int kWords = static_cast<int>(sizeof(ServeJob) / 4);
+  constexpr int kPerLane = (kWords + 31) / 32;
+  static_assert(sizeof(ServeJob) % 4 == 0, "descriptor copied as 32-bit words");
+  __threadfence_system();
+  const volatile uint32_t* src = reinterpret_cast<const volatile uint32_t*>(&mb->desc[slot]);
+  uint32_t w[kPerLane];
+#pragma unroll
+  for (int j = 0; j < kPerLane; ++j) w[j] = lane + 32 * j < kWords ? src[lane + 32 * j] : 0u;
+  if (__shfl_sync(kFullMask, w[0], 0) != gen) return false;  // word 0 is the descriptor's generation
+  constexpr int kGateWord = static_cast<int>(offsetof(ServeJob, rows_gate) / 4);
+  static_assert(kGateWord < 32, "the gate word is in the first 32 words");
+  if (__shfl_sync(kFullMask, w[0], kGateWord) != 0) {
+    if (volatile_load(&ctl->rows_ready[slot]) != gen) return false;
+    __threadfence();  // the rows before the install that lets workers read them
+  }
+  if (lane == 0) {
+    reinterpret_cast<volatile uint32_t*>(ctl->state)[slot] = 0u;
+    reinterpret_cast<volatile int32_t*>(ctl->slot_error)[slot] = 0;
+  }
+  __threadfence();
+  __syncwarp();
+  volatile uint32_t* dst = reinterpret_cast<volatile uint32_t*>(&ctl->jobs[slot]);
+#pragma unroll
+  for (int j = 0; j < kPerLane; ++j) {
+    if (lane + 32 * j < kWords) dst[lane + 32 * j] = w[j];
+  }
+  __threadfence();
+  __syncwarp();
+  if (lane == 0) {
+    atomicExch(&ctl->ticket[slot], static_cast<unsigned long long>(gen) << 32);
+    atomicExch(&ctl->done[slot], static_cast<unsigned long long>(gen) << 32);
+    __threadfence();
+    reinterpret_cast<volatile uint32_t*>(ctl->state)[slot] = gen;
+  }
+  __syncwarp();
+  return true;
+}
+
+// The dispatcher warp: installs every posted job whose generation the slot table does not hold
+// yet. It stays while any installed job has unclaimed items or it installed a job within
+// `idle_limit` passes (about 2 us each: a PCIe read of the posted words and a 1 us sleep), or until
+// the stop word. A post it cannot install yet (rows not landed) counts as an idle pass, so the wait
+// for it is bounded too: if the warp leaves, the host relaunches the kernel for the waiting job.
+__device__ void serve_dispatch(ServeControl* ctl, const ServeMailbox* mb, int32_t slots, long long idle_limit,
+                               int lane) {
+  long long idle = 0;
+  while (idle < idle_limit) {
+    if (volatile_load(&ctl->stop) != 0) return;
+    bool active = false;
+    for (int base = 0; base < slots; base += 32) {
+      const int s = base + lane;
+      uint32_t posted = 0, cur = 0;
+      bool open = false;
+      if (s < slots) {
+        posted = acquire_load_sys(&mb->posted[s]);
+        cur = volatile_load(&ctl->state[s]);
+        if (cur != 0) {
+          const unsigned long long t = volatile_load(&ctl->ticket[s]);
+          open = static_cast<uint32_t>(t >> 32) == cur && static_cast<uint32_t>(t) < volatile_load(&ctl->jobs[s].items);
+        }
+      }
+      unsigned fresh = __ballot_sync(kFullMask, posted != 0 && posted != cur);
+      active = active || __any_sync(kFullMask, open);
+      while (fresh != 0) {
+        const int b = __ffs(fresh) - 1;
+        fresh &= fresh - 1;
+        if (serve_install(ctl, mb, base + b, __shfl_sync(kFullMask, posted, b), lane)) active = true;
+      }
+    }
+    if (active) {
+      idle = 0;
+    } else {
+      ++idle;
+      __nanosleep(1000);
+    }
+  }
+}
+
 // Rows [r0, r1) of a segment: the proper-template row routine 32 rows at a time (coordinates of span
 // < 2^26), else the chunked class-code routine.
 template <int K>
@@ -344,8 +451,8 @@ __device__ __forceinline__ void serve_kopt_item(const ServeJob& job, const Serve
 // 45 pair distances at this budget, and 3 or 2 blocks (80 / 128 registers) measured no faster for
 // k-opt jobs, whose results are bound by the PCIe download, and slower for JV jobs.
 static __global__ void __launch_bounds__(kServeWarps * 32, 4)
-    serve_kernel(ServeControl* ctl, uint32_t* finished, const uint8_t* templates, int32_t slots,
-                 long long idle_limit) {
+    serve_kernel(ServeControl* ctl, const ServeMailbox* mailbox, uint32_t* finished, const uint8_t* templates,
+                 int32_t slots, long long idle_limit) {
   __shared__ JvWarpScratch jv_scratch[kServeWarps];
   __shared__ __align__(16) unsigned char kopt_scratch[kServeWarps][kServeKoptScratch];
   __shared__ ServeJob job_copy[kServeWarps];
@@ -353,6 +460,10 @@ static __global__ void __launch_bounds__(kServeWarps * 32, 4)
   for (int i = threadIdx.x; i < kServeTemplateBytes; i += blockDim.x) tpairs[i] = templates[i];
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (blockIdx.x == 0 && warp == kServeWarps - 1) {  // no block-wide barrier follows
+    serve_dispatch(ctl, mailbox, slots, idle_limit, lane);
+    return;
+  }
   ServeJob& job = job_copy[warp];
   int held = -1;  // slot whose descriptor `job` holds
   long long idle = 0;

@@ -508,6 +508,13 @@ int cee_serve_submit_kopt_improving(cee_ctx* ctx, int32_t snapshot, int32_t segm
 int cee_serve_poll(cee_ctx* ctx, cee_serve_event* events, int32_t capacity, int32_t* count);
 /* Jobs admitted and not yet returned by cee_serve_poll, and arena bytes in use. */
 int cee_serve_pending(const cee_ctx* ctx, int32_t* jobs, uint64_t* arena_used);
+/* Totals since cee_serve_start. */
+typedef struct {
+  uint64_t jobs;           /* jobs posted to the kernel */
+  uint64_t rows_bytes;     /* k-opt rows copied to the device */
+  uint64_t download_bytes; /* results copied back to the host */
+} cee_serve_stats;
+int cee_serve_get_stats(const cee_ctx* ctx, cee_serve_stats* stats);
 /* Stops the kernel and frees the arena. Outstanding jobs are dropped; a dropped job's downloads
  * (results complete or not) may still write its output buffers until this call returns. */
 int cee_serve_stop(cee_ctx* ctx);

@@ -340,6 +340,37 @@ def test_malformed_requests(snapshots):
         c.close()
 
 
+def test_rows_pinned_unaligned_and_pageable(ctx, snapshots):
+    """k-opt rows from page-locked memory (16-byte aligned or not) and from pageable memory all give
+    the regular entry point's cells; the loop's counters record the jobs and the bytes moved."""
+    import torch
+    g, kt = snapshots["kopt"], snapshots["_ktasks"]
+    rows = np.ascontiguousarray(kt[5][:2000])
+    want = ctx.kopt_costs_multi(g, [5], [rows])[0][0]
+    nb = rows.nbytes
+    owner = torch.empty(nb + 64, dtype=torch.uint8).pin_memory()
+    base = owner.numpy()
+    aligned = base[:nb].view(KOPT_TASK_DTYPE)
+    unaligned = base[4:4 + nb].view(KOPT_TASK_DTYPE)
+    c = Context(0)
+    try:
+        c.serve_start(ServeConfig(hbm_budget_bytes=256 << 20, slots=4, idle_ms=20))
+        sid = c.serve_add_snapshot(g)
+        for tag, arr in ((1, unaligned), (2, aligned), (3, rows.copy())):
+            arr[:] = rows
+            before = c.serve_stats()
+            assert c.serve_submit_kopt(sid, [5], [arr], tag) is not None
+            got = drain(c, 1)[tag]
+            np.testing.assert_array_equal(got[0], want)
+            after = c.serve_stats()
+            assert after["rows_bytes"] - before["rows_bytes"] == nb
+            assert after["download_bytes"] - before["download_bytes"] == want.nbytes
+        assert after["jobs"] == 3
+        c.serve_stop()
+    finally:
+        c.close()
+
+
 def test_job_errors_stay_with_their_job(ctx, snapshots):
     """Device bounds checks are reported per job. A k-opt job whose pinned rows the caller rewrites
     with an out-of-range node after the submit-time check (the device copies them late) may fail
