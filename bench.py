@@ -89,12 +89,41 @@ KERNEL_SOURCES = {
 }
 
 
-def source_digest(kernel: str) -> str:
+def strip_comments(text: str) -> str:
+    """C/C++ source without its comments and trailing blanks (string and character literals kept),
+    so that a digest names the code, not its commentary."""
+    out, i, n = [], 0, len(text)
+    while i < n:
+        c = text[i]
+        if c in "\"'":
+            j = i + 1
+            while j < n and text[j] != c:
+                j += 2 if text[j] == "\\" else 1
+            out.append(text[i:j + 1])
+            i = j + 1
+        elif text.startswith("//", i):
+            j = text.find("\n", i)
+            i = n if j < 0 else j
+        elif text.startswith("/*", i):
+            j = text.find("*/", i + 2)
+            i = n if j < 0 else j + 2
+        else:
+            out.append(c)
+            i += 1
+    lines = ("".join(out)).split("\n")
+    return "\n".join(line.rstrip() for line in lines if line.strip())
+
+
+def source_digest(kernel: str, read=None) -> str:
+    """sha256 over the kernel's source files, comments stripped (`read(name)` gives a file's text;
+    default: the working tree)."""
     import hashlib
+    if read is None:
+        read = lambda name: (ROOT / "cudaedgeelimination_b200" / "csrc" / name).read_text()
     h = hashlib.sha256()
     for name in KERNEL_SOURCES[kernel]:
         h.update(name.encode())
-        h.update((ROOT / "cudaedgeelimination_b200" / "csrc" / name).read_bytes())
+        h.update(strip_comments(read(name)).encode())
     return h.hexdigest()
 
 
@@ -786,7 +815,7 @@ def _latency_summary(lat_s):
 def serve_drive(ctx, wl, sids, ksids, arrivals, buffers, keep_every: int, leaf: bool = False):
     """Feeds the jobs into the serving loop at their arrival times (admitting while it accepts
     them), polls completions, and returns (completion - arrival latencies, wall seconds, kept
-    sample outputs)."""
+    sample outputs: every keep_every-th job's, none for 0)."""
     n = len(wl.jobs)
     free = list(range(len(buffers)))
     inflight = {}
@@ -812,7 +841,7 @@ def serve_drive(ctx, wl, sids, ksids, arrivals, buffers, keep_every: int, leaf: 
         for jid, tag, res in ctx.serve_poll():
             idx, b = inflight.pop(jid)
             latency[idx] = time.perf_counter() - t0 - arrivals[idx]
-            if idx % keep_every == 0:
+            if keep_every and idx % keep_every == 0:
                 kept[idx] = _copy_result(res)
             free.append(b)
             done += 1
@@ -844,7 +873,7 @@ def plain_drive(ctx, wl, arrivals, buffer, keep_every: int, leaf: bool = False):
         end = time.perf_counter()
         service[idx] = end - s0
         latency[idx] = end - t0 - arrivals[idx]
-        if idx % keep_every == 0:
+        if keep_every and idx % keep_every == 0:
             kept[idx] = _copy_result(out)
     return latency, service, time.perf_counter() - t0, kept
 
@@ -922,12 +951,13 @@ def run_serve(args, device, world, parity=None, leaf: bool = False, wl=None):
     ksids = [ctx.serve_add_snapshot(g) for g, _ in wl.kopt]
     assert None not in sids and None not in ksids
     keep_every = max(1, len(wl.jobs) // 100)
-    # warm-up on the first jobs, then capacity: every job queued at t = 0 (closed loop)
+    # warm-up on the first jobs, then capacity: every job queued at t = 0 (closed loop); the parity
+    # sample is kept from the Poisson run, so the capacity runs of both arms copy no results aside
     warm = synth.ServeWorkload.__new__(synth.ServeWorkload)
     warm.__dict__.update(wl.__dict__)
     warm.jobs = wl.jobs[:min(200, len(wl.jobs))]
-    serve_drive(ctx, warm, sids, ksids, np.zeros(len(warm.jobs)), buffers[:slots], keep_every, leaf)
-    _, cap_s, _ = serve_drive(ctx, wl, sids, ksids, np.zeros(len(wl.jobs)), buffers[:slots], keep_every, leaf)
+    serve_drive(ctx, warm, sids, ksids, np.zeros(len(warm.jobs)), buffers[:slots], 0, leaf)
+    _, cap_s, _ = serve_drive(ctx, wl, sids, ksids, np.zeros(len(wl.jobs)), buffers[:slots], 0, leaf)
     capacity = len(wl.jobs) / cap_s
     lam = 0.8 * capacity
     arrivals = np.cumsum(wl.gaps) / lam
@@ -936,10 +966,8 @@ def run_serve(args, device, world, parity=None, leaf: bool = False, wl=None):
     ctx.close()
 
     plain_ctx = Context(device)
-    _, service, plain_closed_s, _ = plain_drive(plain_ctx, warm, np.zeros(len(warm.jobs)), buffers[slots], keep_every,
-                                                leaf)
-    _, service, plain_closed_s, _ = plain_drive(plain_ctx, wl, np.zeros(len(wl.jobs)), buffers[slots], keep_every,
-                                                leaf)
+    _, service, plain_closed_s, _ = plain_drive(plain_ctx, warm, np.zeros(len(warm.jobs)), buffers[slots], 0, leaf)
+    _, service, plain_closed_s, _ = plain_drive(plain_ctx, wl, np.zeros(len(wl.jobs)), buffers[slots], 0, leaf)
     plain_capacity = len(wl.jobs) / plain_closed_s
     plain_lat, _, plain_wall, plain_kept = plain_drive(plain_ctx, wl, arrivals, buffers[slots], keep_every, leaf)
     plain_ctx.close()

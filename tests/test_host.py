@@ -85,3 +85,15 @@ def test_tuning_cache_roundtrip(tmp_path):
     assert again.get(key) == {"jv_tile": 64, "blocks_per_sm": 8, "chunks": 8}
     path.write_text('{"version": 0, "entries": {"x": 1}}')  # another format: ignored, not an error
     assert TuningCache(path).get("x") is None
+
+
+def test_traffic_digest_ignores_comments_only():
+    """The digest that ties a recorded ncu traffic figure to its kernel's sources changes with the
+    code and not with its comments; string and character literals count as code."""
+    import bench
+    src = 'int a = 1; // one\n/* block\n comment */ const char* s = "//x"; char c = \'/\';\n'
+    assert bench.strip_comments(src) == 'int a = 1;\n const char* s = "//x"; char c = \'/\';'
+    assert bench.strip_comments(src.replace("// one", "// other")) == bench.strip_comments(src)
+    assert bench.strip_comments(src.replace('"//x"', '"//y"')) != bench.strip_comments(src)
+    for kernel in bench.KERNEL_SOURCES:
+        assert len(bench.source_digest(kernel)) == 64
