@@ -110,7 +110,8 @@ class ServeEvent(ctypes.Structure):
 
 
 class ServeStats(ctypes.Structure):
-    _fields_ = [("jobs", ctypes.c_uint64), ("rows_bytes", ctypes.c_uint64), ("download_bytes", ctypes.c_uint64)]
+    _fields_ = [("jobs", ctypes.c_uint64), ("rows_bytes", ctypes.c_uint64), ("download_bytes", ctypes.c_uint64),
+                ("direct_bytes", ctypes.c_uint64)]
 
 
 class NativeError(RuntimeError):

@@ -347,7 +347,8 @@ class ServeMixin:
         return jobs.value, used.value
 
     def serve_stats(self) -> dict:
-        """Totals since serve_start: jobs posted, k-opt row bytes uploaded, result bytes downloaded."""
+        """Totals since serve_start: jobs posted, k-opt row bytes uploaded, result bytes downloaded, and
+        result bytes the kernel wrote in place into page-locked buffers."""
         st = _native.ServeStats()
         _native.check(self.handle, _native.lib().cee_serve_get_stats(self.handle, ctypes.byref(st)))
         return {name: int(getattr(st, name)) for name, _ in st._fields_}

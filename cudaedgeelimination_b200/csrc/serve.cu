@@ -97,6 +97,7 @@ struct ServeJobHost {
   int snapshot = -1;
   uint64_t tag = 0;
   int phase = 0;  // 0: on the GPU, 1: downloading, 2: done (no device work)
+  bool direct = false;  // the kernel writes the outputs straight into page-locked host memory
   int status = CEE_OK;
   std::vector<std::pair<size_t, size_t>> regions;  // arena (offset, bytes) to free
   std::vector<Download> downloads;
@@ -212,6 +213,46 @@ int FreeSlot(const ServeState& s) {
     if (!s.slot_busy[slot]) return slot;
   }
   return -1;
+}
+
+// cuPointerGetAttribute, from the driver through the runtime (the library links only cudart).
+using PointerAttributeFn = CUresult (*)(void*, CUpointer_attribute, CUdeviceptr);
+PointerAttributeFn PointerAttribute() {
+  static const PointerAttributeFn fn = [] {
+    void* entry = nullptr;
+    cudaDriverEntryPointQueryResult found = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuPointerGetAttribute", &entry, 12000, cudaEnableDefault, &found) !=
+            cudaSuccess ||
+        found != cudaDriverEntryPointSuccess) {
+      return static_cast<PointerAttributeFn>(nullptr);
+    }
+    return reinterpret_cast<PointerAttributeFn>(entry);
+  }();
+  return fn;
+}
+
+// The device address of the `bytes` bytes at `p` when all of them lie in one page-locked,
+// device-mapped host allocation and `p` is `align`-byte aligned (the kernel may then write them in
+// place), else null.
+void* MappedRange(void* p, size_t bytes, size_t align) {
+  if (p == nullptr || bytes == 0 || reinterpret_cast<uintptr_t>(p) % align != 0) return nullptr;
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  if (a.type != cudaMemoryTypeHost || a.devicePointer == nullptr) return nullptr;
+  const PointerAttributeFn get = PointerAttribute();
+  if (get == nullptr) return nullptr;
+  const CUdeviceptr d = reinterpret_cast<CUdeviceptr>(a.devicePointer);
+  CUdeviceptr start = 0;
+  size_t size = 0;
+  if (get(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, d) != CUDA_SUCCESS ||
+      get(&size, CU_POINTER_ATTRIBUTE_RANGE_SIZE, d) != CUDA_SUCCESS) {
+    return nullptr;
+  }
+  if (d % align != 0 || d < start || d - start > size || bytes > size - (d - start)) return nullptr;
+  return a.devicePointer;
 }
 
 // Posts `desc` in `slot`: the descriptor, then (release) its generation, into the mapped mailbox,
@@ -644,13 +685,17 @@ int cee_serve_submit_jv(cee_ctx* ctx, int32_t snapshot, int32_t* witness_out, ui
   if (slot < 0) return CEE_BUSY;  // every slot holds a job
   size_t out = 0;
   const size_t out_bytes = static_cast<size_t>(snap.m) * 4;
-  if (!s.arena.Allocate(out_bytes, &out)) return CEE_BUSY;
+  // a page-locked witness array is written by the kernel in place: no arena room, no download
+  void* direct = MappedRange(witness_out, out_bytes, 4);
+  if (direct == nullptr && !s.arena.Allocate(out_bytes, &out)) return CEE_BUSY;
   ServeJob desc{};
   desc.generation = s.next_generation++;
   desc.type = kServeJv;
   desc.span = snap.span;
   desc.g = snap.g;
-  desc.witness = reinterpret_cast<int32_t*>(static_cast<uint8_t*>(s.arena_buf.ptr) + out);
+  desc.witness = direct != nullptr ? static_cast<int32_t*>(direct)
+                                   : reinterpret_cast<int32_t*>(static_cast<uint8_t*>(s.arena_buf.ptr) + out);
+  desc.host_outputs = direct != nullptr ? 1u : 0u;
   desc.items = static_cast<uint32_t>((snap.m + kServeJvTile - 1) / kServeJvTile);
   s.slot_busy[slot] = true;
   s.next_slot = (slot + 1) % s.cfg.slots;
@@ -658,15 +703,20 @@ int cee_serve_submit_jv(cee_ctx* ctx, int32_t snapshot, int32_t* witness_out, ui
   job.slot = slot;
   job.generation = desc.generation;
   job.snapshot = snapshot;
-  job.regions.push_back({out, out_bytes});
-  job.downloads.push_back({witness_out, out, out_bytes});
+  job.direct = direct != nullptr;
   ++snap.refs;
   ++s.pending;
   *job_out = id;
-  rc = ArmDownloads(ctx, s, job);
-  if (rc != CEE_OK) {
-    ReleaseJob(s, job);
-    return rc;
+  if (job.direct) {
+    s.stats.direct_bytes += out_bytes;
+  } else {
+    job.regions.push_back({out, out_bytes});
+    job.downloads.push_back({witness_out, out, out_bytes});
+    rc = ArmDownloads(ctx, s, job);
+    if (rc != CEE_OK) {
+      ReleaseJob(s, job);
+      return rc;
+    }
   }
   return Publish(ctx, s, slot, desc);
 }
@@ -862,6 +912,11 @@ int cee_serve_poll(cee_ctx* ctx, cee_serve_event* events, int32_t capacity, int3
       }
       if (reinterpret_cast<volatile uint32_t*>(s.finished_host)[kServeMaxSlots + job.slot] != 0) {
         job.status = Fail(ctx, CEE_ERR_INVALID, "serving loop: device bounds check rejected an out-of-range index");
+      }
+      if (job.direct) {  // the outputs are in place (the kernel fenced them before the finished word)
+        std::atomic_thread_fence(std::memory_order_acquire);
+        if (!report(id, job)) break;
+        continue;
       }
       IssueDownloads(s, job.slot);  // unless the downloader thread already has
       int state = kTicketIssuing;

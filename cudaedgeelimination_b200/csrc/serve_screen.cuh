@@ -61,6 +61,8 @@ struct ServeJob {
   int32_t segments;
   uint32_t items;
   uint32_t rows_gate;  // 1: install only once the slot's rows-ready word equals the generation
+  uint32_t host_outputs;  // 1: the outputs are page-locked host memory, written in place
+  uint32_t pad;
   JvGraph g;  // JV jobs; k-opt jobs use g.xy / g.n / g.dist_type
   int32_t* witness;
   ServeSegment seg[3];
@@ -537,14 +539,17 @@ static __global__ void __launch_bounds__(kServeWarps * 32, 4)
     if (job.type == kServeJv) {
       const int64_t e0 = local * kServeJvTile;
       const int64_t e1 = min(e0 + kServeJvTile, job.g.m);
+      int32_t mine = -1;  // the witness of edge e0 + lane
       for (int64_t e = e0; e < e1; ++e) {
         const int32_t wv =
             job.span == kSpanSmall    ? jv_screen_edge_warp<kSpanSmall, true>(job.g, e, jv_scratch[warp], lane, error)
             : job.span == kSpanNarrow ? jv_screen_edge_warp<kSpanNarrow, true>(job.g, e, jv_scratch[warp], lane, error)
                                       : jv_screen_edge_warp<kSpanWide, true>(job.g, e, jv_scratch[warp], lane, error);
-        if (lane == 0) job.witness[e] = wv;
+        const int32_t w0 = __shfl_sync(kFullMask, wv, 0);
+        if (lane == static_cast<int>(e - e0)) mine = w0;
         __syncwarp();
       }
+      if (e0 + lane < e1) job.witness[e0 + lane] = mine;  // one 128-byte store per item
     } else {
       int si = 0;
       while (si + 1 < job.segments && local >= job.seg[si + 1].item_begin) ++si;
@@ -562,7 +567,12 @@ static __global__ void __launch_bounds__(kServeWarps * 32, 4)
         serve_kopt_item<5>(job, S, r0, r1, tp, valid, ks, lane, error);
       }
     }
-    __threadfence();  // this warp's outputs before its done count
+    // this warp's outputs before its done count (a release at GPU scope). Outputs in page-locked host
+    // memory need no system-scope fence here: the warp finishing the job acquires every done count
+    // and then releases at system scope (fence + finished word), and causality order is transitive
+    // across those synchronizations, so the host that acquires the finished word sees every warp's
+    // writes.
+    __threadfence();
     __syncwarp();
     if (lane == 0) {
       const unsigned long long d = atomicAdd(&ctl->done[slot], 1ull);

@@ -481,7 +481,10 @@ int cee_serve_add_snapshot(cee_ctx* ctx, const cee_graph_view* graph, int32_t* s
 /* The snapshot's memory returns to the arena once its last job has completed. */
 int cee_serve_release_snapshot(cee_ctx* ctx, int32_t snapshot);
 /* Screens every edge of the snapshot; witness_out (m entries) is written before the job's
- * completion event is returned by cee_serve_poll. CEE_BUSY: no slot or arena room now. */
+ * completion event is returned by cee_serve_poll. A witness_out that lies in one page-locked host
+ * allocation (cudaHostAlloc, a pinned torch tensor), 4-byte aligned, is written by the kernel in
+ * place as the job runs (no arena room, no copy); other buffers get a copy when the job ends.
+ * CEE_BUSY: no slot or arena room now. */
 int cee_serve_submit_jv(cee_ctx* ctx, int32_t snapshot, int32_t* witness_out, uint64_t tag,
                         int32_t* job);
 /* k-opt leaf costs of 1..3 segments (k = ks[s], rows[s] rows at tasks[s], output costs_out[s],
@@ -513,6 +516,7 @@ typedef struct {
   uint64_t jobs;           /* jobs posted to the kernel */
   uint64_t rows_bytes;     /* k-opt rows copied to the device */
   uint64_t download_bytes; /* results copied back to the host */
+  uint64_t direct_bytes;   /* results the kernel wrote straight into page-locked host memory */
 } cee_serve_stats;
 int cee_serve_get_stats(const cee_ctx* ctx, cee_serve_stats* stats);
 /* Stops the kernel and frees the arena. Outstanding jobs are dropped; a dropped job's downloads

@@ -371,6 +371,37 @@ def test_rows_pinned_unaligned_and_pageable(ctx, snapshots):
         c.close()
 
 
+def test_jv_witness_written_in_place(ctx, snapshots):
+    """A page-locked witness buffer is written by the kernel in place (no download), a pageable one
+    and a page-locked one at an address that is not 4-byte aligned get a copy; all three equal the
+    regular entry point's witnesses, and the counters say which path each took."""
+    import torch
+    g = snapshots["clustered"]
+    want = ctx.jv_screen(g)[0]
+    nb = 4 * g.m
+    owner = torch.empty(nb + 64, dtype=torch.uint8).pin_memory()
+    base = owner.numpy()
+    in_place = base[:nb].view(np.int32)
+    odd = np.frombuffer(base[2:2 + nb].data, dtype=np.int32)
+    c = Context(0)
+    try:
+        c.serve_start(ServeConfig(hbm_budget_bytes=64 << 20, slots=4, idle_ms=20))
+        sid = c.serve_add_snapshot(g)
+        for tag, out, direct in ((1, in_place, True), (2, np.empty(g.m, np.int32), False), (3, odd, False)):
+            out[:] = -7
+            before = c.serve_stats()
+            assert c.serve_submit_jv(sid, g.m, tag, out=out) is not None
+            got = drain(c, 1)[tag]
+            np.testing.assert_array_equal(got, want)
+            np.testing.assert_array_equal(out, want)
+            after = c.serve_stats()
+            moved = (after["direct_bytes"] - before["direct_bytes"], after["download_bytes"] - before["download_bytes"])
+            assert moved == ((nb, 0) if direct else (0, nb)), (tag, moved)
+        c.serve_stop()
+    finally:
+        c.close()
+
+
 def test_job_errors_stay_with_their_job(ctx, snapshots):
     """Device bounds checks are reported per job. A k-opt job whose pinned rows the caller rewrites
     with an out-of-range node after the submit-time check (the device copies them late) may fail
