@@ -7,6 +7,7 @@ import pathlib
 
 PKG = pathlib.Path(__file__).resolve().parent
 LIB_PATH = PKG / "libcee.so"
+CEE_JV_STATIC_UNCHANGED = 1  # include/cee.h
 
 c_i32p = ctypes.POINTER(ctypes.c_int32)
 c_i64p = ctypes.POINTER(ctypes.c_int64)
@@ -150,6 +151,8 @@ def lib() -> ctypes.CDLL:
             "cee_ctx_clear": (ctypes.c_int, [vp, ctypes.c_uint]),
             "cee_ctx_set_option": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int64]),
             "cee_jv_screen": (ctypes.c_int, [vp, ctypes.POINTER(GraphView), c_i32p, ctypes.POINTER(JvStats)]),
+            "cee_jv_screen_ex": (ctypes.c_int, [vp, ctypes.POINTER(GraphView), c_i32p, ctypes.POINTER(JvStats),
+                                                ctypes.c_uint32]),
             "cee_jv_prepare": (ctypes.c_int, [vp, ctypes.POINTER(GraphView), ctypes.POINTER(JvStats)]),
             "cee_jv_launch": (ctypes.c_int, [vp]),
             "cee_jv_fetch": (ctypes.c_int, [vp, c_i32p]),

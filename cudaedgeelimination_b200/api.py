@@ -442,13 +442,17 @@ class Context(BatchMixin, ServeMixin):
         _native.check(self.handle, _native.lib().cee_ctx_clear(self.handle, what))
 
     # ---- JV -------------------------------------------------------------------------
-    def jv_screen(self, graph: GraphSnapshot, out: np.ndarray | None = None) -> tuple[np.ndarray, _native.JvStats]:
+    def jv_screen(self, graph: GraphSnapshot, out: np.ndarray | None = None,
+                  static_unchanged: bool = False) -> tuple[np.ndarray, _native.JvStats]:
+        """cee_jv_screen; with static_unchanged, cee_jv_screen_ex's CEE_JV_STATIC_UNCHANGED hint (the
+        caller vouches that coordinates, endpoints and weights equal this context's previous JV call's)."""
         witness = np.empty(graph.m, np.int32) if out is None else out
         assert witness.dtype == np.int32 and witness.flags.c_contiguous and witness.shape[0] >= graph.m
         stats = _native.JvStats()
         view = graph.view()
-        _native.check(self.handle, _native.lib().cee_jv_screen(
-            self.handle, ctypes.byref(view), witness.ctypes.data_as(_native.c_i32p), ctypes.byref(stats)))
+        flags = _native.CEE_JV_STATIC_UNCHANGED if static_unchanged else 0
+        _native.check(self.handle, _native.lib().cee_jv_screen_ex(
+            self.handle, ctypes.byref(view), witness.ctypes.data_as(_native.c_i32p), ctypes.byref(stats), flags))
         return witness, stats
 
     def jv_prepare(self, graph: GraphSnapshot) -> _native.JvStats:

@@ -225,16 +225,19 @@ static __global__ void root_error_kernel(uint32_t lo, uint32_t hi, unsigned long
 
 // ---------------------------------------------------------------- JV --------------------
 
-int JvPrepare(cee_ctx* ctx, const cee_graph_view* g, cee_jv_stats* stats) {
+// flags: CEE_JV_STATIC_UNCHANGED skips the element-wise comparison of the static arrays with the
+// cached ones (the caller vouches for them); the sizes and the distance type are compared always.
+int JvPrepare(cee_ctx* ctx, const cee_graph_view* g, cee_jv_stats* stats, uint32_t flags = 0) {
   int rc = ValidateView(ctx, g);
   if (rc != CEE_OK) return rc;
   JvState& s = ctx->jv;
   s.prepared = false;
   cudaStream_t st = ctx->stream;
+  const bool vouched = (flags & CEE_JV_STATIC_UNCHANGED) != 0;
   const bool static_hit = s.has_static && s.n == g->n && s.dist_type == g->dist_type && s.m == g->m &&
-                          SameArray(s.hx, g->x, g->n) && SameArray(s.hy, g->y, g->n) &&
-                          SameArray(s.heu, g->edge_u, g->m) && SameArray(s.hev, g->edge_v, g->m) &&
-                          SameArray(s.hw, g->edge_w, g->m);
+                          (vouched || (SameArray(s.hx, g->x, g->n) && SameArray(s.hy, g->y, g->n) &&
+                                       SameArray(s.heu, g->edge_u, g->m) && SameArray(s.hev, g->edge_v, g->m) &&
+                                       SameArray(s.hw, g->edge_w, g->m)));
   cudaEventRecord(ctx->ev[0], st);
   int64_t h2d = 0;
   if (!static_hit) {
@@ -305,8 +308,8 @@ int JvPrepare(cee_ctx* ctx, const cee_graph_view* g, cee_jv_stats* stats) {
   s.prepared = true;
   s.last_h2d_bytes = h2d;
   s.edges_screened = 0;
-  for (int64_t e = 0; e < g->m; ++e) s.edges_screened += g->active[e] != 0;
   if (stats != nullptr) {
+    for (int64_t e = 0; e < g->m; ++e) s.edges_screened += g->active[e] != 0;
     stats->static_hit = static_hit ? 1 : 0;
     stats->workspace_hit = grew ? 0 : 1;
     stats->resident_bytes = JvResident(s);
@@ -1048,10 +1051,16 @@ int cee_jv_fetch(cee_ctx* ctx, int32_t* witness_out) {
 }
 
 int cee_jv_screen(cee_ctx* ctx, const cee_graph_view* graph, int32_t* witness_out, cee_jv_stats* stats) {
+  return cee_jv_screen_ex(ctx, graph, witness_out, stats, 0u);
+}
+
+int cee_jv_screen_ex(cee_ctx* ctx, const cee_graph_view* graph, int32_t* witness_out, cee_jv_stats* stats,
+                     uint32_t flags) {
   int rc = Activate(ctx);
   if (rc != CEE_OK) return rc;
+  if ((flags & ~CEE_JV_STATIC_UNCHANGED) != 0) return Fail(ctx, CEE_ERR_INVALID, "unknown JV screen flags");
   cee_jv_stats local{};
-  rc = JvPrepare(ctx, graph, &local);
+  rc = JvPrepare(ctx, graph, stats != nullptr ? &local : nullptr, flags);
   if (rc != CEE_OK) return Drained(ctx, rc);
   cudaEventRecord(ctx->ev[2], ctx->stream);
   rc = JvLaunch(ctx);

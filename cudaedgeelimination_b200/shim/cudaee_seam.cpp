@@ -24,8 +24,10 @@
 #include "cuda_edge_elimination/hamilton_tutte.hpp"
 #include "cuda_edge_elimination/local_search.hpp"
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <omp.h>
 #include <limits>
 #include <stdexcept>
 #include <string>
@@ -97,33 +99,66 @@ cee_ctx* RequireContext(int* selected_device, const char* what) {
   return ContextFor(device);
 }
 
-// Flat host arrays behind a cee_graph_view of a GraphSnapshot (Point and Edge are structs).
+// Flat host arrays behind a cee_graph_view of a GraphSnapshot (Point and Edge are structs), kept
+// across calls. Bind refreshes them in one pass that compares each static value (coordinates,
+// edge endpoints and weights: the reference's resident-cache key, src/cuda/jv_cuda.cu:360-382)
+// with the kept one and writes only what differs, so that it knows whether the static content
+// changed. `jv_ctx` is the context whose JV static cache was last loaded from this content.
+constexpr int64_t kParallelElements = 1 << 16;
+
 struct SnapshotArrays {
   std::vector<int64_t> x, y, w;
   std::vector<int32_t> u, v;
   std::vector<uint8_t> active;
+  std::vector<int32_t> witness;
+  int32_t dimension = -1, distance_type = -1;
+  cee_ctx* jv_ctx = nullptr;
   cee_graph_view view{};
 
-  void Bind(const GraphSnapshot& graph, bool with_edges) {
-    const size_t n = graph.points.size();
-    x.resize(n);
-    y.resize(n);
-    for (size_t i = 0; i < n; ++i) {
-      x[i] = graph.points[i].integer_x;
-      y[i] = graph.points[i].integer_y;
+  // Returns true when the static content equals the previous Bind's. Each element is compared
+  // and stored in the same pass (an OR of XORs), on the OpenMP team for large snapshots.
+  bool Bind(const GraphSnapshot& graph, bool with_edges) {
+    const int64_t n = static_cast<int64_t>(graph.points.size());
+    const int64_t m = with_edges ? static_cast<int64_t>(graph.edges.size()) : 0;
+    const bool sized = static_cast<int64_t>(x.size()) == n && static_cast<int64_t>(u.size()) == m &&
+                       dimension == graph.dimension && distance_type == static_cast<int32_t>(graph.distance_type);
+    x.resize(static_cast<size_t>(n));
+    y.resize(static_cast<size_t>(n));
+    u.resize(static_cast<size_t>(m));
+    v.resize(static_cast<size_t>(m));
+    w.resize(static_cast<size_t>(m));
+    active.resize(static_cast<size_t>(m));
+    const Point* pts = graph.points.data();
+    const Edge* eds = graph.edges.data();
+    int64_t* px = x.data();
+    int64_t* py = y.data();
+    int32_t* pu = u.data();
+    int32_t* pv = v.data();
+    int64_t* pw = w.data();
+    uint8_t* pa = active.data();
+    uint64_t diff = 0;
+#pragma omp parallel for schedule(static) reduction(| : diff) if (n + m > kParallelElements)
+    for (int64_t i = 0; i < n + m; ++i) {
+      if (i < n) {
+        const int64_t a = pts[i].integer_x, b = pts[i].integer_y;
+        diff |= static_cast<uint64_t>(px[i] ^ a) | static_cast<uint64_t>(py[i] ^ b);
+        px[i] = a;
+        py[i] = b;
+      } else {
+        const int64_t e = i - n;
+        const Edge& edge = eds[e];
+        diff |= static_cast<uint64_t>(static_cast<uint32_t>(pu[e] ^ edge.u) | static_cast<uint32_t>(pv[e] ^ edge.v)) |
+                static_cast<uint64_t>(pw[e] ^ edge.weight);
+        pu[e] = edge.u;
+        pv[e] = edge.v;
+        pw[e] = edge.weight;
+        pa[e] = edge.active ? 1 : 0;
+      }
     }
-    const size_t m = with_edges ? graph.edges.size() : 0;
-    u.resize(m);
-    v.resize(m);
-    w.resize(m);
-    active.resize(m);
-    for (size_t e = 0; e < m; ++e) {
-      const Edge& edge = graph.edges[e];
-      u[e] = edge.u;
-      v[e] = edge.v;
-      w[e] = edge.weight;
-      active[e] = edge.active ? 1 : 0;
-    }
+    const bool same = sized && diff == 0;
+    dimension = graph.dimension;
+    distance_type = static_cast<int32_t>(graph.distance_type);
+    if (!same) jv_ctx = nullptr;
     view = cee_graph_view{};
     view.n = graph.dimension;
     view.dist_type = static_cast<int32_t>(graph.distance_type);
@@ -138,6 +173,7 @@ struct SnapshotArrays {
     view.row_offsets = graph.row_offsets.data();
     view.neighbors = graph.neighbors.data();
     view.csr_edge_ids = graph.csr_edge_ids.data();
+    return same;
   }
 };
 
@@ -158,11 +194,17 @@ std::vector<Candidate> FindJvCandidatesCuda(const GraphSnapshot& graph, int* con
   }
   cee_ctx* ctx = RequireContext(selected_device, "CUDA JV backend");
   if (graph.edges.empty()) return {};
-  g_arrays.Bind(graph, true);
-  std::vector<int32_t> witness(graph.edges.size());
+  const bool same = g_arrays.Bind(graph, true);
+  // this context's static cache holds exactly the kept content: skip its second comparison
+  const uint32_t hint = same && g_arrays.jv_ctx == ctx ? CEE_JV_STATIC_UNCHANGED : 0u;
+  std::vector<int32_t>& witness = g_arrays.witness;
+  witness.resize(graph.edges.size());
   cee_jv_stats stats{};
-  const int status = cee_jv_screen(ctx, &g_arrays.view, witness.data(), &stats);
+  g_arrays.jv_ctx = nullptr;
+  const int status =
+      cee_jv_screen_ex(ctx, &g_arrays.view, witness.data(), cache_usage != nullptr ? &stats : nullptr, hint);
   if (status != CEE_OK) Raise(status, ctx, "B200 JV screen");
+  g_arrays.jv_ctx = ctx;
   if (cache_usage != nullptr) {
     cache_usage->static_hit = stats.static_hit != 0;
     cache_usage->workspace_hit = stats.workspace_hit != 0;
@@ -177,9 +219,27 @@ std::vector<Candidate> FindJvCandidatesCuda(const GraphSnapshot& graph, int* con
     cache_usage->kernel_ms = stats.kernel_ms;
     cache_usage->d2h_ms = stats.d2h_ms;
   }
-  std::vector<Candidate> candidates;
-  for (size_t e = 0; e < witness.size(); ++e) {
-    if (witness[e] >= 0) candidates.push_back({static_cast<int32_t>(e), witness[e], EliminationMethod::kJv});
+  // the edges with a witness, ascending: counted per block of edges, then written at each block's
+  // offset (on the OpenMP team for large snapshots)
+  const int64_t m = static_cast<int64_t>(witness.size());
+  const int64_t blocks = m > kParallelElements ? std::min<int64_t>(4 * omp_get_max_threads(), m / 4096 + 1) : 1;
+  std::vector<int64_t> at(static_cast<size_t>(blocks) + 1, 0);
+  const int32_t* wit = witness.data();
+#pragma omp parallel for schedule(static) if (blocks > 1)
+  for (int64_t b = 0; b < blocks; ++b) {
+    int64_t count = 0;
+    for (int64_t e = m * b / blocks; e < m * (b + 1) / blocks; ++e) count += wit[e] >= 0 ? 1 : 0;
+    at[static_cast<size_t>(b) + 1] = count;
+  }
+  for (int64_t b = 0; b < blocks; ++b) at[static_cast<size_t>(b) + 1] += at[static_cast<size_t>(b)];
+  std::vector<Candidate> candidates(static_cast<size_t>(at[static_cast<size_t>(blocks)]));
+  Candidate* out = candidates.data();
+#pragma omp parallel for schedule(static) if (blocks > 1)
+  for (int64_t b = 0; b < blocks; ++b) {
+    int64_t k = at[static_cast<size_t>(b)];
+    for (int64_t e = m * b / blocks; e < m * (b + 1) / blocks; ++e) {
+      if (wit[e] >= 0) out[k++] = Candidate{static_cast<int32_t>(e), wit[e], EliminationMethod::kJv};
+    }
   }
   return candidates;
 }
@@ -187,6 +247,7 @@ std::vector<Candidate> FindJvCandidatesCuda(const GraphSnapshot& graph, int* con
 void ClearJvCudaCache() {
   for (auto& entry : g_threads.contexts) cee_ctx_clear(entry.second, 1u);
   g_threads.preferred = -1;
+  g_arrays.jv_ctx = nullptr;
 }
 
 namespace detail {

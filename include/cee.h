@@ -162,6 +162,15 @@ typedef struct {
  * active bits and the CSR are uploaded on every call. */
 int cee_jv_screen(cee_ctx* ctx, const cee_graph_view* graph, int32_t* witness_out,
                   cee_jv_stats* stats);
+/* cee_jv_screen with hints (no counterpart in the reference). CEE_JV_STATIC_UNCHANGED: the caller
+ * vouches that x, y, edge_u, edge_v and edge_w hold the values of this context's previous JV call,
+ * as a binding that keeps its own copy and compares it element-wise (the reference's resident-cache
+ * key) knows; the cached static data are then reused without comparing them again. The node and
+ * edge counts and the distance type are still compared, and the hint does nothing once the cache
+ * was cleared. Other flag bits: CEE_ERR_INVALID. */
+#define CEE_JV_STATIC_UNCHANGED 1u
+int cee_jv_screen_ex(cee_ctx* ctx, const cee_graph_view* graph, int32_t* witness_out,
+                     cee_jv_stats* stats, uint32_t flags);
 /* The three phases of cee_jv_screen, for callers that keep the snapshot resident and time
  * the kernel alone: prepare uploads (and waits for the copies), launch enqueues the screen on
  * the context stream (no synchronisation), fetch copies the witnesses back and checks the

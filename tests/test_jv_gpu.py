@@ -1,5 +1,7 @@
 """JV screen on the B200 against the CPU oracle: witness arrays must be identical (bit-exact
 integer work), epoch after epoch, including the reference's edge cases."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -135,3 +137,32 @@ def test_cache_contract(ctx, port):
     assert not s4.static_hit and s4.workspace_hit
     for s in (s1, s2, s3, s4):
         assert np.isfinite(s.h2d_ms) and s.h2d_ms >= 0 and s.kernel_ms >= 0 and s.d2h_ms >= 0
+
+
+def test_static_unchanged_hint(ctx, port):
+    """cee_jv_screen_ex's CEE_JV_STATIC_UNCHANGED: with the cached static data the witnesses equal the
+    oracle's and the cache is hit without comparing; a snapshot of other sizes, or a cleared cache,
+    makes the hint do nothing; unknown flag bits fail."""
+    ctx.clear(1)
+    g = synth.jv_small()
+    first, s1 = ctx.jv_screen(g, static_unchanged=True)  # nothing cached yet: a full upload
+    assert not s1.static_hit
+    np.testing.assert_array_equal(first, port.jv_screen(g))
+    g2 = g.copy()
+    g2.active[: g2.m // 3] = 0
+    g2.rebuild_csr()
+    w, s2 = ctx.jv_screen(g2, static_unchanged=True)  # same static arrays, fewer active edges
+    assert s2.static_hit
+    np.testing.assert_array_equal(w, port.jv_screen(g2))
+    other = synth.jv_clustered()
+    w, s3 = ctx.jv_screen(other, static_unchanged=True)  # other sizes: the hint is not taken
+    assert not s3.static_hit
+    np.testing.assert_array_equal(w, port.jv_screen(other))
+    ctx.clear(1)
+    w, s4 = ctx.jv_screen(other, static_unchanged=True)
+    assert not s4.static_hit
+    np.testing.assert_array_equal(w, port.jv_screen(other))
+    out = np.empty(other.m, np.int32)
+    view = other.view()
+    rc = _native.lib().cee_jv_screen_ex(ctx.handle, ctypes.byref(view), out.ctypes.data_as(_native.c_i32p), None, 2)
+    assert rc == _native.CEE_ERR_INVALID
