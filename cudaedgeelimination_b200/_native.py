@@ -110,6 +110,10 @@ class ServeEvent(ctypes.Structure):
     _fields_ = [("job", ctypes.c_int32), ("status", ctypes.c_int32), ("tag", ctypes.c_uint64)]
 
 
+class HtReplyStats(ctypes.Structure):
+    _fields_ = [("graph_hit", ctypes.c_int32), ("workspace_hit", ctypes.c_int32), ("resident_bytes", ctypes.c_uint64)]
+
+
 class ServeStats(ctypes.Structure):
     _fields_ = [("jobs", ctypes.c_uint64), ("rows_bytes", ctypes.c_uint64), ("download_bytes", ctypes.c_uint64),
                 ("direct_bytes", ctypes.c_uint64)]
@@ -212,6 +216,11 @@ def lib() -> ctypes.CDLL:
                                                                ctypes.POINTER(vp), ctypes.c_uint64, c_i32p]),
             "cee_serve_poll": (ctypes.c_int, [vp, ctypes.POINTER(ServeEvent), ctypes.c_int32, c_i32p]),
             "cee_serve_pending": (ctypes.c_int, [vp, c_i32p, c_u64p]),
+            "cee_ht_replies": (ctypes.c_int, [vp, ctypes.POINTER(GraphView), ctypes.c_int32, ctypes.c_int32, c_i32p,
+                                              ctypes.c_int64, c_u64p, ctypes.POINTER(HtReplyStats)]),
+            "cee_ht_end_replies": (ctypes.c_int, [vp, ctypes.POINTER(GraphView), c_i32p, ctypes.c_int64, c_u64p,
+                                                  ctypes.POINTER(HtReplyStats)]),
+            "cee_ht_replies_fetch": (ctypes.c_int, [vp, vp]),
             "cee_serve_get_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServeStats)]),
             "cee_serve_stop": (ctypes.c_int, [vp]),
         }

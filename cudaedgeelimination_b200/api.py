@@ -455,6 +455,40 @@ class Context(BatchMixin, ServeMixin):
             self.handle, ctypes.byref(view), witness.ctypes.data_as(_native.c_i32p), ctypes.byref(stats), flags))
         return witness, stats
 
+    def ht_replies(self, graph: GraphSnapshot, u: int, v: int, centers) -> tuple[np.ndarray, np.ndarray]:
+        """cee_ht_replies + cee_ht_replies_fetch: the Hamilton replies of each center for target
+        (u, v) (detail::EvaluateHtHamiltonRepliesCuda): (offsets [len + 1] uint64, replies [total, 3]
+        int32 rows (center, first, second)). The stats of the call are kept in `last_reply_stats`."""
+        centers = np.ascontiguousarray(centers, np.int32)
+        offsets = np.zeros(centers.shape[0] + 1, np.uint64)
+        stats = _native.HtReplyStats()
+        view = graph.view()
+        lib = _native.lib()
+        _native.check(self.handle, lib.cee_ht_replies(self.handle, ctypes.byref(view), min(u, v), max(u, v),
+                                                       centers.ctypes.data_as(_native.c_i32p), centers.shape[0],
+                                                       offsets.ctypes.data_as(_native.c_u64p), ctypes.byref(stats)))
+        replies = np.empty((int(offsets[-1]), 3), np.int32)
+        _native.check(self.handle, lib.cee_ht_replies_fetch(self.handle, replies.ctypes.data_as(ctypes.c_void_p)))
+        self.last_reply_stats = stats
+        return offsets, replies
+
+    def ht_end_replies(self, graph: GraphSnapshot, tasks) -> tuple[np.ndarray, np.ndarray]:
+        """cee_ht_end_replies + cee_ht_replies_fetch: for each (endpoint, internal neighbour) task the
+        endpoint's other edges (detail::EvaluateHtEndRepliesCuda): (offsets, replies [total, 2] int32
+        rows (lower, higher))."""
+        tasks = np.ascontiguousarray(np.asarray(tasks, np.int32).reshape(-1, 2))
+        offsets = np.zeros(tasks.shape[0] + 1, np.uint64)
+        stats = _native.HtReplyStats()
+        view = graph.view()
+        lib = _native.lib()
+        _native.check(self.handle, lib.cee_ht_end_replies(self.handle, ctypes.byref(view),
+                                                           tasks.ctypes.data_as(_native.c_i32p), tasks.shape[0],
+                                                           offsets.ctypes.data_as(_native.c_u64p), ctypes.byref(stats)))
+        replies = np.empty((int(offsets[-1]), 2), np.int32)
+        _native.check(self.handle, lib.cee_ht_replies_fetch(self.handle, replies.ctypes.data_as(ctypes.c_void_p)))
+        self.last_reply_stats = stats
+        return offsets, replies
+
     def jv_prepare(self, graph: GraphSnapshot) -> _native.JvStats:
         stats = _native.JvStats()
         view = graph.view()

@@ -40,7 +40,7 @@ def reference_dir() -> pathlib.Path | None:
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-Wall", f"-I{INCLUDE}", f"-I{CSRC}"]
-CUDA_SOURCES = ["cee_api.cu", "batch.cu", "noalloc.cu", "serve.cu", "epoch.cu", "proof.cu", "host_copy.cu"]
+CUDA_SOURCES = ["cee_api.cu", "batch.cu", "noalloc.cu", "serve.cu", "epoch.cu", "proof.cu", "host_copy.cu", "ht_replies.cu"]
 
 
 def _host_cxx() -> str:

@@ -942,6 +942,7 @@ void cee_destroy(cee_ctx* ctx) {
   ReleaseServe(ctx);
   ReleaseBatch(ctx);
   ReleaseEpoch(ctx);
+  ReleaseReplies(ctx);
   ctx->jv.Release();
   ctx->kopt.Release();
   ctx->cd.Release();
@@ -977,7 +978,8 @@ int cee_ctx_synchronize(cee_ctx* ctx) {
 uint64_t cee_ctx_resident_bytes(const cee_ctx* ctx) {
   if (ctx == nullptr) return 0;
   return JvResident(ctx->jv) + KoptResident(ctx->kopt) + ctx->cd.xy.capacity + ctx->cd.tasks.capacity +
-         ctx->cd.flags.capacity + BatchResident(ctx) + ServeResident(ctx) + EpochResident(ctx);
+         ctx->cd.flags.capacity + BatchResident(ctx) + ServeResident(ctx) + EpochResident(ctx) +
+         RepliesResident(ctx);
 }
 
 int cee_ctx_clear(cee_ctx* ctx, unsigned what) {
@@ -990,6 +992,7 @@ int cee_ctx_clear(cee_ctx* ctx, unsigned what) {
   if (what & 8u) ReleaseBatch(ctx);
   if (what & 16u) ReleaseServe(ctx);
   if (what & 32u) ReleaseEpoch(ctx);
+  if (what & 64u) ReleaseReplies(ctx);
   return CEE_OK;
 }
 

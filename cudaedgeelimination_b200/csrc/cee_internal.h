@@ -118,6 +118,7 @@ struct CdState {
 struct BatchState;
 struct ServeState;
 struct EpochState;
+struct ReplyState;
 
 }  // namespace cee
 
@@ -157,6 +158,7 @@ struct cee_ctx {
   cee::BatchState* batch = nullptr;
   cee::ServeState* serve = nullptr;
   cee::EpochState* epoch = nullptr;
+  cee::ReplyState* replies = nullptr;
   cee::HostStage stage;
 };
 
@@ -193,5 +195,11 @@ void ReleaseServe(cee_ctx* ctx, int32_t* error_word = nullptr);
 uint64_t ServeResident(const cee_ctx* ctx);
 void ReleaseEpoch(cee_ctx* ctx);
 uint64_t EpochResident(const cee_ctx* ctx);
+void ReleaseReplies(cee_ctx* ctx);
+uint64_t RepliesResident(const cee_ctx* ctx);
+// Snapshot view checks shared by the entry points (sizes, distance type, edge arrays, CSR offsets).
+int ValidateView(cee_ctx* ctx, const cee_graph_view* g);
+// Whether v is in u's CSR row (rows ascending by neighbour).
+bool HostHasActiveEdge(const cee_graph_view* g, int32_t u, int32_t v);
 
 }  // namespace cee

@@ -16,7 +16,9 @@
 //     std::invalid_argument, out of the exact range -> std::overflow_error, everything else ->
 //     std::runtime_error; *Available() returns false with a reason instead of throwing;
 //   * the HT wavefront propagation entry points keep the stub behaviour
-//     (src/cuda/ht_cd_stub.cpp:20-33): unavailable, and throwing when called.
+//     (src/cuda/ht_cd_stub.cpp:20-33): unavailable, and throwing when called;
+//   * the HT reply seam (src/cuda/ht_replies.cu:583-758) replaces the reference's stub
+//     (src/cuda/ht_replies_stub.cpp) as well.
 #include "cee.h"
 
 #include "cuda_edge_elimination/cuda_device_affinity.hpp"
@@ -311,6 +313,63 @@ std::vector<std::uint8_t> ScreenHtCdCandidatesCuda(const GraphSnapshot& graph, c
                                    static_cast<int64_t>(tasks.size()), static_cast<int32_t>(mode), flags.data());
   if (status != CEE_OK) Raise(status, ctx, "B200 HT c,d screen");
   return flags;
+}
+
+bool HtHamiltonReplyCudaAvailable(std::string* const reason) { return SelectDevice(reason) >= 0; }
+
+HtHamiltonReplyDeviceBatch EvaluateHtHamiltonRepliesCuda(const GraphSnapshot& graph, const NodeEdge target_edge,
+                                                         const std::vector<std::int32_t>& centers,
+                                                         int* const selected_device,
+                                                         HtReplyCudaCacheUsage* const cache_usage) {
+  static_assert(sizeof(HtNeighborPair) == sizeof(cee_ht_pair), "HtNeighborPair layout");
+  if (cache_usage != nullptr) *cache_usage = {};
+  cee_ctx* ctx = RequireContext(selected_device, "CUDA HT reply backend");
+  g_arrays.Bind(graph, true);
+  HtHamiltonReplyDeviceBatch result;
+  result.offsets.assign(centers.size() + 1U, 0U);
+  cee_ht_reply_stats stats{};
+  int status = cee_ht_replies(ctx, &g_arrays.view, target_edge.u, target_edge.v, centers.data(),
+                              static_cast<int64_t>(centers.size()), result.offsets.data(), &stats);
+  if (status != CEE_OK) Raise(status, ctx, "B200 HT Hamilton replies");
+  result.replies.resize(static_cast<size_t>(result.offsets.back()));
+  status = cee_ht_replies_fetch(ctx, result.replies.data());
+  if (status != CEE_OK) Raise(status, ctx, "B200 HT Hamilton reply download");
+  if (cache_usage != nullptr) {
+    cache_usage->graph_hit = stats.graph_hit != 0;
+    cache_usage->workspace_hit = stats.workspace_hit != 0;
+    cache_usage->resident_bytes = stats.resident_bytes;
+  }
+  return result;
+}
+
+bool HtEndReplyCudaAvailable(std::string* const reason) { return SelectDevice(reason) >= 0; }
+
+HtEndReplyDeviceBatch EvaluateHtEndRepliesCuda(const GraphSnapshot& graph, const std::vector<HtEndReplyTask>& tasks,
+                                               int* const selected_device, HtReplyCudaCacheUsage* const cache_usage) {
+  static_assert(sizeof(HtEndReplyTask) == sizeof(cee_ht_end_task), "HtEndReplyTask layout");
+  static_assert(sizeof(NodeEdge) == sizeof(cee_node_edge), "NodeEdge layout");
+  if (cache_usage != nullptr) *cache_usage = {};
+  cee_ctx* ctx = RequireContext(selected_device, "CUDA HT end reply backend");
+  g_arrays.Bind(graph, true);
+  HtEndReplyDeviceBatch result;
+  result.offsets.assign(tasks.size() + 1U, 0U);
+  cee_ht_reply_stats stats{};
+  int status = cee_ht_end_replies(ctx, &g_arrays.view, reinterpret_cast<const cee_ht_end_task*>(tasks.data()),
+                                  static_cast<int64_t>(tasks.size()), result.offsets.data(), &stats);
+  if (status != CEE_OK) Raise(status, ctx, "B200 HT end replies");
+  result.replies.resize(static_cast<size_t>(result.offsets.back()));
+  status = cee_ht_replies_fetch(ctx, result.replies.data());
+  if (status != CEE_OK) Raise(status, ctx, "B200 HT end reply download");
+  if (cache_usage != nullptr) {
+    cache_usage->graph_hit = stats.graph_hit != 0;
+    cache_usage->workspace_hit = stats.workspace_hit != 0;
+    cache_usage->resident_bytes = stats.resident_bytes;
+  }
+  return result;
+}
+
+void ClearHtReplyCudaCache() {
+  for (auto& entry : g_threads.contexts) cee_ctx_clear(entry.second, 64u);
 }
 
 bool HtWavefrontCudaAvailable(std::string* const reason) {

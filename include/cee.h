@@ -90,7 +90,8 @@ enum cee_option {
 /* Sets a launch-shape option of this context; results never depend on it. */
 int cee_ctx_set_option(cee_ctx* ctx, int32_t option, int64_t value);
 /* Frees cached device state: bit 1 = JV, bit 2 = k-opt, bit 4 = c,d, bit 8 = batch,
- * bit 16 = serving loop (stops it; its jobs are dropped), bit 32 = JV epoch loop workspace.
+ * bit 16 = serving loop (stops it; its jobs are dropped), bit 32 = JV epoch loop workspace,
+ * bit 64 = HT replies (ClearHtReplyCudaCache, hamilton_tutte.hpp:544-545).
  * Replaces ClearJvCudaCache (include/cuda_edge_elimination/elimination.hpp:338) and
  * ClearKOptCostCudaCache (include/cuda_edge_elimination/local_search.hpp:242). */
 int cee_ctx_clear(cee_ctx* ctx, unsigned what);
@@ -390,6 +391,51 @@ typedef struct {
  * validated as the reference does (c < d, no target endpoint, active bit equal to the CSR). */
 int cee_cd_screen(cee_ctx* ctx, const cee_graph_view* graph, int32_t u, int32_t v,
                   const cee_cd_task* tasks, int64_t count, int32_t mode, uint8_t* flags_out);
+
+/* ---- HT Hamilton and end replies -------------------------------------------------------- */
+
+/* HtNeighborPair (include/cuda_edge_elimination/hamilton_tutte.hpp:26-32) and HtEndReplyTask
+ * (:76-81); an end reply is a NodeEdge (local_search.hpp:17-22) with u < v. */
+typedef struct {
+  int32_t center;
+  int32_t first;
+  int32_t second;
+} cee_ht_pair;
+typedef struct {
+  int32_t endpoint;
+  int32_t internal_neighbor;
+} cee_ht_end_task;
+typedef struct {
+  int32_t u;
+  int32_t v;
+} cee_node_edge;
+
+/* HtReplyCudaCacheUsage (hamilton_tutte.hpp:515-519). */
+typedef struct {
+  int32_t graph_hit;     /* coordinates and CSR equal the previous reply call's: not uploaded */
+  int32_t workspace_hit; /* no device buffer had to grow */
+  uint64_t resident_bytes;
+} cee_ht_reply_stats;
+
+/* Replaces detail::EvaluateHtHamiltonRepliesCuda (include/cuda_edge_elimination/hamilton_tutte.hpp:
+ * 533-537, src/cuda/ht_replies.cu:585-663): for target (u, v), u < v, an active edge, and each of
+ * `count` centers (in [0, n), not u or v), the Hamilton replies of AppendHtHamiltonRepliesUnchecked
+ * (src/cpu/hamilton_tutte.cpp:230-269) in its order. offsets_out[count + 1]: center i's replies are
+ * [offsets_out[i], offsets_out[i + 1]) of the list that cee_ht_replies_fetch copies out (kept on the
+ * device until the next reply call). The snapshot is validated as the reference does
+ * (src/cuda/ht_replies.cu:521-566: CSR rows strictly ascending, symmetric, the active edges only,
+ * at least 4 nodes): CEE_ERR_INVALID otherwise. stats may be null. */
+int cee_ht_replies(cee_ctx* ctx, const cee_graph_view* graph, int32_t u, int32_t v, const int32_t* centers,
+                   int64_t count, uint64_t* offsets_out, cee_ht_reply_stats* stats);
+/* Replaces detail::EvaluateHtEndRepliesCuda (hamilton_tutte.hpp:539-542, src/cuda/ht_replies.cu:
+ * 667-751): for each task, the edges at its endpoint other than the one to its internal neighbour
+ * (AppendHtEndRepliesUnchecked, src/cpu/hamilton_tutte.cpp:271-282), as (lower, higher) node pairs in
+ * CSR order; every task's edge must be active (CEE_ERR_INVALID otherwise). Offsets and fetch as above. */
+int cee_ht_end_replies(cee_ctx* ctx, const cee_graph_view* graph, const cee_ht_end_task* tasks, int64_t count,
+                       uint64_t* offsets_out, cee_ht_reply_stats* stats);
+/* Copies the last reply call's list: offsets_out[count] records of cee_ht_pair (cee_ht_replies) or
+ * cee_node_edge (cee_ht_end_replies). */
+int cee_ht_replies_fetch(cee_ctx* ctx, void* replies_out);
 
 /* ---- batched screen (many instances, one persistent graph-captured launch) ---------------- */
 

@@ -87,6 +87,10 @@ class Port:
         L.ceo_ht_targets.argtypes = [G, ctypes.c_int32, i32p]
         L.ceo_ht_reply_count.restype = ctypes.c_int64
         L.ceo_ht_reply_count.argtypes = [G, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
+        L.ceo_ht_replies.restype = ctypes.c_int64
+        L.ceo_ht_replies.argtypes = [G, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, i32p, ctypes.c_int64]
+        L.ceo_ht_end_replies.restype = ctypes.c_int64
+        L.ceo_ht_end_replies.argtypes = [G, ctypes.c_int32, ctypes.c_int32, i32p, ctypes.c_int64]
         L.ceo_cd_finalize.restype = ctypes.c_int64
         L.ceo_cd_finalize.argtypes = [G, ctypes.c_int32, ctypes.c_int32, i32p, i32p, u8p, ctypes.c_int64,
                                       ctypes.c_uint32, i32p, i32p, u64p]
@@ -298,6 +302,39 @@ class Port:
     def ht_reply_count(self, g, u: int, v: int, center: int) -> int:
         return int(self.L.ceo_ht_reply_count(self.graph(g), min(u, v), max(u, v), center))
 
+    def ht_replies(self, g, u: int, v: int, centers) -> tuple[np.ndarray, np.ndarray]:
+        """The Hamilton replies of each center for target (u, v), concatenated in center order:
+        (offsets [len + 1] uint64, replies [total, 3] int32 rows (center, first, second))."""
+        view = self.graph(g)
+        lists = []
+        for c in centers:
+            k = int(self.L.ceo_ht_replies(view, min(u, v), max(u, v), int(c), None, 0))
+            out = np.empty((max(k, 1), 3), np.int32)
+            self.L.ceo_ht_replies(view, min(u, v), max(u, v), int(c), _p(out, ctypes.c_int32), k)
+            lists.append(out[:k])
+        return _concat(lists, 3)
+
+    def ht_end_replies(self, g, tasks) -> tuple[np.ndarray, np.ndarray]:
+        """The end replies of each (endpoint, internal neighbour) task: (offsets, replies [total, 2]
+        int32 rows (lower, higher)); a task whose internal neighbour is not adjacent raises."""
+        view = self.graph(g)
+        lists = []
+        for e, w in np.asarray(tasks, np.int64).reshape(-1, 2):
+            k = int(self.L.ceo_ht_end_replies(view, int(e), int(w), None, 0))
+            if k < 0:
+                raise ValueError(f"internal neighbour {w} is not adjacent to {e}")
+            out = np.empty((max(k, 1), 2), np.int32)
+            self.L.ceo_ht_end_replies(view, int(e), int(w), _p(out, ctypes.c_int32), k)
+            lists.append(out[:k])
+        return _concat(lists, 2)
+
+
+def _concat(lists, width: int) -> tuple[np.ndarray, np.ndarray]:
+    offsets = np.zeros(len(lists) + 1, np.uint64)
+    offsets[1:] = np.cumsum([len(x) for x in lists], dtype=np.uint64)
+    rows = np.concatenate(lists) if lists else np.empty((0, width), np.int32)
+    return offsets, rows.reshape(-1, width).astype(np.int32)
+
 
 def reference_available(dropin: bool = False, variant: str | None = None) -> bool:
     return LIBS[variant or ("dropin" if dropin else "ref")].exists()
@@ -351,6 +388,12 @@ class Reference:
         L.ref_seam_kopt_timed.argtypes = [vp, ctypes.c_uint32, vp, ctypes.c_int64, ctypes.c_int32, dp, i64p]
         L.ref_seam_cd_timed.argtypes = [vp, ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                         ctypes.c_int, dp, i64p, i64p]
+        L.ref_ht_hamilton_replies.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, i32p, ctypes.c_int64, ctypes.c_int,
+                                              ctypes.c_int, u64p, i32p, ctypes.c_int64, i64p, i32p]
+        L.ref_ht_end_replies.argtypes = [vp, i32p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, u64p, i32p,
+                                         ctypes.c_int64, i64p, i32p]
+        L.ref_seam_ht_replies_timed.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, i32p, ctypes.c_int64,
+                                                ctypes.c_int32, dp, i64p]
         self.L = L
 
     def error(self) -> str:
@@ -563,6 +606,44 @@ class RefGraph:
         count = self.ref._check(self.ref.L.ref_cd_candidates(self.handle, u, v, max_neighborhood, max_cd, max_degree,
                                                              mode, backend, _p(out, ctypes.c_int64), cap))
         return out[:count].copy()
+
+    def ht_hamilton_replies(self, u: int, v: int, centers, backend: int = 1, dedup: bool = True):
+        """EvaluateHtHamiltonReplies (backend 1 = kCpu, 2 = kCuda): (offsets, replies [total, 3],
+        used: 2 = the CUDA seam's lists, checked by the reference against its CPU lists; 1 = CPU;
+        0 = CPU fallback)."""
+        centers = np.ascontiguousarray(centers, np.int32)
+        offsets = np.zeros(centers.shape[0] + 1, np.uint64)
+        total, used = ctypes.c_int64(0), ctypes.c_int32(0)
+        cap = 1 << 20
+        out = np.empty((cap, 3), np.int32)
+        self.ref._check(self.ref.L.ref_ht_hamilton_replies(
+            self.handle, u, v, _p(centers, ctypes.c_int32), centers.shape[0], backend, int(dedup),
+            _p(offsets, ctypes.c_uint64), _p(out, ctypes.c_int32), cap, ctypes.byref(total), ctypes.byref(used)))
+        assert total.value <= cap
+        return offsets, out[:total.value].copy(), used.value
+
+    def ht_end_replies(self, tasks, backend: int = 1, dedup: bool = True):
+        """EvaluateHtEndReplies, as ht_hamilton_replies; tasks [k, 2] (endpoint, internal neighbour)."""
+        tasks = np.ascontiguousarray(np.asarray(tasks, np.int32).reshape(-1, 2))
+        offsets = np.zeros(tasks.shape[0] + 1, np.uint64)
+        total, used = ctypes.c_int64(0), ctypes.c_int32(0)
+        cap = 1 << 20
+        out = np.empty((cap, 2), np.int32)
+        self.ref._check(self.ref.L.ref_ht_end_replies(
+            self.handle, _p(tasks, ctypes.c_int32), tasks.shape[0], backend, int(dedup), _p(offsets, ctypes.c_uint64),
+            _p(out, ctypes.c_int32), cap, ctypes.byref(total), ctypes.byref(used)))
+        assert total.value <= cap
+        return offsets, out[:total.value].copy(), used.value
+
+    def seam_ht_replies_timed(self, u: int, v: int, centers, reps: int):
+        """ref_seam_ht_replies_timed: (ms of each detail::EvaluateHtHamiltonRepliesCuda call, reply total)."""
+        centers = np.ascontiguousarray(centers, np.int32)
+        ms = np.zeros(reps, np.float64)
+        total = ctypes.c_int64(0)
+        self.ref._check(self.ref.L.ref_seam_ht_replies_timed(self.handle, u, v, _p(centers, ctypes.c_int32),
+                                                             centers.shape[0], reps, _p(ms, ctypes.c_double),
+                                                             ctypes.byref(total)))
+        return ms, total.value
 
     def ht_targets(self, order: int = 1) -> np.ndarray:
         out = np.empty(max(1, self.m), np.int32)

@@ -608,11 +608,12 @@ void ceo_cd_screen(const ceo_graph* g, int32_t u, int32_t v, const int32_t* c, c
 
 /* ---- FinalizeCdCandidates: src/cpu/hamilton_tutte.cpp:283-327 ---- */
 
-/* AppendHtHamiltonRepliesUnchecked (:230-269), counted: pairs of neighbours (first < second in
- * CSR order) of `center` whose edges to the center both survive 2-opt against the target, whose
- * node pair is not the target, and for which the target plus the two center edges cost no more
- * than the pair's edge plus the center's two target edges. */
-int64_t ceo_ht_reply_count(const ceo_graph* g, int32_t tu, int32_t tv, int32_t center) {
+/* AppendHtHamiltonRepliesUnchecked (:230-269): pairs of neighbours (first < second in CSR order)
+ * of `center` whose edges to the center both survive 2-opt against the target, whose node pair is
+ * not the target, and for which the target plus the two center edges cost no more than the pair's
+ * edge plus the center's two target edges. Writes the first `capacity` of them to `out` as
+ * (center, first, second) triples (NULL: none) and returns how many there are. */
+int64_t ceo_ht_replies(const ceo_graph* g, int32_t tu, int32_t tv, int32_t center, int32_t* out, int64_t capacity) {
   const int32_t begin = g->row_offsets[center], end = g->row_offsets[center + 1];
   const int32_t deg = end - begin;
   if (deg < 2) return 0;
@@ -635,13 +636,48 @@ int64_t ceo_ht_reply_count(const ceo_graph* g, int32_t tu, int32_t tv, int32_t c
         if ((lo == tu && hi == tv) || !survives[a] || !survives[b]) continue;
         const __int128 original = target_cost + cost[a] + cost[b];
         const __int128 replacement = (__int128)dist_nodes(g, na, nb) + center_target;
-        if (original <= replacement) ++count;
+        if (original <= replacement) {
+          if (out != NULL && count < capacity) {
+            out[3 * count] = center;
+            out[3 * count + 1] = na;
+            out[3 * count + 2] = nb;
+          }
+          ++count;
+        }
       }
     }
   }
   free(cost);
   free(survives);
   return count;
+}
+
+int64_t ceo_ht_reply_count(const ceo_graph* g, int32_t tu, int32_t tv, int32_t center) {
+  return ceo_ht_replies(g, tu, tv, center, NULL, 0);
+}
+
+/* AppendHtEndRepliesUnchecked (:271-282): the edges at `endpoint` other than the one to
+ * `internal_neighbor`, each as (lower id, higher id), in CSR order; writes the first `capacity`
+ * pairs to `out` (NULL: none) and returns their number, or -1 when `internal_neighbor` is not a
+ * neighbour of `endpoint`. */
+int64_t ceo_ht_end_replies(const ceo_graph* g, int32_t endpoint, int32_t internal_neighbor, int32_t* out,
+                           int64_t capacity) {
+  const int32_t begin = g->row_offsets[endpoint], end = g->row_offsets[endpoint + 1];
+  int found = 0;
+  int64_t count = 0;
+  for (int32_t s = begin; s < end; ++s) {
+    const int32_t nb = g->neighbors[s];
+    if (nb == internal_neighbor) {
+      found = 1;
+      continue;
+    }
+    if (out != NULL && count < capacity) {
+      out[2 * count] = endpoint < nb ? endpoint : nb;
+      out[2 * count + 1] = endpoint < nb ? nb : endpoint;
+    }
+    ++count;
+  }
+  return found ? count : -1;
 }
 
 typedef struct {

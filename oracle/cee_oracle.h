@@ -97,6 +97,13 @@ void ceo_cd_screen(const ceo_graph* g, int32_t u, int32_t v, const int32_t* c, c
                    const uint8_t* active, int64_t count, int32_t mode, uint8_t* flags);
 /* FinalizeCdCandidates (hamilton_tutte.cpp:283-327) and its Hamilton reply count (:230-269). */
 int64_t ceo_ht_reply_count(const ceo_graph* g, int32_t tu, int32_t tv, int32_t center);
+/* The Hamilton replies of `center` (AppendHtHamiltonRepliesUnchecked, hamilton_tutte.cpp:230-269)
+ * as (center, first, second) triples in CSR pair order, and the end replies of a path end
+ * (AppendHtEndRepliesUnchecked, :271-282) as (lower, higher) pairs in CSR order (-1: the internal
+ * neighbour is not adjacent). Up to `capacity` records go to `out`; the return value is the count. */
+int64_t ceo_ht_replies(const ceo_graph* g, int32_t tu, int32_t tv, int32_t center, int32_t* out, int64_t capacity);
+int64_t ceo_ht_end_replies(const ceo_graph* g, int32_t endpoint, int32_t internal_neighbor, int32_t* out,
+                           int64_t capacity);
 int64_t ceo_cd_finalize(const ceo_graph* g, int32_t u, int32_t v, const int32_t* c, const int32_t* d,
                         const uint8_t* flags, int64_t count, uint32_t max_cd, int32_t* out_c, int32_t* out_d,
                         uint64_t* out_product);

@@ -393,6 +393,71 @@ int ref_cd_candidates(void* handle, int32_t u, int32_t v, uint32_t max_neighborh
   });
 }
 
+// EvaluateHtHamiltonReplies (src/cpu/hamilton_tutte.cpp:604-611; backend 1 = kCpu, 2 = kCuda: its
+// CUDA seam, whose lists the reference compares with its CPU lists before returning) for target
+// (u, v) and `count` centers: offsets[count + 1], replies[3 i ..] = (center, first, second) for the
+// first `capacity` replies, *total = their number, *used = 2 when the result came from the CUDA
+// seam, 1 from the CPU, 0 from the CPU fallback.
+int ref_ht_hamilton_replies(void* handle, int32_t u, int32_t v, const int32_t* centers, int64_t count, int backend,
+                            int dedup, uint64_t* offsets, int32_t* replies, int64_t capacity, int64_t* total,
+                            int32_t* used) {
+  return Guard([&] {
+    const std::vector<std::int32_t> list(centers, centers + count);
+    const auto b = backend == 2 ? cudaee::PathCompatibilityBackend::kCuda : cudaee::PathCompatibilityBackend::kCpu;
+    const cudaee::HtHamiltonReplyBatchResult result =
+        cudaee::EvaluateHtHamiltonReplies(*AsGraph(handle), {u, v}, list, b, dedup != 0);
+    std::copy(result.offsets.begin(), result.offsets.end(), offsets);
+    const int64_t n = static_cast<int64_t>(result.replies.size());
+    for (int64_t i = 0; i < n && i < capacity; ++i) {
+      replies[3 * i] = result.replies[i].center;
+      replies[3 * i + 1] = result.replies[i].first;
+      replies[3 * i + 2] = result.replies[i].second;
+    }
+    *total = n;
+    *used = result.backend == "cuda" ? 2 : (result.backend == "cpu" ? 1 : 0);
+    return 0;
+  });
+}
+
+// EvaluateHtEndReplies (src/cpu/hamilton_tutte.cpp:625-631), as ref_ht_hamilton_replies; tasks are
+// (endpoint, internal neighbour) pairs and replies (lower, higher) node pairs.
+int ref_ht_end_replies(void* handle, const int32_t* tasks, int64_t count, int backend, int dedup, uint64_t* offsets,
+                       int32_t* replies, int64_t capacity, int64_t* total, int32_t* used) {
+  return Guard([&] {
+    std::vector<cudaee::HtEndReplyTask> list(static_cast<std::size_t>(count));
+    for (int64_t i = 0; i < count; ++i) list[static_cast<std::size_t>(i)] = {tasks[2 * i], tasks[2 * i + 1]};
+    const auto b = backend == 2 ? cudaee::PathCompatibilityBackend::kCuda : cudaee::PathCompatibilityBackend::kCpu;
+    const cudaee::HtEndReplyBatchResult result = cudaee::EvaluateHtEndReplies(*AsGraph(handle), list, b, dedup != 0);
+    std::copy(result.offsets.begin(), result.offsets.end(), offsets);
+    const int64_t n = static_cast<int64_t>(result.replies.size());
+    for (int64_t i = 0; i < n && i < capacity; ++i) {
+      replies[2 * i] = result.replies[i].u;
+      replies[2 * i + 1] = result.replies[i].v;
+    }
+    *total = n;
+    *used = result.backend == "cuda" ? 2 : (result.backend == "cpu" ? 1 : 0);
+    return 0;
+  });
+}
+
+// detail::EvaluateHtHamiltonRepliesCuda (include/cuda_edge_elimination/hamilton_tutte.hpp:533-537),
+// `reps` calls on the host clock; returns the reply total of the last call.
+int ref_seam_ht_replies_timed(void* handle, int32_t u, int32_t v, const int32_t* centers, int64_t count, int32_t reps,
+                              double* ms, int64_t* total) {
+  return Guard([&] {
+    const std::vector<std::int32_t> list(centers, centers + count);
+    cudaee::detail::HtHamiltonReplyDeviceBatch batch;
+    for (int32_t i = 0; i < reps; ++i) {
+      int device = -1;
+      const auto t0 = std::chrono::steady_clock::now();
+      batch = cudaee::detail::EvaluateHtHamiltonRepliesCuda(*AsGraph(handle), {u, v}, list, &device, nullptr);
+      ms[i] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    *total = static_cast<int64_t>(batch.replies.size());
+    return 0;
+  });
+}
+
 // SelectHtTargetEdgeIds (src/cpu/ht_scan.cpp:316-345), order 1 = weight descending.
 int ref_ht_targets(void* handle, int order, int32_t* out, int32_t capacity) {
   return Guard([&] {

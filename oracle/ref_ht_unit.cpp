@@ -3,13 +3,14 @@
 // against the reference with this project's CUDA seam, built with CUDAEE_HAS_CUDA as the
 // reference's CUDA build is.
 //
-// This project replaces three CUDA units of the reference (JV candidates, k-opt costs, c,d screen);
-// the HT prover's own CUDA units (wavefront propagation, path append, Hamilton and end replies)
+// This project replaces four CUDA units of the reference (JV candidates, k-opt costs, c,d screen,
+// Hamilton and end replies); the HT prover's other CUDA units (wavefront propagation, path append)
 // stay the reference's stubs, outside its scope. One test, TestRecursivePointProof, takes the
 // c,d backend answering as the sign of a full CUDA build and then drives every HT CUDA unit
 // (test_hamilton_tutte.cpp:1303-1330), so this driver leaves it out; its CPU checks run in the
 // reference's CPU-only build of the same file. Every other test runs, including the c,d CPU/CUDA
-// parity test (TestCdCandidatesCpuCuda) on this project's kernels.
+// parity test (TestCdCandidatesCpuCuda) and the CUDA sections of the reply batch tests
+// (TestHamiltonReplyBatch, TestEndReplyBatch: exact lists, cache hits) on this project's kernels.
 #define main cee_reference_ht_unit_main
 #include "tests/unit/test_hamilton_tutte.cpp"
 #undef main

@@ -130,6 +130,35 @@ def cd_case(ref: oracle.Reference) -> dict:
     return out
 
 
+def ht_replies_case(ref: oracle.Reference) -> dict:
+    """EvaluateHtHamiltonReplies / EvaluateHtEndReplies (kCpu) on the recursive-point fixture and on a
+    small ceiling instance: every center of a few active target edges, and every (endpoint, internal
+    neighbour) direction of the first active edges."""
+    out = {}
+    i = np.arange(40)
+    xs, ys = (29 * i + 5) % 89, (i * i * 7 + 3 * i) % 83
+    edges = [(a, b) for a in range(40) for b in range(a + 1, 40) if (11 * a + 7 * b) % 6 == 0 or b == a + 1]
+    for name, g in (("point", read_fixture()), ("ceil", GraphSnapshot.from_edges(xs, ys, edges, 1))):
+        rg = ref.graph(g)
+        out.update({f"{name}_{k}": v for k, v in snapshot_arrays(g).items()})
+        active = np.flatnonzero(g.active)
+        targets = active[:: max(1, len(active) // 4)][:4]
+        for j, e in enumerate(targets):
+            u, v = int(min(g.edge_u[e], g.edge_v[e])), int(max(g.edge_u[e], g.edge_v[e]))
+            centers = np.array([c for c in range(g.n) if c not in (u, v)], np.int32)
+            offsets, replies, _ = rg.ht_hamilton_replies(u, v, centers, backend=1)
+            out[f"{name}_target_{j}"] = np.array([u, v], np.int32)
+            out[f"{name}_offsets_{j}"] = offsets
+            out[f"{name}_replies_{j}"] = replies
+        tasks = np.array([(a, b) for e in active[:60] for a, b in ((g.edge_u[e], g.edge_v[e]), (g.edge_v[e], g.edge_u[e]))],
+                         np.int32)
+        offsets, replies, _ = rg.ht_end_replies(tasks, backend=1)
+        out[f"{name}_end_tasks"] = tasks
+        out[f"{name}_end_offsets"] = offsets
+        out[f"{name}_end_replies"] = replies
+    return out
+
+
 def main() -> None:
     ref = oracle.Reference()
     (HERE / "distance_kats.json").write_text(json.dumps(distance_kats(ref), indent=0))
@@ -137,6 +166,7 @@ def main() -> None:
     np.savez_compressed(HERE / "jv_recursive_point.npz", **jv_case(ref, read_fixture()))
     np.savez_compressed(HERE / "kopt_small.npz", **kopt_case(ref))
     np.savez_compressed(HERE / "cd_small.npz", **cd_case(ref))
+    np.savez_compressed(HERE / "ht_replies.npz", **ht_replies_case(ref))
     print("golden fixtures written to", HERE)
 
 

@@ -134,3 +134,44 @@ def test_kopt_and_cd_match_reference_live(port, ref):
             np.testing.assert_array_equal(flags, rg.cd_screen(u, v, c, d, a, mode))
             np.testing.assert_array_equal(port.cd_finalize(g, u, v, c, d, flags, 5),
                                           rg.cd_candidates(u, v, 25, 5, 50, mode, backend=1))
+
+
+def test_ht_replies_golden(port):
+    """Hamilton and end reply lists (AppendHtHamiltonRepliesUnchecked / AppendHtEndRepliesUnchecked,
+    src/cpu/hamilton_tutte.cpp:230-282) against the reference's own EvaluateHt*Replies(kCpu) output."""
+    d = load("ht_replies.npz")
+    for name in ("point", "ceil"):
+        g = GraphSnapshot(int(d[f"{name}_n"]), int(d[f"{name}_dist_type"]), d[f"{name}_x"], d[f"{name}_y"],
+                          d[f"{name}_edge_u"], d[f"{name}_edge_v"], d[f"{name}_edge_w"], d[f"{name}_active"])
+        j = 0
+        while f"{name}_target_{j}" in d:
+            u, v = (int(t) for t in d[f"{name}_target_{j}"])
+            centers = [c for c in range(g.n) if c not in (u, v)]
+            offsets, replies = port.ht_replies(g, u, v, centers)
+            np.testing.assert_array_equal(offsets, d[f"{name}_offsets_{j}"])
+            np.testing.assert_array_equal(replies, d[f"{name}_replies_{j}"])
+            j += 1
+        assert j > 0
+        offsets, replies = port.ht_end_replies(g, d[f"{name}_end_tasks"])
+        np.testing.assert_array_equal(offsets, d[f"{name}_end_offsets"])
+        np.testing.assert_array_equal(replies, d[f"{name}_end_replies"])
+
+
+def test_ht_replies_match_reference_live(port, ref):
+    rng = np.random.default_rng(7)
+    for g in (knn_graph(220, 7, seed=3), knn_graph(160, 12, seed=4, dist_type=1), random_graph(90, 500, seed=5)):
+        rg = ref.graph(g)
+        active = np.flatnonzero(g.active)
+        for e in active[rng.integers(len(active), size=3)]:
+            u, v = int(min(g.edge_u[e], g.edge_v[e])), int(max(g.edge_u[e], g.edge_v[e]))
+            centers = np.array([c for c in rng.integers(0, g.n, 50) if c not in (u, v)], np.int32)
+            offsets, replies = port.ht_replies(g, u, v, centers)
+            r_offsets, r_replies, used = rg.ht_hamilton_replies(u, v, centers, backend=1)
+            assert used == 1
+            np.testing.assert_array_equal(offsets, r_offsets)
+            np.testing.assert_array_equal(replies, r_replies)
+        tasks = np.stack([g.edge_u[active[:40]], g.edge_v[active[:40]]], axis=1)
+        offsets, replies = port.ht_end_replies(g, tasks)
+        r_offsets, r_replies, _ = rg.ht_end_replies(tasks, backend=1)
+        np.testing.assert_array_equal(offsets, r_offsets)
+        np.testing.assert_array_equal(replies, r_replies)
