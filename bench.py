@@ -1160,6 +1160,19 @@ def run_reference_gpu(args, device):
     cd["same_flags_checksum"] = flags["reference"] == flags["ours"]
     cd["speedup"] = cd["reference"]["seconds"] / cd["ours"]["seconds"]
     out["cd_seam"] = cd
+    # detail::EvaluateHtHamiltonRepliesCuda: every other node of the 50,000-node case as a center
+    g = cases[1][1]
+    e = int(np.flatnonzero(g.active)[0])
+    u, v = int(min(g.edge_u[e], g.edge_v[e])), int(max(g.edge_u[e], g.edge_v[e]))
+    centers = np.array([c for c in range(g.n) if c not in (u, v)], np.int32)
+    replies = {"workload": f"{cases[1][0]}; target ({u}, {v}), {centers.shape[0]:,} centers"}
+    totals = {}
+    for arm, ref in arms.items():
+        ms, totals[arm] = ref.graph(g).seam_ht_replies_timed(u, v, centers, 5)
+        replies[arm] = {"first_call_ms": float(ms[0]), "ms_per_call": float(np.median(ms[1:])), "replies": totals[arm]}
+    replies["same_total"] = totals["reference"] == totals["ours"]
+    replies["speedup"] = replies["reference"]["ms_per_call"] / replies["ours"]["ms_per_call"]
+    out["ht_reply_seam"] = replies
     return out
 
 

@@ -5,6 +5,8 @@ from .api import (  # noqa: F401
     CD_TASK_DTYPE, KOPT_TASK_DTYPE, Candidate, Context, BuildKOptReconnectTable, ClearJvCudaCache,
     ClearKOptCostCudaCache, CudaBackendAvailable, EvaluateKOptTemplateCostsCuda, FindJvCandidatesCuda,
     HtCdCudaAvailable, KOptCostCudaAvailable, KOptReconnectTable, ScreenHtCdCandidatesCuda, device_count,
+    ClearHtReplyCudaCache, EvaluateHtEndRepliesCuda, EvaluateHtHamiltonRepliesCuda, HtEndReplyCudaAvailable,
+    HtHamiltonReplyCudaAvailable,
     JV_EPOCH_METRICS_DTYPE, JV_PROOF_RECORD_DTYPE, TuningCache, content_hash, jv_proof, write_active_edges,
     write_jv_proof,
 )

@@ -776,3 +776,28 @@ def ClearKOptCostCudaCache() -> None:
 
 def ScreenHtCdCandidatesCuda(graph: GraphSnapshot, target, tasks: np.ndarray, mode: int) -> np.ndarray:
     return _context().cd_screen(graph, target, tasks, mode)
+
+
+def HtHamiltonReplyCudaAvailable() -> tuple[bool, str]:
+    return HtCdCudaAvailable()
+
+
+def EvaluateHtHamiltonRepliesCuda(graph: GraphSnapshot, target, centers) -> tuple[np.ndarray, np.ndarray]:
+    """HtHamiltonReplyDeviceBatch: (offsets [len + 1] uint64, replies [total, 3] int32 rows
+    (center, first, second)) for target (u, v) and each center."""
+    return _context().ht_replies(graph, int(target[0]), int(target[1]), centers)
+
+
+def HtEndReplyCudaAvailable() -> tuple[bool, str]:
+    return HtCdCudaAvailable()
+
+
+def EvaluateHtEndRepliesCuda(graph: GraphSnapshot, tasks) -> tuple[np.ndarray, np.ndarray]:
+    """HtEndReplyDeviceBatch: (offsets, replies [total, 2] int32 rows (lower, higher)) for each
+    (endpoint, internal neighbour) task."""
+    return _context().ht_end_replies(graph, tasks)
+
+
+def ClearHtReplyCudaCache() -> None:
+    for ctx in getattr(_tls, "contexts", {}).values():
+        ctx.clear(64)

@@ -116,3 +116,19 @@ def test_reference_batches_through_the_dropin(port):
         offsets, replies, used = rg.ht_end_replies(tasks, backend=2)
         assert used == 2
         np.testing.assert_array_equal(replies, port.ht_end_replies(g, tasks)[1])
+
+
+def test_python_seam_mirrors(port):
+    import cudaedgeelimination_b200 as cee
+    ok, _ = cee.HtHamiltonReplyCudaAvailable()
+    assert ok and cee.HtEndReplyCudaAvailable()[0]
+    g = knn_graph(250, 8, seed=31)
+    u, v = next(targets(g, np.random.default_rng(1), 1))
+    centers = np.array([c for c in range(g.n) if c not in (u, v)], np.int32)
+    offsets, replies = cee.EvaluateHtHamiltonRepliesCuda(g, (u, v), centers)
+    want_offsets, want = port.ht_replies(g, u, v, centers)
+    np.testing.assert_array_equal(offsets, want_offsets)
+    np.testing.assert_array_equal(replies, want)
+    tasks = np.array([[u, v], [v, u]], np.int32)
+    np.testing.assert_array_equal(cee.EvaluateHtEndRepliesCuda(g, tasks)[1], port.ht_end_replies(g, tasks)[1])
+    cee.ClearHtReplyCudaCache()
