@@ -20,6 +20,7 @@ struct ReplyState {
   int span = kSpanSmall;
   std::vector<int64_t> hx, hy;
   std::vector<int32_t> hro, hnbr;
+  std::vector<uint8_t> hactive;  // with the CSR: the content the last validation passed on
   DevBuf xy, ro, nbr;
   // per call
   DevBuf items, counts, offsets, out;
@@ -79,17 +80,25 @@ int ValidateReplyGraph(cee_ctx* ctx, const cee_graph_view* g) {
   return CEE_OK;
 }
 
-// Uploads coordinates and CSR unless they equal the previous call's.
-int PrepareReplyGraph(cee_ctx* ctx, const cee_graph_view* g, bool* hit, bool* grew) {
+// Whether the snapshot equals the last one validated and uploaded: coordinates, CSR and active flags
+// (ValidateReplyGraph's outcome is a function of exactly these and of the sizes, so it need not run
+// again).
+bool SameReplyGraph(const ReplyState* s, const cee_graph_view* g) {
+  if (s == nullptr || !s->has_graph || s->n != g->n || s->dist_type != g->dist_type) return false;
+  const size_t n = static_cast<size_t>(g->n), adj = static_cast<size_t>(g->adjacency), m = static_cast<size_t>(g->m);
+  return g->adjacency >= 0 && g->m >= 0 && Same(s->hro, g->row_offsets, n + 1) && Same(s->hnbr, g->neighbors, adj) &&
+         Same(s->hactive, g->active, m) && Same(s->hx, g->x, n) && Same(s->hy, g->y, n);
+}
+
+// Uploads coordinates and CSR of a validated snapshot unless `same` (it equals the last upload).
+int PrepareReplyGraph(cee_ctx* ctx, const cee_graph_view* g, bool same, bool* grew) {
   if (ctx->replies == nullptr) ctx->replies = new ReplyState();
   ReplyState& s = *ctx->replies;
   const size_t n = static_cast<size_t>(g->n), adj = static_cast<size_t>(g->adjacency);
-  *hit = s.has_graph && s.n == g->n && s.dist_type == g->dist_type && Same(s.hx, g->x, n) && Same(s.hy, g->y, n) &&
-         Same(s.hro, g->row_offsets, n + 1) && Same(s.hnbr, g->neighbors, adj);
-  if (*hit) return CEE_OK;
+  if (same) return CEE_OK;
   s.has_graph = false;
   std::vector<int2> xy;
-  int rc = PackCoordinates(ctx, g->n, g->x, g->y, &xy, &s.span);
+  const int rc = PackCoordinates(ctx, g->n, g->x, g->y, &xy, &s.span);
   if (rc != CEE_OK) return rc;
   bool g1 = false, g2 = false, g3 = false;
   cudaError_t status = s.xy.Reserve(n * sizeof(int2) + 16, &g1);
@@ -105,6 +114,7 @@ int PrepareReplyGraph(cee_ctx* ctx, const cee_graph_view* g, bool* hit, bool* gr
   s.hy.assign(g->y, g->y + n);
   s.hro.assign(g->row_offsets, g->row_offsets + n + 1);
   s.hnbr.assign(g->neighbors, g->neighbors + adj);
+  s.hactive.assign(g->active, g->active + g->m);
   s.n = g->n;
   s.dist_type = g->dist_type;
   s.has_graph = true;
@@ -162,8 +172,13 @@ int cee_ht_replies(cee_ctx* ctx, const cee_graph_view* graph, int32_t u, int32_t
   if (graph == nullptr || count < 0 || offsets_out == nullptr || (count > 0 && centers == nullptr)) {
     return Fail(ctx, CEE_ERR_INVALID, "bad HT reply arguments");
   }
-  rc = ValidateReplyGraph(ctx, graph);
+  rc = ValidateView(ctx, graph);
   if (rc != CEE_OK) return rc;
+  const bool same = SameReplyGraph(ctx->replies, graph);  // validated and uploaded last time
+  if (!same) {
+    rc = ValidateReplyGraph(ctx, graph);
+    if (rc != CEE_OK) return rc;
+  }
   // ValidateInputs (src/cuda/ht_replies.cu:555-566)
   if (u < 0 || v >= graph->n || u >= v || !HostHasActiveEdge(graph, u, v)) {
     return Fail(ctx, CEE_ERR_INVALID, "HT replies: the target must be an active edge (u < v)");
@@ -178,8 +193,9 @@ int cee_ht_replies(cee_ctx* ctx, const cee_graph_view* graph, int32_t u, int32_t
   ctx->replies->kind = 1;
   ctx->replies->total = 0;
   if (count == 0) return CEE_OK;
-  bool hit = false, grew = false;
-  rc = PrepareReplyGraph(ctx, graph, &hit, &grew);
+  const bool hit = same;
+  bool grew = false;
+  rc = PrepareReplyGraph(ctx, graph, same, &grew);
   if (rc != CEE_OK) return Drained(ctx, rc);
   ReplyState& s = *ctx->replies;
   s.kind = 1;
@@ -242,8 +258,13 @@ int cee_ht_end_replies(cee_ctx* ctx, const cee_graph_view* graph, const cee_ht_e
   if (graph == nullptr || count < 0 || offsets_out == nullptr || (count > 0 && tasks == nullptr)) {
     return Fail(ctx, CEE_ERR_INVALID, "bad HT end reply arguments");
   }
-  rc = ValidateReplyGraph(ctx, graph);
+  rc = ValidateView(ctx, graph);
   if (rc != CEE_OK) return rc;
+  const bool same = SameReplyGraph(ctx->replies, graph);
+  if (!same) {
+    rc = ValidateReplyGraph(ctx, graph);
+    if (rc != CEE_OK) return rc;
+  }
   // ValidateEndInputs (src/cuda/ht_replies.cu:568-581)
   for (int64_t i = 0; i < count; ++i) {
     const cee_ht_end_task t = tasks[i];
@@ -257,8 +278,9 @@ int cee_ht_end_replies(cee_ctx* ctx, const cee_graph_view* graph, const cee_ht_e
   ctx->replies->kind = 2;
   ctx->replies->total = 0;
   if (count == 0) return CEE_OK;
-  bool hit = false, grew = false;
-  rc = PrepareReplyGraph(ctx, graph, &hit, &grew);
+  const bool hit = same;
+  bool grew = false;
+  rc = PrepareReplyGraph(ctx, graph, same, &grew);
   if (rc != CEE_OK) return Drained(ctx, rc);
   ReplyState& s = *ctx->replies;
   s.kind = 2;
