@@ -61,6 +61,7 @@ def parse():
     p.add_argument("--no-kopt", action="store_true")
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--serve-jobs", type=int, default=10_000)
+    p.add_argument("--serve-slots", type=int, default=32, help="job slots of the serving loop (1..256)")
     p.add_argument("--no-epochs", action="store_true")
     p.add_argument("--no-refgpu", action="store_true")
     p.add_argument("--part", default="all", choices=["all", "batch", "kopt", "serve", "epochs", "refgpu"],
@@ -942,7 +943,7 @@ def run_serve(args, device, world, parity=None, leaf: bool = False, wl=None):
             pinned_pools.append(owner)
             pinned[k] = view
         wl.kopt[i] = (g, pinned)
-    slots = 32
+    slots = args.serve_slots
     max_bytes = max(_job_output_bytes(wl, j, leaf) for j in wl.jobs)
     owners, buffers = _pinned_pool(slots + 1, max_bytes)
     ctx = Context(device)
