@@ -64,7 +64,7 @@ def parse():
     p.add_argument("--serve-slots", type=int, default=32, help="job slots of the serving loop (1..256)")
     p.add_argument("--no-epochs", action="store_true")
     p.add_argument("--no-refgpu", action="store_true")
-    p.add_argument("--part", default="all", choices=["all", "batch", "kopt", "serve", "epochs", "refgpu"],
+    p.add_argument("--part", default="all", choices=["all", "batch", "kopt", "serve", "epochs", "refgpu", "replies"],
                    help="profiling aid: run only the batched screen, the k-opt part or the serving loop")
     p.add_argument("--cpu-budget-s", type=float, default=12.0)
     p.add_argument("--cpu-leg", default=None, help=argparse.SUPPRESS)
@@ -400,6 +400,8 @@ def run_ours(args, rank: int, world: int, device: int):
         return run_fixed_point(args, device)
     if args.part == "refgpu":
         return run_reference_gpu(args, device)
+    if args.part == "replies":
+        return run_replies(args, device)
     from cudaedgeelimination_b200.api import BatchOptions
     batch = synth.BatchUnion(args.instances)
     g = batch.graph
@@ -1044,6 +1046,45 @@ def run_serve(args, device, world, parity=None, leaf: bool = False, wl=None):
         "checked_jobs": len(plain_kept),
         **extra,
     }
+
+
+def run_replies(args, device):
+    """HT Hamilton replies (cee_ht_replies + fetch) of every other node of the 50,000-node 10-NN
+    case as a center, against the oracle's lists: the device span of one call (count pass, offsets,
+    write pass) on the context's stream and the host time of the whole call."""
+    import torch
+    import oracle
+    from cudaedgeelimination_b200 import Context, synth
+    g = synth.uniform_knn(50_000, 10_000_000, 10, 0, 7)
+    e = int(np.flatnonzero(g.active)[0])
+    u, v = int(min(g.edge_u[e], g.edge_v[e])), int(max(g.edge_u[e], g.edge_v[e]))
+    centers = np.array([c for c in range(g.n) if c not in (u, v)], np.int32)
+    ctx = Context(device)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=device)
+    for _ in range(max(args.warmup, 1)):
+        offsets, replies = ctx.ht_replies(g, u, v, centers)
+    dev_ms, host_ms = [], []
+    for _ in range(max(args.steps, 1)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        offsets, replies = ctx.ht_replies(g, u, v, centers)
+        e1.record(stream)
+        e1.synchronize()
+        host_ms.append((time.perf_counter() - t0) * 1e3)
+        dev_ms.append(e0.elapsed_time(e1))
+    ctx.close()
+    want_offsets, want = oracle.Port().ht_replies(g, u, v, centers)
+    assert np.array_equal(offsets, want_offsets) and np.array_equal(replies, want), "replies differ from the oracle"
+    deg = np.diff(g.row_offsets)[centers].astype(np.int64)
+    pairs = int((deg * (deg - 1) // 2).sum())
+    ms = float(np.median(host_ms))
+    return {"metric": "HT Hamilton replies/s", "value": len(replies) / (ms / 1e3), "unit": "replies/s",
+            "replies": int(len(replies)), "centers": int(centers.shape[0]), "pairs_tested": pairs,
+            "ms_per_call": ms, "device_span_ms": float(np.median(dev_ms)), "pairs_per_s": pairs / (ms / 1e3),
+            "parity": "offsets and every reply equal the oracle's (oracle/cee_oracle.c)",
+            "config": f"50,000-node uniform 10-NN EUC_2D, target ({u}, {v}), every other node a center; "
+                      "snapshot resident (graph_hit), 36 MB of replies copied to host memory per call"}
 
 
 def run_fixed_point(args, device):
