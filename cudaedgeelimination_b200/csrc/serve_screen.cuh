@@ -316,8 +316,9 @@ __device__ __forceinline__ unsigned long long volatile_load(const unsigned long 
 
 // Copies slot `slot`'s descriptor into `out` (all lanes) and returns true when it is the
 // published, complete descriptor: state read before and after the copy (with fences) equals the
-// copy's generation. The host unpublishes a slot (state = 0) before rewriting its descriptor and
-// republishes it after, all with ordered copies, so a torn copy always fails this check.
+// copy's generation. The dispatcher warp unpublishes a slot (state = 0) before rewriting its
+// descriptor and republishes it after, with fences between the steps (serve_install), so a torn copy
+// always fails this check.
 __device__ __forceinline__ bool serve_read_job(const ServeControl* ctl, int slot, ServeJob& out, int lane) {
   const uint32_t s1 = volatile_load(&ctl->state[slot]);
   __threadfence();
@@ -504,7 +505,7 @@ static __global__ void __launch_bounds__(kServeWarps * 32, 4)
     const uint32_t index = static_cast<uint32_t>(t);
     if (gen != job.generation) {
       // the slot was republished after this warp read it: the claimed item belongs to the newer
-      // job, whose descriptor was written before its ticket (ordered copies); read it, bounded
+      // job, whose descriptor was written before its ticket (serve_install); read it, bounded
       bool found = false;
       for (int w = 0; w < kServeDescriptorWaits && !found; ++w) {
         const uint32_t state = __shfl_sync(kFullMask, lane == 0 ? volatile_load(&ctl->state[slot]) : 0u, 0);
