@@ -575,6 +575,16 @@ def run_ours(args, rank: int, world: int, device: int):
             "value": cpu_edges / cpu_s, "unit": UNIT, "cores": threads, "kind": step.kind,
             "sample": f"all {batch.count} instances ({cpu_edges} edges, JV screen + 64 c,d root screens each) in "
                       f"{cpu_s:.1f} s, one C++ call on {threads} host threads, snapshots built before timing"}
+        if step.kind == "reference":
+            # the two parts apart on one core (FindJvCandidatesCpu; BuildCdScreenTasks + ScreenCdTasksCpu),
+            # on every 16th instance
+            sample = list(range(0, batch.count, 16))
+            jv_s, cd_s, e1, t1 = step.graphs.parts_1core(sample)
+            result["cpu_baseline"]["parts_1core"] = {
+                "jv_edges_per_s": e1 / jv_s, "cd_tasks_per_s": t1 / cd_s, "cores": 1,
+                "sample": f"every 16th instance ({len(sample)} instances, {e1} edges, {t1} c,d tasks): "
+                          f"JV {jv_s:.2f} s, c,d {cd_s:.2f} s on one thread",
+                "api": "FindJvCandidatesCpu; SelectHtTargetEdgeIds + BuildCdScreenTasks + ScreenCdTasksCpu"}
         result["host_cpu"] = host_cpu()
         # full-size parity: every instance of the timed step against the C oracle
         parity["batch"] = check_batch_full(batch, res, fin_cand, fin_opt)

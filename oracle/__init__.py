@@ -383,6 +383,9 @@ class Reference:
         L.ref_graph_new_many.argtypes = [ctypes.c_int32, ctypes.c_int] + [vp] * 9
         L.ref_batch_step.argtypes = [vp, ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                      ctypes.c_int, ctypes.c_int32, i64p, i64p]
+        L.ref_batch_parts_1core.argtypes = [vp, ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                            ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_double), i64p, i64p]
         dp = ctypes.POINTER(ctypes.c_double)
         L.ref_seam_jv_timed.argtypes = [vp, ctypes.c_int32, dp, i32p]
         L.ref_seam_kopt_timed.argtypes = [vp, ctypes.c_uint32, vp, ctypes.c_int64, ctypes.c_int32, dp, i64p]
@@ -452,6 +455,17 @@ class RefBatch:
         self.ref._check(self.ref.L.ref_batch_step(chosen, len(instances), targets, nb, max_deg, mode, threads,
                                                   ctypes.byref(edges), ctypes.byref(tasks)))
         return int(edges.value), int(tasks.value)
+
+    def parts_1core(self, instances, targets: int = 64, nb: int = 25, max_deg: int = 50, mode: int = 0):
+        """ref_batch_parts_1core: (JV seconds, c,d seconds, edges screened, c,d tasks screened) of the
+        batched step's CPU work on one thread, the two parts timed apart."""
+        chosen = (vp * len(instances))(*[self.handles[i] for i in instances])
+        jv, cd = ctypes.c_double(0), ctypes.c_double(0)
+        edges, tasks = ctypes.c_int64(0), ctypes.c_int64(0)
+        self.ref._check(self.ref.L.ref_batch_parts_1core(chosen, len(instances), targets, nb, max_deg, mode,
+                                                         ctypes.byref(jv), ctypes.byref(cd), ctypes.byref(edges),
+                                                         ctypes.byref(tasks)))
+        return jv.value, cd.value, int(edges.value), int(tasks.value)
 
     def seam_cd_timed(self, instances, targets: int = 64, nb: int = 25, max_deg: int = 50, mode: int = 0):
         """ref_seam_cd_timed over the given instances: (seconds, c,d tasks screened, flags set)."""

@@ -102,6 +102,49 @@ int ref_batch_step(void* const* handles, int32_t count, uint32_t targets, uint32
   return failed ? -1 : 0;
 }
 
+// The same work as ref_batch_step on the calling thread alone, with the two parts timed apart
+// (steady clock, accumulated per instance): FindJvCandidatesCpu, and SelectHtTargetEdgeIds +
+// BuildCdScreenTasks + ScreenCdTasksCpu. Writes the seconds of each part and what each screened.
+int ref_batch_parts_1core(void* const* handles, int32_t count, uint32_t targets, uint32_t max_neighborhood,
+                          uint32_t max_candidate_degree, int mode, double* jv_seconds, double* cd_seconds,
+                          int64_t* edges_out, int64_t* cd_tasks_out) {
+  try {
+    cudaee::HtShallowOptions options;
+    options.max_neighborhood = max_neighborhood;
+    options.max_candidate_degree = max_candidate_degree;
+    double jv = 0.0, cd = 0.0;
+    int64_t edges = 0, tasks_screened = 0;
+    for (int32_t i = 0; i < count; ++i) {
+      const auto* graph = static_cast<const cudaee::GraphSnapshot*>(handles[i]);
+      const auto t0 = std::chrono::steady_clock::now();
+      const auto candidates = cudaee::FindJvCandidatesCpu(*graph);
+      const auto t1 = std::chrono::steady_clock::now();
+      (void)candidates;
+      for (const auto& edge : graph->edges) edges += edge.active ? 1 : 0;
+      const auto t2 = std::chrono::steady_clock::now();
+      const auto ids = cudaee::SelectHtTargetEdgeIds(*graph, cudaee::HtTargetOrder::kWeightDescending);
+      const std::size_t used = std::min<std::size_t>(ids.size(), targets);
+      for (std::size_t t = 0; t < used; ++t) {
+        const cudaee::Edge& e = graph->edges[static_cast<std::size_t>(ids[t])];
+        const cudaee::NodeEdge target{e.u, e.v};
+        const auto tasks = cudaee::BuildCdScreenTasks(*graph, target, options);
+        const auto flags = cudaee::ScreenCdTasksCpu(*graph, target, tasks, static_cast<cudaee::HtCdMode>(mode));
+        tasks_screened += static_cast<int64_t>(flags.size());
+      }
+      const auto t3 = std::chrono::steady_clock::now();
+      jv += std::chrono::duration<double>(t1 - t0).count();
+      cd += std::chrono::duration<double>(t3 - t2).count();
+    }
+    *jv_seconds = jv;
+    *cd_seconds = cd;
+    *edges_out = edges;
+    *cd_tasks_out = tasks_screened;
+    return 0;
+  } catch (...) {
+    return -1;
+  }
+}
+
 // detail::ScreenHtCdCandidatesCuda (include/cuda_edge_elimination/hamilton_tutte.hpp:527-531)
 // over prebuilt snapshots: for each snapshot its first `targets` SelectHtTargetEdgeIds targets,
 // their BuildCdScreenTasks lists built before the clock starts, then every (snapshot, target)
