@@ -618,10 +618,33 @@ __device__ void batch_finalize_target(const BatchArgs& A, int32_t inst, int32_t 
   int32_t* cc_out = A.cand_c + slot * A.max_cd;
   int32_t* cd_out = A.cand_d + slot * A.max_cd;
   int64_t* cp_out = A.cand_product + slot * A.max_cd;
-  // FinalizeCdCandidates: reply count of every neighbourhood node (lane k keeps node k's)
+  // FinalizeCdCandidates: the reply count of every neighbourhood node that is an end of a flagged
+  // pair (lane k keeps node k's; the products need no other count)
+  uint32_t need = 0;
+  for (int base = 0; base < A.flag_words * 32 && any_flag; base += 32) {
+    const int p = base + lane;
+    const uint32_t word = __shfl_sync(kFullMask, my_word, base >> 5);
+    if (p < pairs && ((word >> lane) & 1u) != 0) {
+      int i = 0, j = 1;
+      if (size == NB) {
+        i = pair_i[p];
+        j = pair_j[p];
+      } else {
+        int rest = p;
+        while (rest >= size - 1 - i) {
+          rest -= size - 1 - i;
+          ++i;
+        }
+        j = i + 1 + rest;
+      }
+      need |= (1u << i) | (1u << j);
+    }
+  }
+  need = __reduce_or_sync(kFullMask, need);
   int32_t my_replies = 0;
   if (any_flag) {
-    for (int k = 0; k < size; ++k) {
+    for (uint32_t rest = need; rest != 0; rest &= rest - 1) {
+      const int k = __ffs(rest) - 1;
       const int32_t x = __shfl_sync(kFullMask, ln, k);
       const int2 pxk = make_int2(__shfl_sync(kFullMask, px.x, k), __shfl_sync(kFullMask, px.y, k));
       const uint32_t cuk = __shfl_sync(kFullMask, cu, k), cvk = __shfl_sync(kFullMask, cv, k);
