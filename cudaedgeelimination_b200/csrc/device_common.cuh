@@ -134,19 +134,20 @@ __device__ __forceinline__ uint64_t warp_sort_asc(uint64_t key, int lane) {
   return key;
 }
 
-// The same network on 32-bit keys.
-__device__ __forceinline__ uint32_t warp_sort_asc32(uint32_t key, int lane) {
+// The kCount smallest of the warp's 32-bit keys, ascending: lane i < kCount ends with the i-th
+// smallest, every other lane with 0xffffffff. Keys other than 0xffffffff (the empty key) must be
+// distinct. kCount warp min-reductions, each knocking its key out, cost fewer instructions than
+// the 15-stage bitonic network when only the head of the order is wanted.
+template <int kCount>
+__device__ __forceinline__ uint32_t warp_smallest_asc32(uint32_t key, int lane) {
+  uint32_t out = 0xffffffffu;
 #pragma unroll
-  for (int k = 2; k <= 32; k <<= 1) {
-#pragma unroll
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      const uint32_t other = __shfl_xor_sync(kFullMask, key, j);
-      const bool ascending = (lane & k) == 0;
-      const bool lower = (lane & j) == 0;
-      key = (lower == ascending) ? min(key, other) : max(key, other);
-    }
+  for (int r = 0; r < kCount; ++r) {
+    const uint32_t smallest = __reduce_min_sync(kFullMask, key);
+    if (lane == r) out = smallest;
+    if (key == smallest) key = 0xffffffffu;
   }
-  return key;
+  return out;
 }
 
 // Given two ascending warp-wide lists, returns the 32 smallest keys of their union,

@@ -19,8 +19,9 @@
 //     edge; lanes of a warp diverge on loop lengths.
 //   * jv_screen_warp_kernel, one warp per edge: the lanes score up to 32 candidates at once (when
 //     N(a) and N(b) fit one round, a node of N(b) already in N(a) is found by matching lane
-//     values, otherwise by a binary search of row a) and keep the top-10 as a warp-wide
-//     bitonic-sorted list; the witness search tests the first
+//     values, otherwise by a binary search of row a) and keep the top-10 (one round of 32-bit keys:
+//     ten warp min-reductions; otherwise a warp-wide bitonic-sorted list merged round by round);
+//     the witness search tests the first
 //     three neighbours of all ten candidates at once, then flattens the remaining pairs of the
 //     still-open candidates over the lanes, accepting a candidate only once all of its pairs
 //     are tested and every earlier candidate is closed (so the sequential choice is kept).
@@ -232,7 +233,7 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
       if (__all_sync(kFullMask, !ok || score < (1u << 18) - 1u)) {
         uint32_t k32 = ok ? (static_cast<uint32_t>(score) << 14) | static_cast<uint32_t>(c - a + kJvLocalSpan)
                           : 0xffffffffu;
-        k32 = warp_sort_asc32(k32, lane);
+        k32 = warp_smallest_asc32<kJvMaxCandidates>(k32, lane);  // keys are distinct: distinct nodes
         top = k32 == 0xffffffffu ? kEmptyKey
                                  : (static_cast<uint64_t>(k32 >> 14) << 32) |
                                        static_cast<uint32_t>(static_cast<int32_t>(k32 & 0x3fffu) - kJvLocalSpan + a);
@@ -249,7 +250,7 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
       const int node_bits = span == 0 ? 1 : 32 - __clz(span);
       if (narrow_scores && node_bits < 31 && smax < (1u << (32 - node_bits)) - 1u) {
         uint32_t k32 = ok ? (static_cast<uint32_t>(score) << node_bits) | (static_cast<uint32_t>(c) - cmin) : 0xffffffffu;
-        k32 = warp_sort_asc32(k32, lane);
+        k32 = warp_smallest_asc32<kJvMaxCandidates>(k32, lane);
         top = k32 == 0xffffffffu ? kEmptyKey
                                  : (static_cast<uint64_t>(k32 >> node_bits) << 32) |
                                        (cmin + (k32 & ((1u << node_bits) - 1u)));
