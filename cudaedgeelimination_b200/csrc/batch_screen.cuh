@@ -568,7 +568,7 @@ static __global__ void __launch_bounds__(kBatchWarps * 32, 8) batch_screen_kerne
       const int64_t e0 = A.jv_first + (q - n_select) * A.jv_tile;
       const int64_t e1 = min(e0 + A.jv_tile, A.jv_last);
       for (int64_t e = e0; e < e1; ++e) {
-        const int32_t w = jv_screen_edge_warp<kSpan, true, kLocal>(A.g, e, scratch[warp].jv, lane, A.error);
+        const int32_t w = jv_screen_edge_warp<kSpan, true, kLocal, true>(A.g, e, scratch[warp].jv, lane, A.error);
         if (lane == 0) A.witness[e] = w;
         __syncwarp();
       }

@@ -51,6 +51,7 @@ struct JvGraph {
   const int32_t* __restrict__ nbr;          // [adjacency], rows ascending
   const int32_t* __restrict__ slot_w;       // [adjacency], weight of the CSR slot's edge
   const int4* __restrict__ slot4;           // [adjacency] {neighbour, slot weight, x, y} (batched screen)
+  const int4* __restrict__ node4;           // [n] {x, y, row_offsets[x], row_offsets[x + 1]} (batched screen)
 };
 
 // ------------------------------------------------------------------ thread per edge -----
@@ -165,18 +166,36 @@ struct JvWarpScratch {
 // Screens edge e with the calling (full) warp; returns the witness or -1 on every lane. With
 // kSlot4 a CSR slot's neighbour, weight and neighbour coordinates come from one 16-byte load; with
 // kLocal the caller guarantees that every neighbour of a or b has an id within kJvLocalSpan - 1 of a
-// (the snapshot, or each instance of a batch union, has at most kJvLocalSpan nodes).
-template <int kSpan, bool kSlot4 = false, bool kLocal = false>
+// (the snapshot, or each instance of a batch union, has at most kJvLocalSpan nodes); with kNode4 a
+// node's coordinates and CSR row come from one 16-byte load.
+template <int kSpan, bool kSlot4 = false, bool kLocal = false, bool kNode4 = false>
 __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t e, JvWarpScratch& s,
                                                        int lane, int32_t* __restrict__ error) {
   if (__ldg(g.active + e) == 0) return -1;
   const int2 uv = __ldg(g.edge_uv + e);
   const int32_t a = uv.x, b = uv.y;
-  const int32_t ra0 = __ldg(g.row_offsets + a), ra1 = __ldg(g.row_offsets + a + 1);
-  const int32_t rb0 = __ldg(g.row_offsets + b), rb1 = __ldg(g.row_offsets + b + 1);
+  int32_t ra0, ra1, rb0, rb1;
+  int2 pa, pb;
+  if constexpr (kNode4) {
+    const int4 na = __ldg(g.node4 + a), nb = __ldg(g.node4 + b);
+    pa = make_int2(na.x, na.y);
+    pb = make_int2(nb.x, nb.y);
+    ra0 = na.z;
+    ra1 = na.w;
+    rb0 = nb.z;
+    rb1 = nb.w;
+  } else {
+    ra0 = __ldg(g.row_offsets + a);
+    ra1 = __ldg(g.row_offsets + a + 1);
+    rb0 = __ldg(g.row_offsets + b);
+    rb1 = __ldg(g.row_offsets + b + 1);
+  }
   const int32_t da = ra1 - ra0, db = rb1 - rb0;
   if (da <= 2 || db <= 2) return -1;
-  const int2 pa = __ldg(g.xy + a), pb = __ldg(g.xy + b);
+  if constexpr (!kNode4) {
+    pa = __ldg(g.xy + a);
+    pb = __ldg(g.xy + b);
+  }
   const int64_t cab = __ldg(g.edge_w + e);
   // neighbours must lie in [lo, lo + range): the snapshot's ids, or with kLocal also within
   // kJvLocalSpan - 1 of a (the one test bounds both the gathers and the instance-relative keys)
@@ -268,11 +287,25 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
     const uint64_t key = __shfl_sync(kFullMask, top, ci);
     if (lane < 2 * kJvMaxCandidates && ci < nc) {
       const int32_t c = static_cast<int32_t>(key & 0xffffffffu);
-      const uint32_t dist = exact_distance<kSpan>(lane < kJvMaxCandidates ? pa : pb, __ldg(g.xy + c), g.dist_type);
+      int2 pc;
+      int32_t row0 = 0, row1 = 0;
+      if constexpr (kNode4) {
+        const int4 nc4 = __ldg(g.node4 + c);
+        pc = make_int2(nc4.x, nc4.y);
+        row0 = nc4.z;
+        row1 = nc4.w;
+      } else {
+        pc = __ldg(g.xy + c);
+        if (lane < kJvMaxCandidates) {
+          row0 = __ldg(g.row_offsets + c);
+          row1 = __ldg(g.row_offsets + c + 1);
+        }
+      }
+      const uint32_t dist = exact_distance<kSpan>(lane < kJvMaxCandidates ? pa : pb, pc, g.dist_type);
       if (lane < kJvMaxCandidates) {
         s.c[ci] = c;
-        s.row[ci] = __ldg(g.row_offsets + c);
-        s.end[ci] = __ldg(g.row_offsets + c + 1);
+        s.row[ci] = row0;
+        s.end[ci] = row1;
         s.cac[ci] = dist;
       } else {
         s.cbc[ci] = dist;
