@@ -263,8 +263,8 @@ __device__ void batch_select_targets(const BatchArgs& A, int32_t inst, int lane)
     uint64_t key = kEmptyKey;
     if (e < e1 && g.active[e] != 0) {
       const int2 uv = g.edge_uv[e];
-      const int32_t du = __ldg(g.row_offsets + uv.x + 1) - __ldg(g.row_offsets + uv.x);
-      const int32_t dv = __ldg(g.row_offsets + uv.y + 1) - __ldg(g.row_offsets + uv.y);
+      const int4 nu = __ldg(g.node4 + uv.x), nv = __ldg(g.node4 + uv.y);
+      const int32_t du = nu.w - nu.z, dv = nv.w - nv.z;
       if (du > 2 && dv > 2) {
         // weight descending, then the instance's edge order (= (u, v) order, edges canonical)
         key = (static_cast<uint64_t>(0x7fffffffu - static_cast<uint32_t>(__ldg(g.edge_w + e))) << 32) |
@@ -309,13 +309,15 @@ template <int kSpan>
 __device__ int32_t ht_reply_count(const JvGraph& g, int32_t u, int32_t v, int2 pu, int2 pv, uint32_t cuv,
                                   int32_t center, int2 pc, uint32_t cuc, uint32_t cvc, const uint16_t* reply_pairs,
                                   int lane) {
-  const int32_t r0 = __ldg(g.row_offsets + center), deg = __ldg(g.row_offsets + center + 1) - r0;
+  const int4 c4 = __ldg(g.node4 + center);
+  const int32_t r0 = c4.z, deg = c4.w - c4.z;
   if (deg < 2) return 0;
   const uint64_t center_target = static_cast<uint64_t>(cuc) + cvc;
   // neighbour j: node, C(center, j), 2-opt survival of edge (center, j) against the target
   auto neighbour = [&](int j, int32_t& node, int2& p, uint32_t& cost, bool& survives) {
-    node = __ldg(g.nbr + r0 + j);
-    p = __ldg(g.xy + node);
+    const int4 s4 = __ldg(g.slot4 + r0 + j);
+    node = s4.x;
+    p = make_int2(s4.z, s4.w);
     cost = exact_distance<kSpan>(pc, p, g.dist_type);
     const bool center_low = center < node;  // canonical edge (ou, ov)
     const uint32_t cu_o = exact_distance<kSpan>(pu, p, g.dist_type), cv_o = exact_distance<kSpan>(pv, p, g.dist_type);
@@ -443,9 +445,9 @@ __device__ void batch_cd_target(const BatchArgs& A, int32_t inst, int32_t t, con
       if (n0 + j < n1) {
         const int32_t x = __ldg(A.perm + n0 + j);
         if (x != u && x != v) {
-          const int32_t deg = __ldg(g.row_offsets + x + 1) - __ldg(g.row_offsets + x);
-          if (A.max_degree == 0 || deg <= A.max_degree) {
-            const int2 p = __ldg(g.xy + x);
+          const int4 x4 = __ldg(g.node4 + x);
+          if (A.max_degree == 0 || x4.w - x4.z <= A.max_degree) {
+            const int2 p = make_int2(x4.x, x4.y);
             const int64_t dx = 2 * static_cast<int64_t>(p.x) - mx, dy = 2 * static_cast<int64_t>(p.y) - my;
             s = static_cast<uint64_t>(dx * dx) + static_cast<uint64_t>(dy * dy);
             node = x;
@@ -463,9 +465,9 @@ __device__ void batch_cd_target(const BatchArgs& A, int32_t inst, int32_t t, con
     uint64_t s = kEmptyKey;
     int32_t node = INT32_MAX;
     if (x < n1 && x != u && x != v) {
-      const int32_t deg = __ldg(g.row_offsets + x + 1) - __ldg(g.row_offsets + x);
-      if (A.max_degree == 0 || deg <= A.max_degree) {
-        const int2 p = __ldg(g.xy + x);
+      const int4 x4 = __ldg(g.node4 + x);
+      if (A.max_degree == 0 || x4.w - x4.z <= A.max_degree) {
+        const int2 p = make_int2(x4.x, x4.y);
         const int64_t dx = 2 * static_cast<int64_t>(p.x) - mx, dy = 2 * static_cast<int64_t>(p.y) - my;
         s = static_cast<uint64_t>(dx * dx) + static_cast<uint64_t>(dy * dy);
         node = static_cast<int32_t>(x);
@@ -521,7 +523,8 @@ __device__ void batch_cd_target(const BatchArgs& A, int32_t inst, int32_t t, con
       const int32_t c = i_is_c ? ni : nj, d = i_is_c ? nj : ni;
       const uint32_t cuc = i_is_c ? cui : cuj, cud = i_is_c ? cuj : cui;
       const uint32_t cvc = i_is_c ? cvi : cvj, cvd = i_is_c ? cvj : cvi;
-      const bool active = row_contains(g.nbr, __ldg(g.row_offsets + c), __ldg(g.row_offsets + c + 1), d);
+      const int4 c4 = __ldg(g.node4 + c);
+      const bool active = row_contains(g.nbr, c4.z, c4.w, d);
       const uint64_t original = static_cast<uint64_t>(cuv) + exact_distance<kSpan>(pi, pj, g.dist_type);
       const uint64_t orient0 = static_cast<uint64_t>(cud) + cvc;
       const uint64_t orient1 = static_cast<uint64_t>(cuc) + cvd;
