@@ -47,7 +47,7 @@ struct BatchState {
   int spatial_keys = 0;               // padded key count of the largest chunked instance
   bool local = false;                 // every instance has at most kJvLocalSpan nodes
   // the union snapshot in the kernels' layout
-  DevBuf d_node_begin, d_edge_begin, xy, uv, w32, active, ro, nbr, ids, slot4, node4;
+  DevBuf d_node_begin, d_edge_begin, xy, uv, w32, active, ro, nbr, ids, slot4, node4, edge4;
   // raw uploads of the end-to-end call (converted on the device)
   DevBuf raw_x, raw_y, raw_u, raw_v;
   int32_t* w32_host = nullptr;  // pinned staging of the end-to-end call's int32 weights
@@ -71,7 +71,7 @@ struct BatchState {
   }
   void Release() {
     ReleaseGraph();
-    for (DevBuf* b : {&d_node_begin, &d_edge_begin, &xy, &uv, &w32, &active, &ro, &nbr, &ids, &slot4, &node4, &raw_x, &raw_y,
+    for (DevBuf* b : {&d_node_begin, &d_edge_begin, &xy, &uv, &w32, &active, &ro, &nbr, &ids, &slot4, &node4, &edge4, &raw_x, &raw_y,
                       &raw_u, &raw_v, &witness, &target_ids, &target_count, &nbhd, &flags, &counter, &ready,
                       &cand_c, &cand_d, &cand_product, &cand_count, &perm, &chunk_box, &d_chunk_begin}) {
       b->Release();
@@ -107,7 +107,7 @@ uint64_t BatchResident(const cee_ctx* ctx) {
   if (s == nullptr) return 0;
   uint64_t bytes = 0;
   for (const DevBuf* b : {&s->d_node_begin, &s->d_edge_begin, &s->xy, &s->uv, &s->w32, &s->active, &s->ro, &s->nbr,
-                          &s->ids, &s->slot4, &s->node4, &s->raw_x, &s->raw_y, &s->raw_u, &s->raw_v, &s->witness,
+                          &s->ids, &s->slot4, &s->node4, &s->edge4, &s->raw_x, &s->raw_y, &s->raw_u, &s->raw_v, &s->witness,
                           &s->target_ids, &s->target_count, &s->nbhd, &s->flags, &s->counter, &s->ready, &s->perm,
                           &s->chunk_box, &s->d_chunk_begin}) {
     bytes += b->capacity;
@@ -228,7 +228,7 @@ int ReserveAll(cee_ctx* ctx, BatchState& s) {
   const std::pair<DevBuf*, size_t> wants[] = {
       {&s.d_node_begin, (I + 1) * 8}, {&s.d_edge_begin, (I + 1) * 8}, {&s.xy, n * 8}, {&s.uv, m * 8},
       {&s.w32, m * 4}, {&s.active, m}, {&s.ro, (n + 1) * 4}, {&s.nbr, adj * 4}, {&s.ids, adj * 4},
-      {&s.slot4, adj * 16}, {&s.node4, n * 16}, {&s.witness, m * 4}, {&s.target_ids, I * T * 4}, {&s.target_count, I * 4},
+      {&s.slot4, adj * 16}, {&s.node4, n * 16}, {&s.edge4, m * 16}, {&s.witness, m * 4}, {&s.target_ids, I * T * 4}, {&s.target_count, I * 4},
       {&s.nbhd, I * T * NB * 4}, {&s.flags, I * T * static_cast<size_t>(s.flag_words) * 4},
       {&s.counter, kMaxChunks * 8}, {&s.ready, I * 4}, {&s.perm, n * 4},
       {&s.chunk_box, static_cast<size_t>(s.chunk_begin.back()) * 16}, {&s.d_chunk_begin, (I + 1) * 8}};
@@ -299,6 +299,7 @@ BatchArgs MakeArgs(cee_ctx* ctx, BatchState& s, int32_t first, int32_t count, in
   A.g.slot_w = nullptr;
   A.g.slot4 = static_cast<const int4*>(s.slot4.ptr);
   A.g.node4 = static_cast<const int4*>(s.node4.ptr);
+  A.g.edge4 = static_cast<const int4*>(s.edge4.ptr);
   A.node_begin = static_cast<const int64_t*>(s.d_node_begin.ptr);
   A.edge_begin = static_cast<const int64_t*>(s.d_edge_begin.ptr);
   A.first_instance = first;
@@ -420,14 +421,21 @@ __global__ void batch_gather(const int32_t* __restrict__ ids, const int32_t* __r
   }
 }
 
-// node4[x] = {xy[x], row_offsets[x], row_offsets[x + 1]} over nodes [n0, n1) (the JV screen's one-load
-// view of an edge's end or a candidate: coordinates and CSR row).
-__global__ void batch_nodes(const int2* __restrict__ xy, const int32_t* __restrict__ ro, int64_t n0, int64_t n1,
-                            int4* __restrict__ node4) {
-  for (int64_t i = n0 + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n1;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+// node4[x] = {xy[x], row_offsets[x], row_offsets[x + 1]} over nodes [n0, n1) and edge4[e] =
+// {uv[e], w32[e], active[e]} over edges [e0, e1): the batched screen's one-load views of a node
+// (coordinates and CSR row) and of an edge (ends, weight, active flag).
+__global__ void batch_records(const int2* __restrict__ xy, const int32_t* __restrict__ ro, int64_t n0, int64_t n1,
+                              int4* __restrict__ node4, const int2* __restrict__ uv, const int32_t* __restrict__ w32,
+                              const uint8_t* __restrict__ active, int64_t e0, int64_t e1, int4* __restrict__ edge4) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t first = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (int64_t i = n0 + first; i < n1; i += stride) {
     const int2 p = xy[i];
     node4[i] = make_int4(p.x, p.y, ro[i], ro[i + 1]);
+  }
+  for (int64_t e = e0 + first; e < e1; e += stride) {
+    const int2 q = uv[e];
+    edge4[e] = make_int4(q.x, q.y, w32[e], active[e]);
   }
 }
 
@@ -526,9 +534,11 @@ int cee_batch_prepare(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opt
         static_cast<const int32_t*>(s.ids.ptr), static_cast<const int32_t*>(s.nbr.ptr), static_cast<const int2*>(s.xy.ptr),
         0, g.adjacency, static_cast<const int32_t*>(s.w32.ptr), g.m, g.n, static_cast<int4*>(s.slot4.ptr), ctx->d_error);
   }
-  if (g.n > 0) {
-    batch_nodes<<<GridFor(g.n, 256, ctx->sm_count * 8), 256, 0, st>>>(
-        static_cast<const int2*>(s.xy.ptr), static_cast<const int32_t*>(s.ro.ptr), 0, g.n, static_cast<int4*>(s.node4.ptr));
+  if (g.n > 0 || g.m > 0) {
+    batch_records<<<GridFor(std::max<int64_t>(g.n, g.m), 256, ctx->sm_count * 8), 256, 0, st>>>(
+        static_cast<const int2*>(s.xy.ptr), static_cast<const int32_t*>(s.ro.ptr), 0, g.n, static_cast<int4*>(s.node4.ptr),
+        static_cast<const int2*>(s.uv.ptr), static_cast<const int32_t*>(s.w32.ptr),
+        static_cast<const uint8_t*>(s.active.ptr), 0, g.m, static_cast<int4*>(s.edge4.ptr));
   }
   cudaError_t status = LaunchSpatial(s, 0, b->instances, st);
   if (status == cudaSuccess) status = cudaStreamSynchronize(st);  // host staging vectors die at return
@@ -811,10 +821,10 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
         static_cast<const int64_t*>(s.raw_x.ptr), static_cast<const int64_t*>(s.raw_y.ptr), n0, n1, min_x, min_y,
         static_cast<int2*>(s.xy.ptr), static_cast<const int32_t*>(s.raw_u.ptr), static_cast<const int32_t*>(s.raw_v.ptr),
         e0, e1, g.n, static_cast<int2*>(s.uv.ptr), ctx->d_error);
-    if (n1 > n0) {
-      batch_nodes<<<GridFor(n1 - n0, 256, ctx->sm_count * 8), 256, 0, s.prep>>>(
-          static_cast<const int2*>(s.xy.ptr), static_cast<const int32_t*>(s.ro.ptr), n0, n1, static_cast<int4*>(s.node4.ptr));
-    }
+    batch_records<<<GridFor(std::max(n1 - n0, e1 - e0), 256, ctx->sm_count * 8), 256, 0, s.prep>>>(
+        static_cast<const int2*>(s.xy.ptr), static_cast<const int32_t*>(s.ro.ptr), n0, n1, static_cast<int4*>(s.node4.ptr),
+        static_cast<const int2*>(s.uv.ptr), static_cast<const int32_t*>(s.w32.ptr),
+        static_cast<const uint8_t*>(s.active.ptr), e0, e1, static_cast<int4*>(s.edge4.ptr));
     if (s1 > s0) {
       batch_gather<<<GridFor(s1 - s0, 256, ctx->sm_count * 8), 256, 0, s.prep>>>(
           static_cast<const int32_t*>(s.ids.ptr), static_cast<const int32_t*>(s.nbr.ptr), static_cast<const int2*>(s.xy.ptr),

@@ -261,13 +261,13 @@ __device__ void batch_select_targets(const BatchArgs& A, int32_t inst, int lane)
   for (int64_t base = e0; base < e1; base += 32) {
     const int64_t e = base + lane;
     uint64_t key = kEmptyKey;
-    if (e < e1 && g.active[e] != 0) {
-      const int2 uv = g.edge_uv[e];
-      const int4 nu = __ldg(g.node4 + uv.x), nv = __ldg(g.node4 + uv.y);
+    const int4 er = e < e1 ? __ldg(g.edge4 + e) : make_int4(0, 0, 0, 0);
+    if (er.w != 0) {
+      const int4 nu = __ldg(g.node4 + er.x), nv = __ldg(g.node4 + er.y);
       const int32_t du = nu.w - nu.z, dv = nv.w - nv.z;
       if (du > 2 && dv > 2) {
         // weight descending, then the instance's edge order (= (u, v) order, edges canonical)
-        key = (static_cast<uint64_t>(0x7fffffffu - static_cast<uint32_t>(__ldg(g.edge_w + e))) << 32) |
+        key = (static_cast<uint64_t>(0x7fffffffu - static_cast<uint32_t>(er.z)) << 32) |
               static_cast<uint32_t>(e - e0);
       }
     }

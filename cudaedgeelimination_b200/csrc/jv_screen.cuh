@@ -52,6 +52,7 @@ struct JvGraph {
   const int32_t* __restrict__ slot_w;       // [adjacency], weight of the CSR slot's edge
   const int4* __restrict__ slot4;           // [adjacency] {neighbour, slot weight, x, y} (batched screen)
   const int4* __restrict__ node4;           // [n] {x, y, row_offsets[x], row_offsets[x + 1]} (batched screen)
+  const int4* __restrict__ edge4;           // [m] {u, v, weight, active} (batched screen)
 };
 
 // ------------------------------------------------------------------ thread per edge -----
@@ -166,17 +167,29 @@ struct JvWarpScratch {
 // Screens edge e with the calling (full) warp; returns the witness or -1 on every lane. With
 // kSlot4 a CSR slot's neighbour, weight and neighbour coordinates come from one 16-byte load; with
 // kLocal the caller guarantees that every neighbour of a or b has an id within kJvLocalSpan - 1 of a
-// (the snapshot, or each instance of a batch union, has at most kJvLocalSpan nodes); with kNode4 a
-// node's coordinates and CSR row come from one 16-byte load.
-template <int kSpan, bool kSlot4 = false, bool kLocal = false, bool kNode4 = false>
+// (the snapshot, or each instance of a batch union, has at most kJvLocalSpan nodes); with kRecords
+// an edge's ends, weight and active flag, and a node's coordinates and CSR row, each come from one
+// 16-byte load.
+template <int kSpan, bool kSlot4 = false, bool kLocal = false, bool kRecords = false>
 __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t e, JvWarpScratch& s,
                                                        int lane, int32_t* __restrict__ error) {
-  if (__ldg(g.active + e) == 0) return -1;
-  const int2 uv = __ldg(g.edge_uv + e);
-  const int32_t a = uv.x, b = uv.y;
+  int32_t a, b;
+  int64_t cab;
+  if constexpr (kRecords) {
+    const int4 er = __ldg(g.edge4 + e);
+    if (er.w == 0) return -1;
+    a = er.x;
+    b = er.y;
+    cab = er.z;
+  } else {
+    if (__ldg(g.active + e) == 0) return -1;
+    const int2 uv = __ldg(g.edge_uv + e);
+    a = uv.x;
+    b = uv.y;
+  }
   int32_t ra0, ra1, rb0, rb1;
   int2 pa, pb;
-  if constexpr (kNode4) {
+  if constexpr (kRecords) {
     const int4 na = __ldg(g.node4 + a), nb = __ldg(g.node4 + b);
     pa = make_int2(na.x, na.y);
     pb = make_int2(nb.x, nb.y);
@@ -192,11 +205,11 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
   }
   const int32_t da = ra1 - ra0, db = rb1 - rb0;
   if (da <= 2 || db <= 2) return -1;
-  if constexpr (!kNode4) {
+  if constexpr (!kRecords) {
     pa = __ldg(g.xy + a);
     pb = __ldg(g.xy + b);
+    cab = __ldg(g.edge_w + e);
   }
-  const int64_t cab = __ldg(g.edge_w + e);
   // neighbours must lie in [lo, lo + range): the snapshot's ids, or with kLocal also within
   // kJvLocalSpan - 1 of a (the one test bounds both the gathers and the instance-relative keys)
   const int32_t lo = kLocal ? max(a - (kJvLocalSpan - 1), 0) : 0;
@@ -289,7 +302,7 @@ __device__ __forceinline__ int32_t jv_screen_edge_warp(const JvGraph& g, int64_t
       const int32_t c = static_cast<int32_t>(key & 0xffffffffu);
       int2 pc;
       int32_t row0 = 0, row1 = 0;
-      if constexpr (kNode4) {
+      if constexpr (kRecords) {
         const int4 nc4 = __ldg(g.node4 + c);
         pc = make_int2(nc4.x, nc4.y);
         row0 = nc4.z;
