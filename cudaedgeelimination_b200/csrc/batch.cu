@@ -541,8 +541,13 @@ int cee_batch_prepare(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opt
         static_cast<const uint8_t*>(s.active.ptr), 0, g.m, static_cast<int4*>(s.edge4.ptr));
   }
   cudaError_t status = LaunchSpatial(s, 0, b->instances, st);
+  if (status == cudaSuccess) {
+    status = cudaMemcpyAsync(ctx->h_error, ctx->d_error, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+  }
   if (status == cudaSuccess) status = cudaStreamSynchronize(st);  // host staging vectors die at return
   if (status != cudaSuccess) return CudaFail(ctx, status, "batch upload");
+  rc = BatchCheck(ctx);  // the upload kernels' checks (edge ids, neighbours)
+  if (rc != CEE_OK) return rc;
   cudaEventRecord(ctx->ev[1], st);
   status = QueryBatchOccupancy(s);
   if (status != cudaSuccess) return CudaFail(ctx, status, "batch occupancy");
