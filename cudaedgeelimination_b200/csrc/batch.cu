@@ -49,9 +49,9 @@ struct BatchState {
   // the union snapshot in the kernels' layout
   DevBuf d_node_begin, d_edge_begin, xy, uv, w32, active, ro, nbr, ids, slot4, node4, edge4;
   // raw uploads of the end-to-end call (converted on the device)
-  DevBuf raw_x, raw_y, raw_u, raw_v;
-  int32_t* w32_host = nullptr;  // pinned staging of the end-to-end call's int32 weights
-  size_t w32_host_count = 0;
+  DevBuf raw_x, raw_y, raw_v, estart;  // estart[x]: the first edge whose lower end is x or above
+  int32_t* stage_host = nullptr;  // pinned int32 staging of the end-to-end call: weights [m], edge starts [n + 1]
+  size_t stage_count = 0;
   // outputs and work-queue state
   DevBuf witness, target_ids, target_count, nbhd, flags, counter, ready;
   DevBuf perm, chunk_box, d_chunk_begin;  // spatial chunks of the instances
@@ -72,7 +72,7 @@ struct BatchState {
   void Release() {
     ReleaseGraph();
     for (DevBuf* b : {&d_node_begin, &d_edge_begin, &xy, &uv, &w32, &active, &ro, &nbr, &ids, &slot4, &node4, &edge4, &raw_x, &raw_y,
-                      &raw_u, &raw_v, &witness, &target_ids, &target_count, &nbhd, &flags, &counter, &ready,
+                      &raw_v, &estart, &witness, &target_ids, &target_count, &nbhd, &flags, &counter, &ready,
                       &cand_c, &cand_d, &cand_product, &cand_count, &perm, &chunk_box, &d_chunk_begin}) {
       b->Release();
     }
@@ -82,9 +82,9 @@ struct BatchState {
       if (prepped[i] != nullptr) cudaEventDestroy(prepped[i]);
       up[i] = done[i] = prepped[i] = nullptr;
     }
-    if (w32_host != nullptr) cudaFreeHost(w32_host);
-    w32_host = nullptr;
-    w32_host_count = 0;
+    if (stage_host != nullptr) cudaFreeHost(stage_host);
+    stage_host = nullptr;
+    stage_count = 0;
     if (h2d != nullptr) cudaStreamDestroy(h2d);
     if (prep != nullptr) cudaStreamDestroy(prep);
     prep = nullptr;
@@ -107,7 +107,7 @@ uint64_t BatchResident(const cee_ctx* ctx) {
   if (s == nullptr) return 0;
   uint64_t bytes = 0;
   for (const DevBuf* b : {&s->d_node_begin, &s->d_edge_begin, &s->xy, &s->uv, &s->w32, &s->active, &s->ro, &s->nbr,
-                          &s->ids, &s->slot4, &s->node4, &s->edge4, &s->raw_x, &s->raw_y, &s->raw_u, &s->raw_v, &s->witness,
+                          &s->ids, &s->slot4, &s->node4, &s->edge4, &s->raw_x, &s->raw_y, &s->raw_v, &s->estart, &s->witness,
                           &s->target_ids, &s->target_count, &s->nbhd, &s->flags, &s->counter, &s->ready, &s->perm,
                           &s->chunk_box, &s->d_chunk_begin}) {
     bytes += b->capacity;
@@ -439,12 +439,15 @@ __global__ void batch_records(const int2* __restrict__ xy, const int32_t* __rest
   }
 }
 
-// Raw host layout -> kernel layout for nodes [n0, n1) and edges [e0, e1): coordinates relative to
-// (min_x, min_y), (u, v) pairs, int32 weights. Out-of-range values are recorded in *error and
-// replaced by harmless ones (node 0, weight 0) so that no later access leaves its array.
+// Raw host layout -> kernel layout for nodes [n0, n1) and their edges [e0, e1): coordinates relative
+// to (min_x, min_y), and each edge's ends (u, v) with u from estart (estart[x], x in [n0, n1], is the
+// first edge whose lower end is x or above; the host builds it from the checked, (u, v)-sorted edge
+// list). A warp takes 32 consecutive nodes and walks their edges with coalesced loads, finding each
+// edge's lower end by a binary search over the lanes' estart values. Out-of-range values are
+// recorded in *error and replaced by harmless ones ((0, 0)) so that no later access leaves its array.
 __global__ void batch_pack(const int64_t* __restrict__ x, const int64_t* __restrict__ y, int64_t n0, int64_t n1,
-                           int64_t min_x, int64_t min_y, int2* __restrict__ xy, const int32_t* __restrict__ u,
-                           const int32_t* __restrict__ v, int64_t e0, int64_t e1, int64_t n, int2* __restrict__ uv,
+                           int64_t min_x, int64_t min_y, int2* __restrict__ xy, const int32_t* __restrict__ estart,
+                           const int32_t* __restrict__ v, int64_t e0, int64_t e1, int2* __restrict__ uv,
                            int32_t* __restrict__ error) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   const int64_t first = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -457,18 +460,37 @@ __global__ void batch_pack(const int64_t* __restrict__ x, const int64_t* __restr
       xy[i] = make_int2(static_cast<int32_t>(dx), static_cast<int32_t>(dy));
     }
   }
-  for (int64_t e = e0 + first; e < e1; e += stride) {
-    int32_t a = u[e], b = v[e];
-    if (static_cast<uint64_t>(static_cast<uint32_t>(a)) >= static_cast<uint64_t>(n) ||
-        static_cast<uint64_t>(static_cast<uint32_t>(b)) >= static_cast<uint64_t>(n) || a >= b) {
-      atomicOr(error, 32);
-      a = b = 0;
+  const int lane = static_cast<int>(threadIdx.x & 31);
+  const int64_t warps = stride >> 5;
+  for (int64_t g0 = n0 + (first >> 5) * 32; g0 < n1; g0 += warps * 32) {
+    const int64_t node = g0 + lane;
+    const int32_t start = node < n1 ? estart[node] : INT32_MAX;
+    const int32_t begin = __shfl_sync(kFullMask, start, 0);
+    const int32_t end = estart[min(g0 + 32, n1)];
+    if (begin < e0 || end > e1 || begin > end) {  // estart is built on the host; checked all the same
+      if (lane == 0) atomicOr(error, 32);
+      continue;
     }
-    if (e > 0) {  // canonical order (u, v) ascending over the union
-      const int32_t pa = u[e - 1], pb = v[e - 1];
-      if (pa > a || (pa == a && pb >= b)) atomicOr(error, 32);
+    for (int64_t base = begin; base < end; base += 32) {
+      const int64_t e = base + lane;
+      int lo = 0;  // the last lane whose first edge is at or before e (starts are non-decreasing)
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        if (__shfl_sync(kFullMask, start, lo + step) <= e) lo += step;
+      }
+      const int32_t first_of_a = __shfl_sync(kFullMask, start, lo);
+      if (e < end) {
+        const int32_t a = static_cast<int32_t>(g0 + lo), b = v[e];
+        // canonical, inside the chunk, and v ascending among the edges of lower end a
+        const bool sorted = e == first_of_a || v[e - 1] < b;
+        if (b <= a || b >= n1 || !sorted) {
+          atomicOr(error, 32);
+          uv[e] = make_int2(0, 0);
+        } else {
+          uv[e] = make_int2(a, b);
+        }
+      }
     }
-    uv[e] = make_int2(a, b);
   }
 }
 
@@ -712,21 +734,22 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
   SetShape(s, b, options);
   rc = ReserveAll(ctx, s);
   for (const auto& [buf, bytes] : {std::pair<DevBuf*, size_t>{&s.raw_x, g.n * 8ull}, {&s.raw_y, g.n * 8ull},
-                                   {&s.raw_u, g.m * 4ull}, {&s.raw_v, g.m * 4ull}}) {
+                                   {&s.raw_v, g.m * 4ull}, {&s.estart, (g.n + 1) * 4ull}}) {
     if (rc == CEE_OK) rc = Reserve(ctx, *buf, bytes);
   }
   if (rc != CEE_OK) return rc;
-  if (s.w32_host_count < static_cast<size_t>(g.m)) {  // pinned int32 weight staging, grown geometrically
-    if (s.w32_host != nullptr) cudaFreeHost(s.w32_host);
-    s.w32_host = nullptr;
-    s.w32_host_count = 0;
-    const size_t count = std::max<size_t>(static_cast<size_t>(g.m), 1);
-    if (cudaHostAlloc(reinterpret_cast<void**>(&s.w32_host), count * sizeof(int32_t), cudaHostAllocDefault) != cudaSuccess) {
+  const size_t stage_need = static_cast<size_t>(g.m) + static_cast<size_t>(g.n) + 1;
+  if (s.stage_count < stage_need) {  // pinned int32 staging, reallocated when it grows
+    if (s.stage_host != nullptr) cudaFreeHost(s.stage_host);
+    s.stage_host = nullptr;
+    s.stage_count = 0;
+    const size_t count = stage_need;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&s.stage_host), count * sizeof(int32_t), cudaHostAllocDefault) != cudaSuccess) {
       cudaGetLastError();
-      s.w32_host = nullptr;
+      s.stage_host = nullptr;
       return Fail(ctx, CEE_ERR_NOMEM, "pinned weight staging");
     }
-    s.w32_host_count = count;
+    s.stage_count = count;
   }
   cudaError_t status = cudaSuccess;
   if (s.h2d == nullptr) status = cudaStreamCreateWithFlags(&s.h2d, cudaStreamNonBlocking);
@@ -786,27 +809,49 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
     cudaMemcpyAsync(static_cast<int64_t*>(s.raw_x.ptr) + n0, g.x + n0, (n1 - n0) * 8, cudaMemcpyHostToDevice, s.h2d);
     cudaMemcpyAsync(static_cast<int64_t*>(s.raw_y.ptr) + n0, g.y + n0, (n1 - n0) * 8, cudaMemcpyHostToDevice, s.h2d);
     cudaMemcpyAsync(static_cast<int32_t*>(s.ro.ptr) + n0, g.row_offsets + n0, (n1 - n0 + 1) * 4, cudaMemcpyHostToDevice, s.h2d);
-    cudaMemcpyAsync(static_cast<int32_t*>(s.raw_u.ptr) + e0, g.edge_u + e0, (e1 - e0) * 4, cudaMemcpyHostToDevice, s.h2d);
     cudaMemcpyAsync(static_cast<int32_t*>(s.raw_v.ptr) + e0, g.edge_v + e0, (e1 - e0) * 4, cudaMemcpyHostToDevice, s.h2d);
     cudaMemcpyAsync(static_cast<uint8_t*>(s.active.ptr) + e0, g.active + e0, e1 - e0, cudaMemcpyHostToDevice, s.h2d);
     if (s1 > s0) {
       cudaMemcpyAsync(static_cast<int32_t*>(s.nbr.ptr) + s0, g.neighbors + s0, (s1 - s0) * 4, cudaMemcpyHostToDevice, s.h2d);
       cudaMemcpyAsync(static_cast<int32_t*>(s.ids.ptr) + s0, g.csr_edge_ids + s0, (s1 - s0) * 4, cudaMemcpyHostToDevice, s.h2d);
     }
-    std::vector<uint8_t> bad_weight(16, 0);
+    // On host threads: the weights narrowed to int32, and the lower ends checked (inside this
+    // chunk's nodes, ascending) while estart is built from them: estart[x], x in [n0, n1], is the
+    // first edge whose lower end is x or above. The device rebuilds each u from estart, so the lower
+    // ends never cross PCIe, and checks the upper ends (batch_pack).
+    std::vector<uint8_t> bad_weight(16, 0), bad_edge(16, 0);
+    int32_t* const estart_host = s.stage_host + g.m;
     ParallelRanges(e1 - e0, [&](int64_t a0, int64_t a1, int t) {
+      int64_t pu = n0 - 1;
+      if (a0 > 0) pu = std::min<int64_t>(std::max<int64_t>(g.edge_u[e0 + a0 - 1], n0 - 1), n1);
       for (int64_t e = e0 + a0; e < e0 + a1; ++e) {
         const int64_t w = g.edge_w[e];
         if (w < 0 || w > INT32_MAX) bad_weight[t] = 1;
-        s.w32_host[e] = static_cast<int32_t>(w);
+        s.stage_host[e] = static_cast<int32_t>(w);
+        const int64_t u = g.edge_u[e];
+        if (u < n0 || u < pu || u >= n1) {
+          bad_edge[t] = 1;
+          return;
+        }
+        for (int64_t node = pu + 1; node <= u; ++node) estart_host[node] = static_cast<int32_t>(e);
+        pu = u;
+      }
+      if (a1 == e1 - e0) {
+        for (int64_t node = pu + 1; node <= n1; ++node) estart_host[node] = static_cast<int32_t>(e1);
       }
     });
     if (std::any_of(bad_weight.begin(), bad_weight.end(), [](uint8_t v) { return v != 0; })) {
       drain();
       return Fail(ctx, CEE_ERR_RANGE, "edge weight outside [0, 2^31)");
     }
-    cudaMemcpyAsync(static_cast<int32_t*>(s.w32.ptr) + e0, s.w32_host + e0, (e1 - e0) * 4, cudaMemcpyHostToDevice, s.h2d);
-    h2d_bytes += (n1 - n0) * 20 + 4 + (e1 - e0) * 13 + (s1 - s0) * 8;
+    if (std::any_of(bad_edge.begin(), bad_edge.end(), [](uint8_t v) { return v != 0; })) {
+      drain();
+      return Fail(ctx, CEE_ERR_INVALID, "edges must be canonical, inside their instance and sorted by (u, v)");
+    }
+    cudaMemcpyAsync(static_cast<int32_t*>(s.w32.ptr) + e0, s.stage_host + e0, (e1 - e0) * 4, cudaMemcpyHostToDevice, s.h2d);
+    cudaMemcpyAsync(static_cast<int32_t*>(s.estart.ptr) + n0, estart_host + n0, (n1 - n0 + 1) * 4, cudaMemcpyHostToDevice,
+                    s.h2d);
+    h2d_bytes += (n1 - n0) * 24 + 8 + (e1 - e0) * 9 + (s1 - s0) * 8;
     cudaEventRecord(s.up[c], s.h2d);
     if (c == 0) {  // row offsets and the bounding box on host threads, while the first copies run
       int64_t box[4];
@@ -824,8 +869,8 @@ int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* b, const cee_batch_opti
     cudaStreamWaitEvent(s.prep, s.up[c], 0);
     batch_pack<<<GridFor(std::max(n1 - n0, e1 - e0), 256, ctx->sm_count * 8), 256, 0, s.prep>>>(
         static_cast<const int64_t*>(s.raw_x.ptr), static_cast<const int64_t*>(s.raw_y.ptr), n0, n1, min_x, min_y,
-        static_cast<int2*>(s.xy.ptr), static_cast<const int32_t*>(s.raw_u.ptr), static_cast<const int32_t*>(s.raw_v.ptr),
-        e0, e1, g.n, static_cast<int2*>(s.uv.ptr), ctx->d_error);
+        static_cast<int2*>(s.xy.ptr), static_cast<const int32_t*>(s.estart.ptr), static_cast<const int32_t*>(s.raw_v.ptr),
+        e0, e1, static_cast<int2*>(s.uv.ptr), ctx->d_error);
     batch_records<<<GridFor(std::max(n1 - n0, e1 - e0), 256, ctx->sm_count * 8), 256, 0, s.prep>>>(
         static_cast<const int2*>(s.xy.ptr), static_cast<const int32_t*>(s.ro.ptr), n0, n1, static_cast<int4*>(s.node4.ptr),
         static_cast<const int2*>(s.uv.ptr), static_cast<const int32_t*>(s.w32.ptr),

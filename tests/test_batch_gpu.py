@@ -170,6 +170,26 @@ def test_unsorted_instance_rejected(ctx):
         ctx.batch_screen(batch, BatchOptions())
 
 
+def test_upper_ends_out_of_order_rejected(ctx):
+    """Two edges with the same lower end, their upper ends swapped: the end-to-end call checks the
+    lower ends on host threads and the upper ends on the device; both paths reject the list."""
+    from cudaedgeelimination_b200._native import CEE_ERR_INVALID, NativeError
+    g = synth.batch_instance(0, n_lo=300, n_hi=300)
+    e = int(np.flatnonzero(g.edge_u[:-1] == g.edge_u[1:])[0])
+    u, v, w = g.edge_u.copy(), g.edge_v.copy(), g.edge_w.copy()
+    v[[e, e + 1]] = v[[e + 1, e]]
+    w[[e, e + 1]] = w[[e + 1, e]]
+    batch = TinyBatch([synth.batch_instance(1, n_lo=300, n_hi=300), GraphSnapshot(g.n, g.dist_type, g.x, g.y, u, v, w,
+                                                                                   g.active)])
+    with pytest.raises(NativeError) as err:
+        ctx.batch_screen(batch, BatchOptions())
+    assert err.value.code == CEE_ERR_INVALID
+    with pytest.raises(NativeError):
+        ctx.batch_prepare(batch, BatchOptions())
+    res, _ = ctx.batch_screen(TinyBatch([g]), BatchOptions())  # the context stays usable
+    assert res.witness.shape == (g.m,)
+
+
 def test_csr_row_leaving_its_instance(ctx):
     """Every instance here has at most 8,192 nodes, so the screen keys candidates by node id relative
     to the edge's endpoint; a CSR row that names a node of another instance more than 8,191 ids away
