@@ -496,7 +496,9 @@ int cee_batch_fetch(cee_ctx* ctx, int32_t* witness, int32_t* target_ids, int32_t
                     int32_t* nbhd, uint32_t* flags);
 /* End to end from host buffers: uploads, screens and downloads chunk by chunk, overlapping the
  * copies of one chunk with the screen of another (pinned buffers overlap; pageable ones too,
- * at the driver's staging speed). Output pointers as in cee_batch_fetch. */
+ * at the driver's staging speed). The edge list must be canonical (u < v) and sorted by (u, v),
+ * CEE_ERR_INVALID otherwise; edge_u itself is not copied (host threads turn it into per-node edge
+ * starts). Output pointers as in cee_batch_fetch. */
 int cee_batch_screen(cee_ctx* ctx, const cee_batch_view* batch, const cee_batch_options* options,
                      int32_t* witness, int32_t* target_ids, int32_t* target_count, int32_t* nbhd,
                      uint32_t* flags, cee_batch_stats* stats);
