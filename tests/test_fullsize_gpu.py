@@ -130,7 +130,11 @@ def test_serve_stream_sample(port):
             for jid, tag, res in ctx.serve_poll():
                 results[tag] = res
                 pending.pop(jid)
-            assert time.time() - t0 < 300, "serving loop stalled"
+            if time.time() - t0 >= 300:
+                kinds_left = sorted({wl.jobs[tag][0] for tag in pending.values()})
+                pytest.fail(f"serving loop stalled: {len(results)} of {len(wl.jobs)} jobs reported, {nxt} "
+                            f"submitted, pending {ctx.serve_pending()} (jobs, arena bytes), kinds still pending "
+                            f"{kinds_left}, loop totals {ctx.serve_stats()}")
         ctx.serve_stop()
     finally:
         ctx.close()
